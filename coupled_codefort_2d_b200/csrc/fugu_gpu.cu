@@ -1,0 +1,1476 @@
+// fugu_gpu.cu -- host orchestration and C ABI of the B200 FUGU-2D hot path.
+//
+// A context owns every device buffer of one case in the uniform padded layout
+// (fugu_internal.cuh) and one CUDA stream.  The step, the Krylov solvers and
+// the PCD preconditioner are sequences of the kernels in kernels.cuh,
+// persistent.cuh and scalars.cuh; Krylov scalars stay on the device, and the
+// host only polls the `active` flag once per Krylov iteration.
+//
+// Compiled for sm_100a with --fmad=false (see build.py): the FP64 plain form
+// then rounds every operation as the CPU oracle does.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstddef>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fugu_gpu.h"
+#include "kernels.cuh"
+#include "persistent.cuh"
+#include "scalars.cuh"
+
+using namespace fugu;
+
+namespace {
+
+struct CudaError {
+  cudaError_t e;
+  const char* what;
+};
+#define CK(x)                                     \
+  do {                                            \
+    cudaError_t e_ = (x);                         \
+    if (e_ != cudaSuccess) throw CudaError{e_, #x}; \
+  } while (0)
+#define CKL(what)                                          \
+  do {                                                     \
+    cudaError_t e_ = cudaGetLastError();                   \
+    if (e_ != cudaSuccess) throw CudaError{e_, what};      \
+  } while (0)
+
+struct ApiError {
+  int code;
+  std::string msg;
+};
+
+template <typename T>
+struct Trip {
+  T* base = nullptr;
+  T* u = nullptr;
+  T* v = nullptr;
+  T* p = nullptr;
+};
+
+template <typename T>
+struct PcgWork {
+  T *cx = nullptr, *cy = nullptr, *dinv = nullptr, *r = nullptr, *z = nullptr, *pb0 = nullptr,
+    *pb1 = nullptr, *ap = nullptr;
+};
+
+template <typename T>
+struct PcdWork {
+  T *phi = nullptr, *zuw = nullptr, *zvw = nullptr, *tmp = nullptr;
+};
+
+// coefficient fields of the coupled operator in one precision
+template <typename T>
+struct CoefBufs {
+  T *u_adv = nullptr, *v_adv = nullptr, *rho_c = nullptr, *rho_u = nullptr, *rho_v = nullptr,
+    *kappa = nullptr, *zeta = nullptr, *eta = nullptr, *pen_u = nullptr, *pen_v = nullptr,
+    *mdu = nullptr, *mdv = nullptr;
+};
+
+// which optional coefficient fields a solve uses
+struct SolveOpt {
+  bool pen = false;
+  bool amp = false;
+};
+
+template <typename T>
+struct KrylovWork {
+  Trip<T> t[13];  // bh, r, rt, uu, vv, ww, ss, tt, z, q + refine r, d, ax
+  PcdWork<T> pcd;
+  PcgWork<T> pcg;
+  CoefBufs<T> cf;  // converted coefficients (FP32 only; FP64 points at the originals)
+};
+
+}  // namespace
+
+struct fugu_ctx {
+  fugu_params prm{};
+  Geo g{};
+  int device = 0;
+  int nsm = 148;
+  cudaStream_t s = nullptr;
+  long n = 0;  // elements per buffer
+  std::vector<void*> allocs;
+  double* f[FUGU_NUM_FIELDS] = {};
+  // step temporaries
+  double *u_nm1 = nullptr, *v_nm1 = nullptr, *u_adv = nullptr, *v_adv = nullptr, *c_new = nullptr,
+         *c_s = nullptr, *svof_w = nullptr, *fcx = nullptr, *fcy = nullptr, *mdu = nullptr,
+         *mdv = nullptr, *pen_u = nullptr, *pen_v = nullptr;
+  Trip<double> B;
+  Trip<double> Xstate;  // u_vel, v_vel, p_field (contiguous)
+  KrylovWork<double> w64;
+  KrylovWork<float> w32;
+  bool w32_ready = false;
+  // routine-level scratch
+  double* scratch[20] = {};
+  // device scalars / state
+  double* sc = nullptr;
+  KState* ks = nullptr;
+  double* part = nullptr;
+  long part_len = 0;
+  GridSync* gs = nullptr;
+  PcgOut* pcg_out = nullptr;
+  int* svof_iters = nullptr;
+  int* svof_status = nullptr;
+  // pinned host mirrors
+  KState* h_ks = nullptr;
+  double* h_sc = nullptr;
+  PcgOut* h_pcg = nullptr;
+  int* h_int = nullptr;
+  int pcg_grid = 0;
+  int svof_grid = 0;
+  int dot_grid = 0;
+  std::string err;
+};
+
+namespace {
+
+constexpr int PCG_TPB = 512;
+constexpr int DOT_TPB = 256;
+
+template <typename T>
+T* dalloc(fugu_ctx* c, long n) {
+  void* p = nullptr;
+  if (cudaMalloc(&p, sizeof(T) * n) != cudaSuccess) throw ApiError{FUGU_ENOMEM, "cudaMalloc failed"};
+  c->allocs.push_back(p);
+  CK(cudaMemsetAsync(p, 0, sizeof(T) * n, c->s));
+  return (T*)p;
+}
+template <typename T>
+Trip<T> talloc(fugu_ctx* c) {
+  Trip<T> t;
+  t.base = dalloc<T>(c, 3 * c->n);
+  t.u = t.base;
+  t.v = t.base + c->n;
+  t.p = t.base + 2 * c->n;
+  return t;
+}
+
+Geo make_geo(const fugu_params& p) {
+  Geo g{};
+  g.nx = p.nx;
+  g.ny = p.ny;
+  g.P = ((p.nx + 5 + 15) / 16) * 16;
+  g.R = p.ny + 5;
+  g.dx = p.dx;
+  g.dy = p.dy;
+  g.idx = 1.0 / p.dx;
+  g.idy = 1.0 / p.dy;
+  g.idx2 = 1.0 / (p.dx * p.dx);
+  g.idy2 = 1.0 / (p.dy * p.dy);
+  g.px = p.periodic_x ? 1 : 0;
+  g.py = p.periodic_y ? 1 : 0;
+  g.fsx = p.free_slip_x ? 1 : 0;
+  return g;
+}
+
+int kind_of_field(int f) {
+  switch (f) {
+    case FUGU_F_U_VEL: case FUGU_F_U_PREV: case FUGU_F_RHO_U: case FUGU_F_F_SIGMA_U: case FUGU_F_PHI_S_U:
+      return K_U;
+    case FUGU_F_V_VEL: case FUGU_F_V_PREV: case FUGU_F_RHO_V: case FUGU_F_F_SIGMA_V: case FUGU_F_PHI_S_V:
+      return K_V;
+    case FUGU_F_ZETA: case FUGU_F_ETA:
+      return K_VERT;
+    default:
+      return K_CELL;
+  }
+}
+
+// Fortran-layout host array <-> uniform device box (strided 2-D copies)
+void copy_kind(fugu_ctx* c, double* dev, const double* host, int kind, bool h2d, double* hostw = nullptr) {
+  const Geo& g = c->g;
+  int i0, i1, j0, j1;
+  g.extent(kind, i0, i1, j0, j1);
+  const size_t w = (size_t)(i1 - i0 + 1), h = (size_t)(j1 - j0 + 1);
+  double* d = dev + g.at(i0, j0);
+  if (h2d)
+    CK(cudaMemcpy2DAsync(d, sizeof(double) * g.P, host, sizeof(double) * w, sizeof(double) * w, h,
+                         cudaMemcpyHostToDevice, c->s));
+  else
+    CK(cudaMemcpy2DAsync(hostw, sizeof(double) * w, d, sizeof(double) * g.P, sizeof(double) * w, h,
+                         cudaMemcpyDeviceToHost, c->s));
+}
+void up(fugu_ctx* c, double* dev, const double* host, int kind) {
+  if (!host) throw ApiError{FUGU_EINVAL, "NULL host array"};
+  copy_kind(c, dev, host, kind, true);
+}
+void down(fugu_ctx* c, double* host, const double* dev, int kind) {
+  if (!host) throw ApiError{FUGU_EINVAL, "NULL host array"};
+  copy_kind(c, (double*)dev, nullptr, kind, false, host);
+}
+void sync(fugu_ctx* c) { CK(cudaStreamSynchronize(c->s)); }
+
+int grid1d(fugu_ctx* c, long n) {
+  long b = (n + 255) / 256;
+  long cap = (long)c->nsm * 8;
+  return (int)(b < 1 ? 1 : (b > cap ? cap : b));
+}
+
+// ------------------------------------------------------------------ launches
+template <typename T>
+void halo(fugu_ctx* c, T* a, int kind, const int* active = nullptr) {
+  if (!c->g.px && !c->g.py) return;
+  k_halo<T><<<1, 1024, 0, c->s>>>(c->g, a, kind, active);
+  CKL("k_halo");
+}
+template <typename T>
+void vbcs(fugu_ctx* c, T* u, T* v, double lid, const int* active = nullptr) {
+  if (c->g.px && c->g.py) return;
+  k_velocity_bcs<T><<<1, 1024, 0, c->s>>>(c->g, u, v, T(lid), active);
+  CKL("k_velocity_bcs");
+}
+
+template <typename T>
+Coefs<T> coefs_of(const CoefBufs<T>& b, const SolveOpt& o) {
+  Coefs<T> cf;
+  cf.u_adv = b.u_adv; cf.v_adv = b.v_adv; cf.rho_c = b.rho_c; cf.rho_u = b.rho_u; cf.rho_v = b.rho_v;
+  cf.kappa = b.kappa; cf.zeta = b.zeta; cf.eta = b.eta;
+  cf.pen_u = o.pen ? b.pen_u : nullptr;
+  cf.pen_v = o.pen ? b.pen_v : nullptr;
+  cf.mdot_u = o.amp ? b.mdu : nullptr;
+  cf.mdot_v = o.amp ? b.mdv : nullptr;
+  return cf;
+}
+
+template <typename T>
+void matvec(fugu_ctx* c, const CoefBufs<T>& cb, const SolveOpt& o, Trip<T> X, Trip<T> Y, double dt,
+            const int* active) {
+  halo(c, X.u, K_U, active);
+  halo(c, X.v, K_V, active);
+  halo(c, X.p, K_CELL, active);
+  Box b = box_launch(c->g);
+  k_matvec<T><<<b.grid, b.block, 0, c->s>>>(c->g, coefs_of(cb, o), X.u, X.v, X.p, Y.u, Y.v, Y.p, T(dt), 1, active,
+                                            &c->ks->matvecs);
+  CKL("k_matvec");
+}
+
+template <typename T>
+void lin(fugu_ctx* c, Trip<T> y, Trip<T> x, double s1 = 0, const double* c1 = nullptr, Trip<T> z1 = {},
+         double s2 = 0, const double* c2 = nullptr, Trip<T> z2 = {}, double s3 = 0,
+         const double* c3 = nullptr, Trip<T> z3 = {}, const int* active = nullptr) {
+  Lin<T> L;
+  L.x = x.base; L.z1 = z1.base; L.z2 = z2.base; L.z3 = z3.base;
+  L.c1 = c1; L.c2 = c2; L.c3 = c3;
+  L.s1 = s1; L.s2 = s2; L.s3 = s3;
+  const long n3 = 3 * c->n;
+  k_lin<T><<<grid1d(c, n3), 256, 0, c->s>>>(n3, y.base, L, active);
+  CKL("k_lin");
+}
+
+template <typename T>
+void dot_op(fugu_ctx* c, std::initializer_list<std::pair<Trip<T>, Trip<T>>> pairs, OpArgs op,
+            bool check_active) {
+  DotArgs<T> d;
+  d.g = c->g;
+  d.n = c->n;
+  int k = 0;
+  for (auto& pr : pairs) {
+    d.a[k] = pr.first.base;
+    d.b[k] = pr.second.base;
+    ++k;
+  }
+  for (; k < 5; ++k) { d.a[k] = nullptr; d.b[k] = nullptr; }
+  d.npairs = (int)pairs.size();
+  d.vol = c->g.dx * c->g.dy;
+  d.part = c->part;
+  d.sc = c->sc;
+  d.ks = c->ks;
+  d.op = op;
+  d.check_active = check_active ? 1 : 0;
+  k_dot_op<T><<<c->dot_grid, DOT_TPB, 0, c->s>>>(d);
+  CKL("k_dot_op");
+}
+void scalar_op(fugu_ctx* c, OpArgs op, bool check_active) {
+  k_scalar_op<<<1, 1, 0, c->s>>>(op, c->sc, c->ks, check_active ? 1 : 0);
+  CKL("k_scalar_op");
+}
+
+// persistent PCG (solve_poisson_pressure)
+template <typename T>
+void pcg(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, double tol, int max_iter, bool phi_zero,
+         const int* active) {
+  PcgArgs<T> a;
+  a.g = c->g;
+  a.rhs = rhs; a.cx = w.cx; a.cy = w.cy; a.dinv = w.dinv;
+  a.phi = phi; a.r = w.r; a.z = w.z; a.pb0 = w.pb0; a.pb1 = w.pb1; a.ap = w.ap;
+  a.part = c->part; a.gs = c->gs; a.out = c->pcg_out; a.active = active;
+  a.tol = tol; a.max_iter = max_iter; a.phi_zero = phi_zero ? 1 : 0;
+  CK(cudaMemsetAsync(c->gs, 0, sizeof(GridSync), c->s));
+  void* args[] = {&a};
+  CK(cudaLaunchCooperativeKernel((void*)k_pcg<T>, dim3(c->pcg_grid), dim3(PCG_TPB), args, 0, c->s));
+}
+
+template <typename T>
+void poisson_coefs(fugu_ctx* c, PcgWork<T>& w, const double* rho_u, const double* rho_v) {
+  Box b = box_launch(c->g);
+  k_poisson_coefs<T><<<b.grid, b.block, 0, c->s>>>(c->g, rho_u, rho_v, w.cx, w.cy, w.dinv);
+  CKL("k_poisson_coefs");
+}
+
+// damped-Jacobi smoother: n sweeps of solve_helmholtz_{u,v} in place on sol
+template <typename T>
+void helmholtz(fugu_ctx* c, bool is_u, T* sol, T* tmp, const T* rhs, const CoefBufs<T>& cb,
+               const SolveOpt& o, double dt, int n_sweeps, const int* active) {
+  Box b = box_launch(c->g);
+  T* cur = sol;
+  T* nxt = tmp;
+  const T* pen = o.pen ? (is_u ? cb.pen_u : cb.pen_v) : nullptr;
+  for (int s = 0; s < n_sweeps; ++s) {
+    halo(c, cur, is_u ? K_U : K_V, active);
+    if (is_u)
+      k_jacobi_u<T><<<b.grid, b.block, 0, c->s>>>(c->g, cur, nxt, rhs, cb.rho_u, cb.kappa, cb.zeta, cb.eta, pen,
+                                                  T(dt), T(c->prm.jacobi_omega), active);
+    else
+      k_jacobi_v<T><<<b.grid, b.block, 0, c->s>>>(c->g, cur, nxt, rhs, cb.rho_v, cb.kappa, cb.zeta, cb.eta, pen,
+                                                  T(dt), T(c->prm.jacobi_omega), active);
+    CKL("k_jacobi");
+    std::swap(cur, nxt);
+  }
+  if (cur != sol) CK(cudaMemcpyAsync(sol, cur, sizeof(T) * c->n, cudaMemcpyDeviceToDevice, c->s));
+}
+
+// apply_pcd_precond, mod_pcd_precond.f90:14-104: z -> r
+template <typename T>
+void pcd(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const SolveOpt& o, Trip<T> z, Trip<T> r,
+         double dt, const int* active) {
+  PcdWork<T>& pw = w.pcd;
+  Box b = box_launch(c->g);
+  // r = zero; phi_p = zero (mod_pcd_precond.f90:44-47).  Plain memsets run
+  // even after an exit; the output of an exited iteration is never read.
+  CK(cudaMemsetAsync(r.base, 0, sizeof(T) * 3 * c->n, c->s));
+  CK(cudaMemsetAsync(pw.phi, 0, sizeof(T) * c->n, c->s));
+  pcg<T>(c, w.pcg, pw.phi, z.p, c->prm.pcg_tol, c->prm.pcg_max_iter, true, active);
+  halo(c, pw.phi, K_CELL, active);
+  k_pcd_schur<T><<<b.grid, b.block, 0, c->s>>>(c->g, pw.phi, cb.u_adv, cb.v_adv, r.p, T(1.0 / dt), active);
+  CKL("k_pcd_schur");
+  halo(c, r.p, K_CELL, active);
+  k_pcd_zwork<T><<<b.grid, b.block, 0, c->s>>>(c->g, z.u, z.v, r.p, pw.zuw, pw.zvw, active);
+  CKL("k_pcd_zwork");
+  helmholtz<T>(c, false, r.v, pw.tmp, pw.zvw, cb, o, dt, c->prm.pcd_sweeps, active);
+  halo(c, r.v, K_V, active);
+  k_pcd_cross<T><<<b.grid, b.block, 0, c->s>>>(c->g, cb.eta, r.v, pw.zuw, active);
+  CKL("k_pcd_cross");
+  helmholtz<T>(c, true, r.u, pw.tmp, pw.zuw, cb, o, dt, c->prm.pcd_sweeps, active);
+  halo(c, r.u, K_U, active);
+}
+
+template <typename T>
+void zero_trip(fugu_ctx* c, Trip<T> t) {
+  CK(cudaMemsetAsync(t.base, 0, sizeof(T) * 3 * c->n, c->s));
+}
+
+// restart the Krylov flags (the matvec counter survives; it is per step)
+void reset_ks(fugu_ctx* c) {
+  static const KState k0 = {1, 0, 0, 0u, 0ull};
+  CK(cudaMemcpyAsync(c->ks, &k0, offsetof(KState, matvecs), cudaMemcpyHostToDevice, c->s));
+}
+// poll the device Krylov state (one round trip)
+KState read_ks(fugu_ctx* c) {
+  CK(cudaMemcpyAsync(c->h_ks, c->ks, sizeof(KState), cudaMemcpyDeviceToHost, c->s));
+  sync(c);
+  return *c->h_ks;
+}
+double read_slot(fugu_ctx* c, int slot) {
+  CK(cudaMemcpyAsync(c->h_sc, c->sc + slot, sizeof(double), cudaMemcpyDeviceToHost, c->s));
+  sync(c);
+  return c->h_sc[0];
+}
+
+struct KrylovResult {
+  int iter = 0;
+  double res = 0.0;
+  int status = FUGU_CONVERGED;
+};
+
+// bicgstab_solve, mod_bicgstab2.f90:77-264
+template <typename T>
+KrylovResult bicgstab1(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const SolveOpt& o, Trip<T> X,
+                       Trip<T> B, double dt, double tol, int max_iter, bool has_lid, double lid) {
+  Trip<T>&bh = w.t[0], &r = w.t[1], &r0 = w.t[2], &p = w.t[3], &v = w.t[4], &s = w.t[5], &t = w.t[6],
+  &z = w.t[7];
+  const int* act = &c->ks->active;
+  double* sc = c->sc;
+  reset_ks(c);
+  vbcs(c, X.u, X.v, 0.0);
+  pcd<T>(c, w, cb, o, B, bh, dt, nullptr);
+  dot_op<T>(c, {{bh, bh}}, OpArgs{OP_NORMB, 0, tol}, false);
+  matvec<T>(c, cb, o, X, z, dt, nullptr);
+  pcd<T>(c, w, cb, o, z, v, dt, nullptr);
+  lin<T>(c, r, bh, -1.0, sc + S_ONE, v);
+  CK(cudaMemcpyAsync(r0.base, r.base, sizeof(T) * 3 * c->n, cudaMemcpyDeviceToDevice, c->s));
+  CK(cudaMemcpyAsync(p.base, r.base, sizeof(T) * 3 * c->n, cudaMemcpyDeviceToDevice, c->s));
+  dot_op<T>(c, {{r0, r}, {r, r}}, OpArgs{OP_B1_INIT, 1, tol}, false);
+  KState ks = read_ks(c);
+  int k = 1;
+  for (; k <= max_iter && ks.active; ++k) {
+    vbcs(c, p.u, p.v, 0.0, act);
+    matvec<T>(c, cb, o, p, z, dt, act);
+    pcd<T>(c, w, cb, o, z, v, dt, act);
+    vbcs(c, v.u, v.v, 0.0, act);
+    dot_op<T>(c, {{r0, v}}, OpArgs{OP_B1_ALPHA, k, tol}, true);
+    lin<T>(c, s, r, -1.0, sc + S_ALPHA, v, 0, nullptr, {}, 0, nullptr, {}, act);
+    vbcs(c, s.u, s.v, 0.0, act);
+    matvec<T>(c, cb, o, s, z, dt, act);
+    pcd<T>(c, w, cb, o, z, t, dt, act);
+    vbcs(c, t.u, t.v, 0.0, act);
+    dot_op<T>(c, {{t, t}, {t, s}}, OpArgs{OP_B1_OMEGA, k, tol}, true);
+    lin<T>(c, X, X, 1.0, sc + S_ALPHA, p, 1.0, sc + S_OMEGA, s, 0, nullptr, {}, act);
+    lin<T>(c, r, s, -1.0, sc + S_OMEGA, t, 0, nullptr, {}, 0, nullptr, {}, act);
+    dot_op<T>(c, {{r, r}, {r0, r}}, OpArgs{OP_B1_END, k, tol}, true);
+    k_pupdate<T><<<grid1d(c, 3 * c->n), 256, 0, c->s>>>(3 * c->n, p.base, r.base, v.base, sc + S_BETA,
+                                                          sc + S_OMEGA, act);
+    CKL("k_pupdate");
+    vbcs(c, X.u, X.v, 0.0, act);
+    ks = read_ks(c);
+  }
+  if (has_lid) vbcs(c, X.u, X.v, lid);
+  ks = read_ks(c);
+  KrylovResult res;
+  res.iter = ks.active ? max_iter : (ks.exit_iter < max_iter ? ks.exit_iter : max_iter);
+  res.res = read_slot(c, S_REL);
+  res.status = ks.nan ? FUGU_NAN : (ks.active ? FUGU_MAXITER : (res.res < tol ? FUGU_CONVERGED : FUGU_BREAKDOWN));
+  return res;
+}
+
+// bicgstab2_solve, mod_bicgstab2.f90:270-570
+template <typename T>
+KrylovResult bicgstab2(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const SolveOpt& o, Trip<T> X,
+                       Trip<T> B, double dt, double tol, int max_iter, bool has_lid, double lid) {
+  Trip<T>&bh = w.t[0], &r = w.t[1], &rt = w.t[2], &uu = w.t[3], &vv = w.t[4], &ww = w.t[5], &ss = w.t[6],
+  &tt = w.t[7], &z = w.t[8], &q = w.t[9];
+  const int* act = &c->ks->active;
+  double* sc = c->sc;
+  reset_ks(c);
+  vbcs(c, X.u, X.v, 0.0);
+  pcd<T>(c, w, cb, o, B, bh, dt, nullptr);
+  dot_op<T>(c, {{bh, bh}}, OpArgs{OP_NORMB, 0, tol}, false);
+  matvec<T>(c, cb, o, X, z, dt, nullptr);
+  pcd<T>(c, w, cb, o, z, q, dt, nullptr);
+  lin<T>(c, r, bh, -1.0, sc + S_ONE, q);
+  CK(cudaMemcpyAsync(rt.base, r.base, sizeof(T) * 3 * c->n, cudaMemcpyDeviceToDevice, c->s));
+  zero_trip(c, uu);
+  zero_trip(c, vv);
+  dot_op<T>(c, {{r, r}}, OpArgs{OP_B2_INIT, 1, tol}, false);
+  KState ks = read_ks(c);
+  int k = 1;
+  for (; k <= max_iter && ks.active; ++k) {
+    // even half
+    dot_op<T>(c, {{rt, r}}, OpArgs{OP_B2_XI_EVEN, k, tol}, true);
+    lin<T>(c, uu, r, -1.0, sc + S_BETA, uu, 0, nullptr, {}, 0, nullptr, {}, act);
+    vbcs(c, uu.u, uu.v, 0.0, act);
+    matvec<T>(c, cb, o, uu, z, dt, act);
+    pcd<T>(c, w, cb, o, z, vv, dt, act);
+    vbcs(c, vv.u, vv.v, 0.0, act);
+    dot_op<T>(c, {{rt, vv}}, OpArgs{OP_B2_GAMMA, k, tol}, true);
+    lin<T>(c, r, r, -1.0, sc + S_ALPHA, vv, 0, nullptr, {}, 0, nullptr, {}, act);
+    if (c->prm.krylov_bc_fix) vbcs(c, r.u, r.v, 0.0, act);
+    matvec<T>(c, cb, o, r, z, dt, act);
+    pcd<T>(c, w, cb, o, z, ss, dt, act);
+    vbcs(c, ss.u, ss.v, 0.0, act);
+    lin<T>(c, X, X, 1.0, sc + S_ALPHA, uu, 0, nullptr, {}, 0, nullptr, {}, act);
+    // odd half
+    dot_op<T>(c, {{rt, ss}}, OpArgs{OP_B2_XI_ODD, k, tol}, true);
+    lin<T>(c, vv, ss, -1.0, sc + S_BETA, vv, 0, nullptr, {}, 0, nullptr, {}, act);
+    vbcs(c, vv.u, vv.v, 0.0, act);
+    matvec<T>(c, cb, o, vv, z, dt, act);
+    pcd<T>(c, w, cb, o, z, ww, dt, act);
+    vbcs(c, ww.u, ww.v, 0.0, act);
+    dot_op<T>(c, {{rt, ww}}, OpArgs{OP_B2_GAMMA, k, tol}, true);
+    lin<T>(c, uu, r, -1.0, sc + S_BETA, uu, 0, nullptr, {}, 0, nullptr, {}, act);
+    lin<T>(c, r, r, -1.0, sc + S_ALPHA, vv, 0, nullptr, {}, 0, nullptr, {}, act);
+    lin<T>(c, ss, ss, -1.0, sc + S_ALPHA, ww, 0, nullptr, {}, 0, nullptr, {}, act);
+    matvec<T>(c, cb, o, ss, z, dt, act);
+    pcd<T>(c, w, cb, o, z, tt, dt, act);
+    vbcs(c, tt.u, tt.v, 0.0, act);
+    // GCR(2)
+    dot_op<T>(c, {{r, ss}, {ss, ss}, {ss, tt}, {tt, tt}, {r, tt}}, OpArgs{OP_B2_GCR, k, tol}, true);
+    lin<T>(c, X, X, 1.0, sc + S_OM1, r, 1.0, sc + S_OM2, ss, 1.0, sc + S_ALPHA, uu, act);
+    lin<T>(c, r, r, -1.0, sc + S_OM1, ss, -1.0, sc + S_OM2, tt, 0, nullptr, {}, act);
+    lin<T>(c, uu, uu, -1.0, sc + S_OM1, vv, -1.0, sc + S_OM2, ww, 0, nullptr, {}, act);
+    dot_op<T>(c, {{r, r}}, OpArgs{OP_B2_REL, k, tol}, true);
+    vbcs(c, X.u, X.v, 0.0, act);
+    scalar_op(c, OpArgs{OP_TOPCHECK, k + 1, tol}, true);
+    ks = read_ks(c);
+  }
+  if (has_lid) vbcs(c, X.u, X.v, lid);
+  ks = read_ks(c);
+  KrylovResult res;
+  res.iter = ks.active ? max_iter : (ks.exit_iter < max_iter ? ks.exit_iter : max_iter);
+  res.res = read_slot(c, S_REL);
+  res.status = ks.nan ? FUGU_NAN : (ks.active ? FUGU_MAXITER : (res.res < tol ? FUGU_CONVERGED : FUGU_BREAKDOWN));
+  return res;
+}
+
+template <typename T>
+KrylovResult krylov_inner(fugu_ctx* c, int solver, KrylovWork<T>& w, const CoefBufs<T>& cb, const SolveOpt& o,
+                          Trip<T> X, Trip<T> B, double dt, double tol, int max_iter, bool has_lid, double lid) {
+  if (solver == 2) return bicgstab2<T>(c, w, cb, o, X, B, dt, tol, max_iter, has_lid, lid);
+  return bicgstab1<T>(c, w, cb, o, X, B, dt, tol, max_iter, has_lid, lid);
+}
+
+void ensure_w32(fugu_ctx* c) {
+  if (c->w32_ready) return;
+  KrylovWork<float>& w = c->w32;
+  for (auto& t : w.t) t = talloc<float>(c);
+  w.pcd.phi = dalloc<float>(c, c->n); w.pcd.zuw = dalloc<float>(c, c->n);
+  w.pcd.zvw = dalloc<float>(c, c->n); w.pcd.tmp = dalloc<float>(c, c->n);
+  PcgWork<float>& p = w.pcg;
+  p.cx = dalloc<float>(c, c->n); p.cy = dalloc<float>(c, c->n); p.dinv = dalloc<float>(c, c->n);
+  p.r = dalloc<float>(c, c->n); p.z = dalloc<float>(c, c->n); p.pb0 = dalloc<float>(c, c->n);
+  p.pb1 = dalloc<float>(c, c->n); p.ap = dalloc<float>(c, c->n);
+  CoefBufs<float>& f = w.cf;
+  f.u_adv = dalloc<float>(c, c->n); f.v_adv = dalloc<float>(c, c->n); f.rho_c = dalloc<float>(c, c->n);
+  f.rho_u = dalloc<float>(c, c->n); f.rho_v = dalloc<float>(c, c->n); f.kappa = dalloc<float>(c, c->n);
+  f.zeta = dalloc<float>(c, c->n); f.eta = dalloc<float>(c, c->n); f.pen_u = dalloc<float>(c, c->n);
+  f.pen_v = dalloc<float>(c, c->n); f.mdu = dalloc<float>(c, c->n); f.mdv = dalloc<float>(c, c->n);
+  c->w32_ready = true;
+}
+
+void cvt(fugu_ctx* c, float* dst, const double* src) {
+  if (!src) return;
+  k_convert<float><<<grid1d(c, c->n), 256, 0, c->s>>>(c->n, dst, src, 1.0);
+  CKL("k_convert");
+}
+
+// FP64 defect correction (extension): X += inner(B - A X) until the true
+// relative residual |B - A X| / |B| < tol (coupled_dot norm).
+KrylovResult refine_solve(fugu_ctx* c, int solver, const CoefBufs<double>& cb64, const SolveOpt& o,
+                          Trip<double> X, Trip<double> B, double dt, double tol, bool has_lid, double lid,
+                          int* outer_out) {
+  KrylovWork<double>& w = c->w64;
+  Trip<double>&r = w.t[10], &d = w.t[11], &ax = w.t[12];
+  const bool mixed = c->prm.precision == FUGU_MIXED;
+  if (mixed) {
+    ensure_w32(c);
+    CoefBufs<float>& f = c->w32.cf;
+    cvt(c, f.u_adv, cb64.u_adv); cvt(c, f.v_adv, cb64.v_adv); cvt(c, f.rho_c, cb64.rho_c);
+    cvt(c, f.rho_u, cb64.rho_u); cvt(c, f.rho_v, cb64.rho_v); cvt(c, f.kappa, cb64.kappa);
+    cvt(c, f.zeta, cb64.zeta); cvt(c, f.eta, cb64.eta);
+    if (o.pen) { cvt(c, f.pen_u, cb64.pen_u); cvt(c, f.pen_v, cb64.pen_v); }
+    if (o.amp) { cvt(c, f.mdu, cb64.mdu); cvt(c, f.mdv, cb64.mdv); }
+    poisson_coefs<float>(c, c->w32.pcg, cb64.rho_u, cb64.rho_v);
+  }
+  reset_ks(c);
+  vbcs(c, X.u, X.v, 0.0);
+  dot_op<double>(c, {{B, B}}, OpArgs{OP_REF_NORMB, 0, tol}, false);
+  KrylovResult res;
+  int outer = 0, inner_total = 0;
+  double rel = 0.0;
+  for (;; ++outer) {
+    matvec<double>(c, cb64, o, X, ax, dt, nullptr);
+    lin<double>(c, r, B, -1.0, c->sc + S_ONE, ax);
+    dot_op<double>(c, {{r, r}}, OpArgs{OP_REF_REL, 0, tol}, false);
+    rel = read_slot(c, S_TRUEREL);
+    KState ks = read_ks(c);
+    if (ks.nan || std::isnan(rel)) { res.status = FUGU_NAN; break; }
+    if (rel < tol) { res.status = FUGU_CONVERGED; break; }
+    if (outer >= c->prm.refine_max_outer) { res.status = FUGU_MAXITER; break; }
+    KrylovResult ir;
+    if (mixed) {
+      // the defect is scaled to unit norm before the FP32 solve (range safety)
+      KrylovWork<float>& w32 = c->w32;
+      Trip<float> r32 = w32.t[10], d32 = w32.t[11];
+      const long n3 = 3 * c->n;
+      k_convert_scaled<float><<<grid1d(c, n3), 256, 0, c->s>>>(n3, r32.base, r.base, c->sc + S_INVRNORM);
+      CKL("k_convert_scaled");
+      zero_trip(c, d32);
+      ir = krylov_inner<float>(c, solver, w32, w32.cf, o, d32, r32, dt, c->prm.refine_inner_tol,
+                               c->prm.refine_max_inner, false, 0.0);
+      k_accumulate<float><<<grid1d(c, n3), 256, 0, c->s>>>(n3, X.base, d32.base, c->sc + S_RNORM);
+      CKL("k_accumulate");
+    } else {
+      zero_trip(c, d);
+      ir = krylov_inner<double>(c, solver, w, cb64, o, d, r, dt, c->prm.refine_inner_tol, c->prm.refine_max_inner,
+                                false, 0.0);
+      lin<double>(c, X, X, 1.0, c->sc + S_ONE, d);
+    }
+    inner_total += ir.iter;
+    reset_ks(c);
+    vbcs(c, X.u, X.v, 0.0);
+  }
+  if (has_lid) vbcs(c, X.u, X.v, lid);
+  res.iter = inner_total;
+  res.res = rel;
+  if (outer_out) *outer_out = outer;
+  return res;
+}
+
+}  // namespace
+
+// ===================================================================== step
+namespace {
+
+Mix mix_of(const fugu_params& p) { return Mix{p.rho1, p.rho2, p.mu1, p.mu2}; }
+
+void properties(fugu_ctx* c, const double* cf, double* rho_c, double* rho_u, double* rho_v, double* kappa,
+                double* zeta, double* eta) {
+  Box b = box_launch(c->g);
+  k_properties<<<b.grid, b.block, 0, c->s>>>(c->g, mix_of(c->prm), cf, rho_c, rho_u, rho_v, kappa, zeta, eta);
+  CKL("k_properties");
+}
+
+// vof_advection_tvd (mod_vof.f90:38-140)
+void vof(fugu_ctx* c, const double* cin, double* cout, const double* u, const double* v, double dt, double* fx,
+         double* fy) {
+  Box b = box_launch(c->g);
+  k_vof_update<<<b.grid, b.block, 0, c->s>>>(c->g, c->prm.limiter, cin, u, v, dt, cout);
+  CKL("k_vof_update");
+  if (fx && fy) {
+    k_vof_fluxes<<<b.grid, b.block, 0, c->s>>>(c->g, c->prm.limiter, cin, u, v, dt, fx, fy);
+    CKL("k_vof_fluxes");
+    halo(c, fx, K_U);
+    halo(c, fy, K_V);
+  }
+  halo(c, cout, K_CELL);
+}
+
+// svof_helmholtz_filter (mod_vof.f90:145-194); returns nothing, adds the
+// iteration count to c->svof_iters
+void svof(fugu_ctx* c, const double* craw, double* cs, double* work, double delta, int max_iter, double tol) {
+  SvofArgs a;
+  a.g = c->g;
+  a.craw = craw;
+  a.out = cs;
+  a.work = work;
+  a.cx = (delta / c->g.dx) * (delta / c->g.dx);
+  a.cy = (delta / c->g.dy) * (delta / c->g.dy);
+  a.diag = 1.0 + 2.0 * (a.cx + a.cy);
+  a.max_iter = max_iter;
+  a.tol = tol;
+  a.part = c->part;
+  a.gs = c->gs;
+  a.iters = c->svof_iters;
+  a.status = c->svof_status;
+  CK(cudaMemsetAsync(c->gs, 0, sizeof(GridSync), c->s));
+  void* args[] = {&a};
+  CK(cudaLaunchCooperativeKernel((void*)k_svof, dim3(c->svof_grid), dim3(PCG_TPB), args, 0, c->s));
+}
+
+void curvature(fugu_ctx* c, const double* cs, double* kc) {
+  Box b = box_launch(c->g);
+  k_curvature<<<b.grid, b.block, 0, c->s>>>(c->g, cs, kc);
+  CKL("k_curvature");
+}
+void csf(fugu_ctx* c, const double* cf, const double* kc, double* fu, double* fv) {
+  Box b = box_launch(c->g);
+  k_csf<<<b.grid, b.block, 0, c->s>>>(c->g, c->prm.sigma, cf, kc, fu, fv);
+  CKL("k_csf");
+}
+
+void reset_counters(fugu_ctx* c) {
+  CK(cudaMemsetAsync(&c->ks->matvecs, 0, sizeof(unsigned long long), c->s));
+  CK(cudaMemsetAsync(c->pcg_out, 0, sizeof(PcgOut), c->s));
+  CK(cudaMemsetAsync(c->svof_iters, 0, sizeof(int), c->s));
+  CK(cudaMemsetAsync(c->svof_status, 0, sizeof(int), c->s));
+}
+// read statistics and the device-wait status; a barrier timeout is an error
+void collect(fugu_ctx* c, fugu_stats* st) {
+  CK(cudaMemcpyAsync(c->h_pcg, c->pcg_out, sizeof(PcgOut), cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(c->h_int, c->svof_iters, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(c->h_int + 1, c->svof_status, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+  CK(cudaMemcpyAsync(c->h_int + 2, &c->gs->error, sizeof(int), cudaMemcpyDeviceToHost, c->s));
+  sync(c);
+  if (c->h_int[1] || c->h_int[2] || c->h_pcg->status)
+    throw ApiError{FUGU_ETIMEOUT, "a persistent kernel's grid barrier gave up waiting"};
+  if (st) {
+    st->pcg_iters = (long long)c->h_pcg->total_iters;
+    st->pcg_calls = (int)c->h_pcg->calls;
+    st->svof_iters = c->h_int[0];
+  }
+}
+
+CoefBufs<double> coef64(fugu_ctx* c, const double* u_adv, const double* v_adv) {
+  CoefBufs<double> b;
+  b.u_adv = (double*)u_adv;
+  b.v_adv = (double*)v_adv;
+  b.rho_c = c->f[FUGU_F_RHO_C];
+  b.rho_u = c->f[FUGU_F_RHO_U];
+  b.rho_v = c->f[FUGU_F_RHO_V];
+  b.kappa = c->f[FUGU_F_KAPPA];
+  b.zeta = c->f[FUGU_F_ZETA];
+  b.eta = c->f[FUGU_F_ETA];
+  b.pen_u = c->pen_u;
+  b.pen_v = c->pen_v;
+  b.mdu = c->mdu;
+  b.mdv = c->mdv;
+  return b;
+}
+
+// the solve used by the step and by fugu_krylov_solve
+KrylovResult solve(fugu_ctx* c, int solver, const CoefBufs<double>& cb, const SolveOpt& o, Trip<double> X,
+                   Trip<double> B, double dt, double tol, int max_iter, bool has_lid, double lid, int* outer) {
+  poisson_coefs<double>(c, c->w64.pcg, cb.rho_u, cb.rho_v);
+  if (c->prm.refine) return refine_solve(c, solver, cb, o, X, B, dt, tol, has_lid, lid, outer);
+  if (outer) *outer = 0;
+  return krylov_inner<double>(c, solver, c->w64, cb, o, X, B, dt, tol, max_iter, has_lid, lid);
+}
+
+// advance_coupled_step, mod_solver_coupled.f90:137-380, on the device state
+void step(fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o, fugu_stats* st) {
+  const fugu_params& p = c->prm;
+  double** f = c->f;
+  const long n = c->n;
+  const bool amp = o->consistent_amp != 0;
+  const bool pen = o->has_penalty != 0;
+  const double tol = o->has_tol ? o->tol : p.tol_bicgstab2;
+  const int max_it = o->has_max_iter ? o->max_iter : p.max_iter_bicgstab2;
+  const double lid = o->has_lid ? o->u_top_lid : 0.0;
+  const bool bdf2 = (p.time_order == 2 && step_idx >= 2);
+  const double dt_eff = bdf2 ? dt / 1.5 : dt;
+  reset_counters(c);
+  // 1. AB extrapolation u_adv = 2u^n - u^(n-1); u_prev <- u^n (u_prev then holds u^n)
+  k_extrapolate<<<grid1d(c, n), 256, 0, c->s>>>(n, f[FUGU_F_U_VEL], f[FUGU_F_U_PREV], c->u_nm1, c->u_adv,
+                                                 step_idx <= 1);
+  k_extrapolate<<<grid1d(c, n), 256, 0, c->s>>>(n, f[FUGU_F_V_VEL], f[FUGU_F_V_PREV], c->v_nm1, c->v_adv,
+                                                 step_idx <= 1);
+  CKL("k_extrapolate");
+  const double* u_n = f[FUGU_F_U_PREV];
+  const double* v_n = f[FUGU_F_V_PREV];
+  // 2. VOF transport with u^n (+ AMP mass fluxes)
+  vof(c, f[FUGU_F_C_FIELD], c->c_new, u_n, v_n, dt, amp ? c->fcx : nullptr, amp ? c->fcy : nullptr);
+  if (amp) {
+    k_axpby<<<grid1d(c, n), 256, 0, c->s>>>(n, c->mdu, p.rho1 - p.rho2, c->fcx, p.rho2, c->u_adv);
+    k_axpby<<<grid1d(c, n), 256, 0, c->s>>>(n, c->mdv, p.rho1 - p.rho2, c->fcy, p.rho2, c->v_adv);
+    CKL("k_axpby");
+  }
+  CK(cudaMemcpyAsync(f[FUGU_F_C_FIELD], c->c_new, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->s));
+  // 3. properties at t^(n+1)
+  properties(c, f[FUGU_F_C_FIELD], f[FUGU_F_RHO_C], f[FUGU_F_RHO_U], f[FUGU_F_RHO_V], f[FUGU_F_KAPPA],
+             f[FUGU_F_ZETA], f[FUGU_F_ETA]);
+  // 4. SVOF + curvature + CSF
+  if (p.sigma > 1.0e-14) {
+    const double delta = p.svof_delta_h * (c->g.dx < c->g.dy ? c->g.dx : c->g.dy);
+    svof(c, f[FUGU_F_C_FIELD], c->c_s, c->svof_w, delta, p.svof_max_iter, p.svof_tol);
+    curvature(c, c->c_s, f[FUGU_F_KAPPA_CURV]);
+    csf(c, f[FUGU_F_C_FIELD], f[FUGU_F_KAPPA_CURV], f[FUGU_F_F_SIGMA_U], f[FUGU_F_F_SIGMA_V]);
+  } else {
+    CK(cudaMemsetAsync(f[FUGU_F_KAPPA_CURV], 0, sizeof(double) * n, c->s));
+    CK(cudaMemsetAsync(f[FUGU_F_F_SIGMA_U], 0, sizeof(double) * n, c->s));
+    CK(cudaMemsetAsync(f[FUGU_F_F_SIGMA_V], 0, sizeof(double) * n, c->s));
+  }
+  // 5. Darcy penalty
+  if (pen) {
+    k_axpby<<<grid1d(c, n), 256, 0, c->s>>>(n, c->pen_u, p.alpha_penalty, f[FUGU_F_PHI_S_U], 0.0, nullptr);
+    k_axpby<<<grid1d(c, n), 256, 0, c->s>>>(n, c->pen_v, p.alpha_penalty, f[FUGU_F_PHI_S_V], 0.0, nullptr);
+    CKL("k_axpby");
+  }
+  // 6. right-hand side
+  RhsArgs ra;
+  ra.rho_u = f[FUGU_F_RHO_U]; ra.rho_v = f[FUGU_F_RHO_V];
+  ra.u_n = u_n; ra.u_nm1 = c->u_nm1; ra.v_n = v_n; ra.v_nm1 = c->v_nm1;
+  ra.fsu = f[FUGU_F_F_SIGMA_U]; ra.fsv = f[FUGU_F_F_SIGMA_V];
+  ra.pen_u = pen ? c->pen_u : nullptr; ra.pen_v = pen ? c->pen_v : nullptr;
+  ra.zeta = f[FUGU_F_ZETA]; ra.eta = f[FUGU_F_ETA];
+  ra.dt = dt; ra.gx = p.gx; ra.gy = p.gy;
+  ra.u_sol = o->has_u_solid ? o->u_solid : 0.0;
+  ra.v_sol = o->has_v_solid ? o->v_solid : 0.0;
+  ra.u_lid = lid;
+  ra.bdf2 = bdf2 ? 1 : 0;
+  ra.has_lid = o->has_lid ? 1 : 0;
+  Box b = box_launch(c->g);
+  k_rhs<<<b.grid, b.block, 0, c->s>>>(c->g, ra, c->B.u, c->B.v, c->B.p);
+  CKL("k_rhs");
+  // 7. monolithic solve (u_top_lid is always present in this call); the
+  // state u_vel, v_vel, p_field is one contiguous coupled triple
+  SolveOpt so;
+  so.pen = pen;
+  so.amp = amp;
+  CoefBufs<double> cb = coef64(c, c->u_adv, c->v_adv);
+  Trip<double> Xc = c->Xstate;
+  KrylovResult kr;
+  int outer = 0;
+  kr = solve(c, o->use_bicgstab2 ? 2 : 1, cb, so, Xc, c->B, dt_eff, tol, max_it, true, lid, &outer);
+  // 8. final halos and BCs
+  halo(c, Xc.u, K_U);
+  halo(c, Xc.v, K_V);
+  halo(c, Xc.p, K_CELL);
+  vbcs(c, Xc.u, Xc.v, lid);
+  collect(c, st);
+  if (st) {
+    st->iter = kr.iter;
+    st->res = kr.res;
+    st->outer = outer;
+    st->status = kr.status;
+    KState ks = read_ks(c);
+    st->matvecs = (int)ks.matvecs;
+  }
+}
+
+}  // namespace
+
+// ================================================================= context
+namespace {
+
+int check_params(const fugu_params* p) {
+  if (!p) return FUGU_EINVAL;
+  if (p->nx < 4 || p->ny < 4 || p->nx > 65536 || p->ny > 65536) return FUGU_EINVAL;
+  if (!(p->dx > 0.0) || !(p->dy > 0.0)) return FUGU_EINVAL;
+  if (p->pcg_max_iter < 0 || p->pcd_sweeps < 0 || p->svof_max_iter < 0) return FUGU_EINVAL;
+  if (p->precision == FUGU_MIXED && !p->refine) return FUGU_EINVAL;
+  if (p->precision != FUGU_FP64 && p->precision != FUGU_MIXED) return FUGU_EINVAL;
+  return FUGU_OK;
+}
+
+int coop_grid(const void* fn, int tpb, int nsm, long work) {
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, tpb, 0) != cudaSuccess || occ < 1) return 0;
+  long want = (work + tpb - 1) / tpb;
+  long cap = (long)nsm * occ;
+  if (cap > nsm) cap = nsm;  // one CTA per SM keeps the barrier short
+  if (want < 1) want = 1;
+  return (int)(want < cap ? want : cap);
+}
+
+void create(fugu_ctx* c) {
+  CK(cudaSetDevice(c->device));
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, c->device));
+  if (!prop.cooperativeLaunch) throw ApiError{FUGU_ECUDA, "device lacks cooperative launch"};
+  c->nsm = prop.multiProcessorCount;
+  CK(cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking));
+  c->g = make_geo(c->prm);
+  c->n = c->g.n();
+  c->Xstate = talloc<double>(c);
+  for (int i = 0; i < FUGU_NUM_FIELDS; ++i) c->f[i] = dalloc<double>(c, c->n);
+  c->f[FUGU_F_U_VEL] = c->Xstate.u;
+  c->f[FUGU_F_V_VEL] = c->Xstate.v;
+  c->f[FUGU_F_P_FIELD] = c->Xstate.p;
+  c->u_nm1 = dalloc<double>(c, c->n); c->v_nm1 = dalloc<double>(c, c->n);
+  c->u_adv = dalloc<double>(c, c->n); c->v_adv = dalloc<double>(c, c->n);
+  c->c_new = dalloc<double>(c, c->n); c->c_s = dalloc<double>(c, c->n); c->svof_w = dalloc<double>(c, c->n);
+  c->fcx = dalloc<double>(c, c->n); c->fcy = dalloc<double>(c, c->n);
+  c->mdu = dalloc<double>(c, c->n); c->mdv = dalloc<double>(c, c->n);
+  c->pen_u = dalloc<double>(c, c->n); c->pen_v = dalloc<double>(c, c->n);
+  c->B = talloc<double>(c);
+  KrylovWork<double>& w = c->w64;
+  for (auto& t : w.t) t = talloc<double>(c);
+  w.pcd.phi = dalloc<double>(c, c->n); w.pcd.zuw = dalloc<double>(c, c->n);
+  w.pcd.zvw = dalloc<double>(c, c->n); w.pcd.tmp = dalloc<double>(c, c->n);
+  PcgWork<double>& p = w.pcg;
+  p.cx = dalloc<double>(c, c->n); p.cy = dalloc<double>(c, c->n); p.dinv = dalloc<double>(c, c->n);
+  p.r = dalloc<double>(c, c->n); p.z = dalloc<double>(c, c->n); p.pb0 = dalloc<double>(c, c->n);
+  p.pb1 = dalloc<double>(c, c->n); p.ap = dalloc<double>(c, c->n);
+  for (auto& sp : c->scratch) sp = dalloc<double>(c, 3 * c->n);
+  c->sc = dalloc<double>(c, NSLOTS);
+  c->ks = dalloc<KState>(c, 1);
+  const long ncell = (long)c->prm.nx * c->prm.ny;
+  c->pcg_grid = coop_grid((const void*)k_pcg<double>, PCG_TPB, c->nsm, ncell);
+  int g32 = coop_grid((const void*)k_pcg<float>, PCG_TPB, c->nsm, ncell);
+  if (g32 < c->pcg_grid) c->pcg_grid = g32;
+  c->svof_grid = coop_grid((const void*)k_svof, PCG_TPB, c->nsm, ncell);
+  if (c->pcg_grid < 1 || c->svof_grid < 1) throw ApiError{FUGU_ECUDA, "no co-resident grid for persistent kernels"};
+  c->dot_grid = c->nsm * 2;
+  c->part_len = 8L * (c->nsm * 8 + 64);
+  c->part = dalloc<double>(c, c->part_len);
+  c->gs = dalloc<GridSync>(c, 1);
+  c->pcg_out = dalloc<PcgOut>(c, 1);
+  c->svof_iters = dalloc<int>(c, 1);
+  c->svof_status = dalloc<int>(c, 1);
+  CK(cudaMallocHost(&c->h_ks, sizeof(KState)));
+  CK(cudaMallocHost(&c->h_sc, sizeof(double) * NSLOTS));
+  CK(cudaMallocHost(&c->h_pcg, sizeof(PcgOut)));
+  CK(cudaMallocHost(&c->h_int, sizeof(int) * 8));
+  const double one = 1.0;
+  CK(cudaMemcpyAsync(c->sc + S_ONE, &one, sizeof(double), cudaMemcpyHostToDevice, c->s));
+  sync(c);
+}
+
+void destroy(fugu_ctx* c) {
+  if (!c) return;
+  if (c->s) cudaStreamSynchronize(c->s);
+  for (void* p : c->allocs) cudaFree(p);
+  if (c->h_ks) cudaFreeHost(c->h_ks);
+  if (c->h_sc) cudaFreeHost(c->h_sc);
+  if (c->h_pcg) cudaFreeHost(c->h_pcg);
+  if (c->h_int) cudaFreeHost(c->h_int);
+  if (c->s) cudaStreamDestroy(c->s);
+  delete c;
+}
+
+// run fn, translating exceptions into an ABI status and a message
+template <typename F>
+int guard(fugu_ctx* c, F fn) {
+  if (!c) return FUGU_EINVAL;
+  try {
+    cudaSetDevice(c->device);
+    fn();
+    return FUGU_OK;
+  } catch (const CudaError& e) {
+    c->err = std::string(e.what) + ": " + cudaGetErrorString(e.e);
+    return FUGU_ECUDA;
+  } catch (const ApiError& e) {
+    c->err = e.msg;
+    return e.code;
+  } catch (const std::exception& e) {
+    c->err = e.what();
+    return FUGU_ECUDA;
+  }
+}
+
+// routine-level helpers: scratch buffer k (single component) / triple view
+double* S(fugu_ctx* c, int k) { return c->scratch[k]; }
+Trip<double> ST(fugu_ctx* c, int k) {
+  Trip<double> t;
+  t.base = c->scratch[k];
+  t.u = t.base;
+  t.v = t.base + c->n;
+  t.p = t.base + 2 * c->n;
+  return t;
+}
+double* upk(fugu_ctx* c, int k, const double* h, int kind) {
+  if (!h) return nullptr;
+  up(c, S(c, k), h, kind);
+  return S(c, k);
+}
+
+}  // namespace
+
+// ================================================================== C ABI
+extern "C" {
+
+void fugu_params_default(fugu_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->nx = 64; p->ny = 64; p->dx = 1.0 / 64; p->dy = 1.0 / 64;
+  p->rho1 = 1000.0; p->rho2 = 1.0; p->mu1 = 1.0; p->mu2 = 0.01;
+  p->sigma = 0.0; p->gx = 0.0; p->gy = -9.81;
+  p->cfl_target = 0.5; p->alpha_penalty = 1.0e12; p->time_order = 1;
+  p->tol_bicgstab2 = 1.0e-6; p->max_iter_bicgstab2 = 500;
+  p->pcg_tol = 1.0e-5; p->pcg_max_iter = 150; p->pcd_sweeps = 3; p->jacobi_omega = 0.8;
+  p->svof_delta_h = 1.5; p->svof_max_iter = 150; p->svof_tol = 1.0e-7;
+  p->refine_inner_tol = 1.0e-2; p->refine_max_inner = 20; p->refine_max_outer = 30;
+  p->precision = FUGU_FP64;
+}
+
+const char* fugu_version(void) { return "fugu-b200 1 (sm_100a)"; }
+
+int fugu_create(const fugu_params* p, int device, fugu_ctx** out) {
+  if (!out) return FUGU_EINVAL;
+  *out = nullptr;
+  int rc = check_params(p);
+  if (rc) return rc;
+  fugu_ctx* c = new fugu_ctx();
+  c->prm = *p;
+  c->device = device;
+  rc = guard(c, [&] { create(c); });
+  if (rc) {
+    fprintf(stderr, "fugu_create: %s\n", c->err.c_str());
+    destroy(c);
+    return rc;
+  }
+  *out = c;
+  return FUGU_OK;
+}
+
+void fugu_destroy(fugu_ctx* ctx) { destroy(ctx); }
+
+int fugu_set_params(fugu_ctx* c, const fugu_params* p) {
+  int rc = check_params(p);
+  if (rc || !c) return rc ? rc : FUGU_EINVAL;
+  if (p->nx != c->prm.nx || p->ny != c->prm.ny) {
+    c->err = "fugu_set_params: the grid size of a context is fixed";
+    return FUGU_EINVAL;
+  }
+  c->prm = *p;
+  c->g = make_geo(*p);
+  return FUGU_OK;
+}
+
+const char* fugu_last_error(const fugu_ctx* c) { return c ? c->err.c_str() : "NULL context"; }
+
+int fugu_upload(fugu_ctx* c, int field, const double* host) {
+  return guard(c, [&] {
+    if (field < 0 || field >= FUGU_NUM_FIELDS) throw ApiError{FUGU_EINVAL, "bad field id"};
+    up(c, c->f[field], host, kind_of_field(field));
+    sync(c);
+  });
+}
+int fugu_download(fugu_ctx* c, int field, double* host) {
+  return guard(c, [&] {
+    if (field < 0 || field >= FUGU_NUM_FIELDS) throw ApiError{FUGU_EINVAL, "bad field id"};
+    down(c, host, c->f[field], kind_of_field(field));
+    sync(c);
+  });
+}
+
+int fugu_step(fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o, fugu_stats* st) {
+  return guard(c, [&] {
+    if (!o) throw ApiError{FUGU_EINVAL, "NULL options"};
+    if (st) std::memset(st, 0, sizeof(*st));
+    step(c, dt, step_idx, o, st);
+  });
+}
+
+int fugu_advance_coupled_step(fugu_ctx* c, double* u_vel, double* v_vel, double* p_field, double* c_field,
+                              double* u_prev, double* v_prev, double* rho_c, double* rho_u, double* rho_v,
+                              double* kappa, double* zeta, double* eta, double* kappa_curv, double* f_sigma_u,
+                              double* f_sigma_v, const double* phi_s_u, const double* phi_s_v, double dt,
+                              int step_idx, const fugu_step_opts* o, fugu_stats* st) {
+  return guard(c, [&] {
+    if (!o) throw ApiError{FUGU_EINVAL, "NULL options"};
+    if (o->has_penalty && (!phi_s_u || !phi_s_v)) throw ApiError{FUGU_EINVAL, "penalty without mask"};
+    double* in[] = {u_vel, v_vel, p_field, c_field, u_prev, v_prev, rho_c, rho_u, rho_v,
+                    kappa, zeta, eta, kappa_curv, f_sigma_u, f_sigma_v};
+    for (int i = 0; i < 15; ++i) up(c, c->f[i], in[i], kind_of_field(i));
+    if (o->has_penalty) {
+      up(c, c->f[FUGU_F_PHI_S_U], phi_s_u, K_U);
+      up(c, c->f[FUGU_F_PHI_S_V], phi_s_v, K_V);
+    }
+    if (st) std::memset(st, 0, sizeof(*st));
+    step(c, dt, step_idx, o, st);
+    for (int i = 0; i < 15; ++i) down(c, in[i], c->f[i], kind_of_field(i));
+    sync(c);
+  });
+}
+
+int fugu_compute_adaptive_dt(fugu_ctx* c, const double* u_vel, const double* v_vel, double dt_max,
+                             double* dt_out) {
+  return guard(c, [&] {
+    if (!dt_out) throw ApiError{FUGU_EINVAL, "NULL dt_out"};
+    double* u = upk(c, 0, u_vel, K_U);
+    double* v = upk(c, 1, v_vel, K_V);
+    const int nb = c->nsm;
+    k_maxvel<<<nb, 256, 0, c->s>>>(c->g, u, v, c->part);
+    CKL("k_maxvel");
+    std::vector<double> part(2 * nb);
+    CK(cudaMemcpyAsync(part.data(), c->part, sizeof(double) * 2 * nb, cudaMemcpyDeviceToHost, c->s));
+    sync(c);
+    double um = 0.0, vm = 0.0;
+    for (int b = 0; b < nb; ++b) {
+      um = part[2 * b] > um ? part[2 * b] : um;
+      vm = part[2 * b + 1] > vm ? part[2 * b + 1] : vm;
+    }
+    // scalar tail of compute_adaptive_dt (mod_solver_coupled.f90:68-90)
+    const fugu_params& p = c->prm;
+    const double h = p.dx < p.dy ? p.dx : p.dy;
+    const double pi = 3.141592653589793238462643383279502884197;
+    double dcfl = (um / p.dx + vm / p.dy > 1.0e-12) ? p.cfl_target / (um / p.dx + vm / p.dy) : dt_max;
+    double dtl = dt_max < dcfl ? dt_max : dcfl;
+    if (p.sigma > 1.0e-14) {
+      const double dcap = 0.5 * std::sqrt((p.rho1 + p.rho2) * (h * h * h) / (4.0 * pi * p.sigma));
+      dtl = dtl < dcap ? dtl : dcap;
+    }
+    const double gm = std::sqrt(p.gx * p.gx + p.gy * p.gy);
+    if (gm > 1.0e-14) {
+      const double dg = 0.5 * std::sqrt(h / gm);
+      dtl = dtl < dg ? dtl : dg;
+    }
+    *dt_out = dtl;
+  });
+}
+
+int fugu_build_cylinder_mask(fugu_ctx* c, double xc, double yc, double rad, double* phi_s_u, double* phi_s_v) {
+  return guard(c, [&] {
+    Box b = box_launch(c->g);
+    k_cylinder<<<b.grid, b.block, 0, c->s>>>(c->g, xc, yc, rad, S(c, 0), S(c, 1));
+    CKL("k_cylinder");
+    halo(c, S(c, 0), K_U);
+    halo(c, S(c, 1), K_V);
+    down(c, phi_s_u, S(c, 0), K_U);
+    down(c, phi_s_v, S(c, 1), K_V);
+    sync(c);
+  });
+}
+
+int fugu_halo_scalar(fugu_ctx* c, double* phi) {
+  return guard(c, [&] { upk(c, 0, phi, K_CELL); halo(c, S(c, 0), K_CELL); down(c, phi, S(c, 0), K_CELL); sync(c); });
+}
+int fugu_halo_u(fugu_ctx* c, double* u) {
+  return guard(c, [&] { upk(c, 0, u, K_U); halo(c, S(c, 0), K_U); down(c, u, S(c, 0), K_U); sync(c); });
+}
+int fugu_halo_v(fugu_ctx* c, double* v) {
+  return guard(c, [&] { upk(c, 0, v, K_V); halo(c, S(c, 0), K_V); down(c, v, S(c, 0), K_V); sync(c); });
+}
+
+int fugu_compute_mixture_densities(fugu_ctx* c, const double* cf, double* rho_c, double* rho_u, double* rho_v) {
+  return guard(c, [&] {
+    double* cc = upk(c, 0, cf, K_CELL);
+    properties(c, cc, S(c, 1), S(c, 2), S(c, 3), S(c, 4), S(c, 5), S(c, 6));
+    down(c, rho_c, S(c, 1), K_CELL);
+    down(c, rho_u, S(c, 2), K_U);
+    down(c, rho_v, S(c, 3), K_V);
+    sync(c);
+  });
+}
+int fugu_compute_mixture_viscosities(fugu_ctx* c, const double* cf, double* kappa, double* zeta, double* eta) {
+  return guard(c, [&] {
+    double* cc = upk(c, 0, cf, K_CELL);
+    properties(c, cc, S(c, 1), S(c, 2), S(c, 3), S(c, 4), S(c, 5), S(c, 6));
+    down(c, kappa, S(c, 4), K_CELL);
+    down(c, zeta, S(c, 5), K_VERT);
+    down(c, eta, S(c, 6), K_VERT);
+    sync(c);
+  });
+}
+
+int fugu_op_divergence(fugu_ctx* c, const double* u, const double* v, double* div) {
+  return guard(c, [&] {
+    double* du = upk(c, 0, u, K_U);
+    double* dv = upk(c, 1, v, K_V);
+    Box b = box_launch(c->g);
+    k_op_divergence<<<b.grid, b.block, 0, c->s>>>(c->g, du, dv, S(c, 2));
+    CKL("k_op_divergence");
+    down(c, div, S(c, 2), K_CELL);
+    sync(c);
+  });
+}
+int fugu_op_grad_pressure(fugu_ctx* c, const double* p, double* gu, double* gv) {
+  return guard(c, [&] {
+    double* dp = upk(c, 0, p, K_CELL);
+    Box b = box_launch(c->g);
+    k_op_grad<<<b.grid, b.block, 0, c->s>>>(c->g, dp, S(c, 1), S(c, 2));
+    CKL("k_op_grad");
+    down(c, gu, S(c, 1), K_U);
+    down(c, gv, S(c, 2), K_V);
+    sync(c);
+  });
+}
+int fugu_op_viscous_stress(fugu_ctx* c, const double* u, const double* v, const double* kappa, const double* zeta,
+                           const double* eta, double* vu, double* vv) {
+  return guard(c, [&] {
+    double *du = upk(c, 0, u, K_U), *dv = upk(c, 1, v, K_V), *dk = upk(c, 2, kappa, K_CELL);
+    double *dz = upk(c, 3, zeta, K_VERT), *de = upk(c, 4, eta, K_VERT);
+    Box b = box_launch(c->g);
+    k_op_visc<<<b.grid, b.block, 0, c->s>>>(c->g, du, dv, dk, dz, de, S(c, 5), S(c, 6));
+    CKL("k_op_visc");
+    down(c, vu, S(c, 5), K_U);
+    down(c, vv, S(c, 6), K_V);
+    sync(c);
+  });
+}
+int fugu_op_advection(fugu_ctx* c, const double* u_adv, const double* v_adv, const double* rho_c,
+                      const double* rho_u, const double* rho_v, const double* u, const double* v, double* adv_u,
+                      double* adv_v, const double* mdot_u, const double* mdot_v) {
+  return guard(c, [&] {
+    Coefs<double> cf{};
+    cf.u_adv = upk(c, 0, u_adv, K_U);
+    cf.v_adv = upk(c, 1, v_adv, K_V);
+    cf.rho_c = upk(c, 2, rho_c, K_CELL);
+    cf.rho_u = upk(c, 3, rho_u, K_U);
+    cf.rho_v = upk(c, 4, rho_v, K_V);
+    const bool cons = mdot_u && mdot_v;
+    cf.mdot_u = cons ? upk(c, 5, mdot_u, K_U) : nullptr;
+    cf.mdot_v = cons ? upk(c, 6, mdot_v, K_V) : nullptr;
+    double *du = upk(c, 7, u, K_U), *dv = upk(c, 8, v, K_V);
+    Box b = box_launch(c->g);
+    k_op_adv<<<b.grid, b.block, 0, c->s>>>(c->g, cf, du, dv, S(c, 9), S(c, 10));
+    CKL("k_op_adv");
+    down(c, adv_u, S(c, 9), K_U);
+    down(c, adv_v, S(c, 10), K_V);
+    sync(c);
+  });
+}
+int fugu_apply_velocity_bcs(fugu_ctx* c, double* u, double* v, int has_lid, double u_lid) {
+  return guard(c, [&] {
+    upk(c, 0, u, K_U);
+    upk(c, 1, v, K_V);
+    vbcs(c, S(c, 0), S(c, 1), has_lid ? u_lid : 0.0);
+    down(c, u, S(c, 0), K_U);
+    down(c, v, S(c, 1), K_V);
+    sync(c);
+  });
+}
+
+}  // extern "C"
+
+namespace {
+// coefficient set of a routine-level call: uploads into scratch 4..15
+CoefBufs<double> up_coefs(fugu_ctx* c, const double* u_adv, const double* v_adv, const double* rho_c,
+                          const double* rho_u, const double* rho_v, const double* kappa, const double* zeta,
+                          const double* eta, const double* pen_u, const double* pen_v, const double* mdu,
+                          const double* mdv) {
+  CoefBufs<double> b;
+  b.u_adv = upk(c, 4, u_adv, K_U);
+  b.v_adv = upk(c, 5, v_adv, K_V);
+  b.rho_c = upk(c, 6, rho_c, K_CELL);
+  b.rho_u = upk(c, 7, rho_u, K_U);
+  b.rho_v = upk(c, 8, rho_v, K_V);
+  b.kappa = upk(c, 9, kappa, K_CELL);
+  b.zeta = upk(c, 10, zeta, K_VERT);
+  b.eta = upk(c, 11, eta, K_VERT);
+  b.pen_u = upk(c, 12, pen_u, K_U);
+  b.pen_v = upk(c, 13, pen_v, K_V);
+  b.mdu = upk(c, 14, mdu, K_U);
+  b.mdv = upk(c, 15, mdv, K_V);
+  return b;
+}
+void up_trip(fugu_ctx* c, Trip<double> t, const double* u, const double* v, const double* p) {
+  up(c, t.u, u, K_U);
+  up(c, t.v, v, K_V);
+  up(c, t.p, p, K_CELL);
+}
+void down_trip(fugu_ctx* c, Trip<double> t, double* u, double* v, double* p) {
+  if (u) down(c, u, t.u, K_U);
+  if (v) down(c, v, t.v, K_V);
+  if (p) down(c, p, t.p, K_CELL);
+}
+
+}  // namespace
+
+extern "C" {
+
+int fugu_matvec_coupled(fugu_ctx* c, double* Xu, double* Xv, double* Xp, double* Yu, double* Yv, double* Yp,
+                        const double* u_adv, const double* v_adv, const double* rho_c, const double* rho_u,
+                        const double* rho_v, const double* kappa, const double* zeta, const double* eta,
+                        double dt, int include_advection, const double* pen_u, const double* pen_v,
+                        const double* mdot_u, const double* mdot_v) {
+  return guard(c, [&] {
+    CoefBufs<double> cb = up_coefs(c, u_adv, v_adv, rho_c, rho_u, rho_v, kappa, zeta, eta, pen_u, pen_v,
+                                   mdot_u, mdot_v);
+    SolveOpt o;
+    o.pen = pen_u && pen_v;
+    o.amp = mdot_u && mdot_v;
+    Trip<double> X = ST(c, 0), Y = ST(c, 1);
+    up_trip(c, X, Xu, Xv, Xp);
+    halo(c, X.u, K_U);
+    halo(c, X.v, K_V);
+    halo(c, X.p, K_CELL);
+    Box b = box_launch(c->g);
+    k_matvec<double><<<b.grid, b.block, 0, c->s>>>(c->g, coefs_of(cb, o), X.u, X.v, X.p, Y.u, Y.v, Y.p, dt,
+                                                    include_advection ? 1 : 0, nullptr, nullptr);
+    CKL("k_matvec");
+    down_trip(c, X, Xu, Xv, Xp);
+    down_trip(c, Y, Yu, Yv, Yp);
+    sync(c);
+  });
+}
+
+int fugu_solve_poisson_pressure(fugu_ctx* c, double* phi, const double* rhs, const double* rho_u,
+                                const double* rho_v, double tol, int max_iter, int* iter_out, double* res_out) {
+  return guard(c, [&] {
+    double* dphi = upk(c, 0, phi, K_CELL);
+    double* drhs = upk(c, 1, rhs, K_CELL);
+    double* dru = upk(c, 2, rho_u, K_U);
+    double* drv = upk(c, 3, rho_v, K_V);
+    reset_counters(c);
+    poisson_coefs<double>(c, c->w64.pcg, dru, drv);
+    pcg<double>(c, c->w64.pcg, dphi, drhs, tol, max_iter, false, nullptr);
+    collect(c, nullptr);
+    down(c, phi, dphi, K_CELL);
+    CK(cudaMemcpyAsync(c->h_pcg, c->pcg_out, sizeof(PcgOut), cudaMemcpyDeviceToHost, c->s));
+    sync(c);
+    if (iter_out) *iter_out = c->h_pcg->iters;
+    if (res_out) *res_out = c->h_pcg->res;
+  });
+}
+
+}  // extern "C"
+
+namespace {
+int helm_entry(fugu_ctx* c, bool is_u, double* sol, const double* rhs, const double* rho,
+                      const double* kappa, const double* zeta, const double* eta, double dt, int n_sweeps,
+                      const double* pen) {
+  return guard(c, [&] {
+    const int kind = is_u ? K_U : K_V;
+    double* ds = upk(c, 0, sol, kind);
+    double* dr = upk(c, 1, rhs, kind);
+    CoefBufs<double> cb;
+    if (is_u) cb.rho_u = upk(c, 2, rho, K_U);
+    else cb.rho_v = upk(c, 2, rho, K_V);
+    cb.kappa = upk(c, 3, kappa, K_CELL);
+    cb.zeta = upk(c, 4, zeta, K_VERT);
+    cb.eta = upk(c, 5, eta, K_VERT);
+    if (is_u) cb.pen_u = upk(c, 6, pen, K_U);
+    else cb.pen_v = upk(c, 6, pen, K_V);
+    SolveOpt o;
+    o.pen = pen != nullptr;
+    helmholtz<double>(c, is_u, ds, S(c, 7), dr, cb, o, dt, n_sweeps, nullptr);
+    down(c, sol, ds, kind);
+    sync(c);
+  });
+}
+}  // namespace
+
+extern "C" {
+
+int fugu_solve_helmholtz_u(fugu_ctx* c, double* u_sol, const double* rhs_u, const double* rho_u,
+                           const double* kappa, const double* zeta, const double* eta, double dt, int n_sweeps,
+                           const double* penalty_u) {
+  return helm_entry(c, true, u_sol, rhs_u, rho_u, kappa, zeta, eta, dt, n_sweeps, penalty_u);
+}
+int fugu_solve_helmholtz_v(fugu_ctx* c, double* v_sol, const double* rhs_v, const double* rho_v,
+                           const double* kappa, const double* zeta, const double* eta, double dt, int n_sweeps,
+                           const double* penalty_v) {
+  return helm_entry(c, false, v_sol, rhs_v, rho_v, kappa, zeta, eta, dt, n_sweeps, penalty_v);
+}
+
+int fugu_apply_pcd_precond(fugu_ctx* c, const double* z_u, const double* z_v, const double* z_p, double* r_u,
+                           double* r_v, double* r_p, const double* u_adv, const double* v_adv,
+                           const double* rho_u, const double* rho_v, const double* kappa, const double* zeta,
+                           const double* eta, double dt, const double* penalty_u, const double* penalty_v) {
+  return guard(c, [&] {
+    CoefBufs<double> cb = up_coefs(c, u_adv, v_adv, nullptr, rho_u, rho_v, kappa, zeta, eta, penalty_u,
+                                   penalty_v, nullptr, nullptr);
+    SolveOpt o;
+    o.pen = penalty_u && penalty_v;
+    Trip<double> Z = ST(c, 0), R = ST(c, 1);
+    up_trip(c, Z, z_u, z_v, z_p);
+    reset_counters(c);
+    poisson_coefs<double>(c, c->w64.pcg, cb.rho_u, cb.rho_v);
+    pcd<double>(c, c->w64, cb, o, Z, R, dt, nullptr);
+    collect(c, nullptr);
+    down_trip(c, R, r_u, r_v, r_p);
+    sync(c);
+  });
+}
+
+int fugu_coupled_dot(fugu_ctx* c, const double* u1, const double* v1, const double* p1, const double* u2,
+                     const double* v2, const double* p2, double* out) {
+  return guard(c, [&] {
+    if (!out) throw ApiError{FUGU_EINVAL, "NULL out"};
+    Trip<double> A = ST(c, 0), B = ST(c, 1);
+    up_trip(c, A, u1, v1, p1);
+    up_trip(c, B, u2, v2, p2);
+    dot_op<double>(c, {{A, B}}, OpArgs{OP_STORE, 0, 0.0}, false);
+    *out = read_slot(c, S_D0);
+  });
+}
+
+int fugu_krylov_solve(fugu_ctx* c, int solver, double* X_u, double* X_v, double* X_p, const double* B_u,
+                      const double* B_v, const double* B_p, const double* u_adv, const double* v_adv,
+                      const double* rho_c, const double* rho_u, const double* rho_v, const double* kappa,
+                      const double* zeta, const double* eta, double dt, double tol, int max_iter, int has_lid,
+                      double u_lid, const double* penalty_u, const double* penalty_v, const double* mdot_u,
+                      const double* mdot_v, fugu_stats* st) {
+  return guard(c, [&] {
+    if (solver != 1 && solver != 2) throw ApiError{FUGU_EINVAL, "solver must be 1 or 2"};
+    CoefBufs<double> cb = up_coefs(c, u_adv, v_adv, rho_c, rho_u, rho_v, kappa, zeta, eta, penalty_u,
+                                   penalty_v, mdot_u, mdot_v);
+    SolveOpt o;
+    o.pen = penalty_u && penalty_v;
+    o.amp = mdot_u && mdot_v;
+    Trip<double> X = ST(c, 0), B = ST(c, 1);
+    up_trip(c, X, X_u, X_v, X_p);
+    up_trip(c, B, B_u, B_v, B_p);
+    reset_counters(c);
+    int outer = 0;
+    KrylovResult kr = solve(c, solver, cb, o, X, B, dt, tol, max_iter, has_lid != 0, u_lid, &outer);
+    if (st) std::memset(st, 0, sizeof(*st));
+    collect(c, st);
+    if (st) {
+      st->iter = kr.iter;
+      st->res = kr.res;
+      st->outer = outer;
+      st->status = kr.status;
+      KState ks = read_ks(c);
+      st->matvecs = (int)ks.matvecs;
+    }
+    down_trip(c, X, X_u, X_v, X_p);
+    sync(c);
+  });
+}
+
+int fugu_vof_advection_tvd(fugu_ctx* c, const double* c_in, double* c_out, const double* u, const double* v,
+                           double dt, double* flux_x, double* flux_y) {
+  return guard(c, [&] {
+    double* ci = upk(c, 0, c_in, K_CELL);
+    double* du = upk(c, 1, u, K_U);
+    double* dv = upk(c, 2, v, K_V);
+    const bool fl = flux_x && flux_y;
+    vof(c, ci, S(c, 3), du, dv, dt, fl ? S(c, 4) : nullptr, fl ? S(c, 5) : nullptr);
+    down(c, c_out, S(c, 3), K_CELL);
+    if (fl) {
+      down(c, flux_x, S(c, 4), K_U);
+      down(c, flux_y, S(c, 5), K_V);
+    }
+    sync(c);
+  });
+}
+
+int fugu_svof_helmholtz_filter(fugu_ctx* c, const double* c_raw, double* c_smooth, double delta, int max_iter,
+                               double tol, int* iters_out) {
+  return guard(c, [&] {
+    double* cr = upk(c, 0, c_raw, K_CELL);
+    reset_counters(c);
+    svof(c, cr, S(c, 1), S(c, 2), delta, max_iter, tol);
+    fugu_stats st{};
+    collect(c, &st);
+    if (iters_out) *iters_out = st.svof_iters;
+    down(c, c_smooth, S(c, 1), K_CELL);
+    sync(c);
+  });
+}
+
+int fugu_compute_interface_curvature(fugu_ctx* c, const double* c_smooth, double* kappa_curv) {
+  return guard(c, [&] {
+    double* cs = upk(c, 0, c_smooth, K_CELL);
+    curvature(c, cs, S(c, 1));
+    down(c, kappa_curv, S(c, 1), K_CELL);
+    sync(c);
+  });
+}
+
+int fugu_compute_csf_force(fugu_ctx* c, const double* c_raw, const double* kappa_curv, double* f_sigma_u,
+                           double* f_sigma_v) {
+  return guard(c, [&] {
+    double* cr = upk(c, 0, c_raw, K_CELL);
+    double* kc = upk(c, 1, kappa_curv, K_CELL);
+    csf(c, cr, kc, S(c, 2), S(c, 3));
+    down(c, f_sigma_u, S(c, 2), K_U);
+    down(c, f_sigma_v, S(c, 3), K_V);
+    sync(c);
+  });
+}
+
+// mod_io.f90:169-225 byte format
+int fugu_write_checkpoint(fugu_ctx* c, const char* path, int step_no, double t) {
+  return guard(c, [&] {
+    if (!path) throw ApiError{FUGU_EINVAL, "NULL path"};
+    const int nx = c->prm.nx, ny = c->prm.ny;
+    const size_t nu = (size_t)(nx + 5) * (ny + 4), nv = (size_t)(nx + 4) * (ny + 5), nc = (size_t)(nx + 4) * (ny + 4);
+    std::vector<double> buf(2 * nu + 2 * nv + 2 * nc);
+    double* b = buf.data();
+    down(c, b, c->f[FUGU_F_U_VEL], K_U); b += nu;
+    down(c, b, c->f[FUGU_F_V_VEL], K_V); b += nv;
+    down(c, b, c->f[FUGU_F_U_PREV], K_U); b += nu;
+    down(c, b, c->f[FUGU_F_V_PREV], K_V); b += nv;
+    down(c, b, c->f[FUGU_F_P_FIELD], K_CELL); b += nc;
+    down(c, b, c->f[FUGU_F_C_FIELD], K_CELL);
+    sync(c);
+    FILE* fp = fopen(path, "wb");
+    if (!fp) throw ApiError{FUGU_EIO, std::string("cannot open ") + path};
+    const int hdr[3] = {nx, ny, 2};
+    bool ok = fwrite(&step_no, sizeof(int), 1, fp) == 1 && fwrite(&t, sizeof(double), 1, fp) == 1 &&
+              fwrite(hdr, sizeof(int), 3, fp) == 3 && fwrite(buf.data(), sizeof(double), buf.size(), fp) == buf.size();
+    ok = (fclose(fp) == 0) && ok;
+    if (!ok) throw ApiError{FUGU_EIO, "checkpoint write failed"};
+  });
+}
+
+int fugu_read_checkpoint(fugu_ctx* c, const char* path, int* step_no, double* t) {
+  return guard(c, [&] {
+    if (!path || !step_no || !t) throw ApiError{FUGU_EINVAL, "NULL argument"};
+    const int nx = c->prm.nx, ny = c->prm.ny;
+    FILE* fp = fopen(path, "rb");
+    if (!fp) throw ApiError{FUGU_EIO, std::string("cannot open ") + path};
+    int hdr[3];
+    if (fread(step_no, sizeof(int), 1, fp) != 1 || fread(t, sizeof(double), 1, fp) != 1 ||
+        fread(hdr, sizeof(int), 3, fp) != 3 || hdr[0] != nx || hdr[1] != ny || hdr[2] != 2) {
+      fclose(fp);
+      throw ApiError{FUGU_EIO, "checkpoint header does not match the context (nx, ny, nh)"};
+    }
+    const size_t nu = (size_t)(nx + 5) * (ny + 4), nv = (size_t)(nx + 4) * (ny + 5), nc = (size_t)(nx + 4) * (ny + 4);
+    std::vector<double> buf(2 * nu + 2 * nv + 2 * nc);
+    const bool ok = fread(buf.data(), sizeof(double), buf.size(), fp) == buf.size();
+    fclose(fp);
+    if (!ok) throw ApiError{FUGU_EIO, "checkpoint body truncated"};
+    const double* b = buf.data();
+    up(c, c->f[FUGU_F_U_VEL], b, K_U); b += nu;
+    up(c, c->f[FUGU_F_V_VEL], b, K_V); b += nv;
+    up(c, c->f[FUGU_F_U_PREV], b, K_U); b += nu;
+    up(c, c->f[FUGU_F_V_PREV], b, K_V); b += nv;
+    up(c, c->f[FUGU_F_P_FIELD], b, K_CELL); b += nc;
+    up(c, c->f[FUGU_F_C_FIELD], b, K_CELL);
+    sync(c);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,177 @@
+// fugu_internal.cuh -- device layout, launch helpers and the bounded grid
+// barrier shared by the B200 kernels of the FUGU-2D coupled-step path.
+//
+// Device layout.  Every field kind (cell, u-face, v-face, vertex) is stored in
+// one uniform padded box: element (i, j) lives at (i + 2) + (j + 2) * P with
+// P >= nx + 5 a multiple of 16 (128-byte rows) and R = ny + 5 rows.  A u-face
+// (i, j), the cell (i, j) and the vertex (i, j) therefore share one linear
+// index, so every stencil offset is +-1 / +-P whatever the kinds involved, and
+// one thread per (i, j) can produce the u, v and p rows of the coupled
+// operator together.  The Fortran extents of each kind are sub-boxes of it:
+//   cell (-1..nx+2, -1..ny+2)  u (-2..nx+2, -1..ny+2)
+//   v    (-1..nx+2, -2..ny+2)  vertex (-2..nx+2, -2..ny+2)
+// Elements outside a kind's extent are padding; they are zero at allocation
+// and every whole-buffer operation keeps them zero.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace fugu {
+
+enum Kind { K_CELL = 0, K_U = 1, K_V = 2, K_VERT = 3 };
+
+struct Geo {
+  int nx, ny;
+  int P, R;            // pitch (elements) and rows of the padded box
+  double dx, dy;
+  double idx, idy;     // 1/dx, 1/dy  (computed as one / dx_grid, as the reference)
+  double idx2, idy2;   // 1/(dx*dx), 1/(dy*dy)
+  int px, py;          // periodic flags
+  int fsx;             // free-slip side walls (extension)
+  __host__ __device__ __forceinline__ int at(int i, int j) const { return (i + 2) + (j + 2) * P; }
+  __host__ __device__ __forceinline__ long n() const { return (long)P * R; }
+  __host__ __device__ __forceinline__ int imax() const { return px ? nx : nx - 1; }  // owned u faces
+  __host__ __device__ __forceinline__ int jmax() const { return py ? ny : ny - 1; }  // owned v faces
+  // extent of a kind in Fortran indices (inclusive)
+  __host__ __device__ __forceinline__ void extent(int kind, int& i0, int& i1, int& j0, int& j1) const {
+    i0 = (kind == K_U || kind == K_VERT) ? -2 : -1;
+    j0 = (kind == K_V || kind == K_VERT) ? -2 : -1;
+    i1 = nx + 2;
+    j1 = ny + 2;
+  }
+};
+
+// 2-D launch over the whole padded box: ii = 0..P-1, jj = 0..R-1 (i = ii - 2)
+struct Box {
+  dim3 grid, block;
+};
+inline Box box_launch(const Geo& g) {
+  Box b;
+  b.block = dim3(32, 8, 1);
+  b.grid = dim3((g.P + 31) / 32, (g.R + 7) / 8, 1);
+  return b;
+}
+
+// --------------------------------------------------------------------------
+// Bounded grid barrier for persistent kernels launched cooperatively (all
+// CTAs co-resident).  One thread per CTA arrives on a counter; the last one
+// resets it and bumps the generation.  Every wait polls at most
+// FUGU_SPIN_LIMIT times (about a second); on timeout, or when another CTA
+// has already flagged an error, the CTA records the error and returns false
+// so the kernel can unwind instead of hanging the GPU.
+// --------------------------------------------------------------------------
+#ifndef FUGU_SPIN_LIMIT
+#define FUGU_SPIN_LIMIT (1u << 24)
+#endif
+
+struct GridSync {
+  unsigned int count;
+  unsigned int gen;
+  int error;       // 0 ok, 1 barrier timeout
+  int pad;
+};
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ int ld_relaxed_i32(const int* p) {
+  int v;
+  asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Returns true when every CTA arrived; false on timeout / error.
+__device__ __forceinline__ bool grid_sync(GridSync* gs, unsigned int nblocks, unsigned int& gen) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    __threadfence();
+    unsigned int my = gen;
+    unsigned int arrived = atomicAdd(&gs->count, 1u);
+    if (arrived == nblocks - 1) {
+      atomicExch(&gs->count, 0u);
+      __threadfence();
+      atomicAdd(&gs->gen, 1u);
+    } else {
+      unsigned int spins = 0;
+      while (ld_acquire_u32(&gs->gen) == my) {
+        if (++spins > FUGU_SPIN_LIMIT || ld_relaxed_i32(&gs->error) != 0) {
+          atomicExch(&gs->error, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(40);
+      }
+    }
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  gen += 1;
+  return s_ok != 0;
+}
+
+// deterministic block reduction (sum) of one double per thread; result valid
+// in thread 0.  blockDim.x must be a multiple of 32 and <= 1024.
+__device__ __forceinline__ double block_sum(double v, double* sh /* >= 32 */) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  if (w == 0) {
+    v = l < nw ? sh[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  return v;
+}
+__device__ __forceinline__ double block_max(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  if (w == 0) {
+    v = l < nw ? sh[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  }
+  return v;
+}
+
+// Sum of n per-CTA partials, identical in every CTA (fixed order): warp 0
+// reads lane-strided and tree-reduces.  Result broadcast through shared.
+__device__ __forceinline__ double sum_partials(const double* part, int n, double* sh) {
+  __shared__ double s_res;
+  if (threadIdx.x < 32) {
+    double v = 0.0;
+    for (int k = threadIdx.x; k < n; k += 32) v += __ldcg(part + k);
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) s_res = v;
+  }
+  __syncthreads();
+  double r = s_res;
+  __syncthreads();
+  (void)sh;
+  return r;
+}
+__device__ __forceinline__ double max_partials(const double* part, int n) {
+  __shared__ double s_res;
+  if (threadIdx.x < 32) {
+    double v = 0.0;
+    for (int k = threadIdx.x; k < n; k += 32) v = fmax(v, __ldcg(part + k));
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0) s_res = v;
+  }
+  __syncthreads();
+  double r = s_res;
+  __syncthreads();
+  return r;
+}
+
+}  // namespace fugu

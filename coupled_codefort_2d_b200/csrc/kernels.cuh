@@ -1,0 +1,798 @@
+// kernels.cuh -- hand-written sm_100a kernels of the FUGU-2D coupled step.
+//
+// Each kernel restates one loop nest of the Fortran reference (file:line in
+// the comment above it) in the uniform device layout of fugu_internal.cuh.
+// Expressions keep the reference's operand order; the FP64 instantiation is
+// compiled with --fmad=false, so element-wise results match the CPU oracle
+// bit for bit.  Templates on T let the mixed-precision inner solve reuse the
+// same code in FP32.
+#pragma once
+
+#include "fugu_internal.cuh"
+
+namespace fugu {
+
+// --------------------------------------------------------------- helpers
+template <typename T>
+__device__ __forceinline__ T clip01(T x) { return fmax(T(0), fmin(T(1), x)); }
+
+#define FUGU_BOX_IJ                                          \
+  const int ii = blockIdx.x * blockDim.x + threadIdx.x;      \
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;      \
+  if (ii >= g.P || jj >= g.R) return;                        \
+  const int i = ii - 2, j = jj - 2;                          \
+  const int k = ii + jj * g.P;                               \
+  (void)k;
+
+__device__ __forceinline__ bool in_kind(const Geo& g, int kind, int i, int j) {
+  int i0, i1, j0, j1;
+  g.extent(kind, i0, i1, j0, j1);
+  return i >= i0 && i <= i1 && j >= j0 && j <= j1;
+}
+
+// ------------------------------------------------------------ halos
+// mpi_exchange_halos_{scalar,u,v} at one rank (mod_mpi.f90:113-245): a
+// periodic direction copies its own opposite interior layers (x pass over the
+// full j range first, then y pass over the full i range); a wall direction is
+// untouched.  One CTA; phases separated by __syncthreads.
+template <typename T>
+__global__ void k_halo(Geo g, T* a, int kind, const int* active) {
+  if (active && !*active) return;
+  int i0, i1, j0, j1;
+  g.extent(kind, i0, i1, j0, j1);
+  const int nx = g.nx, ny = g.ny;
+  if (g.px) {
+    const int nj = j1 - j0 + 1;
+    for (int t = threadIdx.x; t < 2 * nj; t += blockDim.x) {
+      const int kk = t & 1, j = j0 + (t >> 1);
+      a[g.at(-1 + kk, j)] = a[g.at(nx - 1 + kk, j)];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 2 * nj; t += blockDim.x) {
+      const int kk = t & 1, j = j0 + (t >> 1);
+      a[g.at(nx + 1 + kk, j)] = a[g.at(1 + kk, j)];
+    }
+    __syncthreads();
+  }
+  if (g.py) {
+    const int ni = i1 - i0 + 1;
+    for (int t = threadIdx.x; t < 2 * ni; t += blockDim.x) {
+      const int kk = t / ni, i = i0 + t % ni;
+      a[g.at(i, -1 + kk)] = a[g.at(i, ny - 1 + kk)];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < 2 * ni; t += blockDim.x) {
+      const int kk = t / ni, i = i0 + t % ni;
+      a[g.at(i, ny + 1 + kk)] = a[g.at(i, 1 + kk)];
+    }
+  }
+}
+
+// ------------------------------------------------------------ velocity BCs
+// apply_velocity_bcs, mod_operators.f90:254-333: west, east, south, north in
+// that order (each phase reads what the previous one wrote at the corners).
+// Extension fsx: symmetric (free-slip) tangential ghosts at the side walls.
+template <typename T>
+__global__ void k_velocity_bcs(Geo g, T* u, T* v, T u_lid, const int* active) {
+  if (active && !*active) return;
+  const int nx = g.nx, ny = g.ny;
+  const T vs = g.fsx ? T(1) : T(-1);
+  if (!g.px) {
+    for (int t = threadIdx.x; t < ny + 5; t += blockDim.x) {  // west
+      const int j = -2 + t;
+      if (j >= -1) {
+        u[g.at(0, j)] = T(0);
+        u[g.at(-1, j)] = -u[g.at(1, j)];
+        u[g.at(-2, j)] = -u[g.at(2, j)];
+      }
+      v[g.at(0, j)] = vs * v[g.at(1, j)];
+      v[g.at(-1, j)] = vs * v[g.at(2, j)];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < ny + 5; t += blockDim.x) {  // east
+      const int j = -2 + t;
+      if (j >= -1) {
+        u[g.at(nx, j)] = T(0);
+        u[g.at(nx + 1, j)] = -u[g.at(nx - 1, j)];
+        u[g.at(nx + 2, j)] = -u[g.at(nx - 2, j)];
+      }
+      v[g.at(nx + 1, j)] = vs * v[g.at(nx, j)];
+      v[g.at(nx + 2, j)] = vs * v[g.at(nx - 1, j)];
+    }
+    __syncthreads();
+  }
+  if (!g.py) {
+    for (int t = threadIdx.x; t < nx + 5; t += blockDim.x) {  // south
+      const int i = -2 + t;
+      if (i >= -1) {
+        v[g.at(i, 0)] = T(0);
+        v[g.at(i, -1)] = -v[g.at(i, 1)];
+        v[g.at(i, -2)] = -v[g.at(i, 2)];
+      }
+      u[g.at(i, 0)] = -u[g.at(i, 1)];
+      u[g.at(i, -1)] = -u[g.at(i, 2)];
+    }
+    __syncthreads();
+    const T two_lid = T(2) * u_lid;
+    for (int t = threadIdx.x; t < nx + 5; t += blockDim.x) {  // north
+      const int i = -2 + t;
+      if (i >= -1) {
+        v[g.at(i, ny)] = T(0);
+        v[g.at(i, ny + 1)] = -v[g.at(i, ny - 1)];
+        v[g.at(i, ny + 2)] = -v[g.at(i, ny - 2)];
+      }
+      u[g.at(i, ny + 1)] = two_lid - u[g.at(i, ny)];
+      u[g.at(i, ny + 2)] = two_lid - u[g.at(i, ny - 1)];
+    }
+  }
+}
+
+// ------------------------------------------------------------ properties
+struct Mix {
+  double rho1, rho2, mu1, mu2;
+};
+
+// harmonic_viscosity, mod_viscosity.f90:28-46
+__device__ __forceinline__ double harmonic_mu(const Mix& m, double c) {
+  const double cc = clip01(c);
+  if (fabs(m.mu1 - m.mu2) < 1.0e-14) return m.mu1;
+  const double den = m.mu2 * cc + m.mu1 * (1.0 - cc);
+  if (den > 1.0e-15) return (m.mu1 * m.mu2) / den;
+  return fmin(m.mu1, m.mu2);
+}
+__device__ __forceinline__ double rho_of(const Mix& m, double c) {
+  const double cv = clip01(c);
+  return m.rho1 * cv + m.rho2 * (1.0 - cv);
+}
+
+// compute_mixture_densities + compute_mixture_viscosities
+// (mod_viscosity.f90:54-151) in one pass: every output element is computed
+// from C directly; the border copies of the reference become index clamps.
+__global__ void k_properties(Geo g, Mix m, const double* __restrict__ c, double* rho_c, double* rho_u,
+                             double* rho_v, double* kappa, double* zeta, double* eta) {
+  FUGU_BOX_IJ
+  const int nx = g.nx, ny = g.ny;
+  if (in_kind(g, K_CELL, i, j)) {
+    rho_c[k] = rho_of(m, c[k]);
+    kappa[k] = 2.0 * harmonic_mu(m, c[k]);
+  }
+  if (in_kind(g, K_U, i, j)) {
+    const int ie = min(max(i, -1), nx + 1);
+    rho_u[k] = 0.5 * (rho_of(m, c[g.at(ie, j)]) + rho_of(m, c[g.at(ie + 1, j)]));
+  }
+  if (in_kind(g, K_V, i, j)) {
+    const int je = min(max(j, -1), ny + 1);
+    rho_v[k] = 0.5 * (rho_of(m, c[g.at(i, je)]) + rho_of(m, c[g.at(i, je + 1)]));
+  }
+  {  // vertex extent is the whole box's kind range
+    if (in_kind(g, K_VERT, i, j)) {
+      const int ie = min(max(i, -1), nx + 1), je = min(max(j, -1), ny + 1);
+      const double cv = 0.25 * (c[g.at(ie, je)] + c[g.at(ie + 1, je)] + c[g.at(ie, je + 1)] +
+                                c[g.at(ie + 1, je + 1)]);
+      const double mu = harmonic_mu(m, cv);
+      zeta[k] = 2.0 * mu;
+      eta[k] = mu;
+    }
+  }
+}
+
+// ------------------------------------------------------------ operators
+// T_xx, T_yy at cells and T_xy, T_yx at vertices (mod_operators.f90:119-140)
+template <typename T>
+__device__ __forceinline__ T txx(const Geo& g, const T* u, const T* kap, int i, int j, T idx) {
+  return kap[g.at(i, j)] * (u[g.at(i, j)] - u[g.at(i - 1, j)]) * idx;
+}
+template <typename T>
+__device__ __forceinline__ T tyy(const Geo& g, const T* v, const T* kap, int i, int j, T idy) {
+  return kap[g.at(i, j)] * (v[g.at(i, j)] - v[g.at(i, j - 1)]) * idy;
+}
+template <typename T>
+__device__ __forceinline__ void txy_tyx(const Geo& g, const T* u, const T* v, const T* zeta,
+                                        const T* eta, int i, int j, T idx, T idy, T& txy, T& tyx) {
+  const T du_dy = (u[g.at(i, j + 1)] - u[g.at(i, j)]) * idy;
+  const T dv_dx = (v[g.at(i + 1, j)] - v[g.at(i, j)]) * idx;
+  const T z = zeta[g.at(i, j)], e = eta[g.at(i, j)];
+  txy = (z - e) * du_dy + e * dv_dx;
+  tyx = e * du_dy + (z - e) * dv_dx;
+}
+// -div(T) on a u face (mod_operators.f90:145-150)
+template <typename T>
+__device__ __forceinline__ T visc_u_at(const Geo& g, const T* u, const T* v, const T* kap,
+                                       const T* zeta, const T* eta, int i, int j, T idx, T idy) {
+  T a0, b0, a1, b1;
+  txy_tyx(g, u, v, zeta, eta, i, j, idx, idy, a0, b0);
+  txy_tyx(g, u, v, zeta, eta, i, j - 1, idx, idy, a1, b1);
+  return -((txx(g, u, kap, i + 1, j, idx) - txx(g, u, kap, i, j, idx)) * idx + (a0 - a1) * idy);
+}
+// -div(T) on a v face (mod_operators.f90:155-160)
+template <typename T>
+__device__ __forceinline__ T visc_v_at(const Geo& g, const T* u, const T* v, const T* kap,
+                                       const T* zeta, const T* eta, int i, int j, T idx, T idy) {
+  T a0, b0, a1, b1;
+  txy_tyx(g, u, v, zeta, eta, i, j, idx, idy, a0, b0);
+  txy_tyx(g, u, v, zeta, eta, i - 1, j, idx, idy, a1, b1);
+  return -((b0 - b1) * idx + (tyy(g, v, kap, i, j + 1, idy) - tyy(g, v, kap, i, j, idy)) * idy);
+}
+
+// op_advection, mod_operators.f90:201-222 (u component)
+template <typename T>
+__device__ __forceinline__ T adv_u_at(const Geo& g, const T* ua, const T* va, const T* rc,
+                                      const T* rv, const T* u, const T* mdu, const T* mdv, int i,
+                                      int j, T idx, T idy) {
+  const T h = T(0.5);
+  T mE, mW, mN, mS;
+  if (mdu) {
+    mE = h * (mdu[g.at(i, j)] + mdu[g.at(i + 1, j)]);
+    mW = h * (mdu[g.at(i - 1, j)] + mdu[g.at(i, j)]);
+    mN = h * (mdv[g.at(i, j)] + mdv[g.at(i + 1, j)]);
+    mS = h * (mdv[g.at(i, j - 1)] + mdv[g.at(i + 1, j - 1)]);
+  } else {
+    mE = rc[g.at(i + 1, j)] * h * (ua[g.at(i, j)] + ua[g.at(i + 1, j)]);
+    mW = rc[g.at(i, j)] * h * (ua[g.at(i - 1, j)] + ua[g.at(i, j)]);
+    mN = h * (rv[g.at(i, j)] + rv[g.at(i + 1, j)]) * h * (va[g.at(i, j)] + va[g.at(i + 1, j)]);
+    mS = h * (rv[g.at(i, j - 1)] + rv[g.at(i + 1, j - 1)]) * h * (va[g.at(i, j - 1)] + va[g.at(i + 1, j - 1)]);
+  }
+  const T uE = h * (u[g.at(i, j)] + u[g.at(i + 1, j)]);
+  const T uW = h * (u[g.at(i - 1, j)] + u[g.at(i, j)]);
+  const T uN = h * (u[g.at(i, j)] + u[g.at(i, j + 1)]);
+  const T uS = h * (u[g.at(i, j - 1)] + u[g.at(i, j)]);
+  return (mE * uE - mW * uW) * idx + (mN * uN - mS * uS) * idy;
+}
+// op_advection, mod_operators.f90:225-247 (v component)
+template <typename T>
+__device__ __forceinline__ T adv_v_at(const Geo& g, const T* ua, const T* va, const T* rc,
+                                      const T* ru, const T* v, const T* mdu, const T* mdv, int i,
+                                      int j, T idx, T idy) {
+  const T h = T(0.5);
+  T mE, mW, mN, mS;
+  if (mdu) {
+    mE = h * (mdu[g.at(i, j)] + mdu[g.at(i, j + 1)]);
+    mW = h * (mdu[g.at(i - 1, j)] + mdu[g.at(i - 1, j + 1)]);
+    mN = h * (mdv[g.at(i, j)] + mdv[g.at(i, j + 1)]);
+    mS = h * (mdv[g.at(i, j - 1)] + mdv[g.at(i, j)]);
+  } else {
+    mE = h * (ru[g.at(i, j)] + ru[g.at(i, j + 1)]) * h * (ua[g.at(i, j)] + ua[g.at(i, j + 1)]);
+    mW = h * (ru[g.at(i - 1, j)] + ru[g.at(i - 1, j + 1)]) * h * (ua[g.at(i - 1, j)] + ua[g.at(i - 1, j + 1)]);
+    mN = rc[g.at(i, j + 1)] * h * (va[g.at(i, j)] + va[g.at(i, j + 1)]);
+    mS = rc[g.at(i, j)] * h * (va[g.at(i, j - 1)] + va[g.at(i, j)]);
+  }
+  const T vE = h * (v[g.at(i, j)] + v[g.at(i + 1, j)]);
+  const T vW = h * (v[g.at(i - 1, j)] + v[g.at(i, j)]);
+  const T vN = h * (v[g.at(i, j)] + v[g.at(i, j + 1)]);
+  const T vS = h * (v[g.at(i, j - 1)] + v[g.at(i, j)]);
+  return (mE * vE - mW * vW) * idx + (mN * vN - mS * vS) * idy;
+}
+
+// Coefficient fields of the coupled operator for one precision.
+template <typename T>
+struct Coefs {
+  const T *u_adv, *v_adv, *rho_c, *rho_u, *rho_v, *kappa, *zeta, *eta;
+  const T *pen_u, *pen_v;   // nullable
+  const T *mdot_u, *mdot_v; // nullable (AMP)
+};
+
+// matvec_coupled, mod_operators.f90:341-443, as ONE pass: the thread at
+// (i, j) writes Y_u(i,j), Y_v(i,j) and Y_p(i,j) of the whole padded box (zero
+// where the reference zeroes), computing the viscous stresses, the pressure
+// gradient, the advection and the divergence from X on the fly.  X must
+// already hold its periodic halo (k_halo).
+template <typename T>
+__global__ void k_matvec(Geo g, Coefs<T> c, const T* __restrict__ Xu, const T* __restrict__ Xv,
+                         const T* __restrict__ Xp, T* __restrict__ Yu, T* __restrict__ Yv,
+                         T* __restrict__ Yp, T dt, int with_adv, const int* active,
+                         unsigned long long* count) {
+  if (active && !*active) return;
+  if (count && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) atomicAdd(count, 1ull);
+  FUGU_BOX_IJ
+  const int nx = g.nx, ny = g.ny;
+  const T idx = T(g.idx), idy = T(g.idy);
+  // u row
+  T yu = T(0);
+  if (j >= 1 && j <= ny) {
+    if (i >= 1 && i <= g.imax()) {
+      const T adv = with_adv ? adv_u_at(g, c.u_adv, c.v_adv, c.rho_c, c.rho_v, Xu, c.mdot_u, c.mdot_v, i, j, idx, idy) : T(0);
+      const T vis = visc_u_at(g, Xu, Xv, c.kappa, c.zeta, c.eta, i, j, idx, idy);
+      const T gp = (Xp[g.at(i + 1, j)] - Xp[g.at(i, j)]) * idx;
+      yu = (c.rho_u[k] / dt) * Xu[k] + adv + vis + gp;
+      if (c.pen_u) yu = yu + c.pen_u[k] * Xu[k];
+    } else if (!g.px && (i == 0 || i == nx)) {
+      yu = Xu[k];
+    }
+  }
+  Yu[k] = yu;
+  // v row
+  T yv = T(0);
+  if (i >= 1 && i <= nx) {
+    if (j >= 1 && j <= g.jmax()) {
+      const T adv = with_adv ? adv_v_at(g, c.u_adv, c.v_adv, c.rho_c, c.rho_u, Xv, c.mdot_u, c.mdot_v, i, j, idx, idy) : T(0);
+      const T vis = visc_v_at(g, Xu, Xv, c.kappa, c.zeta, c.eta, i, j, idx, idy);
+      const T gp = (Xp[g.at(i, j + 1)] - Xp[g.at(i, j)]) * idy;
+      yv = (c.rho_v[k] / dt) * Xv[k] + adv + vis + gp;
+      if (c.pen_v) yv = yv + c.pen_v[k] * Xv[k];
+    } else if (!g.py && (j == 0 || j == ny)) {
+      yv = Xv[k];
+    }
+  }
+  Yv[k] = yv;
+  // p row: op_divergence (mod_operators.f90:34-53)
+  T yp = T(0);
+  if (i >= 1 && i <= nx && j >= 1 && j <= ny)
+    yp = (Xu[k] - Xu[g.at(i - 1, j)]) * idx + (Xv[k] - Xv[g.at(i, j - 1)]) * idy;
+  Yp[k] = yp;
+}
+
+// The individual operators of mod_operators.f90 (routine-level entries).
+__global__ void k_op_divergence(Geo g, const double* u, const double* v, double* div) {
+  FUGU_BOX_IJ
+  double d = 0.0;
+  if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny)
+    d = (u[k] - u[g.at(i - 1, j)]) * g.idx + (v[k] - v[g.at(i, j - 1)]) * g.idy;
+  div[k] = d;
+}
+__global__ void k_op_grad(Geo g, const double* p, double* gu, double* gv) {
+  FUGU_BOX_IJ
+  gu[k] = (j >= 1 && j <= g.ny && i >= 0 && i <= g.nx) ? (p[g.at(i + 1, j)] - p[k]) * g.idx : 0.0;
+  gv[k] = (i >= 1 && i <= g.nx && j >= 0 && j <= g.ny) ? (p[g.at(i, j + 1)] - p[k]) * g.idy : 0.0;
+}
+__global__ void k_op_visc(Geo g, const double* u, const double* v, const double* kap,
+                          const double* zeta, const double* eta, double* vu, double* vv) {
+  FUGU_BOX_IJ
+  vu[k] = (j >= 1 && j <= g.ny && i >= 0 && i <= g.nx) ? visc_u_at(g, u, v, kap, zeta, eta, i, j, g.idx, g.idy) : 0.0;
+  vv[k] = (i >= 1 && i <= g.nx && j >= 0 && j <= g.ny) ? visc_v_at(g, u, v, kap, zeta, eta, i, j, g.idx, g.idy) : 0.0;
+}
+__global__ void k_op_adv(Geo g, Coefs<double> c, const double* u, const double* v, double* au, double* av) {
+  FUGU_BOX_IJ
+  au[k] = (j >= 1 && j <= g.ny && i >= 1 && i <= g.imax())
+              ? adv_u_at(g, c.u_adv, c.v_adv, c.rho_c, c.rho_v, u, c.mdot_u, c.mdot_v, i, j, g.idx, g.idy) : 0.0;
+  av[k] = (i >= 1 && i <= g.nx && j >= 1 && j <= g.jmax())
+              ? adv_v_at(g, c.u_adv, c.v_adv, c.rho_c, c.rho_u, v, c.mdot_u, c.mdot_v, i, j, g.idx, g.idy) : 0.0;
+}
+
+// ------------------------------------------------------------ PCD pieces
+// Poisson face coefficients with zero flux through walls
+// (mod_subsolvers.f90:61-87): cx on u faces (i = 0..nx), cy on v faces
+// (j = 0..ny), and the Jacobi inverse diagonal at cells.
+template <typename T>
+__global__ void k_poisson_coefs(Geo g, const double* rho_u, const double* rho_v, T* cx, T* cy, T* dinv) {
+  FUGU_BOX_IJ
+  const int nx = g.nx, ny = g.ny;
+  T vx = T(0), vy = T(0), di = T(1);
+  if (j >= 1 && j <= ny && i >= 0 && i <= nx) {
+    double cxv = g.idx2 / rho_u[k];
+    if (!g.px && (i == 0 || i == nx)) cxv = 0.0;
+    vx = T(cxv);
+  }
+  if (i >= 1 && i <= nx && j >= 0 && j <= ny) {
+    double cyv = g.idy2 / rho_v[k];
+    if (!g.py && (j == 0 || j == ny)) cyv = 0.0;
+    vy = T(cyv);
+  }
+  if (i >= 1 && i <= nx && j >= 1 && j <= ny) {
+    double cE = g.idx2 / rho_u[k], cW = g.idx2 / rho_u[g.at(i - 1, j)];
+    double cN = g.idy2 / rho_v[k], cS = g.idy2 / rho_v[g.at(i, j - 1)];
+    if (!g.px) { if (i == 1) cW = 0.0; if (i == nx) cE = 0.0; }
+    if (!g.py) { if (j == 1) cS = 0.0; if (j == ny) cN = 0.0; }
+    const double d = cE + cW + cN + cS;
+    di = T(d > 1.0e-14 ? 1.0 / d : 1.0);
+  }
+  cx[k] = vx;
+  cy[k] = vy;
+  dinv[k] = di;
+}
+
+// PCD Schur step r_p = -((1/dt) phi + u.grad phi) (mod_pcd_precond.f90:54-62);
+// r_p is zero outside the interior (as after r_p = zero).
+template <typename T>
+__global__ void k_pcd_schur(Geo g, const T* phi, const T* ua, const T* va, T* rp, T inv_dt, const int* active) {
+  if (active && !*active) return;
+  FUGU_BOX_IJ
+  T r = T(0);
+  if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny) {
+    const T h = T(0.5);
+    const T uavg = h * (ua[k] + ua[g.at(i - 1, j)]);
+    const T vavg = h * (va[k] + va[g.at(i, j - 1)]);
+    const T conv = uavg * (phi[g.at(i + 1, j)] - phi[g.at(i - 1, j)]) * (h * T(g.idx)) +
+                   vavg * (phi[g.at(i, j + 1)] - phi[g.at(i, j - 1)]) * (h * T(g.idy));
+    r = -(inv_dt * phi[k] + conv);
+  }
+  rp[k] = r;
+}
+
+// velocity residual update z - B_p^T r_p (mod_pcd_precond.f90:66-84)
+template <typename T>
+__global__ void k_pcd_zwork(Geo g, const T* zu, const T* zv, const T* rp, T* zuw, T* zvw, const int* active) {
+  if (active && !*active) return;
+  FUGU_BOX_IJ
+  const int nx = g.nx, ny = g.ny;
+  T a = T(0), b = T(0);
+  if (j >= 1 && j <= ny) {
+    if (i >= 1 && i <= nx - 1) a = zu[k] - (rp[g.at(i + 1, j)] - rp[k]) * T(g.idx);
+    else if (i == 0 || i == nx) a = zu[k];
+  }
+  if (i >= 1 && i <= nx) {
+    if (j >= 1 && j <= ny - 1) b = zv[k] - (rp[g.at(i, j + 1)] - rp[k]) * T(g.idy);
+    else if (j == 0 || j == ny) b = zv[k];
+  }
+  zuw[k] = a;
+  zvw[k] = b;
+}
+
+// cross term from r_v into the u residual (mod_pcd_precond.f90:91-98)
+template <typename T>
+__global__ void k_pcd_cross(Geo g, const T* eta, const T* rv, T* zuw, const int* active) {
+  if (active && !*active) return;
+  FUGU_BOX_IJ
+  if (j >= 1 && j <= g.ny && i >= 1 && i <= g.nx - 1) {
+    const T idx = T(g.idx), idy = T(g.idy);
+    const T cross = -idy * (eta[k] * (rv[g.at(i + 1, j)] - rv[k]) * idx -
+                            eta[g.at(i, j - 1)] * (rv[g.at(i + 1, j - 1)] - rv[g.at(i, j - 1)]) * idx);
+    zuw[k] = zuw[k] - cross;
+  }
+}
+
+// One damped-Jacobi sweep of solve_helmholtz_u (mod_subsolvers.f90:284-306):
+// un = Jacobi(uo) on owned faces, rhs on wall faces, uo elsewhere (the
+// reference's u_old = u_sol copy).
+template <typename T>
+__global__ void k_jacobi_u(Geo g, const T* uo, T* un, const T* rhs, const T* rho_u, const T* kap,
+                           const T* zeta, const T* eta, const T* pen, T dt, T om, const int* active) {
+  if (active && !*active) return;
+  FUGU_BOX_IJ
+  const int nx = g.nx, ny = g.ny;
+  T val = uo[k];
+  if (j >= 1 && j <= ny) {
+    if (i >= 1 && i <= g.imax()) {
+      const T ix2 = T(g.idx2), iy2 = T(g.idy2);
+      const T cE = kap[g.at(i + 1, j)] * ix2;
+      const T cW = kap[k] * ix2;
+      const T cN = (zeta[k] - eta[k]) * iy2;
+      const T cS = (zeta[g.at(i, j - 1)] - eta[g.at(i, j - 1)]) * iy2;
+      T diag = (rho_u[k] / dt) + cE + cW + cN + cS;
+      if (pen) diag = diag + pen[k];
+      const T off = cE * uo[g.at(i + 1, j)] + cW * uo[g.at(i - 1, j)] + cN * uo[g.at(i, j + 1)] +
+                    cS * uo[g.at(i, j - 1)];
+      if (diag > T(1.0e-15)) val = (T(1) - om) * uo[k] + om * ((rhs[k] + off) / diag);
+    } else if (!g.px && (i == 0 || i == nx)) {
+      val = rhs[k];
+    }
+  }
+  un[k] = val;
+}
+
+// One damped-Jacobi sweep of solve_helmholtz_v (mod_subsolvers.f90:346-369)
+template <typename T>
+__global__ void k_jacobi_v(Geo g, const T* vo, T* vn, const T* rhs, const T* rho_v, const T* kap,
+                           const T* zeta, const T* eta, const T* pen, T dt, T om, const int* active) {
+  if (active && !*active) return;
+  FUGU_BOX_IJ
+  const int nx = g.nx, ny = g.ny;
+  T val = vo[k];
+  if (i >= 1 && i <= nx) {
+    if (j >= 1 && j <= g.jmax()) {
+      const T ix2 = T(g.idx2), iy2 = T(g.idy2);
+      const T cE = (zeta[k] - eta[k]) * ix2;
+      const T cW = (zeta[g.at(i - 1, j)] - eta[g.at(i - 1, j)]) * ix2;
+      const T cN = kap[g.at(i, j + 1)] * iy2;
+      const T cS = kap[k] * iy2;
+      T diag = (rho_v[k] / dt) + cE + cW + cN + cS;
+      if (pen) diag = diag + pen[k];
+      const T off = cE * vo[g.at(i + 1, j)] + cW * vo[g.at(i - 1, j)] + cN * vo[g.at(i, j + 1)] +
+                    cS * vo[g.at(i, j - 1)];
+      if (diag > T(1.0e-15)) val = (T(1) - om) * vo[k] + om * ((rhs[k] + off) / diag);
+    } else if (!g.py && (j == 0 || j == ny)) {
+      val = rhs[k];
+    }
+  }
+  vn[k] = val;
+}
+
+// ------------------------------------------------------------ Krylov vectors
+// Whole-buffer linear combinations over a coupled triple (u, v, p buffers of
+// n elements each, contiguous in one allocation of 3n).  Coefficients are
+// read from device scalars so the sequence can run without host round trips;
+// sgn flips the sign exactly.  Evaluation order is the reference's
+// left-to-right: y = ((x + c1 z1) + c2 z2) + c3 z3.
+template <typename T>
+struct Lin {
+  const T* x;
+  const T* z1;
+  const T* z2;
+  const T* z3;
+  const double* c1;
+  const double* c2;
+  const double* c3;
+  double s1, s2, s3;
+};
+template <typename T>
+__global__ void k_lin(long n3, T* y, Lin<T> L, const int* active) {
+  if (active && !*active) return;
+  const T c1 = L.c1 ? T(L.s1 * *L.c1) : T(0);
+  const T c2 = L.c2 ? T(L.s2 * *L.c2) : T(0);
+  const T c3 = L.c3 ? T(L.s3 * *L.c3) : T(0);
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n3; q += (long)gridDim.x * blockDim.x) {
+    T a = L.x[q];
+    if (L.z1) a = a + c1 * L.z1[q];
+    if (L.z2) a = a + c2 * L.z2[q];
+    if (L.z3) a = a + c3 * L.z3[q];
+    y[q] = a;
+  }
+}
+// bicgstab_solve direction update p = r + beta (p - omega v) (mod_bicgstab2.f90:244-246)
+template <typename T>
+__global__ void k_pupdate(long n3, T* p, const T* r, const T* v, const double* beta,
+                          const double* omega, const int* active) {
+  if (active && !*active) return;
+  const T b = T(*beta), w = T(*omega);
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n3; q += (long)gridDim.x * blockDim.x)
+    p[q] = r[q] + b * (p[q] - w * v[q]);
+}
+
+// coupled_dot (mod_bicgstab2.f90:32-72) for up to 5 pairs at once: block
+// partial sums of (a*b)*vol over owned u faces, v faces and cells, FP64
+// accumulation whatever T.  part[pair * nblk + block].
+template <typename T>
+struct DotPairs {
+  const T* a[5];
+  const T* b[5];
+  int npairs;
+};
+template <typename T>
+__global__ void k_dots(Geo g, long n, DotPairs<T> dp, double vol, double* part, const int* active) {
+  if (active && !*active) return;
+  __shared__ double sh[32];
+  double acc[5] = {0, 0, 0, 0, 0};
+  const int nx = g.nx, ny = g.ny, imax = g.imax(), jmax = g.jmax();
+  const long total = (long)imax * ny + (long)nx * jmax + (long)nx * ny;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
+    long off;
+    int i, j;
+    if (q < (long)imax * ny) {
+      i = 1 + (int)(q % imax); j = 1 + (int)(q / imax); off = 0;
+    } else if (q < (long)imax * ny + (long)nx * jmax) {
+      const long r = q - (long)imax * ny;
+      i = 1 + (int)(r % nx); j = 1 + (int)(r / nx); off = n;
+    } else {
+      const long r = q - (long)imax * ny - (long)nx * jmax;
+      i = 1 + (int)(r % nx); j = 1 + (int)(r / nx); off = 2 * n;
+    }
+    const long e = off + g.at(i, j);
+#pragma unroll
+    for (int p = 0; p < 5; ++p)
+      if (p < dp.npairs) acc[p] += (double(dp.a[p][e]) * double(dp.b[p][e])) * vol;
+  }
+  for (int p = 0; p < dp.npairs; ++p) {
+    const double s = block_sum(acc[p], sh);
+    if (threadIdx.x == 0) part[p * gridDim.x + blockIdx.x] = s;
+  }
+}
+
+// ------------------------------------------------------------ VOF transport
+__device__ __forceinline__ double limiter_psi(int lim, double r) {
+  if (lim == 1) {  // Superbee (extension)
+    const double a = fmin(2.0 * r, 1.0), b = fmin(r, 2.0);
+    return fmax(0.0, fmax(a, b));
+  }
+  if (r <= 0.0) return 0.0;  // van_leer_limiter, mod_vof.f90:25-33
+  return (2.0 * r) / (1.0 + r);
+}
+// face fluxes of vof_advection_tvd (mod_vof.f90:59-114)
+__device__ __forceinline__ double flux_x_at(const Geo& g, int lim, const double* c, const double* u,
+                                            int i, int j, double dt) {
+  const double uf = u[g.at(i, j)];
+  double num, den, r, cfl, cf;
+  if (uf >= 0.0) {
+    num = c[g.at(i, j)] - c[g.at(i - 1, j)];
+    den = c[g.at(i + 1, j)] - c[g.at(i, j)];
+    r = fabs(den) > 1.0e-12 ? num / den : 0.0;
+    cfl = fabs(uf) * dt * g.idx;
+    cf = c[g.at(i, j)] + 0.5 * (1.0 - cfl) * limiter_psi(lim, r) * den;
+  } else {
+    num = c[g.at(i + 2, j)] - c[g.at(i + 1, j)];
+    den = c[g.at(i + 1, j)] - c[g.at(i, j)];
+    r = fabs(den) > 1.0e-12 ? num / den : 0.0;
+    cfl = fabs(uf) * dt * g.idx;
+    cf = c[g.at(i + 1, j)] - 0.5 * (1.0 - cfl) * limiter_psi(lim, r) * den;
+  }
+  return uf * clip01(cf);
+}
+__device__ __forceinline__ double flux_y_at(const Geo& g, int lim, const double* c, const double* v,
+                                            int i, int j, double dt) {
+  const double vf = v[g.at(i, j)];
+  double num, den, r, cfl, cf;
+  if (vf >= 0.0) {
+    num = c[g.at(i, j)] - c[g.at(i, j - 1)];
+    den = c[g.at(i, j + 1)] - c[g.at(i, j)];
+    r = fabs(den) > 1.0e-12 ? num / den : 0.0;
+    cfl = fabs(vf) * dt * g.idy;
+    cf = c[g.at(i, j)] + 0.5 * (1.0 - cfl) * limiter_psi(lim, r) * den;
+  } else {
+    num = c[g.at(i, j + 2)] - c[g.at(i, j + 1)];
+    den = c[g.at(i, j + 1)] - c[g.at(i, j)];
+    r = fabs(den) > 1.0e-12 ? num / den : 0.0;
+    cfl = fabs(vf) * dt * g.idy;
+    cf = c[g.at(i, j + 1)] - 0.5 * (1.0 - cfl) * limiter_psi(lim, r) * den;
+  }
+  return vf * clip01(cf);
+}
+// conservative update + clipping (mod_vof.f90:117-126); ghosts copied from C_in
+__global__ void k_vof_update(Geo g, int lim, const double* c, const double* u, const double* v,
+                             double dt, double* cout) {
+  FUGU_BOX_IJ
+  double val = c[k];
+  if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny) {
+    const double fe = flux_x_at(g, lim, c, u, i, j, dt), fw = flux_x_at(g, lim, c, u, i - 1, j, dt);
+    const double fn = flux_y_at(g, lim, c, v, i, j, dt), fs = flux_y_at(g, lim, c, v, i, j - 1, dt);
+    val = clip01(c[k] - dt * ((fe - fw) * g.idx + (fn - fs) * g.idy));
+  }
+  cout[k] = val;
+}
+// optional flux outputs for the AMP mass fluxes (mod_vof.f90:128-137)
+__global__ void k_vof_fluxes(Geo g, int lim, const double* c, const double* u, const double* v,
+                             double dt, double* fx, double* fy) {
+  FUGU_BOX_IJ
+  fx[k] = (j >= 1 && j <= g.ny && i >= 0 && i <= g.nx) ? flux_x_at(g, lim, c, u, i, j, dt) : 0.0;
+  fy[k] = (i >= 1 && i <= g.nx && j >= 0 && j <= g.ny) ? flux_y_at(g, lim, c, v, i, j, dt) : 0.0;
+}
+
+// ------------------------------------------------------------ SVOF, curvature, CSF
+// Index maps of a ghost onto the interior after halo exchange + Neumann BC
+// (mod_vof.f90:169-170, :199-237): periodic wraps, a wall mirrors.
+__device__ __forceinline__ int map_x(const Geo& g, int i) {
+  if (i >= 1 && i <= g.nx) return i;
+  if (g.px) return i < 1 ? i + g.nx : i - g.nx;
+  return i < 1 ? 1 - i : 2 * g.nx + 1 - i;
+}
+__device__ __forceinline__ int map_y(const Geo& g, int j) {
+  if (j >= 1 && j <= g.ny) return j;
+  if (g.py) return j < 1 ? j + g.ny : j - g.ny;
+  return j < 1 ? 1 - j : 2 * g.ny + 1 - j;
+}
+// fill every ghost cell of a cell array from its interior (halo + Neumann)
+__global__ void k_fill_ghost_neumann(Geo g, double* a) {
+  FUGU_BOX_IJ
+  if (!in_kind(g, K_CELL, i, j)) return;
+  if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny) return;
+  a[k] = a[g.at(map_x(g, i), map_y(g, j))];
+}
+
+// compute_interface_curvature (mod_surface_tension.f90:25-72): face normals
+// on the fly, kappa = -div n at cells; ghosts 0 at walls or wrapped (halo).
+__device__ __forceinline__ double nx_face(const Geo& g, const double* cs, int i, int j) {
+  const double gx = (cs[g.at(i + 1, j)] - cs[g.at(i, j)]) * g.idx;
+  const double gy = 0.25 * (cs[g.at(i, j + 1)] + cs[g.at(i + 1, j + 1)] - cs[g.at(i, j - 1)] -
+                            cs[g.at(i + 1, j - 1)]) * g.idy;
+  return gx / sqrt(gx * gx + gy * gy + 1.0e-12);
+}
+__device__ __forceinline__ double ny_face(const Geo& g, const double* cs, int i, int j) {
+  const double gx = 0.25 * (cs[g.at(i + 1, j)] + cs[g.at(i + 1, j + 1)] - cs[g.at(i - 1, j)] -
+                            cs[g.at(i - 1, j + 1)]) * g.idx;
+  const double gy = (cs[g.at(i, j + 1)] - cs[g.at(i, j)]) * g.idy;
+  return gy / sqrt(gx * gx + gy * gy + 1.0e-12);
+}
+__global__ void k_curvature(Geo g, const double* cs, double* kc) {
+  FUGU_BOX_IJ
+  if (!in_kind(g, K_CELL, i, j)) { kc[k] = 0.0; return; }
+  int ci = i, cj = j;
+  const bool gi = (i < 1 || i > g.nx), gj = (j < 1 || j > g.ny);
+  if ((gi && !g.px) || (gj && !g.py)) { kc[k] = 0.0; return; }
+  if (gi) ci = map_x(g, i);
+  if (gj) cj = map_y(g, j);
+  kc[k] = -((nx_face(g, cs, ci, cj) - nx_face(g, cs, ci - 1, cj)) * g.idx +
+            (ny_face(g, cs, ci, cj) - ny_face(g, cs, ci, cj - 1)) * g.idy);
+}
+// compute_csf_force (mod_surface_tension.f90:78-109)
+__global__ void k_csf(Geo g, double sigma, const double* c, const double* kc, double* fu, double* fv) {
+  FUGU_BOX_IJ
+  double a = 0.0, b = 0.0;
+  if (j >= 1 && j <= g.ny && i >= 0 && i <= g.nx) {
+    const double kf = 0.5 * (kc[k] + kc[g.at(i + 1, j)]);
+    a = sigma * kf * (c[g.at(i + 1, j)] - c[k]) * g.idx;
+  }
+  if (i >= 1 && i <= g.nx && j >= 0 && j <= g.ny) {
+    const double kf = 0.5 * (kc[k] + kc[g.at(i, j + 1)]);
+    b = sigma * kf * (c[g.at(i, j + 1)] - c[k]) * g.idy;
+  }
+  fu[k] = a;
+  fv[k] = b;
+}
+
+// ------------------------------------------------------------ step pieces
+// AB extrapolation + history shift (mod_solver_coupled.f90:209-222):
+// adv = step<=1 ? x : 2x - prev; nm1 = prev; prev = x.
+__global__ void k_extrapolate(long n, const double* x, double* prev, double* nm1, double* adv, int first) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x) {
+    const double xv = x[q], pv = prev[q];
+    adv[q] = first ? xv : 2.0 * xv - pv;
+    nm1[q] = pv;
+    prev[q] = xv;
+  }
+}
+// a = s1 * x + s2 * y (AMP mass flux, penalty scaling; whole buffers)
+__global__ void k_axpby(long n, double* a, double s1, const double* x, double s2, const double* y) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+    a[q] = y ? s1 * x[q] + s2 * y[q] : s1 * x[q];
+}
+template <typename T>
+__global__ void k_convert(long n, T* dst, const double* src, double scale) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+    dst[q] = T(src[q] * scale);
+}
+template <typename T>
+__global__ void k_convert_scaled(long n, T* dst, const double* src, const double* scale) {
+  const double s = *scale;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+    dst[q] = T(src[q] * s);
+}
+template <typename T>
+__global__ void k_accumulate(long n, double* x, const T* d, const double* scale) {
+  const double s = *scale;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
+    x[q] = x[q] + s * double(d[q]);
+}
+
+// monolithic right-hand side (mod_solver_coupled.f90:261-303)
+struct RhsArgs {
+  const double *rho_u, *rho_v, *u_n, *u_nm1, *v_n, *v_nm1, *fsu, *fsv, *pen_u, *pen_v, *zeta, *eta;
+  double dt, gx, gy, u_sol, v_sol, u_lid;
+  int bdf2, has_lid;
+};
+__global__ void k_rhs(Geo g, RhsArgs a, double* Bu, double* Bv, double* Bp) {
+  FUGU_BOX_IJ
+  double bu = 0.0, bv = 0.0;
+  if (j >= 1 && j <= g.ny && i >= 1 && i <= g.imax()) {
+    if (a.bdf2)
+      bu = (a.rho_u[k] / a.dt) * (2.0 * a.u_n[k] - 0.5 * a.u_nm1[k]) + a.rho_u[k] * a.gx + a.fsu[k];
+    else
+      bu = (a.rho_u[k] / a.dt) * a.u_n[k] + a.rho_u[k] * a.gx + a.fsu[k];
+    if (a.pen_u) bu = bu + a.pen_u[k] * a.u_sol;
+    if (a.has_lid && !g.py && j == g.ny)
+      bu = bu + (2.0 * (a.zeta[k] - a.eta[k]) / (g.dy * g.dy)) * a.u_lid;
+  }
+  if (i >= 1 && i <= g.nx && j >= 1 && j <= g.jmax()) {
+    if (a.bdf2)
+      bv = (a.rho_v[k] / a.dt) * (2.0 * a.v_n[k] - 0.5 * a.v_nm1[k]) + a.rho_v[k] * a.gy + a.fsv[k];
+    else
+      bv = (a.rho_v[k] / a.dt) * a.v_n[k] + a.rho_v[k] * a.gy + a.fsv[k];
+    if (a.pen_v) bv = bv + a.pen_v[k] * a.v_sol;
+  }
+  Bu[k] = bu;
+  Bv[k] = bv;
+  Bp[k] = 0.0;
+}
+
+// max |u| over faces 0..nx x 1..ny and |v| over 1..nx x 0..ny
+// (compute_adaptive_dt, mod_solver_coupled.f90:54-66); part[2*blk]
+__global__ void k_maxvel(Geo g, const double* u, const double* v, double* part) {
+  __shared__ double sh[32];
+  double mu = 0.0, mv = 0.0;
+  const long nu = (long)(g.nx + 1) * g.ny, nv = (long)g.nx * (g.ny + 1);
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nu + nv; q += (long)gridDim.x * blockDim.x) {
+    if (q < nu) mu = fmax(mu, fabs(u[g.at((int)(q % (g.nx + 1)), 1 + (int)(q / (g.nx + 1)))]));
+    else {
+      const long r = q - nu;
+      mv = fmax(mv, fabs(v[g.at(1 + (int)(r % g.nx), (int)(r / g.nx))]));
+    }
+  }
+  mu = block_max(mu, sh);
+  if (threadIdx.x == 0) part[2 * blockIdx.x] = mu;
+  mv = block_max(mv, sh);
+  if (threadIdx.x == 0) part[2 * blockIdx.x + 1] = mv;
+}
+
+// build_cylinder_mask (mod_solver_coupled.f90:96-132), i_start = j_start = 1
+__global__ void k_cylinder(Geo g, double xc, double yc, double rad, double* pu, double* pv) {
+  FUGU_BOX_IJ
+  double a = 0.0, b = 0.0;
+  if (j >= 1 && j <= g.ny && i >= 0 && i <= g.nx) {
+    const double x = (double)i * g.dx, y = ((double)j - 0.5) * g.dy;
+    if (sqrt((x - xc) * (x - xc) + (y - yc) * (y - yc)) <= rad) a = 1.0;
+  }
+  if (i >= 1 && i <= g.nx && j >= 0 && j <= g.ny) {
+    const double x = ((double)i - 0.5) * g.dx, y = (double)j * g.dy;
+    if (sqrt((x - xc) * (x - xc) + (y - yc) * (y - yc)) <= rad) b = 1.0;
+  }
+  pu[k] = a;
+  pv[k] = b;
+}
+
+}  // namespace fugu

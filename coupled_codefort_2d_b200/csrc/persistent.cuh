@@ -1,0 +1,285 @@
+// persistent.cuh -- persistent (cooperative) kernels: the Jacobi-PCG pressure
+// Poisson solve and the SVOF Helmholtz filter.  One launch runs every
+// iteration; CTAs meet at bounded grid barriers (fugu_internal.cuh), the
+// convergence tests are evaluated identically by every CTA from the same
+// deterministic reductions, so no host round trip is needed per iteration.
+#pragma once
+
+#include "fugu_internal.cuh"
+
+namespace fugu {
+
+struct PcgOut {
+  int iters;            // iter_out of the last solve
+  int status;           // 0 ok, 1 barrier timeout
+  double res;           // res_out of the last solve
+  unsigned long long total_iters;  // accumulated over solves (statistics)
+  unsigned long long calls;
+};
+
+template <typename T>
+struct PcgArgs {
+  Geo g;
+  const T* rhs;        // right-hand side (cell layout)
+  const T* cx;         // u-face coefficients idx2/rho_u, zero on wall faces
+  const T* cy;         // v-face coefficients idy2/rho_v, zero on wall faces
+  const T* dinv;       // Jacobi inverse diagonal at cells
+  T* phi;              // in: initial guess; out: solution (ghosts as the reference)
+  T* r;                // work (interior)
+  T* z;
+  T* pb0;
+  T* pb1;
+  T* ap;
+  double* part;        // 6 * gridDim.x partial sums
+  GridSync* gs;
+  PcgOut* out;
+  const int* active;   // skip when *active == 0 (nullable)
+  double tol;
+  int max_iter;
+  int phi_zero;        // phi is identically zero on entry (preconditioner use)
+};
+
+// stencil of the variable-density Poisson operator at cell (i,j) applied to
+// a field given by accessor f (mod_subsolvers.f90:142-144, :182-184)
+template <typename T, typename F>
+__device__ __forceinline__ T poisson_ap(const Geo& g, const T* cx, const T* cy, int i, int j, F f) {
+  const T cE = __ldg(cx + g.at(i, j)), cW = __ldg(cx + g.at(i - 1, j));
+  const T cN = __ldg(cy + g.at(i, j)), cS = __ldg(cy + g.at(i, j - 1));
+  const int ie = (i < g.nx) ? i + 1 : (g.px ? 1 : g.nx);
+  const int iw = (i > 1) ? i - 1 : (g.px ? g.nx : 1);
+  const int jn = (j < g.ny) ? j + 1 : (g.py ? 1 : g.ny);
+  const int js = (j > 1) ? j - 1 : (g.py ? g.ny : 1);
+  return (cE + cW + cN + cS) * f(i, j) - (cE * f(ie, j) + cW * f(iw, j) + cN * f(i, jn) + cS * f(i, js));
+}
+
+// solve_poisson_pressure, mod_subsolvers.f90:32-246.
+template <typename T>
+__global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
+  if (a.active && !*a.active) return;
+  __shared__ double sh[32];
+  const Geo g = a.g;
+  const int G = gridDim.x;
+  const long N = (long)g.nx * g.ny;
+  const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long nthr = (long)G * blockDim.x;
+  const bool closed = !g.px && !g.py;
+  unsigned int gen = 0;
+  double* P0 = a.part;          // setup sum / final mean
+  double* P1 = a.part + G;      // rhs norm
+  double* P2 = a.part + 2 * G;  // initial r.z
+  double* PA = a.part + 3 * G;  // p.Ap
+  double* PB = a.part + 4 * G;  // r.r
+  double* PC = a.part + 5 * G;  // r.z
+#define CELL_LOOP for (long q = tid; q < N; q += nthr)
+#define CELL_IJ const int i = 1 + (int)(q % g.nx), j = 1 + (int)(q / g.nx); const int c = g.at(i, j);
+
+  // (b) zero-mean projection of the right-hand side when no direction is periodic
+  double mean = 0.0;
+  if (closed) {
+    double s = 0.0;
+    CELL_LOOP { CELL_IJ s += double(a.rhs[c]); }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) P0[blockIdx.x] = s;
+    if (!grid_sync(a.gs, G, gen)) return;
+    mean = sum_partials(P0, G, sh) / (double)(g.nx * g.ny);
+  }
+  double ss = 0.0;
+  CELL_LOOP {
+    CELL_IJ
+    const T rw = closed ? T(double(a.rhs[c]) - mean) : a.rhs[c];
+    a.r[c] = rw;  // r holds rhs_work until the initial residual is formed
+    ss += double(rw) * double(rw);
+  }
+  ss = block_sum(ss, sh);
+  if (threadIdx.x == 0) P1[blockIdx.x] = ss;
+  if (!grid_sync(a.gs, G, gen)) return;
+  const double rhs_norm = sqrt(sum_partials(P1, G, sh));
+  if (rhs_norm < 1.0e-14) {
+    for (long q = tid; q < g.n(); q += nthr) a.phi[q] = T(0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.out->iters = 0;
+      a.out->res = 0.0;
+      a.out->calls += 1;
+    }
+    return;
+  }
+  // (c) ghosts of phi from halo exchange + Neumann BC, then r = rhs_work - A phi
+  if (!a.phi_zero) {
+    for (long q = tid; q < g.n(); q += nthr) {
+      const int i = (int)(q % g.P) - 2, j = (int)(q / g.P) - 2;
+      if (i < -1 || j < -1 || i > g.nx + 2 || j > g.ny + 2) continue;
+      if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny) continue;
+      const int mi = (i >= 1 && i <= g.nx) ? i : (g.px ? (i < 1 ? i + g.nx : i - g.nx) : (i < 1 ? 1 - i : 2 * g.nx + 1 - i));
+      const int mj = (j >= 1 && j <= g.ny) ? j : (g.py ? (j < 1 ? j + g.ny : j - g.ny) : (j < 1 ? 1 - j : 2 * g.ny + 1 - j));
+      a.phi[q] = a.phi[g.at(mi, mj)];
+    }
+  }
+  double rz = 0.0;
+  CELL_LOOP {
+    CELL_IJ
+    T rr = a.r[c];
+    if (!a.phi_zero) {
+      const T* ph = a.phi;
+      const T apv = poisson_ap<T>(g, a.cx, a.cy, i, j, [&](int x, int y) { return ph[g.at(x, y)]; });
+      rr = rr - apv;
+    }
+    const T zz = a.dinv[c] * rr;
+    a.r[c] = rr;
+    a.z[c] = zz;
+    a.pb0[c] = zz;
+    rz += double(rr) * double(zz);
+  }
+  rz = block_sum(rz, sh);
+  if (threadIdx.x == 0) P2[blockIdx.x] = rz;
+  if (!grid_sync(a.gs, G, gen)) return;
+  double rz_old = sum_partials(P2, G, sh);
+
+  // (d) PCG iterations; the direction update p = z + beta p of iteration k-1
+  // is evaluated where iteration k needs it (own cell and stencil
+  // neighbours, identical arithmetic), double-buffered in pb0 / pb1.
+  double res_norm = 0.0, beta = 0.0;
+  int iter;
+  for (iter = 1; iter <= a.max_iter; ++iter) {
+    T* pcur = (iter & 1) ? a.pb0 : a.pb1;        // p of this iteration
+    const T* pprev = (iter & 1) ? a.pb1 : a.pb0; // p of the previous one
+    const T tb = T(beta);
+    double pap = 0.0;
+    CELL_LOOP {
+      CELL_IJ
+      T apv, pown;
+      if (iter == 1) {
+        const T* p0 = a.pb0;
+        pown = __ldcg(p0 + c);
+        apv = poisson_ap<T>(g, a.cx, a.cy, i, j, [&](int x, int y) { return __ldcg(p0 + g.at(x, y)); });
+      } else {
+        const T* zz = a.z;
+        auto pf = [&](int x, int y) {
+          const int e = g.at(x, y);
+          return __ldcg(zz + e) + tb * __ldcg(pprev + e);
+        };
+        pown = pf(i, j);
+        apv = poisson_ap<T>(g, a.cx, a.cy, i, j, pf);
+        pcur[c] = pown;
+      }
+      a.ap[c] = apv;
+      pap += double(pown) * double(apv);
+    }
+    pap = block_sum(pap, sh);
+    if (threadIdx.x == 0) PA[blockIdx.x] = pap;
+    if (!grid_sync(a.gs, G, gen)) return;
+    pap = sum_partials(PA, G, sh);
+    if (fabs(pap) < 1.0e-30) break;
+    const double alpha = rz_old / pap;
+    const T ta = T(alpha);
+    double rr = 0.0, rzn = 0.0;
+    CELL_LOOP {
+      CELL_IJ
+      const T pown = pcur[c];
+      const T rv = a.r[c] - ta * a.ap[c];
+      const T zv = a.dinv[c] * rv;
+      a.phi[c] = a.phi[c] + ta * pown;
+      a.r[c] = rv;
+      a.z[c] = zv;
+      rr += double(rv) * double(rv);
+      rzn += double(rv) * double(zv);
+    }
+    rr = block_sum(rr, sh);
+    if (threadIdx.x == 0) PB[blockIdx.x] = rr;
+    rzn = block_sum(rzn, sh);
+    if (threadIdx.x == 0) PC[blockIdx.x] = rzn;
+    if (!grid_sync(a.gs, G, gen)) return;
+    res_norm = sqrt(sum_partials(PB, G, sh));
+    if (res_norm / rhs_norm < a.tol) break;
+    const double rz_new = sum_partials(PC, G, sh);
+    beta = rz_new / rz_old;
+    rz_old = rz_new;
+  }
+  if (closed) {
+    double s = 0.0;
+    CELL_LOOP { CELL_IJ s += double(a.phi[c]); }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) P0[blockIdx.x] = s;
+    if (!grid_sync(a.gs, G, gen)) return;
+    const double m = sum_partials(P0, G, sh) / (double)(g.nx * g.ny);
+    CELL_LOOP { CELL_IJ a.phi[c] = T(double(a.phi[c]) - m); }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const int it = iter < a.max_iter ? iter : a.max_iter;
+    a.out->iters = it;
+    a.out->res = res_norm / rhs_norm;
+    a.out->total_iters += (unsigned long long)it;
+    a.out->calls += 1;
+  }
+#undef CELL_LOOP
+#undef CELL_IJ
+}
+
+// The mean subtraction above uses (phi - mean) in double for both T; for T =
+// double it is exactly phi(i,j) - mean_val of mod_subsolvers.f90:238.
+
+struct SvofArgs {
+  Geo g;
+  const double* craw;
+  double* out;    // C_smooth
+  double* work;   // second Jacobi buffer
+  double cx, cy, diag;
+  int max_iter;
+  double tol;
+  double* part;
+  GridSync* gs;
+  int* iters;     // accumulated iteration count
+  int* status;
+};
+
+// svof_helmholtz_filter, mod_vof.f90:145-194.  Ghost reads go through the
+// halo + Neumann index maps, which reproduce the ghosts the reference
+// refreshes before every sweep.
+__global__ void __launch_bounds__(512) k_svof(SvofArgs a) {
+  __shared__ double sh[32];
+  const Geo g = a.g;
+  const int G = gridDim.x;
+  const long N = (long)g.nx * g.ny;
+  const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long nthr = (long)G * blockDim.x;
+  unsigned int gen = 0;
+  for (long q = tid; q < g.n(); q += nthr) a.out[q] = a.craw[q];
+  if (!grid_sync(a.gs, G, gen)) { if (threadIdx.x == 0) *a.status = 1; return; }
+  auto mx = [&](int i) { return (i >= 1 && i <= g.nx) ? i : (g.px ? (i < 1 ? i + g.nx : i - g.nx) : (i < 1 ? 1 - i : 2 * g.nx + 1 - i)); };
+  auto my = [&](int j) { return (j >= 1 && j <= g.ny) ? j : (g.py ? (j < 1 ? j + g.ny : j - g.ny) : (j < 1 ? 1 - j : 2 * g.ny + 1 - j)); };
+  int it, used = 0;
+  const double* fin = a.out;
+  for (it = 1; it <= a.max_iter; ++it) {
+    used = it;
+    const double* src = (it & 1) ? a.out : a.work;
+    double* dst = (it & 1) ? a.work : a.out;
+    double res = 0.0;
+    for (long q = tid; q < N; q += nthr) {
+      const int i = 1 + (int)(q % g.nx), j = 1 + (int)(q / g.nx);
+      const int c = g.at(i, j);
+      const double old = __ldcg(src + c);
+      const double val = (a.craw[c] + a.cx * (__ldcg(src + g.at(mx(i + 1), j)) + __ldcg(src + g.at(mx(i - 1), j))) +
+                          a.cy * (__ldcg(src + g.at(i, my(j + 1))) + __ldcg(src + g.at(i, my(j - 1))))) / a.diag;
+      dst[c] = val;
+      res = fmax(res, fabs(val - old));
+    }
+    res = block_max(res, sh);
+    if (threadIdx.x == 0) a.part[blockIdx.x] = res;
+    if (!grid_sync(a.gs, G, gen)) { if (threadIdx.x == 0) *a.status = 1; return; }
+    fin = dst;
+    if (max_partials(a.part, G) < a.tol) break;
+  }
+  // final halo + Neumann: every ghost of C_smooth from its interior
+  for (long q = tid; q < g.n(); q += nthr) {
+    const int i = (int)(q % g.P) - 2, j = (int)(q / g.P) - 2;
+    if (i < -1 || j < -1 || i > g.nx + 2 || j > g.ny + 2) continue;
+    const bool inner = (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny);
+    if (inner) {
+      if (fin != a.out) a.out[q] = __ldcg(fin + q);
+    } else {
+      a.out[q] = __ldcg(fin + g.at(mx(i), my(j)));
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *a.iters += used;
+}
+
+}  // namespace fugu

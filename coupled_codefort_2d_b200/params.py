@@ -1,0 +1,54 @@
+"""Physics and solver parameters (the module globals of ``src/mod_params.f90``).
+
+The reference keeps these as mutable module variables read by every routine
+(``mod_params.f90:9-50``).  Here they are one explicit value object, passed
+through the C ABI as ``fugu_params`` (``include/fugu_gpu.h``).  Defaults are
+the reference's module defaults; knobs the reference hard-codes at call sites
+are exposed with the reference's constants as defaults.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, replace
+
+
+@dataclass(frozen=True)
+class Params:
+    # mod_params.f90:37-43
+    rho1: float = 1000.0
+    rho2: float = 1.0
+    mu1: float = 1.0
+    mu2: float = 0.01
+    sigma: float = 0.0
+    gx: float = 0.0
+    gy: float = -9.81
+    # mod_params.f90:48-54
+    cfl_target: float = 0.5
+    time_order: int = 1
+    # mod_params.f90:59-68
+    tol_bicgstab2: float = 1.0e-6
+    max_iter_bicgstab2: int = 500
+    alpha_penalty: float = 1.0e12
+    # call-site constants of the reference
+    pcg_tol: float = 1.0e-5  # mod_subsolvers.f90:53
+    pcg_max_iter: int = 150  # mod_subsolvers.f90:55
+    pcd_sweeps: int = 3  # mod_pcd_precond.f90:88,101
+    jacobi_omega: float = 0.8  # mod_subsolvers.f90:272,334
+    svof_delta_h: float = 1.5  # mod_solver_coupled.f90:243
+    svof_max_iter: int = 150  # mod_solver_coupled.f90:245
+    svof_tol: float = 1.0e-7  # mod_solver_coupled.f90:245
+    # extensions; 0 keeps the reference behaviour
+    limiter: int = 0  # 0 van Leer (mod_vof.f90:25-33), 1 Superbee
+    free_slip_x: int = 0  # 1: side walls free-slip
+    krylov_bc_fix: int = 0  # 1: BiCGStab(2) applies wall BCs to r before A*r
+    # FP64 defect-correction outer loop (0 = reference Krylov stopping rule)
+    refine: int = 0
+    refine_inner_tol: float = 1.0e-2
+    refine_max_inner: int = 20
+    refine_max_outer: int = 30
+
+    def with_(self, **kw) -> "Params":
+        return replace(self, **kw)
+
+
+VAN_LEER = 0
+SUPERBEE = 1

@@ -1,0 +1,255 @@
+/*
+ * fugu_gpu.h -- C ABI of the B200 (sm_100a) FUGU-2D coupled-step hot path.
+ *
+ * This is the boundary a Fortran caller binds with ISO_C_BINDING (see
+ * INTEGRATION.md for the interface block).  Plain pointers and sizes only.
+ *
+ * Host arrays follow the reference's own convention (src/main.f90:97-103):
+ * column-major, nh = 2 ghost layers, passed by the address of the lower-bound
+ * element (c_loc(a(lbound(a,1), lbound(a,2)))).  Extents per kind:
+ *   cell   (1-nh:nx+nh, 1-nh:ny+nh)   (nx+4) x (ny+4)
+ *   u-face (0-nh:nx+nh, 1-nh:ny+nh)   (nx+5) x (ny+4)
+ *   v-face (1-nh:nx+nh, 0-nh:ny+nh)   (nx+4) x (ny+5)
+ *   vertex (0-nh:nx+nh, 0-nh:ny+nh)   (nx+5) x (ny+5)
+ *
+ * Every entry point returns an int status: FUGU_OK (0); a negative value for
+ * misuse or a CUDA / device error (the message is in fugu_last_error()).
+ * Numerical outcomes (converged, max-iter, breakdown, NaN) are reported in
+ * fugu_stats.status, never as a failure of the call, because the reference
+ * routines return silently in those cases.  Nothing aborts or throws across
+ * the ABI.
+ *
+ * Threading: a context belongs to one host thread and owns one CUDA stream on
+ * one device.  Several contexts (one per GPU) may run concurrently.
+ */
+#ifndef FUGU_GPU_H
+#define FUGU_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FUGU_ABI_VERSION 1
+
+/* return codes */
+#define FUGU_OK 0
+#define FUGU_EINVAL (-1)   /* bad argument (NULL, size, option)          */
+#define FUGU_ECUDA (-2)    /* CUDA runtime error                          */
+#define FUGU_ENOMEM (-3)   /* device allocation failed                    */
+#define FUGU_EIO (-4)      /* checkpoint file error                       */
+#define FUGU_ETIMEOUT (-5) /* a device-side wait gave up (see message)    */
+
+/* numerical status in fugu_stats.status */
+#define FUGU_CONVERGED 0
+#define FUGU_MAXITER 1
+#define FUGU_BREAKDOWN 2
+#define FUGU_NAN 3
+
+/* precision of the Krylov solve */
+#define FUGU_FP64 0  /* plain form: FP64 throughout                       */
+#define FUGU_MIXED 1 /* FP32 inner Krylov+PCD inside FP64 defect correction */
+
+/* Physics, grid and solver knobs: the module globals of src/mod_params.f90:9-50
+ * and src/mod_mpi.f90:10-26 as one explicit struct.  fugu_params_default()
+ * fills the reference's module defaults and call-site constants. */
+typedef struct {
+  int nx, ny;                 /* cells (Nx_global = nx_loc at one rank)     */
+  double dx, dy;              /* dx_grid, dy_grid                           */
+  int periodic_x, periodic_y; /* periods(1:2)                               */
+  double rho1, rho2, mu1, mu2, sigma, gx, gy;
+  double cfl_target, alpha_penalty;
+  int time_order;             /* 1 = BDF1, 2 = BDF2                         */
+  double tol_bicgstab2;
+  int max_iter_bicgstab2;
+  double pcg_tol;             /* 1e-5  (mod_subsolvers.f90:53)              */
+  int pcg_max_iter;           /* 150   (mod_subsolvers.f90:55)              */
+  int pcd_sweeps;             /* 3     (mod_pcd_precond.f90:88,101)         */
+  double jacobi_omega;        /* 0.8   (mod_subsolvers.f90:272,334)         */
+  double svof_delta_h;        /* 1.5   (mod_solver_coupled.f90:243)         */
+  int svof_max_iter;          /* 150   (mod_solver_coupled.f90:245)         */
+  double svof_tol;            /* 1e-7  (mod_solver_coupled.f90:245)         */
+  /* extensions; 0 keeps the reference behaviour */
+  int limiter;                /* 0 van Leer (mod_vof.f90:25-33), 1 Superbee */
+  int free_slip_x;            /* 1: side walls free-slip                    */
+  int krylov_bc_fix;          /* 1: BiCGStab(2) applies wall BCs to r before
+                                 A*r (mod_bicgstab2.f90:430 does not)       */
+  int refine;                 /* 1: FP64 defect-correction outer loop on the
+                                 true residual |B-AX|/|B| < tol             */
+  double refine_inner_tol;
+  int refine_max_inner;
+  int refine_max_outer;
+  int precision;              /* FUGU_FP64 or FUGU_MIXED (needs refine = 1) */
+} fugu_params;
+
+/* Optional arguments of advance_coupled_step (src/mod_solver_coupled.f90:137-160):
+ * a has_* flag mirrors Fortran present(). */
+typedef struct {
+  int use_bicgstab2;          /* 1 = bicgstab2_solve, 0 = bicgstab_solve    */
+  int has_lid;  double u_top_lid;
+  int has_tol;  double tol;
+  int has_max_iter; int max_iter;
+  int consistent_amp;
+  int has_penalty;            /* phi_s_u / phi_s_v uploaded (FUGU_F_PHI_S_*) */
+  int has_u_solid; double u_solid;
+  int has_v_solid; double v_solid;
+} fugu_step_opts;
+
+typedef struct {
+  int iter;                   /* iter_out (refine: total inner iterations) */
+  double res;                 /* res_out: left-preconditioned relative
+                                 residual (refine: true relative residual)  */
+  long long pcg_iters;        /* inner PCG iterations summed over the step  */
+  int pcg_calls;              /* Poisson solves = preconditioner applications */
+  int svof_iters;
+  int matvecs;
+  int outer;                  /* defect-correction outer iterations        */
+  int status;                 /* FUGU_CONVERGED / MAXITER / BREAKDOWN / NAN */
+} fugu_stats;
+
+/* field identifiers of a context's device-resident state */
+enum {
+  FUGU_F_U_VEL = 0, FUGU_F_V_VEL, FUGU_F_P_FIELD, FUGU_F_C_FIELD,
+  FUGU_F_U_PREV, FUGU_F_V_PREV,
+  FUGU_F_RHO_C, FUGU_F_RHO_U, FUGU_F_RHO_V,
+  FUGU_F_KAPPA, FUGU_F_ZETA, FUGU_F_ETA,
+  FUGU_F_KAPPA_CURV, FUGU_F_F_SIGMA_U, FUGU_F_F_SIGMA_V,
+  FUGU_F_PHI_S_U, FUGU_F_PHI_S_V,
+  FUGU_NUM_FIELDS
+};
+
+typedef struct fugu_ctx fugu_ctx;
+
+/* ---------------------------------------------------------------- context */
+void fugu_params_default(fugu_params* p);
+const char* fugu_version(void);
+/* Create a context on CUDA device `device` for the grid in *p. */
+int fugu_create(const fugu_params* p, int device, fugu_ctx** out);
+void fugu_destroy(fugu_ctx* ctx);
+/* Replace the module globals (grid size must not change). */
+int fugu_set_params(fugu_ctx* ctx, const fugu_params* p);
+const char* fugu_last_error(const fugu_ctx* ctx);
+/* Copy one device-resident field from / to a host array (reference layout). */
+int fugu_upload(fugu_ctx* ctx, int field, const double* host);
+int fugu_download(fugu_ctx* ctx, int field, double* host);
+
+/* One coupled time step on the device-resident state (u_vel ... f_sigma_v,
+ * phi_s_*).  Replaces advance_coupled_step, src/mod_solver_coupled.f90:137. */
+int fugu_step(fugu_ctx* ctx, double dt, int step_idx, const fugu_step_opts* o, fugu_stats* st);
+
+/* Drop-in for advance_coupled_step (src/mod_solver_coupled.f90:137-380) with
+ * the reference's host arrays: uploads the state, steps, downloads it.
+ * phi_s_u / phi_s_v may be NULL (no Darcy penalty). */
+int fugu_advance_coupled_step(fugu_ctx* ctx,
+                              double* u_vel, double* v_vel, double* p_field, double* c_field,
+                              double* u_prev, double* v_prev,
+                              double* rho_c, double* rho_u, double* rho_v,
+                              double* kappa, double* zeta, double* eta,
+                              double* kappa_curv, double* f_sigma_u, double* f_sigma_v,
+                              const double* phi_s_u, const double* phi_s_v,
+                              double dt, int step_idx, const fugu_step_opts* o, fugu_stats* st);
+
+/* compute_adaptive_dt (src/mod_solver_coupled.f90:41-91) on host arrays */
+int fugu_compute_adaptive_dt(fugu_ctx* ctx, const double* u_vel, const double* v_vel,
+                             double dt_max, double* dt_out);
+/* build_cylinder_mask (src/mod_solver_coupled.f90:96-132) */
+int fugu_build_cylinder_mask(fugu_ctx* ctx, double xc, double yc, double rad,
+                             double* phi_s_u, double* phi_s_v);
+
+/* ------------------------------------------------ routine-level entries
+ * Each takes the reference routine's dummy arguments as host arrays, runs the
+ * device kernels the step uses, and writes the intent(out)/(inout) arrays
+ * back.  NULL marks an absent optional argument. */
+
+/* mod_mpi.f90:113-245 (single rank: periodic self-wrap, walls untouched) */
+int fugu_halo_scalar(fugu_ctx* ctx, double* phi);
+int fugu_halo_u(fugu_ctx* ctx, double* u);
+int fugu_halo_v(fugu_ctx* ctx, double* v);
+
+/* mod_viscosity.f90:54-93, :105-151 */
+int fugu_compute_mixture_densities(fugu_ctx* ctx, const double* c_field,
+                                   double* rho_c, double* rho_u, double* rho_v);
+int fugu_compute_mixture_viscosities(fugu_ctx* ctx, const double* c_field,
+                                     double* kappa, double* zeta, double* eta);
+
+/* mod_operators.f90:34-53, :60-88, :99-162, :168-249, :254-333 */
+int fugu_op_divergence(fugu_ctx* ctx, const double* u, const double* v, double* div);
+int fugu_op_grad_pressure(fugu_ctx* ctx, const double* p, double* grad_u, double* grad_v);
+int fugu_op_viscous_stress(fugu_ctx* ctx, const double* u, const double* v,
+                           const double* kappa, const double* zeta, const double* eta,
+                           double* visc_u, double* visc_v);
+int fugu_op_advection(fugu_ctx* ctx, const double* u_adv, const double* v_adv,
+                      const double* rho_c, const double* rho_u, const double* rho_v,
+                      const double* u, const double* v, double* adv_u, double* adv_v,
+                      const double* mdot_u, const double* mdot_v);
+int fugu_apply_velocity_bcs(fugu_ctx* ctx, double* u, double* v, int has_lid, double u_lid);
+
+/* matvec_coupled, mod_operators.f90:341-443 (X is intent(inout): its ghosts
+ * receive the periodic halo, as in the reference) */
+int fugu_matvec_coupled(fugu_ctx* ctx, double* X_u, double* X_v, double* X_p,
+                        double* Y_u, double* Y_v, double* Y_p,
+                        const double* u_adv, const double* v_adv,
+                        const double* rho_c, const double* rho_u, const double* rho_v,
+                        const double* kappa, const double* zeta, const double* eta,
+                        double dt, int include_advection,
+                        const double* penalty_u, const double* penalty_v,
+                        const double* mdot_u, const double* mdot_v);
+
+/* mod_subsolvers.f90:32-246, :252-309, :314-372 */
+int fugu_solve_poisson_pressure(fugu_ctx* ctx, double* phi, const double* rhs,
+                                const double* rho_u, const double* rho_v,
+                                double tol, int max_iter, int* iter_out, double* res_out);
+int fugu_solve_helmholtz_u(fugu_ctx* ctx, double* u_sol, const double* rhs_u,
+                           const double* rho_u, const double* kappa, const double* zeta,
+                           const double* eta, double dt, int n_sweeps, const double* penalty_u);
+int fugu_solve_helmholtz_v(fugu_ctx* ctx, double* v_sol, const double* rhs_v,
+                           const double* rho_v, const double* kappa, const double* zeta,
+                           const double* eta, double dt, int n_sweeps, const double* penalty_v);
+
+/* apply_pcd_precond, mod_pcd_precond.f90:14-104 */
+int fugu_apply_pcd_precond(fugu_ctx* ctx, const double* z_u, const double* z_v, const double* z_p,
+                           double* r_u, double* r_v, double* r_p,
+                           const double* u_adv, const double* v_adv,
+                           const double* rho_u, const double* rho_v,
+                           const double* kappa, const double* zeta, const double* eta,
+                           double dt, const double* penalty_u, const double* penalty_v);
+
+/* coupled_dot, mod_bicgstab2.f90:32-72 */
+int fugu_coupled_dot(fugu_ctx* ctx, const double* u1, const double* v1, const double* p1,
+                     const double* u2, const double* v2, const double* p2, double* out);
+
+/* bicgstab_solve (mod_bicgstab2.f90:77-264) when solver = 1,
+ * bicgstab2_solve (:270-570) when solver = 2.  has_lid mirrors
+ * present(u_top_lid).  With params.refine = 1 the solve is the FP64
+ * defect-correction loop around the chosen inner solver. */
+int fugu_krylov_solve(fugu_ctx* ctx, int solver,
+                      double* X_u, double* X_v, double* X_p,
+                      const double* B_u, const double* B_v, const double* B_p,
+                      const double* u_adv, const double* v_adv,
+                      const double* rho_c, const double* rho_u, const double* rho_v,
+                      const double* kappa, const double* zeta, const double* eta,
+                      double dt, double tol, int max_iter, int has_lid, double u_lid,
+                      const double* penalty_u, const double* penalty_v,
+                      const double* mdot_u, const double* mdot_v, fugu_stats* st);
+
+/* mod_vof.f90:38-140 (flux_x/flux_y may be NULL), :145-194 */
+int fugu_vof_advection_tvd(fugu_ctx* ctx, const double* c_in, double* c_out,
+                           const double* u, const double* v, double dt,
+                           double* flux_x, double* flux_y);
+int fugu_svof_helmholtz_filter(fugu_ctx* ctx, const double* c_raw, double* c_smooth,
+                               double delta, int max_iter, double tol, int* iters_out);
+
+/* mod_surface_tension.f90:25-72, :78-109 */
+int fugu_compute_interface_curvature(fugu_ctx* ctx, const double* c_smooth, double* kappa_curv);
+int fugu_compute_csf_force(fugu_ctx* ctx, const double* c_raw, const double* kappa_curv,
+                           double* f_sigma_u, double* f_sigma_v);
+
+/* mod_io.f90:169-225: checkpoint of the device-resident state in the
+ * reference's stream-binary format (header step, t, nx, ny, nh; then
+ * u, v, u_prev, v_prev, p, c with halos). */
+int fugu_write_checkpoint(fugu_ctx* ctx, const char* path, int step, double t);
+int fugu_read_checkpoint(fugu_ctx* ctx, const char* path, int* step, double* t);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FUGU_GPU_H */

@@ -1,0 +1,160 @@
+"""Step-level parity: ``advance_coupled_step`` on the GPU against the CPU
+oracle for every case family the reference tests exercise (cavity with lid,
+static droplet with SVOF/CSF, rising bubble with AMP, periodic two-phase
+Poiseuille with BDF2, Darcy cylinder with alpha = 1e12), both Krylov solvers,
+and the FP64 / mixed defect-correction forms.
+
+Tolerances (the hot path's parity targets): u, v, p relative L2 <= 1e-8 after
+N steps on identical inputs; VOF volume equal to 1e-12 relative.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from coupled_codefort_2d_b200 import cases
+from coupled_codefort_2d_b200.context import Context
+from coupled_codefort_2d_b200.layout import Grid
+from coupled_codefort_2d_b200.params import Params
+
+pytestmark = pytest.mark.gpu
+
+STATE = ["u_vel", "v_vel", "p_field", "c_field", "u_prev", "v_prev", "rho_c", "rho_u", "rho_v", "kappa",
+         "zeta", "eta", "kappa_curv", "f_sigma_u", "f_sigma_v"]
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def case(name):
+    """(grid, params, initial colour, step kwargs, dt, nsteps, phi_s)"""
+    if name == "cavity":
+        g = Grid(24, 24)
+        p = Params(rho1=1.0, rho2=1.0, mu1=0.01, mu2=0.01, sigma=0.0, gx=0.0, gy=0.0, time_order=1,
+                   tol_bicgstab2=1e-8, max_iter_bicgstab2=100)
+        return g, p, g.full("cell", 1.0), dict(u_top_lid=1.0, use_bicgstab2=False), 1e-2, 3, None
+    if name == "droplet":
+        g = Grid(32, 32)
+        p = Params(rho1=1.0, rho2=0.1, mu1=0.1, mu2=0.01, sigma=1.0, gx=0.0, gy=0.0, time_order=2,
+                   tol_bicgstab2=1e-6, max_iter_bicgstab2=100)
+        c = cases.circle_fraction(g, 0.5, 0.5, 0.25, inside=1.0, ns=8)
+        return g, p, c, dict(use_bicgstab2=False), 1e-4, 3, None
+    if name == "bubble_amp":
+        g = Grid(16, 32, 1.0, 2.0)
+        p = Params(rho1=1000.0, rho2=100.0, mu1=10.0, mu2=1.0, sigma=24.5, gx=0.0, gy=-0.98, time_order=2,
+                   tol_bicgstab2=1e-6, max_iter_bicgstab2=100)
+        c = cases.initial_colour(g, "rising_bubble")
+        return g, p, c, dict(use_bicgstab2=False, consistent_amp=True), 1e-3, 3, None
+    if name == "poiseuille":
+        g = Grid(8, 16, periodic_x=True)
+        p = Params(rho1=1.0, rho2=1.0, mu1=1.0, mu2=0.25, sigma=0.0, gx=1.0, gy=0.0, time_order=2,
+                   tol_bicgstab2=1e-7, max_iter_bicgstab2=200)
+        return g, p, cases.initial_colour(g, "poiseuille"), dict(use_bicgstab2=False), 0.05, 3, None
+    if name == "cylinder":
+        g = Grid(16, 16, periodic_x=True)
+        p = Params(rho1=1.0, rho2=1.0, mu1=0.1, mu2=0.1, sigma=0.0, gx=1.0, gy=0.0, time_order=2,
+                   alpha_penalty=1e12, tol_bicgstab2=1e-5, max_iter_bicgstab2=150)
+        return g, p, g.full("cell", 1.0), dict(use_bicgstab2=False), 0.01, 3, (0.5, 0.5, 0.15)
+    if name == "cavity_b2":
+        g = Grid(16, 16)
+        p = Params(rho1=1.0, rho2=1.0, mu1=0.01, mu2=0.01, sigma=0.0, gx=0.0, gy=0.0, time_order=1,
+                   tol_bicgstab2=1e-10, max_iter_bicgstab2=4)
+        return g, p, g.full("cell", 1.0), dict(u_top_lid=1.0, use_bicgstab2=True), 1e-2, 2, None
+    raise KeyError(name)
+
+
+def run_pair(oracle_mod, name, prm_override=None, precision=0, nsteps=None):
+    g, p, c0, kw, dt, n, cyl = case(name)
+    if prm_override:
+        p = p.with_(**prm_override)
+    n = nsteps or n
+    st_o = oracle_mod.new_state(g, c0, p)
+    st_g = {k: a.copy(order="F") for k, a in st_o.items()}
+    o = oracle_mod.Oracle(g, p)
+    phi = o.cylinder_mask(*cyl) if cyl else None
+    hist = []
+    with Context(g, p, precision=precision) as ctx:
+        for step in range(1, n + 1):
+            so = o.step(st_o, dt, step, phi_s=phi, **kw)
+            sg = ctx.advance_coupled_step(*[st_g[k] for k in STATE], dt, step,
+                                          phi_s_u=None if phi is None else phi[0],
+                                          phi_s_v=None if phi is None else phi[1], **kw)
+            hist.append((so, sg))
+    return g, st_o, st_g, hist
+
+
+@pytest.mark.parametrize("name", ["cavity", "droplet", "bubble_amp", "poiseuille", "cylinder", "cavity_b2"])
+def test_step_parity_plain_fp64(gpu, oracle_mod, name):
+    g, st_o, st_g, hist = run_pair(oracle_mod, name)
+    for so, sg in hist:
+        assert sg["iter"] == so.iter, (sg["iter"], so.iter)
+        assert sg["pcg_calls"] == so.pcg_calls
+        assert sg["svof_iters"] == so.svof_iters
+    for k in ("u_vel", "v_vel", "p_field"):
+        assert rel(st_g[k], st_o[k]) <= 1e-8, (k, rel(st_g[k], st_o[k]))
+    vo = cases.fluid1_volume(g, st_o["c_field"])
+    vg = cases.fluid1_volume(g, st_g["c_field"])
+    assert abs(vg - vo) <= 1e-12 * max(abs(vo), 1e-300)
+    for k in ("c_field", "rho_c", "rho_u", "rho_v", "kappa", "zeta", "eta"):
+        assert rel(st_g[k], st_o[k]) <= 1e-10, k
+
+
+def test_refine_fp64_parity(gpu, oracle_mod):
+    over = dict(refine=1, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=30, krylov_bc_fix=1,
+                tol_bicgstab2=1e-9)
+    g, st_o, st_g, hist = run_pair(oracle_mod, "droplet", over)
+    for so, sg in hist:
+        assert sg["res"] < 1e-9 and so.res < 1e-9
+        assert sg["outer"] == so.outer
+    for k in ("u_vel", "v_vel", "p_field"):
+        assert rel(st_g[k], st_o[k]) <= 1e-8, (k, rel(st_g[k], st_o[k]))
+
+
+@pytest.mark.parametrize("name", ["cavity", "droplet", "bubble_amp"])
+def test_mixed_precision_error_vs_fp64_oracle(gpu, oracle_mod, name):
+    """FP32 inner Krylov+PCD inside FP64 defect correction: every step reaches
+    the FP64 true residual tolerance, and the state stays within 1e-6 relative
+    L2 of the FP64 oracle solving the same steps to the same tolerance."""
+    over = dict(refine=1, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=40, krylov_bc_fix=1,
+                tol_bicgstab2=1e-9)
+    g, st_o, st_g, hist = run_pair(oracle_mod, name, over, precision=1)
+    for so, sg in hist:
+        assert sg["res"] < 1e-9, sg
+        assert sg["status"] == 0
+    for k in ("u_vel", "v_vel", "p_field"):
+        assert rel(st_g[k], st_o[k]) <= 1e-6, (k, rel(st_g[k], st_o[k]))
+
+
+def test_checkpoint_restart_bitwise(gpu, oracle_mod):
+    """mod_io.f90:169-225 format: the GPU writes the reference's byte layout,
+    the oracle reads it back, and a restart reproduces the run bit for bit
+    (tests/test_week6_advanced.f90:125-156)."""
+    g, p, c0, kw, dt, n, cyl = case("cylinder")
+    o = oracle_mod.Oracle(g, p)
+    phi = o.cylinder_mask(*cyl)
+    st0 = oracle_mod.new_state(g, c0, p)
+    with tempfile.TemporaryDirectory() as d, Context(g, p) as ctx:
+        ctx.upload_state(st0)
+        ctx.upload("phi_s_u", phi[0])
+        ctx.upload("phi_s_v", phi[1])
+        opts = ctx.step_opts(use_bicgstab2=False, penalty=True)
+        for s in (1, 2):
+            ctx.step(dt, s, opts)
+        path = os.path.join(d, "chk_r0000.bin")
+        ctx.write_checkpoint(path, 2, 2 * dt)
+        st_chk = {k: g.zeros(kd) for k, kd in oracle_mod.STATE_KINDS.items()}
+        rc, step, t = o.read_checkpoint(path, st_chk)
+        assert rc == 0 and step == 2 and t == 2 * dt
+        for k in ("u_vel", "v_vel", "u_prev", "v_prev", "p_field", "c_field"):
+            np.testing.assert_array_equal(st_chk[k], ctx.download(k))
+        for s in (3, 4):
+            ctx.step(dt, s, opts)
+        ref = ctx.download_state(["u_vel", "v_vel", "p_field"])
+        step, t = ctx.read_checkpoint(path)
+        assert step == 2
+        for s in (3, 4):
+            ctx.step(dt, s, opts)
+        for k, a in ref.items():
+            np.testing.assert_array_equal(ctx.download(k), a)
