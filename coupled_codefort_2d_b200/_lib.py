@@ -65,6 +65,16 @@ class FuguStats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class FuguProfile(C.Structure):
+    _fields_ = [
+        ("kernel_launches", C.c_ulonglong), ("pcg_ms", C.c_double), ("pcg_launches", C.c_ulonglong),
+        ("pcg_iters", C.c_ulonglong), ("pcg_cells", C.c_ulonglong), ("pcg_grid", C.c_int), ("svof_grid", C.c_int),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 # name -> (restype, argtypes); every pointer is c_void_p, NULL allowed
 _vp, _i, _d = C.c_void_p, C.c_int, C.c_double
 SIGNATURES = {
@@ -74,6 +84,8 @@ SIGNATURES = {
     "fugu_destroy": (None, [_vp]),
     "fugu_set_params": (_i, [_vp, _vp]),
     "fugu_last_error": (C.c_char_p, [_vp]),
+    "fugu_get_stream": (_i, [_vp, _vp]),
+    "fugu_profile": (_i, [_vp, _i, _vp]),
     "fugu_upload": (_i, [_vp, _i, _vp]),
     "fugu_download": (_i, [_vp, _i, _vp]),
     "fugu_step": (_i, [_vp, _d, _i, _vp, _vp]),

@@ -74,6 +74,19 @@ class Context:
         self._p = make_params(self.g, prm, self.precision)
         self._ck(self.L.fugu_set_params(self.h, C.byref(self._p)))
 
+    def stream_handle(self) -> int:
+        """cudaStream_t of the context (for torch.cuda.ExternalStream)."""
+        s = C.c_void_p()
+        self._ck(self.L.fugu_get_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def profile(self, enable: int = -1) -> dict:
+        """Read the measurement counters; enable >= 0 resets them and turns
+        PCG event timing on (1) or off (0)."""
+        out = _lib.FuguProfile()
+        self._ck(self.L.fugu_profile(self.h, int(enable), C.byref(out)))
+        return out.as_dict()
+
     def _f(self, a, kind):
         return ptr(as_fortran(a, self.g, kind))
 

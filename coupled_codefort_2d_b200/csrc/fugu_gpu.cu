@@ -36,10 +36,13 @@ struct CudaError {
     cudaError_t e_ = (x);                         \
     if (e_ != cudaSuccess) throw CudaError{e_, #x}; \
   } while (0)
+// every kernel launch site is followed by CKL: it checks the launch and
+// counts it (c is the context in scope at each site)
 #define CKL(what)                                          \
   do {                                                     \
     cudaError_t e_ = cudaGetLastError();                   \
     if (e_ != cudaSuccess) throw CudaError{e_, what};      \
+    ++c->launches;                                         \
   } while (0)
 
 struct ApiError {
@@ -127,6 +130,13 @@ struct fugu_ctx {
   int pcg_grid = 0;
   int svof_grid = 0;
   int dot_grid = 0;
+  // measurement: launch count, CUDA-event timing of the persistent kernels
+  unsigned long long launches = 0;
+  int prof = 0;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pcg;
+  double prof_pcg_ms = 0.0;
+  unsigned long long prof_pcg_launches = 0, prof_pcg_iters = 0, prof_pcg_cells = 0;
   std::string err;
 };
 
@@ -293,6 +303,29 @@ void scalar_op(fugu_ctx* c, OpArgs op, bool check_active) {
   CKL("k_scalar_op");
 }
 
+cudaEvent_t ev_get(fugu_ctx* c) {
+  if (!c->ev_pool.empty()) {
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  CK(cudaEventCreate(&e));
+  return e;
+}
+// fold the recorded PCG launch intervals into the profile (stream synced)
+void prof_drain(fugu_ctx* c) {
+  for (auto& pr : c->ev_pcg) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, pr.first, pr.second));
+    c->prof_pcg_ms += ms;
+    c->prof_pcg_launches += 1;
+    c->ev_pool.push_back(pr.first);
+    c->ev_pool.push_back(pr.second);
+  }
+  c->ev_pcg.clear();
+}
+
 // persistent PCG (solve_poisson_pressure)
 template <typename T>
 void pcg(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, double tol, int max_iter, bool phi_zero,
@@ -305,7 +338,18 @@ void pcg(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, double tol, int max_i
   a.tol = tol; a.max_iter = max_iter; a.phi_zero = phi_zero ? 1 : 0;
   CK(cudaMemsetAsync(c->gs, 0, sizeof(GridSync), c->s));
   void* args[] = {&a};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (c->prof) {
+    e0 = ev_get(c);
+    e1 = ev_get(c);
+    CK(cudaEventRecord(e0, c->s));
+  }
   CK(cudaLaunchCooperativeKernel((void*)k_pcg<T>, dim3(c->pcg_grid), dim3(PCG_TPB), args, 0, c->s));
+  ++c->launches;
+  if (c->prof) {
+    CK(cudaEventRecord(e1, c->s));
+    c->ev_pcg.push_back({e0, e1});
+  }
 }
 
 template <typename T>
@@ -652,6 +696,7 @@ void svof(fugu_ctx* c, const double* craw, double* cs, double* work, double delt
   CK(cudaMemsetAsync(c->gs, 0, sizeof(GridSync), c->s));
   void* args[] = {&a};
   CK(cudaLaunchCooperativeKernel((void*)k_svof, dim3(c->svof_grid), dim3(PCG_TPB), args, 0, c->s));
+  ++c->launches;
 }
 
 void curvature(fugu_ctx* c, const double* cs, double* kc) {
@@ -684,6 +729,11 @@ void collect(fugu_ctx* c, fugu_stats* st) {
     st->pcg_iters = (long long)c->h_pcg->total_iters;
     st->pcg_calls = (int)c->h_pcg->calls;
     st->svof_iters = c->h_int[0];
+  }
+  if (c->prof) {
+    prof_drain(c);
+    c->prof_pcg_iters += c->h_pcg->total_iters;
+    c->prof_pcg_cells = (unsigned long long)c->prm.nx * c->prm.ny;
   }
 }
 
@@ -886,6 +936,8 @@ void create(fugu_ctx* c) {
 void destroy(fugu_ctx* c) {
   if (!c) return;
   if (c->s) cudaStreamSynchronize(c->s);
+  for (auto& pr : c->ev_pcg) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
+  for (auto e : c->ev_pool) cudaEventDestroy(e);
   for (void* p : c->allocs) cudaFree(p);
   if (c->h_ks) cudaFreeHost(c->h_ks);
   if (c->h_sc) cudaFreeHost(c->h_sc);
@@ -985,6 +1037,34 @@ int fugu_set_params(fugu_ctx* c, const fugu_params* p) {
 }
 
 const char* fugu_last_error(const fugu_ctx* c) { return c ? c->err.c_str() : "NULL context"; }
+
+int fugu_get_stream(fugu_ctx* c, void** stream) {
+  if (!c || !stream) return FUGU_EINVAL;
+  *stream = (void*)c->s;
+  return FUGU_OK;
+}
+
+int fugu_profile(fugu_ctx* c, int enable, fugu_profile_stats* out) {
+  return guard(c, [&] {
+    sync(c);
+    prof_drain(c);
+    if (out) {
+      out->kernel_launches = c->launches;
+      out->pcg_ms = c->prof_pcg_ms;
+      out->pcg_launches = c->prof_pcg_launches;
+      out->pcg_iters = c->prof_pcg_iters;
+      out->pcg_cells = c->prof_pcg_cells;
+      out->pcg_grid = c->pcg_grid;
+      out->svof_grid = c->svof_grid;
+    }
+    if (enable >= 0) {
+      c->prof = enable;
+      c->launches = 0;
+      c->prof_pcg_ms = 0.0;
+      c->prof_pcg_launches = c->prof_pcg_iters = 0;
+    }
+  });
+}
 
 int fugu_upload(fugu_ctx* c, int field, const double* host) {
   return guard(c, [&] {

@@ -115,6 +115,85 @@ __device__ __forceinline__ bool grid_sync(GridSync* gs, unsigned int nblocks, un
   return s_ok != 0;
 }
 
+// --------------------------------------------------------------------------
+// Order-independent sums.  Every sum of the hot path (coupled_dot, the PCG
+// scalars, the zero-mean projections) is accumulated as an unevaluated pair
+// hi + lo with error-free transformations (Knuth's TwoSum), then rounded once.
+// The result is the correctly rounded exact sum except when that sum lies
+// within ~1e-30 relative of a rounding boundary, so the GPU tree order and the
+// oracle's serial order give the same double; the reference's own sums depend
+// on its MPI rank count.  Needs IEEE add without contraction or reassociation
+// (the FP64 build uses --fmad=false).
+// --------------------------------------------------------------------------
+struct DD {
+  double hi, lo;
+};
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+  s = a + b;
+  const double bp = s - a;
+  e = (a - (s - bp)) + (b - bp);
+}
+__device__ __forceinline__ void dd_add(DD& d, double x) {
+  double s, e;
+  two_sum(d.hi, x, s, e);
+  d.hi = s;
+  d.lo = d.lo + e;
+}
+__device__ __forceinline__ DD dd_merge(DD a, DD b) {
+  double s, e;
+  two_sum(a.hi, b.hi, s, e);
+  e = e + (a.lo + b.lo);
+  DD r;
+  r.hi = s + e;
+  r.lo = e - (r.hi - s);
+  return r;
+}
+__device__ __forceinline__ DD dd_shfl_down(DD v, int o) {
+  DD r;
+  r.hi = __shfl_down_sync(0xffffffffu, v.hi, o);
+  r.lo = __shfl_down_sync(0xffffffffu, v.lo, o);
+  return r;
+}
+// block reduction of one DD per thread; result valid in thread 0
+__device__ __forceinline__ DD block_sum_dd(DD v, DD* sh /* >= 32 */) {
+  for (int o = 16; o > 0; o >>= 1) v = dd_merge(v, dd_shfl_down(v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) sh[w] = v;
+  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  if (w == 0) {
+    if (l < nw) v = sh[l];
+    else { v.hi = 0.0; v.lo = 0.0; }
+    for (int o = 16; o > 0; o >>= 1) v = dd_merge(v, dd_shfl_down(v, o));
+  }
+  return v;
+}
+// store a CTA's DD partial as two doubles: part[2b], part[2b+1]
+__device__ __forceinline__ void put_partial(double* part, int b, DD v) {
+  part[2 * b] = v.hi;
+  part[2 * b + 1] = v.lo;
+}
+// rounded sum of n DD partials, identical in every CTA (fixed order)
+__device__ __forceinline__ double sum_partials_dd(const double* part, int n) {
+  __shared__ double s_res;
+  if (threadIdx.x < 32) {
+    DD v{0.0, 0.0};
+    for (int k = threadIdx.x; k < n; k += 32) {
+      DD p;
+      p.hi = __ldcg(part + 2 * k);
+      p.lo = __ldcg(part + 2 * k + 1);
+      v = dd_merge(v, p);
+    }
+    for (int o = 16; o > 0; o >>= 1) v = dd_merge(v, dd_shfl_down(v, o));
+    if (threadIdx.x == 0) s_res = v.hi + v.lo;
+  }
+  __syncthreads();
+  const double r = s_res;
+  __syncthreads();
+  return r;
+}
+
 // deterministic block reduction (sum) of one double per thread; result valid
 // in thread 0.  blockDim.x must be a multiple of 32 and <= 1024.
 __device__ __forceinline__ double block_sum(double v, double* sh /* >= 32 */) {

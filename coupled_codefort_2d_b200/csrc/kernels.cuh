@@ -527,45 +527,6 @@ __global__ void k_pupdate(long n3, T* p, const T* r, const T* v, const double* b
     p[q] = r[q] + b * (p[q] - w * v[q]);
 }
 
-// coupled_dot (mod_bicgstab2.f90:32-72) for up to 5 pairs at once: block
-// partial sums of (a*b)*vol over owned u faces, v faces and cells, FP64
-// accumulation whatever T.  part[pair * nblk + block].
-template <typename T>
-struct DotPairs {
-  const T* a[5];
-  const T* b[5];
-  int npairs;
-};
-template <typename T>
-__global__ void k_dots(Geo g, long n, DotPairs<T> dp, double vol, double* part, const int* active) {
-  if (active && !*active) return;
-  __shared__ double sh[32];
-  double acc[5] = {0, 0, 0, 0, 0};
-  const int nx = g.nx, ny = g.ny, imax = g.imax(), jmax = g.jmax();
-  const long total = (long)imax * ny + (long)nx * jmax + (long)nx * ny;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < total; q += (long)gridDim.x * blockDim.x) {
-    long off;
-    int i, j;
-    if (q < (long)imax * ny) {
-      i = 1 + (int)(q % imax); j = 1 + (int)(q / imax); off = 0;
-    } else if (q < (long)imax * ny + (long)nx * jmax) {
-      const long r = q - (long)imax * ny;
-      i = 1 + (int)(r % nx); j = 1 + (int)(r / nx); off = n;
-    } else {
-      const long r = q - (long)imax * ny - (long)nx * jmax;
-      i = 1 + (int)(r % nx); j = 1 + (int)(r / nx); off = 2 * n;
-    }
-    const long e = off + g.at(i, j);
-#pragma unroll
-    for (int p = 0; p < 5; ++p)
-      if (p < dp.npairs) acc[p] += (double(dp.a[p][e]) * double(dp.b[p][e])) * vol;
-  }
-  for (int p = 0; p < dp.npairs; ++p) {
-    const double s = block_sum(acc[p], sh);
-    if (threadIdx.x == 0) part[p * gridDim.x + blockIdx.x] = s;
-  }
-}
-
 // ------------------------------------------------------------ VOF transport
 __device__ __forceinline__ double limiter_psi(int lim, double r) {
   if (lim == 1) {  // Superbee (extension)

@@ -30,7 +30,7 @@ struct PcgArgs {
   T* pb0;
   T* pb1;
   T* ap;
-  double* part;        // 6 * gridDim.x partial sums
+  double* part;        // 12 * gridDim.x partial sums (6 DD slots)
   GridSync* gs;
   PcgOut* out;
   const int* active;   // skip when *active == 0 (nullable)
@@ -38,6 +38,29 @@ struct PcgArgs {
   int max_iter;
   int phi_zero;        // phi is identically zero on entry (preconditioner use)
 };
+
+// Grid-wide order-independent sum of one (or two) DD values per thread: CTA
+// partials, one bounded grid barrier, then every CTA sums the partials in
+// the same order.  Returns false when the barrier gave up.
+__device__ __forceinline__ bool grid_allreduce(GridSync* gs, unsigned int& gen, double* part, DD v, DD* sh,
+                                               double& out) {
+  v = block_sum_dd(v, sh);
+  if (threadIdx.x == 0) put_partial(part, blockIdx.x, v);
+  if (!grid_sync(gs, gridDim.x, gen)) return false;
+  out = sum_partials_dd(part, gridDim.x);
+  return true;
+}
+__device__ __forceinline__ bool grid_allreduce2(GridSync* gs, unsigned int& gen, double* pa, double* pb, DD a,
+                                                DD b, DD* sh, double& oa, double& ob) {
+  a = block_sum_dd(a, sh);
+  if (threadIdx.x == 0) put_partial(pa, blockIdx.x, a);
+  b = block_sum_dd(b, sh);
+  if (threadIdx.x == 0) put_partial(pb, blockIdx.x, b);
+  if (!grid_sync(gs, gridDim.x, gen)) return false;
+  oa = sum_partials_dd(pa, gridDim.x);
+  ob = sum_partials_dd(pb, gridDim.x);
+  return true;
+}
 
 // stencil of the variable-density Poisson operator at cell (i,j) applied to
 // a field given by accessor f (mod_subsolvers.f90:142-144, :182-184)
@@ -56,7 +79,7 @@ __device__ __forceinline__ T poisson_ap(const Geo& g, const T* cx, const T* cy, 
 template <typename T>
 __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
   if (a.active && !*a.active) return;
-  __shared__ double sh[32];
+  __shared__ DD sh[32];
   const Geo g = a.g;
   const int G = gridDim.x;
   const long N = (long)g.nx * g.ny;
@@ -64,36 +87,34 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
   const long nthr = (long)G * blockDim.x;
   const bool closed = !g.px && !g.py;
   unsigned int gen = 0;
-  double* P0 = a.part;          // setup sum / final mean
-  double* P1 = a.part + G;      // rhs norm
-  double* P2 = a.part + 2 * G;  // initial r.z
-  double* PA = a.part + 3 * G;  // p.Ap
-  double* PB = a.part + 4 * G;  // r.r
-  double* PC = a.part + 5 * G;  // r.z
+  double* P0 = a.part;           // setup sum / final mean
+  double* P1 = a.part + 2 * G;   // rhs norm
+  double* P2 = a.part + 4 * G;   // initial r.z
+  double* PA = a.part + 6 * G;   // p.Ap
+  double* PB = a.part + 8 * G;   // r.r
+  double* PC = a.part + 10 * G;  // r.z
 #define CELL_LOOP for (long q = tid; q < N; q += nthr)
 #define CELL_IJ const int i = 1 + (int)(q % g.nx), j = 1 + (int)(q / g.nx); const int c = g.at(i, j);
 
   // (b) zero-mean projection of the right-hand side when no direction is periodic
   double mean = 0.0;
   if (closed) {
-    double s = 0.0;
-    CELL_LOOP { CELL_IJ s += double(a.rhs[c]); }
-    s = block_sum(s, sh);
-    if (threadIdx.x == 0) P0[blockIdx.x] = s;
-    if (!grid_sync(a.gs, G, gen)) return;
-    mean = sum_partials(P0, G, sh) / (double)(g.nx * g.ny);
+    DD s{0.0, 0.0};
+    CELL_LOOP { CELL_IJ dd_add(s, double(a.rhs[c])); }
+    double tot;
+    if (!grid_allreduce(a.gs, gen, P0, s, sh, tot)) return;
+    mean = tot / (double)(g.nx * g.ny);
   }
-  double ss = 0.0;
+  DD ss{0.0, 0.0};
   CELL_LOOP {
     CELL_IJ
     const T rw = closed ? T(double(a.rhs[c]) - mean) : a.rhs[c];
     a.r[c] = rw;  // r holds rhs_work until the initial residual is formed
-    ss += double(rw) * double(rw);
+    dd_add(ss, double(rw) * double(rw));
   }
-  ss = block_sum(ss, sh);
-  if (threadIdx.x == 0) P1[blockIdx.x] = ss;
-  if (!grid_sync(a.gs, G, gen)) return;
-  const double rhs_norm = sqrt(sum_partials(P1, G, sh));
+  double ssum;
+  if (!grid_allreduce(a.gs, gen, P1, ss, sh, ssum)) return;
+  const double rhs_norm = sqrt(ssum);
   if (rhs_norm < 1.0e-14) {
     for (long q = tid; q < g.n(); q += nthr) a.phi[q] = T(0);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -114,7 +135,7 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
       a.phi[q] = a.phi[g.at(mi, mj)];
     }
   }
-  double rz = 0.0;
+  DD rz{0.0, 0.0};
   CELL_LOOP {
     CELL_IJ
     T rr = a.r[c];
@@ -127,12 +148,10 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
     a.r[c] = rr;
     a.z[c] = zz;
     a.pb0[c] = zz;
-    rz += double(rr) * double(zz);
+    dd_add(rz, double(rr) * double(zz));
   }
-  rz = block_sum(rz, sh);
-  if (threadIdx.x == 0) P2[blockIdx.x] = rz;
-  if (!grid_sync(a.gs, G, gen)) return;
-  double rz_old = sum_partials(P2, G, sh);
+  double rz_old;
+  if (!grid_allreduce(a.gs, gen, P2, rz, sh, rz_old)) return;
 
   // (d) PCG iterations; the direction update p = z + beta p of iteration k-1
   // is evaluated where iteration k needs it (own cell and stencil
@@ -143,7 +162,7 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
     T* pcur = (iter & 1) ? a.pb0 : a.pb1;        // p of this iteration
     const T* pprev = (iter & 1) ? a.pb1 : a.pb0; // p of the previous one
     const T tb = T(beta);
-    double pap = 0.0;
+    DD papd{0.0, 0.0};
     CELL_LOOP {
       CELL_IJ
       T apv, pown;
@@ -162,16 +181,14 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
         pcur[c] = pown;
       }
       a.ap[c] = apv;
-      pap += double(pown) * double(apv);
+      dd_add(papd, double(pown) * double(apv));
     }
-    pap = block_sum(pap, sh);
-    if (threadIdx.x == 0) PA[blockIdx.x] = pap;
-    if (!grid_sync(a.gs, G, gen)) return;
-    pap = sum_partials(PA, G, sh);
+    double pap;
+    if (!grid_allreduce(a.gs, gen, PA, papd, sh, pap)) return;
     if (fabs(pap) < 1.0e-30) break;
     const double alpha = rz_old / pap;
     const T ta = T(alpha);
-    double rr = 0.0, rzn = 0.0;
+    DD rrd{0.0, 0.0}, rzd{0.0, 0.0};
     CELL_LOOP {
       CELL_IJ
       const T pown = pcur[c];
@@ -180,27 +197,22 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
       a.phi[c] = a.phi[c] + ta * pown;
       a.r[c] = rv;
       a.z[c] = zv;
-      rr += double(rv) * double(rv);
-      rzn += double(rv) * double(zv);
+      dd_add(rrd, double(rv) * double(rv));
+      dd_add(rzd, double(rv) * double(zv));
     }
-    rr = block_sum(rr, sh);
-    if (threadIdx.x == 0) PB[blockIdx.x] = rr;
-    rzn = block_sum(rzn, sh);
-    if (threadIdx.x == 0) PC[blockIdx.x] = rzn;
-    if (!grid_sync(a.gs, G, gen)) return;
-    res_norm = sqrt(sum_partials(PB, G, sh));
+    double rr, rz_new;
+    if (!grid_allreduce2(a.gs, gen, PB, PC, rrd, rzd, sh, rr, rz_new)) return;
+    res_norm = sqrt(rr);
     if (res_norm / rhs_norm < a.tol) break;
-    const double rz_new = sum_partials(PC, G, sh);
     beta = rz_new / rz_old;
     rz_old = rz_new;
   }
   if (closed) {
-    double s = 0.0;
-    CELL_LOOP { CELL_IJ s += double(a.phi[c]); }
-    s = block_sum(s, sh);
-    if (threadIdx.x == 0) P0[blockIdx.x] = s;
-    if (!grid_sync(a.gs, G, gen)) return;
-    const double m = sum_partials(P0, G, sh) / (double)(g.nx * g.ny);
+    DD s{0.0, 0.0};
+    CELL_LOOP { CELL_IJ dd_add(s, double(a.phi[c])); }
+    double tot;
+    if (!grid_allreduce(a.gs, gen, P0, s, sh, tot)) return;
+    const double m = tot / (double)(g.nx * g.ny);
     CELL_LOOP { CELL_IJ a.phi[c] = T(double(a.phi[c]) - m); }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -235,7 +247,7 @@ struct SvofArgs {
 // halo + Neumann index maps, which reproduce the ghosts the reference
 // refreshes before every sweep.
 __global__ void __launch_bounds__(512) k_svof(SvofArgs a) {
-  __shared__ double sh[32];
+  __shared__ double sh[32];  // max reduction (exact in any order)
   const Geo g = a.g;
   const int G = gridDim.x;
   const long N = (long)g.nx * g.ny;

@@ -191,7 +191,7 @@ struct DotArgs {
   const T* b[5];
   int npairs;
   double vol;
-  double* part;      // >= 5 * gridDim.x
+  double* part;      // >= 10 * gridDim.x (5 DD partials per CTA)
   double* sc;
   KState* ks;
   OpArgs op;
@@ -201,10 +201,12 @@ struct DotArgs {
 template <typename T>
 __global__ void __launch_bounds__(256) k_dot_op(DotArgs<T> d) {
   if (d.check_active && !d.ks->active) return;
-  __shared__ double sh[32];
+  __shared__ DD sh[32];
   __shared__ bool last;
   const Geo g = d.g;
-  double acc[5] = {0, 0, 0, 0, 0};
+  DD acc[5];
+#pragma unroll
+  for (int p = 0; p < 5; ++p) acc[p] = DD{0.0, 0.0};
   const int nx = g.nx, ny = g.ny, imax = g.imax(), jmax = g.jmax();
   const long nu = (long)imax * ny, nv = (long)nx * jmax, np = (long)nx * ny;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nu + nv + np; q += (long)gridDim.x * blockDim.x) {
@@ -220,11 +222,11 @@ __global__ void __launch_bounds__(256) k_dot_op(DotArgs<T> d) {
     }
 #pragma unroll
     for (int p = 0; p < 5; ++p)
-      if (p < d.npairs) acc[p] += (double(d.a[p][e]) * double(d.b[p][e])) * d.vol;
+      if (p < d.npairs) dd_add(acc[p], (double(d.a[p][e]) * double(d.b[p][e])) * d.vol);
   }
   for (int p = 0; p < d.npairs; ++p) {
-    const double s = block_sum(acc[p], sh);
-    if (threadIdx.x == 0) d.part[p * gridDim.x + blockIdx.x] = s;
+    const DD s = block_sum_dd(acc[p], sh);
+    if (threadIdx.x == 0) put_partial(d.part + 2 * p * gridDim.x, blockIdx.x, s);
   }
   if (threadIdx.x == 0) {
     __threadfence();
@@ -235,7 +237,7 @@ __global__ void __launch_bounds__(256) k_dot_op(DotArgs<T> d) {
   if (!last) return;
   __threadfence();
   for (int p = 0; p < d.npairs; ++p) {
-    const double s = sum_partials(d.part + p * gridDim.x, gridDim.x, sh);
+    const double s = sum_partials_dd(d.part + 2 * p * gridDim.x, gridDim.x);
     if (threadIdx.x == 0) d.sc[S_D0 + p] = s;
   }
   if (threadIdx.x == 0) {

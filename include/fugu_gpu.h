@@ -119,6 +119,16 @@ enum {
 
 typedef struct fugu_ctx fugu_ctx;
 
+/* Measurement counters (no counterpart in the reference, which has none). */
+typedef struct {
+  unsigned long long kernel_launches; /* kernels launched since the last reset */
+  double pcg_ms;                      /* CUDA-event time of the PCG launches   */
+  unsigned long long pcg_launches;
+  unsigned long long pcg_iters;       /* PCG iterations in those launches      */
+  unsigned long long pcg_cells;       /* cells per PCG iteration (nx*ny)       */
+  int pcg_grid, svof_grid;            /* CTAs of the persistent kernels        */
+} fugu_profile_stats;
+
 /* ---------------------------------------------------------------- context */
 void fugu_params_default(fugu_params* p);
 const char* fugu_version(void);
@@ -128,6 +138,13 @@ void fugu_destroy(fugu_ctx* ctx);
 /* Replace the module globals (grid size must not change). */
 int fugu_set_params(fugu_ctx* ctx, const fugu_params* p);
 const char* fugu_last_error(const fugu_ctx* ctx);
+/* The context's CUDA stream (cudaStream_t), so a caller can time or order
+ * work against it.  No counterpart in the reference. */
+int fugu_get_stream(fugu_ctx* ctx, void** stream);
+/* Read the counters into *out (may be NULL); enable >= 0 then resets them and
+ * switches PCG event timing on (1) or off (0); enable < 0 only reads.
+ * No counterpart in the reference. */
+int fugu_profile(fugu_ctx* ctx, int enable, fugu_profile_stats* out);
 /* Copy one device-resident field from / to a host array (reference layout). */
 int fugu_upload(fugu_ctx* ctx, int field, const double* host);
 int fugu_download(fugu_ctx* ctx, int field, double* host);

@@ -38,6 +38,22 @@ static double* zalloc(size_t n) {
   if (!p) { fprintf(stderr, "fugu_oracle: out of memory\n"); abort(); }
   return p;
 }
+/* Order-independent sums: the reference accumulates each reduction serially
+ * per MPI rank and then MPI_Allreduce-s the rank partials, so its rounding
+ * depends on the rank count.  The oracle (and the CUDA path) accumulate the
+ * same terms as an unevaluated pair hi + lo with Knuth's TwoSum and round
+ * once, which yields the correctly rounded exact sum except within ~1e-30
+ * relative of a rounding boundary -- the same double in any order. */
+typedef struct { double hi, lo; } dsum;
+static void ds_add(dsum* d, double x) {
+  double s = d->hi + x;
+  double bp = s - d->hi;
+  double e = (d->hi - (s - bp)) + (x - bp);
+  d->hi = s;
+  d->lo = d->lo + e;
+}
+static double ds_val(dsum d) { return d.hi + d.lo; }
+
 static double dmin(double a, double b) { return a < b ? a : b; }
 static double dmax(double a, double b) { return a > b ? a : b; }
 static double clip01(double x) { return dmax(0.0, dmin(1.0, x)); }
@@ -463,17 +479,17 @@ void fo_solve_poisson_pressure(const fo_model* m, double* phi, const double* rhs
 
   memcpy(rw, rhs, nc * sizeof(double));
   if (closed) {
-    double s = 0.0;
+    dsum s = {0.0, 0.0};
     for (int j = 1; j <= ny; ++j)
-      for (int i = 1; i <= nx; ++i) s += AC(rhs, i, j);
-    double mean = s / (double)(nx * ny);
+      for (int i = 1; i <= nx; ++i) ds_add(&s, AC(rhs, i, j));
+    double mean = ds_val(s) / (double)(nx * ny);
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) AC(rw, i, j) = AC(rhs, i, j) - mean;
   }
-  double dot = 0.0;
+  dsum dot = {0.0, 0.0};
   for (int j = 1; j <= ny; ++j)
-    for (int i = 1; i <= nx; ++i) dot += AC(rw, i, j) * AC(rw, i, j);
-  const double rhs_norm = sqrt(dot);
+    for (int i = 1; i <= nx; ++i) ds_add(&dot, AC(rw, i, j) * AC(rw, i, j));
+  const double rhs_norm = sqrt(ds_val(dot));
   if (rhs_norm < 1.0e-14) {
     memset(phi, 0, nc * sizeof(double));
     if (iter_out) *iter_out = 0;
@@ -493,47 +509,50 @@ void fo_solve_poisson_pressure(const fo_model* m, double* phi, const double* rhs
       AC(z, i, j) = AC(dinv, i, j) * AC(r, i, j);
       AC(p, i, j) = AC(z, i, j);
     }
-  double rz_old = 0.0;
+  dsum rz0 = {0.0, 0.0};
   for (int j = 1; j <= ny; ++j)
-    for (int i = 1; i <= nx; ++i) rz_old += AC(r, i, j) * AC(z, i, j);
+    for (int i = 1; i <= nx; ++i) ds_add(&rz0, AC(r, i, j) * AC(z, i, j));
+  double rz_old = ds_val(rz0);
 
   for (iter = 1; iter <= max_iter; ++iter) {
     fo_halo_scalar(m, p);
     neumann_cell(m, p);
-    double pAp = 0.0;
+    dsum pApd = {0.0, 0.0};
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
         poisson_coefs(m, rho_u, rho_v, i, j, idx2, idy2, &cE, &cW, &cN, &cS);
         AC(Ap, i, j) = (cE + cW + cN + cS) * AC(p, i, j) -
                        (cE * AC(p, i + 1, j) + cW * AC(p, i - 1, j) + cN * AC(p, i, j + 1) +
                         cS * AC(p, i, j - 1));
-        pAp += AC(p, i, j) * AC(Ap, i, j);
+        ds_add(&pApd, AC(p, i, j) * AC(Ap, i, j));
       }
+    double pAp = ds_val(pApd);
     if (fabs(pAp) < 1.0e-30) break;
     double alpha = rz_old / pAp;
-    double rr = 0.0;
+    dsum rrd = {0.0, 0.0};
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) {
         AC(phi, i, j) = AC(phi, i, j) + alpha * AC(p, i, j);
         AC(r, i, j) = AC(r, i, j) - alpha * AC(Ap, i, j);
         AC(z, i, j) = AC(dinv, i, j) * AC(r, i, j);
-        rr += AC(r, i, j) * AC(r, i, j);
+        ds_add(&rrd, AC(r, i, j) * AC(r, i, j));
       }
-    res_norm = sqrt(rr);
+    res_norm = sqrt(ds_val(rrd));
     if (res_norm / rhs_norm < tol) break;
-    double rz_new = 0.0;
+    dsum rzn = {0.0, 0.0};
     for (int j = 1; j <= ny; ++j)
-      for (int i = 1; i <= nx; ++i) rz_new += AC(r, i, j) * AC(z, i, j);
+      for (int i = 1; i <= nx; ++i) ds_add(&rzn, AC(r, i, j) * AC(z, i, j));
+    double rz_new = ds_val(rzn);
     double beta = rz_new / rz_old;
     rz_old = rz_new;
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) AC(p, i, j) = AC(z, i, j) + beta * AC(p, i, j);
   }
   if (closed) {
-    double s = 0.0;
+    dsum s = {0.0, 0.0};
     for (int j = 1; j <= ny; ++j)
-      for (int i = 1; i <= nx; ++i) s += AC(phi, i, j);
-    double mean = s / (double)(nx * ny);
+      for (int i = 1; i <= nx; ++i) ds_add(&s, AC(phi, i, j));
+    double mean = ds_val(s) / (double)(nx * ny);
     for (int j = 1; j <= ny; ++j)
       for (int i = 1; i <= nx; ++i) AC(phi, i, j) = AC(phi, i, j) - mean;
   }
@@ -678,14 +697,14 @@ double fo_coupled_dot(const fo_model* m, const double* u1, const double* v1, con
                       const double* u2, const double* v2, const double* p2) {
   const int nx = m->nx, ny = m->ny, imax = iu_max(m), jmax = jv_max(m);
   const double vol = m->dx * m->dy;
-  double s = 0.0;
+  dsum s = {0.0, 0.0};
   for (int j = 1; j <= ny; ++j)
-    for (int i = 1; i <= imax; ++i) s += AU(u1, i, j) * AU(u2, i, j) * vol;
+    for (int i = 1; i <= imax; ++i) ds_add(&s, AU(u1, i, j) * AU(u2, i, j) * vol);
   for (int j = 1; j <= jmax; ++j)
-    for (int i = 1; i <= nx; ++i) s += AV(v1, i, j) * AV(v2, i, j) * vol;
+    for (int i = 1; i <= nx; ++i) ds_add(&s, AV(v1, i, j) * AV(v2, i, j) * vol);
   for (int j = 1; j <= ny; ++j)
-    for (int i = 1; i <= nx; ++i) s += AC(p1, i, j) * AC(p2, i, j) * vol;
-  return s;
+    for (int i = 1; i <= nx; ++i) ds_add(&s, AC(p1, i, j) * AC(p2, i, j) * vol);
+  return ds_val(s);
 }
 
 /* a coupled (u,v,p) work triple allocated over the full padded extents */
