@@ -1,0 +1,446 @@
+"""Benchmark of the B200 FUGU-2D coupled step (one JSON line on rank 0).
+
+Workload (the configuration the headline metric is quoted on): static
+two-phase droplet on the unit square, 256 x 256 MAC grid, R = 0.25 centred,
+inside rho = 1, mu = 0.1, outside rho = 0.1, mu = 0.01, sigma = 1, no gravity,
+colour from 16 x 16 sub-sampled area fractions, BDF2, dt = 1e-4, each coupled
+step solved to a true relative residual |B - AX| / |B| < 1e-8.  A "step" is
+one advance_coupled_step.  Synthetic inputs: the case is fully determined by
+these parameters (no dataset).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value : mixed form (FP32 inner BiCGStab(2)+PCD inside FP64 defect correction),
+        device-resident state, CUDA events on the library's stream around
+        each timed step, L2 flushed (256 MiB write) between timed steps.
+e2e   : the same steps through the drop-in C entry fugu_advance_coupled_step
+        with pinned host arrays (state uploaded and downloaded every step).
+Also reported: the FP64-inner form of the same solver ("fp64"), and the
+reference algorithm as written (BiCGStab + PCD, preconditioned residual,
+max 500 iterations) with the residual it actually reaches.
+
+Multi-GPU (torchrun): the case does not shard; every rank runs an
+independent replica ("replicas only", weak scaling); value = all ranks'
+steps / max over ranks of the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "coupled steps/s at 1e-8 residual: FP32+refine vs FP64 on B200; % HBM roofline"
+UNIT = "coupled steps/s"
+N = 256
+DT = 1e-4
+TOL = 1e-8
+
+
+def case_params():
+    from coupled_codefort_2d_b200.params import Params
+
+    return Params(rho1=1.0, rho2=0.1, mu1=0.1, mu2=0.01, sigma=1.0, gx=0.0, gy=0.0, time_order=2,
+                  tol_bicgstab2=TOL, max_iter_bicgstab2=500, refine=1, refine_inner_tol=1e-2,
+                  refine_max_inner=30, refine_max_outer=60, krylov_bc_fix=1)
+
+
+def initial_state(g, prm):
+    from coupled_codefort_2d_b200 import cases
+    from coupled_codefort_2d_b200._lib import FIELD_KIND
+
+    c0 = cases.circle_fraction(g, 0.5, 0.5, 0.25, inside=1.0, ns=16)
+    st = {k: g.zeros(FIELD_KIND[k]) for k in ("u_vel", "v_vel", "p_field", "c_field", "u_prev", "v_prev", "rho_c",
+                                              "rho_u", "rho_v", "kappa", "zeta", "eta", "kappa_curv",
+                                              "f_sigma_u", "f_sigma_v")}
+    st["c_field"][...] = c0
+    return st
+
+
+def workload_config(solver_name):
+    return {
+        "workload": f"static_droplet_{N}x{N}", "grid": [N, N], "radius": 0.25, "rho_in_out": [1.0, 0.1],
+        "mu_in_out": [0.1, 0.01], "sigma": 1.0, "time_scheme": "BDF2", "dt": DT,
+        "residual": "true |B-AX|/|B| < 1e-8 (coupled_dot norm)",
+        "solver": solver_name, "l2": "flushed between timed steps (256 MiB write)",
+    }
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks and throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = float(rows[0][2]) if rows[0][2].replace(".", "").isdigit() else None
+        loaded = [s for s in sm if smax and s > 0.5 * smax] or sm
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for nm, v in zip(names, r[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(loaded)) if loaded else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+# --------------------------------------------------------------- GPU arm
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+
+    from coupled_codefort_2d_b200 import build
+    from coupled_codefort_2d_b200._lib import FIELD_KIND, MIXED, FP64
+    from coupled_codefort_2d_b200.context import Context
+    from coupled_codefort_2d_b200.layout import Grid
+
+    build.build()
+    torch.cuda.set_device(local_rank)
+    g = Grid(N, N)
+    prm = case_params()
+    st0 = initial_state(g, prm)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
+
+    def run_form(precision, steps, warmup, use_b2=True, prm_=None, profile=False, sampler=None):
+        p = prm_ or prm
+        with Context(g, p, device=local_rank, precision=precision) as ctx:
+            ctx.upload_state(st0)
+            # properties from C (the drivers' set-up, main.f90:185-186)
+            pr = {k: g.zeros(FIELD_KIND[k]) for k in ("rho_c", "rho_u", "rho_v", "kappa", "zeta", "eta")}
+            ctx.compute_mixture_densities(st0["c_field"], pr["rho_c"], pr["rho_u"], pr["rho_v"])
+            ctx.compute_mixture_viscosities(st0["c_field"], pr["kappa"], pr["zeta"], pr["eta"])
+            for k, a in pr.items():
+                ctx.upload(k, a)
+            opts = ctx.step_opts(use_bicgstab2=use_b2)
+            stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=f"cuda:{local_rank}")
+            stats = []
+            for s in range(1, warmup + 1):
+                stats.append(ctx.step(DT, s, opts))
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            if profile:
+                ctx.profile(1)
+            times = []
+            ctx_s = sampler if sampler is not None else _Null()
+            with ctx_s:
+                for s in range(warmup + 1, warmup + steps + 1):
+                    with torch.cuda.stream(stream):
+                        flush.zero_()
+                        e0 = torch.cuda.Event(enable_timing=True)
+                        e1 = torch.cuda.Event(enable_timing=True)
+                        e0.record(stream)
+                    r = ctx.step(DT, s, opts)
+                    with torch.cuda.stream(stream):
+                        e1.record(stream)
+                    e1.synchronize()
+                    times.append(e0.elapsed_time(e1))
+                    stats.append(r)
+            torch.cuda.synchronize()
+            prof = ctx.profile(0) if profile else None
+            state = ctx.download_state(["u_vel", "v_vel", "p_field", "c_field", "u_prev", "v_prev", "rho_c", "rho_u",
+                                        "rho_v", "kappa", "zeta", "eta", "kappa_curv", "f_sigma_u", "f_sigma_v"])
+        return times, stats, prof, state
+
+    sampler = ClockSampler(local_rank)
+    t_mixed, s_mixed, prof, state_w = run_form(MIXED, args.steps, args.warmup, profile=True, sampler=sampler)
+    total_ms = float(np.sum(t_mixed))
+    # max over ranks of the timed region
+    if world > 1:
+        tt = torch.tensor([total_ms], device=f"cuda:{local_rank}", dtype=torch.float64)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    out = {"t_mixed": t_mixed, "s_mixed": s_mixed, "prof": prof, "total_ms": total_ms, "clocks": sampler.summary()}
+
+    if rank == 0 and not args.quick:
+        # FP64 inner form of the same solver, same steps
+        t64, s64, _, _ = run_form(FP64, args.steps, args.warmup)
+        out["t_fp64"], out["s_fp64"] = t64, s64
+        # the reference algorithm as written (preconditioned residual, max 500 its)
+        pref = prm.with_(refine=0, krylov_bc_fix=0)
+        tref, sref, _, _ = run_form(FP64, 2, 1, use_b2=False, prm_=pref)
+        out["t_ref"], out["s_ref"] = tref, sref
+        out["e2e"] = e2e_arm(args, g, prm, st0, local_rank)
+        out["state_w"] = state_w
+    return out
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        pass
+
+
+def pinned_field(g, kind):
+    import torch
+
+    shp = g.shape(kind)
+    t = torch.zeros((shp[1], shp[0]), dtype=torch.float64, pin_memory=True)
+    return t, t.numpy().T  # Fortran-ordered view of pinned memory
+
+
+def e2e_arm(args, g, prm, st0, local_rank):
+    """fugu_advance_coupled_step (the drop-in C entry) on pinned host arrays."""
+    import torch
+
+    from coupled_codefort_2d_b200._lib import FIELD_KIND, MIXED
+    from coupled_codefort_2d_b200.context import Context
+
+    names = ["u_vel", "v_vel", "p_field", "c_field", "u_prev", "v_prev", "rho_c", "rho_u", "rho_v", "kappa",
+             "zeta", "eta", "kappa_curv", "f_sigma_u", "f_sigma_v"]
+    keep, host = [], {}
+    for k in names:
+        t, a = pinned_field(g, FIELD_KIND[k])
+        a[...] = st0[k]
+        keep.append(t)
+        host[k] = a
+    nbytes = sum(a.nbytes for a in host.values())
+    with Context(g, prm, device=local_rank, precision=MIXED) as ctx:
+        ctx.compute_mixture_densities(host["c_field"], host["rho_c"], host["rho_u"], host["rho_v"])
+        ctx.compute_mixture_viscosities(host["c_field"], host["kappa"], host["zeta"], host["eta"])
+        stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=f"cuda:{local_rank}")
+        times = []
+        for s in range(1, args.warmup + args.steps + 1):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            r = ctx.advance_coupled_step(*[host[k] for k in names], DT, s, use_bicgstab2=True)
+            e1.record(stream)
+            e1.synchronize()
+            if s > args.warmup:
+                times.append(e0.elapsed_time(e1))
+            assert r["res"] < TOL, r
+    ms = float(np.mean(times))
+    return {"value": 1000.0 / ms, "unit": UNIT, "h2d_bytes_per_step": int(nbytes), "d2h_bytes_per_step": int(nbytes),
+            "ms_per_step": ms, "entry": "fugu_advance_coupled_step (pinned host arrays, reference layout)"}
+
+
+# --------------------------------------------------------------- CPU legs
+def cpu_step_time(state, step_idx, nsteps=1):
+    """The oracle (a C restatement of the reference) on the same inputs."""
+    from coupled_codefort_2d_b200.layout import Grid
+    from oracle import oracle
+
+    g = Grid(N, N)
+    prm = case_params()
+    o = oracle.Oracle(g, prm)
+    st = {k: a.copy(order="F") for k, a in state.items()}
+    t0 = time.perf_counter()
+    stats = []
+    for s in range(step_idx, step_idx + nsteps):
+        stats.append(o.step(st, DT, s, use_bicgstab2=True))
+    return (time.perf_counter() - t0) / nsteps, stats
+
+
+def _replica_worker(args_tuple):
+    """one replica's step; replica 0 also returns the advanced state"""
+    state, step_idx, keep = args_tuple
+    from coupled_codefort_2d_b200.layout import Grid
+    from oracle import oracle
+
+    o = oracle.Oracle(Grid(N, N), case_params())
+    st = {k: a.copy(order="F") for k, a in state.items()}
+    t0 = time.perf_counter()
+    o.step(st, DT, step_idx, use_bicgstab2=True)
+    return time.perf_counter() - t0, (st if keep else None)
+
+
+def reference_arm(args, rank, world):
+    """The reference's CPU path on the host cores: the oracle port (the
+    Fortran/MPI reference cannot be built here), one independent replica per
+    host core, each timing whole coupled steps."""
+    if rank != 0:
+        return
+    from coupled_codefort_2d_b200.layout import Grid
+    from oracle import oracle
+
+    oracle.build()
+    g = Grid(N, N)
+    prm = case_params()
+    st = initial_state(g, prm)
+    o = oracle.Oracle(g, prm)
+    o.densities(st["c_field"], st["rho_c"], st["rho_u"], st["rho_v"])
+    o.viscosities(st["c_field"], st["kappa"], st["zeta"], st["eta"])
+    cores = os.cpu_count() or 1
+    import multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    for s in range(1, args.warmup + 1):  # untimed, serial
+        o.step(st, DT, s, use_bicgstab2=True)
+    per_step = []
+    with ctx.Pool(cores) as pool:
+        for s in range(args.warmup + 1, args.warmup + args.steps + 1):
+            t0 = time.perf_counter()
+            res = pool.map(_replica_worker, [(st, s, i == 0) for i in range(cores)])
+            per_step.append(time.perf_counter() - t0)
+            st = res[0][1]
+    ms = 1000.0 * float(np.mean(per_step))
+    value = cores * 1000.0 / ms
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / cores, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(
+            "FP64 defect correction around BiCGStab(2)+PCD (oracle port of the reference modules)"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{cores} independent replicas x 1 thread, whole steps of the {N}^2 droplet"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "Fortran/MPI reference unbuildable here (no gfortran, no MPI); the C oracle restates it",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- main
+def roofline(prof, peaks):
+    """Dominant kernel: the persistent PCG of the PCD preconditioner (FP32 in
+    the mixed form).  Algorithmic bytes per PCG iteration and cell: reads of
+    z, p_prev, cx, cy, dinv, phi, r and writes of p, phi, r, z = 11 values."""
+    if not prof or not prof["pcg_launches"]:
+        return None
+    elt = 4  # FP32 inner solve
+    bytes_per_launch = 11 * elt * prof["pcg_cells"] * prof["pcg_iters"] / prof["pcg_launches"]
+    ms_per_launch = prof["pcg_ms"] / prof["pcg_launches"]
+    achieved = bytes_per_launch / (ms_per_launch * 1e-3) / 1e9
+    peak = peaks.get("hbm_gbs") if peaks else None
+    src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "pcg_traffic.json")
+    if os.path.exists(tf):
+        try:
+            t = json.load(open(tf))
+            traffic = t.get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+    return {"kernel": "k_pcg<float> (persistent Jacobi-PCG of the PCD pressure step)", "bound": "hbm",
+            "achieved": achieved, "peak": peak, "peak_source": src, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "bytes_per_launch": bytes_per_launch, "ms_per_launch": ms_per_launch,
+            "iters_per_launch": prof["pcg_iters"] / prof["pcg_launches"]}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--quick", action="store_true", help="skip the secondary arms")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+        return
+
+    out = gpu_arm(args, rank, world, local_rank)
+    if world > 1:
+        import torch
+
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    peaks = {}
+    pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pk):
+        peaks = json.load(open(pk))
+    total_ms = out["total_ms"]
+    value = world * args.steps * 1000.0 / total_ms
+    s_m = out["s_mixed"][args.warmup:]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 outer",
+        "data": "synthetic (droplet case fully determined by its parameters)",
+        "config": workload_config("FP64 defect correction around FP32 BiCGStab(2)+PCD (inner tol 1e-2)"),
+        "max_true_residual": max(r["res"] for r in s_m),
+        "per_step": {"outer": [r["outer"] for r in s_m], "inner_iters": [r["iter"] for r in s_m],
+                     "pcg_calls": [r["pcg_calls"] for r in s_m], "pcg_iters": [r["pcg_iters"] for r in s_m]},
+        "roofline": roofline(out["prof"], peaks),
+        "gpu_launches": int(out["prof"]["kernel_launches"]) if out["prof"] else None,
+        "clocks": out["clocks"],
+    }
+    if "t_fp64" in out:
+        s64 = out["s_fp64"][args.warmup:]
+        line["fp64"] = {"value": 1000.0 * len(out["t_fp64"]) / float(np.sum(out["t_fp64"])), "unit": UNIT,
+                        "max_true_residual": max(r["res"] for r in s64),
+                        "solver": "FP64 defect correction around FP64 BiCGStab(2)+PCD"}
+        line["mixed_over_fp64"] = value / world / line["fp64"]["value"]
+        sref = out["s_ref"][1:]
+        line["reference_algorithm_fp64"] = {
+            "value": 1000.0 * len(out["t_ref"]) / float(np.sum(out["t_ref"])), "unit": UNIT,
+            "iterations": [r["iter"] for r in sref], "preconditioned_residual": [r["res"] for r in sref],
+            "status": ["converged" if r["status"] == 0 else "max-iter/breakdown" for r in sref],
+            "solver": "bicgstab_solve + PCD exactly as the reference (tol 1e-8 on the preconditioned residual)"}
+    if "e2e" in out:
+        line["e2e"] = out["e2e"]
+    if not args.no_cpu and "state_w" in out:
+        nxt = args.warmup + args.steps + 1
+        dt_cpu, st_cpu = cpu_step_time(out["state_w"], nxt)
+        line["cpu_baseline"] = {
+            "value": 1.0 / dt_cpu, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"1 coupled step (step {nxt}) of the same workload from the GPU run's state, "
+                      "oracle C port, FP64 defect correction around BiCGStab(2)+PCD, 1 thread",
+            "true_residual": st_cpu[0].res}
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -20,6 +20,7 @@
 
 #include "fugu_gpu.h"
 #include "kernels.cuh"
+#include "pcg_cluster.cuh"
 #include "persistent.cuh"
 #include "scalars.cuh"
 
@@ -130,6 +131,12 @@ struct fugu_ctx {
   int pcg_grid = 0;
   int svof_grid = 0;
   int dot_grid = 0;
+  // cluster-resident PCG plan per precision (index 0 FP64, 1 FP32)
+  struct ClusterPlan {
+    bool ok = false;
+    int C = 0, rows_per = 0, cpt = 0;
+    size_t smem = 0;
+  } pcgc[2];
   // measurement: launch count, CUDA-event timing of the persistent kernels
   unsigned long long launches = 0;
   int prof = 0;
@@ -303,6 +310,80 @@ void scalar_op(fugu_ctx* c, OpArgs op, bool check_active) {
   CKL("k_scalar_op");
 }
 
+// cluster-resident PCG: kernel for a cells-per-thread count
+template <typename T>
+const void* pcgc_fn(int cpt) {
+  switch (cpt) {
+    case 1: return (const void*)k_pcg_cluster<T, 1>;
+    case 2: return (const void*)k_pcg_cluster<T, 2>;
+    case 4: return (const void*)k_pcg_cluster<T, 4>;
+    case 8: return (const void*)k_pcg_cluster<T, 8>;
+    case 16: return (const void*)k_pcg_cluster<T, 16>;
+  }
+  return nullptr;
+}
+template <typename T>
+cudaLaunchConfig_t pcgc_cfg(int C, size_t smem, cudaStream_t s, cudaLaunchAttribute* at) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(C, 1, 1);
+  cfg.blockDim = dim3(PCGC_TPB, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = C;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+template <typename T>
+cudaError_t launch_pcg_cluster(PcgClusterArgs<T> a, int C, int cpt, size_t smem, cudaStream_t s) {
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg = pcgc_cfg<T>(C, smem, s, at);
+  void* args[] = {&a};
+  return cudaLaunchKernelExC(&cfg, pcgc_fn<T>(cpt), args);
+}
+// Plan the cluster-resident PCG for precision T: up to 16 CTAs of PCGC_TPB
+// threads, every CTA's rows must fit the shared memory and the register
+// arrays (cpt <= 8 in FP64, <= 16 in FP32), and the device must be able to
+// co-schedule such a cluster.
+template <typename T>
+void plan_pcg_cluster(fugu_ctx* c, fugu_ctx::ClusterPlan& pl) {
+  pl = fugu_ctx::ClusterPlan{};
+  const char* env = std::getenv("FUGU_PCG");
+  if (env && std::strcmp(env, "grid") == 0) return;
+  const int nx = c->prm.nx, ny = c->prm.ny;
+  const int cmax = ny < 16 ? ny : 16;
+  const int rows_per = (ny + cmax - 1) / cmax;
+  const int C = (ny + rows_per - 1) / rows_per;
+  const long cells = (long)nx * rows_per;
+  int cpt = 1;
+  while ((long)cpt * PCGC_TPB < cells) cpt *= 2;
+  const int cpt_max = sizeof(T) == 8 ? 8 : 16;
+  const size_t smem = sizeof(T) * (size_t)pcgc_smem_elems(nx, rows_per);
+  const size_t smem_cap = 227 * 1024 - 1024;  // minus the kernel's static shared memory
+  if (cpt > cpt_max || smem > smem_cap) return;
+  const void* fn = pcgc_fn<T>(cpt);
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+      cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  cudaLaunchAttribute at[1];
+  cudaLaunchConfig_t cfg = pcgc_cfg<T>(C, smem, c->s, at);
+  int nclusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&nclusters, fn, &cfg) != cudaSuccess || nclusters < 1) {
+    cudaGetLastError();
+    return;
+  }
+  pl.ok = true;
+  pl.C = C;
+  pl.rows_per = rows_per;
+  pl.cpt = cpt;
+  pl.smem = smem;
+}
+
 cudaEvent_t ev_get(fugu_ctx* c) {
   if (!c->ev_pool.empty()) {
     cudaEvent_t e = c->ev_pool.back();
@@ -336,15 +417,25 @@ void pcg(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, double tol, int max_i
   a.phi = phi; a.r = w.r; a.z = w.z; a.pb0 = w.pb0; a.pb1 = w.pb1; a.ap = w.ap;
   a.part = c->part; a.gs = c->gs; a.out = c->pcg_out; a.active = active;
   a.tol = tol; a.max_iter = max_iter; a.phi_zero = phi_zero ? 1 : 0;
-  CK(cudaMemsetAsync(c->gs, 0, sizeof(GridSync), c->s));
-  void* args[] = {&a};
+  const fugu_ctx::ClusterPlan& cp = c->pcgc[sizeof(T) == 8 ? 0 : 1];
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (c->prof) {
     e0 = ev_get(c);
     e1 = ev_get(c);
     CK(cudaEventRecord(e0, c->s));
   }
-  CK(cudaLaunchCooperativeKernel((void*)k_pcg<T>, dim3(c->pcg_grid), dim3(PCG_TPB), args, 0, c->s));
+  if (cp.ok) {
+    PcgClusterArgs<T> ca;
+    ca.g = c->g;
+    ca.rhs = rhs; ca.cx = w.cx; ca.cy = w.cy; ca.dinv = w.dinv; ca.phi = phi;
+    ca.out = c->pcg_out; ca.active = active; ca.tol = tol; ca.max_iter = max_iter;
+    ca.phi_zero = phi_zero ? 1 : 0; ca.rows_per = cp.rows_per;
+    CK(launch_pcg_cluster<T>(ca, cp.C, cp.cpt, cp.smem, c->s));
+  } else {
+    CK(cudaMemsetAsync(c->gs, 0, sizeof(GridSync), c->s));
+    void* args[] = {&a};
+    CK(cudaLaunchCooperativeKernel((void*)k_pcg<T>, dim3(c->pcg_grid), dim3(PCG_TPB), args, 0, c->s));
+  }
   ++c->launches;
   if (c->prof) {
     CK(cudaEventRecord(e1, c->s));
@@ -917,6 +1008,11 @@ void create(fugu_ctx* c) {
   if (g32 < c->pcg_grid) c->pcg_grid = g32;
   c->svof_grid = coop_grid((const void*)k_svof, PCG_TPB, c->nsm, ncell);
   if (c->pcg_grid < 1 || c->svof_grid < 1) throw ApiError{FUGU_ECUDA, "no co-resident grid for persistent kernels"};
+  plan_pcg_cluster<double>(c, c->pcgc[0]);
+  plan_pcg_cluster<float>(c, c->pcgc[1]);
+  const char* env = std::getenv("FUGU_PCG");
+  if (env && std::strcmp(env, "cluster") == 0 && !(c->pcgc[0].ok && c->pcgc[1].ok))
+    throw ApiError{FUGU_EINVAL, "FUGU_PCG=cluster but this grid does not fit a thread-block cluster"};
   c->dot_grid = c->nsm * 2;
   c->part_len = 8L * (c->nsm * 8 + 64);
   c->part = dalloc<double>(c, c->part_len);
@@ -1056,6 +1152,8 @@ int fugu_profile(fugu_ctx* c, int enable, fugu_profile_stats* out) {
       out->pcg_cells = c->prof_pcg_cells;
       out->pcg_grid = c->pcg_grid;
       out->svof_grid = c->svof_grid;
+      out->pcg_cluster_fp64 = c->pcgc[0].ok ? c->pcgc[0].C : 0;
+      out->pcg_cluster_fp32 = c->pcgc[1].ok ? c->pcgc[1].C : 0;
     }
     if (enable >= 0) {
       c->prof = enable;

@@ -127,6 +127,8 @@ typedef struct {
   unsigned long long pcg_iters;       /* PCG iterations in those launches      */
   unsigned long long pcg_cells;       /* cells per PCG iteration (nx*ny)       */
   int pcg_grid, svof_grid;            /* CTAs of the persistent kernels        */
+  int pcg_cluster_fp64;               /* CTAs of the cluster-resident PCG (0 =  */
+  int pcg_cluster_fp32;               /*   grid-wide kernel used instead)       */
 } fugu_profile_stats;
 
 /* ---------------------------------------------------------------- context */

@@ -221,8 +221,16 @@ def test_coupled_dot(gpu, oracle_mod, grid):
     assert dg == do, (dg, do)
 
 
+@pytest.fixture(params=["auto", "grid"])
+def pcg_variant(request, monkeypatch):
+    """auto: the cluster-resident PCG when the grid fits one thread-block
+    cluster (all the grids here do); grid: the grid-wide persistent kernel."""
+    monkeypatch.setenv("FUGU_PCG", request.param)
+    return request.param
+
+
 @pytest.mark.parametrize("zero_init", [True, False])
-def test_poisson_pcg(gpu, oracle_mod, grid, zero_init):
+def test_poisson_pcg(gpu, oracle_mod, grid, zero_init, pcg_variant):
     rng = np.random.default_rng(10)
     prm = two_phase_params()
     o = oracle_mod.Oracle(grid, prm)
@@ -237,7 +245,7 @@ def test_poisson_pcg(gpu, oracle_mod, grid, zero_init):
     exact(pg, po)
 
 
-def test_pcd_precond(gpu, oracle_mod, grid):
+def test_pcd_precond(gpu, oracle_mod, grid, pcg_variant):
     rng = np.random.default_rng(11)
     prm = two_phase_params()
     o = oracle_mod.Oracle(grid, prm)
