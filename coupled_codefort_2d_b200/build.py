@@ -35,15 +35,32 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not _stale():
-        return LIB
-    nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-o", LIB]
-    cmd += [os.path.join(CSRC, f) for f in SOURCES]
+DRIVER = os.path.join(HERE, "fugu2d")
+DRIVER_SRC = os.path.join(CSRC, "fugu2d_main.cpp")
+
+
+def build_driver(verbose: bool = False) -> str:
+    """The fugu2d driver (input.nml -> time loop) linked against the library."""
+    cxx = os.environ.get("CXX", "g++")
+    cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), DRIVER_SRC, "-o", DRIVER,
+           "-L", HERE, "-lfugu_gpu", "-Wl,-rpath,$ORIGIN"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
+    return DRIVER
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if force or _stale():
+        nvcc = os.environ.get("NVCC", "nvcc")
+        cmd = [nvcc, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-o", LIB]
+        cmd += [os.path.join(CSRC, f) for f in SOURCES]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    if force or not os.path.exists(DRIVER) or os.path.getmtime(DRIVER) < max(os.path.getmtime(LIB),
+                                                                             os.path.getmtime(DRIVER_SRC)):
+        build_driver(verbose)
     return LIB
 
 
