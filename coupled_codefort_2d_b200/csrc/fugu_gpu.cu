@@ -131,6 +131,9 @@ struct fugu_ctx {
   int pcg_grid = 0;
   int svof_grid = 0;
   int dot_grid = 0;
+  // limits for concurrent use (a batch lowers them so many cases fit at once)
+  int max_cluster = 16;  // CTAs of the cluster-resident PCG
+  int max_coop = 1 << 30;  // CTAs of a grid-wide cooperative kernel
   // cluster-resident PCG plan per precision (index 0 FP64, 1 FP32)
   struct ClusterPlan {
     bool ok = false;
@@ -354,12 +357,13 @@ void plan_pcg_cluster(fugu_ctx* c, fugu_ctx::ClusterPlan& pl) {
   const char* env = std::getenv("FUGU_PCG");
   if (env && std::strcmp(env, "grid") == 0) return;
   const int nx = c->prm.nx, ny = c->prm.ny;
-  const int cmax = ny < 16 ? ny : 16;
+  const int cmax = ny < c->max_cluster ? ny : c->max_cluster;
   const int rows_per = (ny + cmax - 1) / cmax;
   const int C = (ny + rows_per - 1) / rows_per;
-  const long cells = (long)nx * rows_per;
+  // every thread owns one column and a strip of cpt rows: nx * strips <= TPB
+  if (nx > PCGC_TPB) return;
   int cpt = 1;
-  while ((long)cpt * PCGC_TPB < cells) cpt *= 2;
+  while ((long)nx * ((rows_per + cpt - 1) / cpt) > PCGC_TPB) cpt *= 2;
   const int cpt_max = sizeof(T) == 8 ? 8 : 16;
   const size_t smem = sizeof(T) * (size_t)pcgc_smem_elems(nx, rows_per);
   const size_t smem_cap = 227 * 1024 - 1024;  // minus the kernel's static shared memory
@@ -960,12 +964,13 @@ int check_params(const fugu_params* p) {
   return FUGU_OK;
 }
 
-int coop_grid(const void* fn, int tpb, int nsm, long work) {
+int coop_grid(const void* fn, int tpb, int nsm, long work, int max_ctas) {
   int occ = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, tpb, 0) != cudaSuccess || occ < 1) return 0;
   long want = (work + tpb - 1) / tpb;
   long cap = (long)nsm * occ;
   if (cap > nsm) cap = nsm;  // one CTA per SM keeps the barrier short
+  if (cap > max_ctas) cap = max_ctas;
   if (want < 1) want = 1;
   return (int)(want < cap ? want : cap);
 }
@@ -999,14 +1004,14 @@ void create(fugu_ctx* c) {
   p.cx = dalloc<double>(c, c->n); p.cy = dalloc<double>(c, c->n); p.dinv = dalloc<double>(c, c->n);
   p.r = dalloc<double>(c, c->n); p.z = dalloc<double>(c, c->n); p.pb0 = dalloc<double>(c, c->n);
   p.pb1 = dalloc<double>(c, c->n); p.ap = dalloc<double>(c, c->n);
-  for (auto& sp : c->scratch) sp = dalloc<double>(c, 3 * c->n);
+  // routine-level scratch (c->scratch) is allocated on first use
   c->sc = dalloc<double>(c, NSLOTS);
   c->ks = dalloc<KState>(c, 1);
   const long ncell = (long)c->prm.nx * c->prm.ny;
-  c->pcg_grid = coop_grid((const void*)k_pcg<double>, PCG_TPB, c->nsm, ncell);
-  int g32 = coop_grid((const void*)k_pcg<float>, PCG_TPB, c->nsm, ncell);
+  c->pcg_grid = coop_grid((const void*)k_pcg<double>, PCG_TPB, c->nsm, ncell, c->max_coop);
+  int g32 = coop_grid((const void*)k_pcg<float>, PCG_TPB, c->nsm, ncell, c->max_coop);
   if (g32 < c->pcg_grid) c->pcg_grid = g32;
-  c->svof_grid = coop_grid((const void*)k_svof, PCG_TPB, c->nsm, ncell);
+  c->svof_grid = coop_grid((const void*)k_svof, PCG_TPB, c->nsm, ncell, c->max_coop);
   if (c->pcg_grid < 1 || c->svof_grid < 1) throw ApiError{FUGU_ECUDA, "no co-resident grid for persistent kernels"};
   plan_pcg_cluster<double>(c, c->pcgc[0]);
   plan_pcg_cluster<float>(c, c->pcgc[1]);
@@ -1064,10 +1069,13 @@ int guard(fugu_ctx* c, F fn) {
 }
 
 // routine-level helpers: scratch buffer k (single component) / triple view
-double* S(fugu_ctx* c, int k) { return c->scratch[k]; }
+double* S(fugu_ctx* c, int k) {
+  if (!c->scratch[k]) c->scratch[k] = dalloc<double>(c, 3 * c->n);
+  return c->scratch[k];
+}
 Trip<double> ST(fugu_ctx* c, int k) {
   Trip<double> t;
-  t.base = c->scratch[k];
+  t.base = S(c, k);
   t.u = t.base;
   t.v = t.base + c->n;
   t.p = t.base + 2 * c->n;

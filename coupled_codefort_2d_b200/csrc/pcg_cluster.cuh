@@ -6,21 +6,26 @@
 // barrier per reduction (~2.5-3 us on a B200 at 16-148 CTAs).  A cluster of
 // up to 16 CTAs synchronises with the hardware cluster barrier and reduces
 // through distributed shared memory (~0.4 us per barrier), so whenever a
-// case fits, the whole solve lives in the cluster's shared memory:
+// case fits, the whole solve lives in the cluster:
 //
-//   CTA r owns cell rows [j0, j0+R) of all nx columns.  Shared memory holds z
-//   and two p buffers with one halo row above and below, the face
-//   coefficients cx (rows x (nx+1)), cy ((rows+1) x nx) and dinv; phi, r and
-//   A p of the CTA's cells live in registers (CPT cells per thread).
-//   After every update a CTA pushes its first and last rows of z and p into
-//   the halo rows of its neighbours' shared memory (st.shared::cluster via
-//   mapped pointers; periodic y wraps rank 0 <-> rank C-1).
+//   CTA r owns cell rows [j0, j0+R).  Thread t owns column i = t % nx + 1 and
+//   a contiguous strip of CPT rows; its cells' phi, r, z, p and A p live in
+//   registers.  Shared memory holds p_k of the CTA (for the east/west and
+//   strip-end neighbours), the face coefficients cx (rows x (nx+1)),
+//   cy ((rows+1) x nx) and dinv, and four halo rows: z and p of the row just
+//   above and just below the CTA, pushed there by the neighbouring CTAs
+//   (st.shared::cluster through mapped pointers; periodic y wraps rank 0 and
+//   rank C-1).  p_k = z + beta p_{k-1} is formed once per cell; at a CTA
+//   boundary it is formed from the halo z and p, which gives the same bits as
+//   the owner's value.
 //
-// Arithmetic is identical to k_pcg and the oracle (same expressions, same
-// error-free DD reductions, merged in rank order), so results are bit-exact.
-// There is no software spin-wait: every wait is a hardware cluster barrier,
-// and every CTA executes the same sequence of barriers because all branch
-// decisions use cluster-reduced values.
+// Arithmetic and reductions of the FP64 instantiation are those of k_pcg
+// and the oracle (error-free DD sums merged in rank order), so results are
+// bit-exact.  The FP32 instantiation (mixed-precision inner solve) sums its
+// exact float products in double in a fixed order.  There is no software
+// spin-wait: every wait is a hardware cluster barrier, and all CTAs execute
+// the same sequence of barriers because every branch uses cluster-reduced
+// values.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -52,8 +57,19 @@ struct PcgClusterArgs {
 
 // shared-memory footprint in elements of T for rows_per rows of nx cells
 __host__ __device__ inline long pcgc_smem_elems(int nx, int rows_per) {
-  return 3L * (rows_per + 2) * nx + (long)rows_per * (nx + 1) + (long)(rows_per + 1) * nx + (long)rows_per * nx;
+  return (long)rows_per * nx + 4L * nx + (long)rows_per * (nx + 1) + (long)(rows_per + 1) * nx + (long)rows_per * nx;
 }
+
+// reduction accumulator: error-free DD for the FP64 parity path, plain
+// double (exact float products, fixed order) for the FP32 inner solve
+template <typename T>
+struct RAcc {
+  DD v{0.0, 0.0};
+  __device__ __forceinline__ void add(double x) {
+    if constexpr (sizeof(T) == 8) dd_add(v, x);
+    else v.hi += x;
+  }
+};
 
 template <typename T, int CPT>
 __global__ void __launch_bounds__(PCGC_TPB, 1) k_pcg_cluster(PcgClusterArgs<T> a) {
@@ -66,77 +82,173 @@ __global__ void __launch_bounds__(PCGC_TPB, 1) k_pcg_cluster(PcgClusterArgs<T> a
   const int j0 = 1 + rank * rp;
   const int R = min(rp, ny - rank * rp);  // rows of this CTA (>= 1)
   const bool closed = !g.px && !g.py;
+  const int S = (R + CPT - 1) / CPT;       // strips per column
+  const int t = threadIdx.x;
+  const bool act = t < nx * S;
+  const int i = act ? t % nx + 1 : 1;
+  const int lr0 = act ? (t / nx) * CPT : 0;
+  const int nr = act ? min(CPT, R - lr0) : 0;
+  const int ie = (i < nx) ? i + 1 : (g.px ? 1 : nx);
+  const int iw = (i > 1) ? i - 1 : (g.px ? nx : 1);
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* zs = reinterpret_cast<T*>(smem_raw);
-  T* ps0 = zs + (rp + 2) * nx;
-  T* ps1 = ps0 + (rp + 2) * nx;
-  T* cxs = ps1 + (rp + 2) * nx;
+  T* pcs = reinterpret_cast<T*>(smem_raw);  // p_k of the CTA's cells, rp x nx
+  T* zt = pcs + rp * nx;                     // z of the row above the CTA
+  T* zb = zt + nx;                           // z of the row below
+  T* pt = zb + nx;                           // p of the row above
+  T* pb = pt + nx;                           // p of the row below
+  T* cxs = pb + nx;
   T* cys = cxs + rp * (nx + 1);
   T* dis = cys + (rp + 1) * nx;
   __shared__ DD sh[32];
   __shared__ DD red[6];  // 0 pAp, 1 rr, 2 rz, 3 sum / mean, 4 rhs norm, 5 initial rz
 
-  auto zi = [&](int lr, int i) { return (lr + 1) * nx + (i - 1); };  // lr in [-1, R]
-
-  // cluster sum of one DD per thread: block sum -> own slot -> barrier ->
-  // every CTA merges the C slots in rank order (identical everywhere)
-  auto csum = [&](DD v, int slot) -> double {
-    v = block_sum_dd(v, sh);
+  // cluster sum: block sum -> own slot -> barrier -> every CTA merges the C
+  // slots in rank order (identical everywhere)
+  auto bsum = [&](RAcc<T> acc) -> DD {
+    if constexpr (sizeof(T) == 8) {
+      return block_sum_dd(acc.v, sh);
+    } else {
+      DD r;
+      r.hi = block_sum(acc.v.hi, reinterpret_cast<double*>(sh));
+      r.lo = 0.0;
+      return r;
+    }
+  };
+  // two block sums in one interleaved pass (results into slots da, db)
+  __shared__ DD sh2[32];
+  auto bsum2 = [&](RAcc<T> a1, RAcc<T> a2, DD& da, DD& db) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    DD v = a1.v, u = a2.v;
+    if constexpr (sizeof(T) == 8) {
+      for (int o = 16; o > 0; o >>= 1) {
+        v = dd_merge(v, dd_shfl_down(v, o));
+        u = dd_merge(u, dd_shfl_down(u, o));
+      }
+    } else {
+      for (int o = 16; o > 0; o >>= 1) {
+        v.hi += __shfl_down_sync(0xffffffffu, v.hi, o);
+        u.hi += __shfl_down_sync(0xffffffffu, u.hi, o);
+      }
+    }
+    __syncthreads();
+    if (l == 0) {
+      sh[w] = v;
+      sh2[w] = u;
+    }
+    __syncthreads();
+    if (w == 0) {
+      v = l < nw ? sh[l] : DD{0.0, 0.0};
+      u = l < nw ? sh2[l] : DD{0.0, 0.0};
+      if constexpr (sizeof(T) == 8) {
+        for (int o = 16; o > 0; o >>= 1) {
+          v = dd_merge(v, dd_shfl_down(v, o));
+          u = dd_merge(u, dd_shfl_down(u, o));
+        }
+      } else {
+        for (int o = 16; o > 0; o >>= 1) {
+          v.hi += __shfl_down_sync(0xffffffffu, v.hi, o);
+          u.hi += __shfl_down_sync(0xffffffffu, u.hi, o);
+        }
+      }
+      if (l == 0) {
+        da = v;
+        db = u;
+      }
+    }
+  };
+  // merge the C slots after a cluster barrier: lane r of warp 0 loads rank
+  // r's slot (one DSMEM round trip for all ranks), a fixed shuffle tree sums
+  // them, and the result is broadcast through shared memory.  Two slots can
+  // be merged in the same pass (slot2 < 0: one).
+  __shared__ double bcast[2];
+  auto merge2 = [&](int slot, int slot2) {
+    if (threadIdx.x < 32) {
+      const int l = threadIdx.x;
+      DD v{0.0, 0.0}, w{0.0, 0.0};
+      if (l < C) {
+        v = *cl.map_shared_rank(&red[slot], l);
+        if (slot2 >= 0) w = *cl.map_shared_rank(&red[slot2], l);
+      }
+      if constexpr (sizeof(T) == 8) {
+        for (int o = 16; o > 0; o >>= 1) {
+          v = dd_merge(v, dd_shfl_down(v, o));
+          if (slot2 >= 0) w = dd_merge(w, dd_shfl_down(w, o));
+        }
+        if (l == 0) {
+          bcast[0] = v.hi + v.lo;
+          bcast[1] = w.hi + w.lo;
+        }
+      } else {
+        double a0 = v.hi, a1 = w.hi;
+        for (int o = 16; o > 0; o >>= 1) {
+          a0 += __shfl_down_sync(0xffffffffu, a0, o);
+          a1 += __shfl_down_sync(0xffffffffu, a1, o);
+        }
+        if (l == 0) {
+          bcast[0] = a0;
+          bcast[1] = a1;
+        }
+      }
+    }
+    __syncthreads();
+  };
+  auto csum = [&](RAcc<T> acc, int slot) -> double {
+    const DD v = bsum(acc);
     if (threadIdx.x == 0) red[slot] = v;
     cl.sync();
-    DD t{0.0, 0.0};
-    for (int r = 0; r < C; ++r) t = dd_merge(t, *cl.map_shared_rank(&red[slot], r));
-    return t.hi + t.lo;
+    merge2(slot, -1);
+    return bcast[0];
   };
-  // push first / last own row of buf (z or a p buffer) into the neighbours' halos
-  auto push_halos = [&](T* buf) {
-    if (rank > 0 || g.py) {
+  // owners of the CTA's first / last row publish z and p into the halo rows
+  // of the neighbouring CTAs (the row above CTA r-1 is my first row, the row
+  // below CTA r+1 is my last row)
+  auto push = [&](int c, T zv, T pv) {
+    const int lr = lr0 + c;
+    if (lr == 0 && (rank > 0 || g.py)) {
       const int dst = (rank - 1 + C) % C;
-      const int Rd = min(rp, ny - dst * rp);
-      T* rem = cl.map_shared_rank(buf, dst);
-      for (int i = 1 + threadIdx.x; i <= nx; i += blockDim.x) rem[(Rd + 1) * nx + (i - 1)] = buf[zi(0, i)];
+      cl.map_shared_rank(zt, dst)[i - 1] = zv;
+      cl.map_shared_rank(pt, dst)[i - 1] = pv;
     }
-    if (rank < C - 1 || g.py) {
+    if (lr == R - 1 && (rank < C - 1 || g.py)) {
       const int dst = (rank + 1) % C;
-      T* rem = cl.map_shared_rank(buf, dst);
-      for (int i = 1 + threadIdx.x; i <= nx; i += blockDim.x) rem[i - 1] = buf[zi(R - 1, i)];
+      cl.map_shared_rank(zb, dst)[i - 1] = zv;
+      cl.map_shared_rank(pb, dst)[i - 1] = pv;
     }
   };
 
-  // ---- load coefficients of the own rows
+  // ---- coefficients of the own rows
   for (int q = threadIdx.x; q < R * (nx + 1); q += blockDim.x) {
-    const int lr = q / (nx + 1), i = q % (nx + 1);
-    cxs[lr * (nx + 1) + i] = a.cx[g.at(i, j0 + lr)];
+    const int lr = q / (nx + 1), ii = q % (nx + 1);
+    cxs[lr * (nx + 1) + ii] = a.cx[g.at(ii, j0 + lr)];
   }
   for (int q = threadIdx.x; q < (R + 1) * nx; q += blockDim.x) {
-    const int lf = q / nx - 1, i = q % nx + 1;  // face rows j0-1 .. j0+R-1
-    cys[(lf + 1) * nx + (i - 1)] = a.cy[g.at(i, j0 + lf)];
+    const int lf = q / nx - 1, ii = q % nx + 1;  // face rows j0-1 .. j0+R-1
+    cys[(lf + 1) * nx + (ii - 1)] = a.cy[g.at(ii, j0 + lf)];
   }
   for (int q = threadIdx.x; q < R * nx; q += blockDim.x) dis[q] = a.dinv[g.at(q % nx + 1, j0 + q / nx)];
 
-  T phi_r[CPT], r_r[CPT], ap_r[CPT], p_r[CPT];
-  const int ncell = R * nx;
+  T phi_r[CPT], r_r[CPT], z_r[CPT], p_r[CPT], ap_r[CPT];
 #define PCGC_CELLS _Pragma("unroll") for (int c = 0; c < CPT; ++c)
-#define PCGC_CELL                                        \
-  const int q = threadIdx.x + c * PCGC_TPB;              \
-  if (q >= ncell) continue;                              \
-  const int lr = q / nx, i = q % nx + 1, j = j0 + lr;    \
+#define PCGC_CELL             \
+  if (c >= nr) continue;      \
+  const int lr = lr0 + c;     \
+  const int j = j0 + lr;      \
   (void)j;
 
   // ---- (b) zero-mean projection and rhs norm
   double mean = 0.0;
   if (closed) {
-    DD s{0.0, 0.0};
-    PCGC_CELLS { PCGC_CELL dd_add(s, double(a.rhs[g.at(i, j)])); }
+    RAcc<T> s;
+    PCGC_CELLS { PCGC_CELL s.add(double(a.rhs[g.at(i, j)])); }
     mean = csum(s, 3) / (double)(nx * ny);
   }
-  DD ss{0.0, 0.0};
+  RAcc<T> ss;
   PCGC_CELLS {
     PCGC_CELL
     const T rw = closed ? T(double(a.rhs[g.at(i, j)]) - mean) : a.rhs[g.at(i, j)];
     r_r[c] = rw;
-    dd_add(ss, double(rw) * double(rw));
+    ss.add(double(rw) * double(rw));
   }
   const double rhs_norm = sqrt(csum(ss, 4));
   if (rhs_norm < 1.0e-14) {
@@ -151,7 +263,7 @@ __global__ void __launch_bounds__(PCGC_TPB, 1) k_pcg_cluster(PcgClusterArgs<T> a
     return;
   }
 
-  // ---- (c) phi ghosts (halo + Neumann), initial residual, z, p = z
+  // ---- (c) phi ghosts (halo + Neumann), initial residual, z, p_1 = z
   if (!a.phi_zero) {
     const long tot = g.n();
     for (long q = rank * (long)blockDim.x + threadIdx.x; q < tot; q += (long)C * blockDim.x) {
@@ -163,7 +275,8 @@ __global__ void __launch_bounds__(PCGC_TPB, 1) k_pcg_cluster(PcgClusterArgs<T> a
       a.phi[q] = a.phi[g.at(mi, mj)];
     }
   }
-  DD rz{0.0, 0.0};
+  __syncthreads();  // coefficients in shared memory
+  RAcc<T> rz;
   PCGC_CELLS {
     PCGC_CELL
     T rr = r_r[c];
@@ -177,91 +290,74 @@ __global__ void __launch_bounds__(PCGC_TPB, 1) k_pcg_cluster(PcgClusterArgs<T> a
     const T zz = dis[lr * nx + (i - 1)] * rr;
     phi_r[c] = ph;
     r_r[c] = rr;
-    zs[zi(lr, i)] = zz;
-    ps1[zi(lr, i)] = zz;  // p_1 = z lives in ps1 (odd iterations)
-    dd_add(rz, double(rr) * double(zz));
+    z_r[c] = zz;
+    p_r[c] = zz;
+    push(c, zz, zz);
+    rz.add(double(rr) * double(zz));
   }
-  __syncthreads();
-  push_halos(zs);
-  push_halos(ps1);
   double rz_old = csum(rz, 5);  // its barrier also publishes the halos
-
-  // stencil at own cell (lr, i) on a field given by accessor f(lr', i')
-  auto stencil = [&](int lr, int i, int j, auto f) -> T {
-    const T cE = cxs[lr * (nx + 1) + i], cW = cxs[lr * (nx + 1) + i - 1];
-    const T cN = cys[(lr + 1) * nx + (i - 1)], cS = cys[lr * nx + (i - 1)];
-    const int ie = (i < nx) ? i + 1 : (g.px ? 1 : nx);
-    const int iw = (i > 1) ? i - 1 : (g.px ? nx : 1);
-    const int ln = (j == ny && !g.py) ? lr : lr + 1;
-    const int ls = (j == 1 && !g.py) ? lr : lr - 1;
-    return (cE + cW + cN + cS) * f(lr, i) - (cE * f(lr, ie) + cW * f(lr, iw) + cN * f(ln, i) + cS * f(ls, i));
-  };
 
   double res_norm = 0.0, beta = 0.0;
   int iter;
   for (iter = 1; iter <= a.max_iter; ++iter) {
-    T* pcur = (iter & 1) ? ps1 : ps0;
-    const T* pprev = (iter & 1) ? ps0 : ps1;
     const T tb = T(beta);
-    // phase A: p_k (on the fly) and A p_k
-    DD papd{0.0, 0.0};
+    // phase A: p_k of the own cells, then A p_k
     PCGC_CELLS {
       PCGC_CELL
-      T apv, pown;
-      if (iter == 1) {
-        pown = ps1[zi(lr, i)];
-        apv = stencil(lr, i, j, [&](int l2, int i2) { return ps1[zi(l2, i2)]; });
-      } else {
-        auto pf = [&](int l2, int i2) {
-          const int e = zi(l2, i2);
-          return zs[e] + tb * pprev[e];
-        };
-        pown = pf(lr, i);
-        apv = stencil(lr, i, j, pf);
-      }
-      p_r[c] = pown;
-      ap_r[c] = apv;
-      dd_add(papd, double(pown) * double(apv));
+      const T pk = (iter == 1) ? z_r[c] : z_r[c] + tb * p_r[c];
+      p_r[c] = pk;
+      pcs[lr * nx + (i - 1)] = pk;
     }
-    const double pap = csum(papd, 0);  // barrier: every CTA is done reading z / pprev
+    __syncthreads();
+    RAcc<T> papd;
+    PCGC_CELLS {
+      PCGC_CELL
+      const T pk = p_r[c];
+      const T cE = cxs[lr * (nx + 1) + i], cW = cxs[lr * (nx + 1) + i - 1];
+      const T cN = cys[(lr + 1) * nx + (i - 1)], cS = cys[lr * nx + (i - 1)];
+      const T pE = pcs[lr * nx + (ie - 1)], pW = pcs[lr * nx + (iw - 1)];
+      T pN, pS;
+      if (j == ny && !g.py) pN = pk;
+      else if (c + 1 < nr) pN = p_r[c + 1];
+      else if (lr + 1 < R) pN = pcs[(lr + 1) * nx + (i - 1)];
+      else pN = (iter == 1) ? zt[i - 1] : zt[i - 1] + tb * pt[i - 1];
+      if (j == 1 && !g.py) pS = pk;
+      else if (c > 0) pS = p_r[c - 1];
+      else if (lr > 0) pS = pcs[(lr - 1) * nx + (i - 1)];
+      else pS = (iter == 1) ? zb[i - 1] : zb[i - 1] + tb * pb[i - 1];
+      const T apv = (cE + cW + cN + cS) * pk - (cE * pE + cW * pW + cN * pN + cS * pS);
+      ap_r[c] = apv;
+      papd.add(double(pk) * double(apv));
+    }
+    const double pap = csum(papd, 0);  // barrier: every CTA is done reading pcs / halos
     if (fabs(pap) < 1.0e-30) break;
     const double alpha = rz_old / pap;
     const T ta = T(alpha);
-    // phase B: phi, r, z updates; publish z and p_k rows
-    DD rrd{0.0, 0.0}, rzd{0.0, 0.0};
+    // phase B: phi, r, z updates; publish the boundary rows' z and p_k
+    RAcc<T> rrd, rzd;
     PCGC_CELLS {
       PCGC_CELL
       const T rv = r_r[c] - ta * ap_r[c];
       const T zv = dis[lr * nx + (i - 1)] * rv;
       phi_r[c] = phi_r[c] + ta * p_r[c];
       r_r[c] = rv;
-      zs[zi(lr, i)] = zv;
-      if (iter > 1) pcur[zi(lr, i)] = p_r[c];
-      dd_add(rrd, double(rv) * double(rv));
-      dd_add(rzd, double(rv) * double(zv));
+      z_r[c] = zv;
+      push(c, zv, p_r[c]);
+      rrd.add(double(rv) * double(rv));
+      rzd.add(double(rv) * double(zv));
     }
-    __syncthreads();
-    push_halos(zs);
-    if (iter > 1) push_halos(pcur);
-    rrd = block_sum_dd(rrd, sh);
-    if (threadIdx.x == 0) red[1] = rrd;
-    rzd = block_sum_dd(rzd, sh);
-    if (threadIdx.x == 0) red[2] = rzd;
+    bsum2(rrd, rzd, red[1], red[2]);
     cl.sync();
-    DD trr{0.0, 0.0}, trz{0.0, 0.0};
-    for (int r = 0; r < C; ++r) {
-      trr = dd_merge(trr, *cl.map_shared_rank(&red[1], r));
-      trz = dd_merge(trz, *cl.map_shared_rank(&red[2], r));
-    }
-    res_norm = sqrt(trr.hi + trr.lo);
+    merge2(1, 2);
+    res_norm = sqrt(bcast[0]);
     if (res_norm / rhs_norm < a.tol) break;
-    const double rz_new = trz.hi + trz.lo;
+    const double rz_new = bcast[1];
     beta = rz_new / rz_old;
     rz_old = rz_new;
   }
   if (closed) {
-    DD s{0.0, 0.0};
-    PCGC_CELLS { PCGC_CELL dd_add(s, double(phi_r[c])); }
+    RAcc<T> s;
+    PCGC_CELLS { PCGC_CELL s.add(double(phi_r[c])); }
     const double m = csum(s, 3) / (double)(nx * ny);
     PCGC_CELLS { PCGC_CELL phi_r[c] = T(double(phi_r[c]) - m); }
   }
