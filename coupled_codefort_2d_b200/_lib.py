@@ -116,6 +116,7 @@ SIGNATURES = {
     "fugu_compute_csf_force": (_i, [_vp] * 5),
     "fugu_write_checkpoint": (_i, [_vp, C.c_char_p, _i, _d]),
     "fugu_read_checkpoint": (_i, [_vp, C.c_char_p, _vp, _vp]),
+    "fugu_solve_poisson_pressure_noalloc": (_i, [_vp] * 6 + [_d, _i, _vp, _vp, _vp, _i]),
 }
 
 _lib = None

@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <cstddef>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1660,3 +1661,142 @@ int fugu_read_checkpoint(fugu_ctx* c, const char* path, int* step_no, double* t)
 }
 
 }  // extern "C"
+
+// ============================================== allocation-free Poisson solve
+//
+// fugu_solve_poisson_pressure_noalloc runs solve_poisson_pressure
+// (mod_subsolvers.f90:32-246) with the grid-wide PCG kernel k_pcg<double>,
+// but every byte of its working memory comes from na_scratch, one file-scope
+// device array, instead of from a context.  The call allocates nothing: no
+// cudaMalloc, cudaFree, cudaMallocHost or library routine that allocates.
+//
+// na_scratch layout (offsets in doubles, every region 256-byte aligned):
+//   [0, 32)               GridSync at 0, PcgOut at 16
+//   [32, 32 + 12*256)     CTA partial sums of k_pcg (12 per CTA, <= 256 CTAs)
+//   [NA_FIELD0, ...)      12 fields of NA_MAX_POINTS each in the padded
+//                         device layout: phi, rhs, rho_u, rho_v, cx, cy,
+//                         dinv, r, z, pb0, pb1, ap
+namespace {
+
+constexpr long NA_MAX_POINTS = FUGU_NOALLOC_MAX_POINTS;  // padded points per field
+constexpr int NA_MAX_CTAS = 256;
+constexpr long NA_PART = 32;
+constexpr long NA_FIELD0 = NA_PART + 12L * NA_MAX_CTAS;
+constexpr int NA_NFIELDS = 12;
+constexpr long NA_TOTAL = NA_FIELD0 + NA_NFIELDS * NA_MAX_POINTS;
+constexpr int NA_MAX_DEVICES = 64;
+static_assert((NA_FIELD0 * sizeof(double)) % 256 == 0, "field region alignment");
+static_assert((NA_MAX_POINTS * sizeof(double)) % 256 == 0, "field stride alignment");
+static_assert(sizeof(GridSync) <= 16 * sizeof(double) && sizeof(PcgOut) <= 16 * sizeof(double), "header");
+
+static __device__ __align__(256) double na_scratch[NA_TOTAL];
+
+// per-device set-up, done by the first call with that device current
+struct NaDevice {
+  bool ready = false;
+  double* base = nullptr;  // device address of na_scratch in this device's context
+  int max_ctas = 0;        // co-resident CTAs of k_pcg<double>, one per SM at most
+};
+std::mutex na_mu;
+NaDevice na_dev[NA_MAX_DEVICES];
+
+// message into the caller's buffer (no heap use on any path of the entry)
+int na_fail(char* err, int err_len, int code, const char* what, const char* detail = "") {
+  if (err && err_len > 0) std::snprintf(err, (size_t)err_len, "%s%s", what, detail);
+  return code;
+}
+
+}  // namespace
+
+extern "C" int fugu_solve_poisson_pressure_noalloc(const fugu_params* p, void* stream, double* phi,
+                                                   const double* rhs, const double* rho_u, const double* rho_v,
+                                                   double tol, int max_iter, int* iter_out, double* res_out,
+                                                   char* err, int err_len) {
+  if (err && err_len > 0) err[0] = '\0';
+  if (check_params(p) != FUGU_OK) return na_fail(err, err_len, FUGU_EINVAL, "invalid fugu_params");
+  if (!phi || !rhs || !rho_u || !rho_v) return na_fail(err, err_len, FUGU_EINVAL, "NULL array argument");
+  if (max_iter < 0) return na_fail(err, err_len, FUGU_EINVAL, "max_iter < 0");
+  const Geo g = make_geo(*p);
+  if (g.n() > NA_MAX_POINTS) {
+    char m[256];
+    std::snprintf(m, sizeof m,
+                  "grid %d x %d needs %ld padded points per field; the allocation-free solve holds at most "
+                  "%ld (round_up(nx+5,16)*(ny+5); every grid up to 256 x 256 fits)",
+                  p->nx, p->ny, g.n(), NA_MAX_POINTS);
+    return na_fail(err, err_len, FUGU_EINVAL, m);
+  }
+  int dev = -1;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return na_fail(err, err_len, FUGU_ECUDA, "cudaGetDevice: ", cudaGetErrorString(e));
+  if (dev < 0 || dev >= NA_MAX_DEVICES) return na_fail(err, err_len, FUGU_EINVAL, "device ordinal out of range");
+  NaDevice d;
+  {
+    std::lock_guard<std::mutex> lk(na_mu);
+    NaDevice& nd = na_dev[dev];
+    if (!nd.ready) {
+      double* ptr = nullptr;
+      e = cudaGetSymbolAddress((void**)&ptr, na_scratch);
+      if (e != cudaSuccess)
+        return na_fail(err, err_len, FUGU_ECUDA, "cudaGetSymbolAddress: ", cudaGetErrorString(e));
+      int nsm = 0, occ = 0;
+      e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_pcg<double>, PCG_TPB, 0);
+      if (e != cudaSuccess || nsm < 1 || occ < 1)
+        return na_fail(err, err_len, FUGU_ECUDA, "no co-resident grid for the PCG kernel on this device");
+      nd.base = ptr;
+      nd.max_ctas = nsm < NA_MAX_CTAS ? nsm : NA_MAX_CTAS;
+      nd.ready = true;
+    }
+    d = nd;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const long n = g.n();
+  GridSync* gs = (GridSync*)d.base;
+  PcgOut* out = (PcgOut*)(d.base + 16);
+  double* part = d.base + NA_PART;
+  double* f[NA_NFIELDS];
+  for (int k = 0; k < NA_NFIELDS; ++k) f[k] = d.base + NA_FIELD0 + k * NA_MAX_POINTS;
+  // caller's array (reference layout, host or device memory) <-> padded field
+  auto copy = [&](double* dst_f, const double* src, double* dst, const double* src_f, int kind) {
+    int i0, i1, j0, j1;
+    g.extent(kind, i0, i1, j0, j1);
+    const size_t w = (size_t)(i1 - i0 + 1), h = (size_t)(j1 - j0 + 1);
+    if (dst_f)
+      return cudaMemcpy2DAsync(dst_f + g.at(i0, j0), sizeof(double) * g.P, src, sizeof(double) * w,
+                               sizeof(double) * w, h, cudaMemcpyDefault, s);
+    return cudaMemcpy2DAsync(dst, sizeof(double) * w, src_f + g.at(i0, j0), sizeof(double) * g.P,
+                             sizeof(double) * w, h, cudaMemcpyDefault, s);
+  };
+  // the barrier counters, the result record and every field start at zero
+  e = cudaMemsetAsync(d.base, 0, sizeof(double) * (size_t)(NA_FIELD0 + (NA_NFIELDS - 1) * NA_MAX_POINTS + n), s);
+  if (e == cudaSuccess) e = copy(f[0], phi, nullptr, nullptr, K_CELL);
+  if (e == cudaSuccess) e = copy(f[1], rhs, nullptr, nullptr, K_CELL);
+  if (e == cudaSuccess) e = copy(f[2], rho_u, nullptr, nullptr, K_U);
+  if (e == cudaSuccess) e = copy(f[3], rho_v, nullptr, nullptr, K_V);
+  if (e != cudaSuccess) return na_fail(err, err_len, FUGU_ECUDA, "copy in: ", cudaGetErrorString(e));
+  Box b = box_launch(g);
+  k_poisson_coefs<double><<<b.grid, b.block, 0, s>>>(g, f[2], f[3], f[4], f[5], f[6]);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return na_fail(err, err_len, FUGU_ECUDA, "k_poisson_coefs: ", cudaGetErrorString(e));
+  PcgArgs<double> a;
+  a.g = g;
+  a.rhs = f[1]; a.cx = f[4]; a.cy = f[5]; a.dinv = f[6];
+  a.phi = f[0]; a.r = f[7]; a.z = f[8]; a.pb0 = f[9]; a.pb1 = f[10]; a.ap = f[11];
+  a.part = part; a.gs = gs; a.out = out; a.active = nullptr;
+  a.tol = tol; a.max_iter = max_iter; a.phi_zero = 0;
+  long want = ((long)p->nx * p->ny + PCG_TPB - 1) / PCG_TPB;
+  const int grid = (int)(want < d.max_ctas ? (want < 1 ? 1 : want) : d.max_ctas);
+  void* args[] = {&a};
+  e = cudaLaunchCooperativeKernel((void*)k_pcg<double>, dim3(grid), dim3(PCG_TPB), args, 0, s);
+  if (e != cudaSuccess) return na_fail(err, err_len, FUGU_ECUDA, "k_pcg: ", cudaGetErrorString(e));
+  e = copy(nullptr, nullptr, phi, f[0], K_CELL);
+  PcgOut h{};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, out, sizeof(PcgOut), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return na_fail(err, err_len, FUGU_ECUDA, "copy out: ", cudaGetErrorString(e));
+  if (h.status != 0) return na_fail(err, err_len, FUGU_ETIMEOUT, "k_pcg: a grid barrier wait gave up");
+  if (iter_out) *iter_out = h.iters;
+  if (res_out) *res_out = h.res;
+  return FUGU_OK;
+}

@@ -268,6 +268,45 @@ int fugu_compute_csf_force(fugu_ctx* ctx, const double* c_raw, const double* kap
 int fugu_write_checkpoint(fugu_ctx* ctx, const char* path, int step, double t);
 int fugu_read_checkpoint(fugu_ctx* ctx, const char* path, int* step, double* t);
 
+/* ------------------------------------------------ allocation-free entry
+ * solve_poisson_pressure (mod_subsolvers.f90:32-246) with no context and no
+ * allocation.  No counterpart in the reference, whose subroutine works on
+ * arrays its caller already owns.  It serves callers that cannot call
+ * cudaMalloc:
+ *   - a host code whose own pool allocator already holds the device memory,
+ *     where a cudaMalloc would fail or fragment that pool;
+ *   - a time loop that cannot take the device-wide synchronisation that
+ *     cudaFree implies.
+ * Its working memory is one static device array of about 7.1 MB, present
+ * on each device once the library's device code is loaded there.  The call
+ * makes no cudaMalloc, cudaFree, cudaMallocHost or other allocating call.
+ *
+ * phi (in: initial guess; out: solution, ghosts as the reference), rhs,
+ * rho_u and rho_v are reference-layout arrays (see the top of this file) in
+ * host or device memory.  stream is a cudaStream_t (NULL: the default
+ * stream).  The call returns once the stream has finished the solve.
+ * iter_out and res_out are those of the reference routine (may be NULL).
+ * A message goes to err (err_len bytes, may be NULL) when the call fails.
+ *
+ * Limit: round_up(nx+5, 16) * (ny+5) <= FUGU_NOALLOC_MAX_POINTS padded
+ * points per field, which every grid up to 256 x 256 cells meets.  Larger
+ * grids are rejected with FUGU_EINVAL.
+ * Set-up: the first call on a device, with that device current, takes the
+ * static array's device address (cudaGetSymbolAddress) and queries the
+ * device.  Make that first call before any stream capture.
+ * Zero state: the grid-barrier counters, the result record and the fields
+ * must start at zero.  Every call clears them on `stream` before its
+ * kernels run.
+ * Concurrency: all calls on one device share the one static array.  Two
+ * calls in flight at the same time on one device (from two host threads)
+ * race, and both results are undefined.  Calls on different devices are
+ * independent. */
+#define FUGU_NOALLOC_MAX_POINTS 73728
+int fugu_solve_poisson_pressure_noalloc(const fugu_params* p, void* stream, double* phi,
+                                        const double* rhs, const double* rho_u, const double* rho_v,
+                                        double tol, int max_iter, int* iter_out, double* res_out,
+                                        char* err, int err_len);
+
 #ifdef __cplusplus
 }
 #endif
