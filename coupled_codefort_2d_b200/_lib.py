@@ -117,7 +117,17 @@ SIGNATURES = {
     "fugu_write_checkpoint": (_i, [_vp, C.c_char_p, _i, _d]),
     "fugu_read_checkpoint": (_i, [_vp, C.c_char_p, _vp, _vp]),
     "fugu_solve_poisson_pressure_noalloc": (_i, [_vp] * 6 + [_d, _i, _vp, _vp, _vp, _i]),
+    "fugu_batch_create": (_i, [_vp, _i, _i, _vp, _vp]),
+    "fugu_batch_destroy": (None, [_vp]),
+    "fugu_batch_last_error": (C.c_char_p, [_vp]),
+    "fugu_batch_size": (_i, [_vp]),
+    "fugu_batch_case": (_i, [_vp, _i, _vp]),
+    "fugu_batch_run": (_i, [_vp, _i] + [_vp] * 6),
 }
+
+
+class FuguBatchOpts(C.Structure):
+    _fields_ = [("nthreads", C.c_int), ("max_cluster", C.c_int), ("max_coop", C.c_int)]
 
 _lib = None
 

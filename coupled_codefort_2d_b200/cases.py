@@ -142,3 +142,39 @@ def max_divergence(g: Grid, u: np.ndarray, v: np.ndarray) -> float:
     du = (at(u, "u", slice(1, g.nx), slice(1, g.ny)) - at(u, "u", slice(0, g.nx - 1), slice(1, g.ny))) / g.dx
     dv = (at(v, "v", slice(1, g.nx), slice(1, g.ny)) - at(v, "v", slice(1, g.nx), slice(0, g.ny - 1))) / g.dy
     return float(np.max(np.abs(du + dv)))
+
+
+# ------------------------------------------------------- batched ensemble
+ENSEMBLE_GRIDS = ((64, 128), (128, 256), (192, 384), (256, 512))
+ENSEMBLE_SEED = 20261203
+
+
+def bubble_ensemble(ncases: int, seed: int = ENSEMBLE_SEED, grids=ENSEMBLE_GRIDS):
+    """Independent two-phase rising-bubble cases in a 1 x 2 box.
+
+    One draw sequence per case, in case order, from
+    ``numpy.random.default_rng(seed)``: grid uniform over ``grids``; radius
+    ``U[0.15, 0.3] * Lx``; centre ``x = U[0.4, 0.6] * Lx``, ``y = 0.5``;
+    ``rho_out / rho_in`` log-uniform in [10, 1000] with ``rho_out = 1000``;
+    ``mu_out / mu_in`` log-uniform in [10, 100] with ``mu_out = 10``;
+    ``sigma = U[1, 50]``; ``g = 0.98`` downwards.  The bubble is fluid 2
+    (``C = 0``, the reference's ``rising_bubble`` colour, ``main.f90:137-150``),
+    top and bottom walls are no-slip and the side walls free-slip.  Returns
+    dicts with the grid, the physics and the bubble geometry; the solver
+    settings are the caller's.
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(ncases):
+        nx, ny = grids[int(rng.integers(len(grids)))]
+        radius = float(rng.uniform(0.15, 0.3))
+        xc = float(rng.uniform(0.4, 0.6))
+        rho_ratio = float(np.exp(rng.uniform(np.log(10.0), np.log(1000.0))))
+        mu_ratio = float(np.exp(rng.uniform(np.log(10.0), np.log(100.0))))
+        sigma = float(rng.uniform(1.0, 50.0))
+        out.append({
+            "case": k, "grid": Grid(nx, ny, 1.0, 2.0), "radius": radius, "xc": xc, "yc": 0.5,
+            "rho1": 1000.0, "rho2": 1000.0 / rho_ratio, "mu1": 10.0, "mu2": 10.0 / mu_ratio,
+            "sigma": sigma, "gx": 0.0, "gy": -0.98,
+        })
+    return out

@@ -45,10 +45,22 @@ class Context:
             raise FuguError(rc, f"fugu_create failed for {g} (see stderr)")
         self.h = h
 
+    @classmethod
+    def view(cls, handle, g: Grid, prm: Params, precision: int = _lib.FP64) -> "Context":
+        """A non-owning Context over a handle another object owns (a batch case)."""
+        self = cls.__new__(cls)
+        self.L = _lib.lib()
+        self.g, self.prm, self.precision = g, prm, precision
+        self._p = make_params(g, prm, precision)
+        self.h = handle
+        self._owned = False
+        return self
+
     # -------------------------------------------------------------- plumbing
     def close(self):
         if getattr(self, "h", None):
-            self.L.fugu_destroy(self.h)
+            if getattr(self, "_owned", True):
+                self.L.fugu_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -10,13 +10,18 @@
 // then rounds every operation as the CPU oracle does.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstddef>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "fugu_gpu.h"
@@ -135,6 +140,7 @@ struct fugu_ctx {
   // limits for concurrent use (a batch lowers them so many cases fit at once)
   int max_cluster = 16;  // CTAs of the cluster-resident PCG
   int max_coop = 1 << 30;  // CTAs of a grid-wide cooperative kernel
+  bool coop_as_cluster = false;  // launch those as one cluster (max_coop <= 8)
   // cluster-resident PCG plan per precision (index 0 FP64, 1 FP32)
   struct ClusterPlan {
     bool ok = false;
@@ -366,11 +372,22 @@ void plan_pcg_cluster(fugu_ctx* c, fugu_ctx::ClusterPlan& pl) {
   int cpt = 1;
   while ((long)nx * ((rows_per + cpt - 1) / cpt) > PCGC_TPB) cpt *= 2;
   const int cpt_max = sizeof(T) == 8 ? 8 : 16;
-  const size_t smem = sizeof(T) * (size_t)pcgc_smem_elems(nx, rows_per);
-  const size_t smem_cap = 227 * 1024 - 1024;  // minus the kernel's static shared memory
-  if (cpt > cpt_max || smem > smem_cap) return;
+  if (cpt > cpt_max) return;
   const void* fn = pcgc_fn<T>(cpt);
-  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+  // The dynamic shared-memory limit is a property of the kernel, shared by
+  // every context in the process, so it is always raised to the device's
+  // maximum (never to one case's need, which would shrink it for another).
+  int optin = 0;
+  cudaFuncAttributes fa;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->device) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, fn) != cudaSuccess) {
+    cudaGetLastError();
+    return;
+  }
+  const size_t smem = sizeof(T) * (size_t)pcgc_smem_elems(nx, rows_per);
+  const size_t smem_cap = (size_t)optin - fa.sharedSizeBytes;
+  if (smem > smem_cap) return;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap) != cudaSuccess ||
       cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
     cudaGetLastError();
     return;
@@ -387,6 +404,33 @@ void plan_pcg_cluster(fugu_ctx* c, fugu_ctx::ClusterPlan& pl) {
   pl.rows_per = rows_per;
   pl.cpt = cpt;
   pl.smem = smem;
+}
+
+// Launch a persistent kernel whose CTAs wait on one another at grid
+// barriers.  A context alone uses a cooperative launch, which makes all CTAs
+// co-resident.  In a batch, many cases' kernels share the device and two
+// partly resident cooperative grids could each wait for CTAs the other's
+// occupy (until the bounded barrier gives up), so there the grid is launched
+// as one thread-block cluster (at most 8 CTAs), whose CTAs the hardware
+// schedules together or not at all.
+void launch_coop(fugu_ctx* c, const void* fn, int grid, void** args) {
+  if (!c->coop_as_cluster) {
+    CK(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(PCG_TPB), args, 0, c->s));
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(PCG_TPB);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = c->s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = grid;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelExC(&cfg, fn, args));
 }
 
 cudaEvent_t ev_get(fugu_ctx* c) {
@@ -439,7 +483,7 @@ void pcg(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, double tol, int max_i
   } else {
     CK(cudaMemsetAsync(c->gs, 0, sizeof(GridSync), c->s));
     void* args[] = {&a};
-    CK(cudaLaunchCooperativeKernel((void*)k_pcg<T>, dim3(c->pcg_grid), dim3(PCG_TPB), args, 0, c->s));
+    launch_coop(c, (const void*)k_pcg<T>, c->pcg_grid, args);
   }
   ++c->launches;
   if (c->prof) {
@@ -791,7 +835,7 @@ void svof(fugu_ctx* c, const double* craw, double* cs, double* work, double delt
   a.status = c->svof_status;
   CK(cudaMemsetAsync(c->gs, 0, sizeof(GridSync), c->s));
   void* args[] = {&a};
-  CK(cudaLaunchCooperativeKernel((void*)k_svof, dim3(c->svof_grid), dim3(PCG_TPB), args, 0, c->s));
+  launch_coop(c, (const void*)k_svof, c->svof_grid, args);
   ++c->launches;
 }
 
@@ -1658,6 +1702,235 @@ int fugu_read_checkpoint(fugu_ctx* c, const char* path, int* step_no, double* t)
     up(c, c->f[FUGU_F_C_FIELD], b, K_CELL);
     sync(c);
   });
+}
+
+}  // extern "C"
+
+// ================================================================ batched form
+//
+// Many independent cases on one GPU.  Each case is a full context (state,
+// Krylov work space, stream); a pool of host threads steps them, so the
+// device runs as many cases' kernels at once as its SMs hold.  Cases are
+// handed out largest first (longest-processing-time order) from one atomic
+// counter.  The cluster size of each case's PCG comes from a measured
+// autotune: per distinct (grid, boundary, precision), every feasible size is
+// timed on the case's own coefficients and the one with the least SM time
+// per iteration (CTAs x microseconds) wins, because a full GPU is limited by
+// SM time, not by one case's latency.
+struct fugu_batch {
+  int device = 0;
+  int nthreads = 1;
+  std::vector<fugu_ctx*> cases;
+  std::vector<int> order;
+  std::string err;
+};
+
+namespace {
+
+template <typename T>
+PcgWork<T>& pcg_work(fugu_ctx* c);
+template <>
+PcgWork<double>& pcg_work<double>(fugu_ctx* c) { return c->w64.pcg; }
+template <>
+PcgWork<float>& pcg_work<float>(fugu_ctx* c) { return c->w32.pcg; }
+
+// time one PCG launch of `iters` iterations (tol 0: never converges) on the
+// context's current cluster plan; returns microseconds per iteration
+template <typename T>
+double time_pcg_iter(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, int iters) {
+  cudaEvent_t e0 = ev_get(c), e1 = ev_get(c);
+  CK(cudaMemsetAsync(phi, 0, sizeof(T) * c->n, c->s));
+  pcg<T>(c, w, phi, rhs, 0.0, iters, false, nullptr);  // warm-up
+  CK(cudaMemsetAsync(phi, 0, sizeof(T) * c->n, c->s));
+  CK(cudaEventRecord(e0, c->s));
+  pcg<T>(c, w, phi, rhs, 0.0, iters, false, nullptr);
+  CK(cudaEventRecord(e1, c->s));
+  sync(c);
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  c->ev_pool.push_back(e0);
+  c->ev_pool.push_back(e1);
+  return 1e3 * ms / iters;
+}
+
+// Autotune the PCG cluster size of context c for precision T: candidates
+// 2, 4, 8, 16 CTAs (those the planner accepts).  The Poisson coefficients
+// are those of uniform unit density, the right-hand side a smooth mode; the
+// iteration cost does not depend on the values.  Returns the chosen size
+// (0 when no cluster plan fits: the grid-wide kernel is used).
+template <typename T>
+int tune_cluster(fugu_ctx* c) {
+  const int idx = sizeof(T) == 8 ? 0 : 1;
+  PcgWork<T>& w = pcg_work<T>(c);
+  const Geo& g = c->g;
+  // scratch: unit density (double), then phi and rhs of type T
+  std::vector<double> host((size_t)c->n, 1.0);
+  double* ones = S(c, 0);
+  T* phi = (T*)S(c, 1);
+  T* rhs = (T*)S(c, 2);
+  CK(cudaMemcpyAsync(ones, host.data(), sizeof(double) * c->n, cudaMemcpyHostToDevice, c->s));
+  poisson_coefs<T>(c, w, ones, ones);
+  std::vector<T> hr((size_t)c->n, T(0));
+  for (int j = 1; j <= g.ny; ++j)
+    for (int i = 1; i <= g.nx; ++i)
+      hr[(size_t)g.at(i, j)] = T(std::sin(6.283185307179586 * i / g.nx) * std::cos(3.141592653589793 * j / g.ny));
+  CK(cudaMemcpyAsync(rhs, hr.data(), sizeof(T) * c->n, cudaMemcpyHostToDevice, c->s));
+  sync(c);  // the host vectors go out of scope
+  int best = 0;
+  double best_cost = 0.0;
+  for (int C = 2; C <= 16; C *= 2) {
+    c->max_cluster = C;
+    plan_pcg_cluster<T>(c, c->pcgc[idx]);
+    if (!c->pcgc[idx].ok || c->pcgc[idx].C != C) continue;
+    const double cost = C * time_pcg_iter<T>(c, w, phi, rhs, 64);
+    if (!best || cost < best_cost) {
+      best = C;
+      best_cost = cost;
+    }
+  }
+  c->max_cluster = best ? best : 16;
+  plan_pcg_cluster<T>(c, c->pcgc[idx]);
+  sync(c);
+  return best;
+}
+
+struct BatchRun {
+  int nsteps;
+  const double* dt;
+  const int* step0;
+  const fugu_step_opts* opts;
+  fugu_stats* last;
+  double* max_res;
+  int* status;
+  std::atomic<int> next{0};
+};
+
+void batch_worker(fugu_batch* b, BatchRun* r) {
+  const int nc = (int)b->cases.size();
+  for (;;) {
+    const int k = r->next.fetch_add(1);
+    if (k >= nc) return;
+    const int i = b->order[k];
+    fugu_ctx* c = b->cases[i];
+    double mres = 0.0;
+    fugu_stats st{};
+    const int rc = guard(c, [&] {
+      for (int s = 0; s < r->nsteps; ++s) {
+        std::memset(&st, 0, sizeof st);
+        step(c, r->dt[i], r->step0[i] + s, &r->opts[i], &st);
+        if (st.res > mres || std::isnan(st.res)) mres = st.res;
+      }
+    });
+    if (r->last) r->last[i] = st;
+    if (r->max_res) r->max_res[i] = mres;
+    if (r->status) r->status[i] = rc;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int fugu_batch_create(const fugu_params* params, int ncases, int device, const fugu_batch_opts* opts,
+                      fugu_batch** out) {
+  if (!out) return FUGU_EINVAL;
+  *out = nullptr;
+  if (!params || ncases < 1) return FUGU_EINVAL;
+  for (int i = 0; i < ncases; ++i)
+    if (check_params(&params[i]) != FUGU_OK) return FUGU_EINVAL;
+  fugu_batch_opts o{};
+  if (opts) o = *opts;
+  if (o.nthreads < 0 || o.max_cluster < 0 || o.max_cluster > 16 || o.max_coop < 0) return FUGU_EINVAL;
+  fugu_batch* b = new fugu_batch();
+  b->device = device;
+  const int hw = (int)std::thread::hardware_concurrency();
+  b->nthreads = o.nthreads ? o.nthreads : (hw > 0 ? hw : 8);
+  if (b->nthreads > ncases) b->nthreads = ncases;
+  // autotune decisions shared by cases of the same grid, boundaries and precision
+  std::map<std::array<int, 5>, int> tuned;
+  for (int i = 0; i < ncases; ++i) {
+    fugu_ctx* c = new fugu_ctx();
+    c->prm = params[i];
+    c->device = device;
+    c->max_coop = o.max_coop ? std::min(o.max_coop, 8) : 8;
+    c->coop_as_cluster = true;
+    c->max_cluster = o.max_cluster ? o.max_cluster : 16;
+    b->cases.push_back(c);
+    const int rc = guard(c, [&] {
+      create(c);
+      if (c->prm.precision == FUGU_MIXED) ensure_w32(c);
+      if (o.max_cluster) return;
+      const std::array<int, 5> key = {c->prm.nx, c->prm.ny, c->prm.periodic_x, c->prm.periodic_y,
+                                      c->prm.precision};
+      auto it = tuned.find(key);
+      if (it == tuned.end()) {
+        const int C = c->prm.precision == FUGU_MIXED ? tune_cluster<float>(c) : tune_cluster<double>(c);
+        it = tuned.emplace(key, C ? C : 16).first;
+      }
+      c->max_cluster = it->second;
+      plan_pcg_cluster<double>(c, c->pcgc[0]);
+      plan_pcg_cluster<float>(c, c->pcgc[1]);
+    });
+    if (rc) {
+      b->err = "case " + std::to_string(i) + ": " + c->err;
+      fprintf(stderr, "fugu_batch_create: %s\n", b->err.c_str());
+      for (fugu_ctx* x : b->cases) destroy(x);
+      delete b;
+      return rc;
+    }
+  }
+  b->order.resize(ncases);
+  for (int i = 0; i < ncases; ++i) b->order[i] = i;
+  std::stable_sort(b->order.begin(), b->order.end(), [&](int a, int z) {
+    return (long)params[a].nx * params[a].ny > (long)params[z].nx * params[z].ny;
+  });
+  *out = b;
+  return FUGU_OK;
+}
+
+void fugu_batch_destroy(fugu_batch* b) {
+  if (!b) return;
+  for (fugu_ctx* c : b->cases) destroy(c);
+  delete b;
+}
+
+const char* fugu_batch_last_error(const fugu_batch* b) { return b ? b->err.c_str() : "NULL batch"; }
+
+int fugu_batch_size(const fugu_batch* b) { return b ? (int)b->cases.size() : 0; }
+
+int fugu_batch_case(fugu_batch* b, int i, fugu_ctx** ctx) {
+  if (!b || !ctx || i < 0 || i >= (int)b->cases.size()) return FUGU_EINVAL;
+  *ctx = b->cases[i];
+  return FUGU_OK;
+}
+
+int fugu_batch_run(fugu_batch* b, int nsteps, const double* dt, const int* step0, const fugu_step_opts* opts,
+                   fugu_stats* last, double* max_res, int* status) {
+  if (!b) return FUGU_EINVAL;
+  if (nsteps < 0 || !dt || !step0 || !opts) {
+    b->err = "fugu_batch_run: NULL dt/step0/opts or nsteps < 0";
+    return FUGU_EINVAL;
+  }
+  BatchRun r;
+  r.nsteps = nsteps;
+  r.dt = dt;
+  r.step0 = step0;
+  r.opts = opts;
+  r.last = last;
+  r.max_res = max_res;
+  std::vector<int> st(b->cases.size(), FUGU_OK);
+  r.status = st.data();
+  std::vector<std::thread> pool;
+  for (int t = 1; t < b->nthreads; ++t) pool.emplace_back(batch_worker, b, &r);
+  batch_worker(b, &r);
+  for (auto& th : pool) th.join();
+  if (status) std::memcpy(status, st.data(), sizeof(int) * st.size());
+  for (size_t i = 0; i < st.size(); ++i)
+    if (st[i] != FUGU_OK) {
+      b->err = "case " + std::to_string(i) + ": " + b->cases[i]->err;
+      return st[i];
+    }
+  return FUGU_OK;
 }
 
 }  // extern "C"

@@ -268,6 +268,37 @@ int fugu_compute_csf_force(fugu_ctx* ctx, const double* c_raw, const double* kap
 int fugu_write_checkpoint(fugu_ctx* ctx, const char* path, int step, double t);
 int fugu_read_checkpoint(fugu_ctx* ctx, const char* path, int* step, double* t);
 
+/* ------------------------------------------------ batched form
+ * Many independent cases (grids, physics and precision may differ) advanced
+ * together on one GPU.  No counterpart in the reference, which runs one case
+ * per mpirun.  Each case is a full context (fugu_batch_case gives it, for
+ * fugu_upload / fugu_download / fugu_profile); a pool of host threads steps
+ * the cases, largest grid first, so the device runs as many cases' kernels
+ * at once as fit.  With max_cluster = 0 the CTAs of each case's
+ * cluster-resident PCG are autotuned at creation: per distinct (grid,
+ * boundaries, precision) every feasible size in {2, 4, 8, 16} is timed on
+ * the device and the least CTAs x time per iteration wins. */
+typedef struct fugu_batch fugu_batch;
+typedef struct {
+  int nthreads;     /* host threads stepping cases (0: hardware threads, <= ncases) */
+  int max_cluster;  /* CTAs of each cluster-resident PCG, 1..16 (0: autotune)     */
+  int max_coop;     /* CTAs of each grid-wide persistent kernel, launched as one  */
+                    /* thread-block cluster so that it is scheduled whole (<= 8; 0: 8) */
+} fugu_batch_opts;
+int fugu_batch_create(const fugu_params* params, int ncases, int device, const fugu_batch_opts* opts,
+                      fugu_batch** out);
+void fugu_batch_destroy(fugu_batch* b);
+const char* fugu_batch_last_error(const fugu_batch* b);
+int fugu_batch_size(const fugu_batch* b);
+int fugu_batch_case(fugu_batch* b, int i, fugu_ctx** ctx);
+/* Advance case i by nsteps steps with dt[i], step indices step0[i] ..
+ * step0[i]+nsteps-1 and options opts[i].  Per case (each output may be
+ * NULL): last[i] = stats of its last step, max_res[i] = largest final
+ * residual over its steps, status[i] = FUGU_OK or the error of the step
+ * that stopped it.  Returns FUGU_OK, or the first failing case's code. */
+int fugu_batch_run(fugu_batch* b, int nsteps, const double* dt, const int* step0, const fugu_step_opts* opts,
+                   fugu_stats* last, double* max_res, int* status);
+
 /* ------------------------------------------------ allocation-free entry
  * solve_poisson_pressure (mod_subsolvers.f90:32-246) with no context and no
  * allocation.  No counterpart in the reference, whose subroutine works on

@@ -63,7 +63,7 @@ def test_ctypes_structs_match_header_layout():
 
     src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
     for cname, py in (("fugu_params", _lib.FuguParams), ("fugu_step_opts", _lib.FuguStepOpts),
-                      ("fugu_stats", _lib.FuguStats)):
+                      ("fugu_stats", _lib.FuguStats), ("fugu_batch_opts", _lib.FuguBatchOpts)):
         body = re.search(r"typedef struct \{([^}]*)\}\s*" + cname + ";", src).group(1)
         names = []
         for decl in body.split(";"):

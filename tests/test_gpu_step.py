@@ -49,6 +49,13 @@ def case(name):
                    tol_bicgstab2=1e-6, max_iter_bicgstab2=100)
         c = cases.initial_colour(g, "rising_bubble")
         return g, p, c, dict(use_bicgstab2=False, consistent_amp=True), 1e-3, 3, None
+    if name == "bubble_freeslip":
+        # the 1 x 2 rising-bubble box with free-slip side walls (extension flag)
+        g = Grid(16, 32, 1.0, 2.0)
+        p = Params(rho1=1000.0, rho2=100.0, mu1=10.0, mu2=1.0, sigma=24.5, gx=0.0, gy=-0.98, time_order=2,
+                   tol_bicgstab2=1e-6, max_iter_bicgstab2=100, free_slip_x=1)
+        c = cases.initial_colour(g, "rising_bubble")
+        return g, p, c, dict(use_bicgstab2=False), 1e-3, 3, None
     if name == "poiseuille":
         g = Grid(8, 16, periodic_x=True)
         p = Params(rho1=1.0, rho2=1.0, mu1=1.0, mu2=0.25, sigma=0.0, gx=1.0, gy=0.0, time_order=2,
@@ -87,7 +94,8 @@ def run_pair(oracle_mod, name, prm_override=None, precision=0, nsteps=None):
     return g, st_o, st_g, hist
 
 
-@pytest.mark.parametrize("name", ["cavity", "droplet", "bubble_amp", "poiseuille", "cylinder", "cavity_b2"])
+@pytest.mark.parametrize("name", ["cavity", "droplet", "bubble_amp", "bubble_freeslip", "poiseuille", "cylinder",
+                                  "cavity_b2"])
 def test_step_parity_plain_fp64(gpu, oracle_mod, name):
     g, st_o, st_g, hist = run_pair(oracle_mod, name)
     for so, sg in hist:
@@ -124,7 +132,7 @@ def test_refine_fp64_parity(gpu, oracle_mod):
         assert rel(st_g[k], st_o[k]) <= 1e-8, (k, rel(st_g[k], st_o[k]))
 
 
-@pytest.mark.parametrize("name", ["cavity", "droplet", "bubble_amp"])
+@pytest.mark.parametrize("name", ["cavity", "droplet", "bubble_amp", "bubble_freeslip"])
 def test_mixed_precision_error_vs_fp64_oracle(gpu, oracle_mod, name):
     """FP32 inner Krylov+PCD inside FP64 defect correction: every step reaches
     the FP64 true residual tolerance (1e-9 relative), and the coupled state
