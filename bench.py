@@ -45,11 +45,17 @@ DT = 1e-4
 TOL = 1e-8
 
 
-def case_params():
+# inner solve of the FP64 defect correction: flexible GMRES (refine 2) or the
+# step's BiCGStab(2) (refine 1); both around the same PCD preconditioner
+INNER = {"fgmres": 2, "bicgstab2": 1}
+INNER_NAME = {2: "flexible GMRES(30)", 1: "BiCGStab(2)"}
+
+
+def case_params(refine=2):
     from coupled_codefort_2d_b200.params import Params
 
     return Params(rho1=1.0, rho2=0.1, mu1=0.1, mu2=0.01, sigma=1.0, gx=0.0, gy=0.0, time_order=2,
-                  tol_bicgstab2=TOL, max_iter_bicgstab2=500, refine=1, refine_inner_tol=1e-2,
+                  tol_bicgstab2=TOL, max_iter_bicgstab2=500, refine=refine, refine_inner_tol=1e-2,
                   refine_max_inner=30, refine_max_outer=60, krylov_bc_fix=1)
 
 
@@ -137,7 +143,7 @@ def gpu_arm(args, rank, world, local_rank):
     build.build()
     torch.cuda.set_device(local_rank)
     g = Grid(N, N)
-    prm = case_params()
+    prm = case_params(INNER[args.inner])
     st0 = initial_state(g, prm)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
 
@@ -258,13 +264,12 @@ def e2e_arm(args, g, prm, st0, local_rank):
 
 
 # --------------------------------------------------------------- CPU legs
-def cpu_step_time(state, step_idx, nsteps=1):
+def cpu_step_time(state, step_idx, prm, nsteps=1):
     """The oracle (a C restatement of the reference) on the same inputs."""
     from coupled_codefort_2d_b200.layout import Grid
     from oracle import oracle
 
     g = Grid(N, N)
-    prm = case_params()
     o = oracle.Oracle(g, prm)
     st = {k: a.copy(order="F") for k, a in state.items()}
     t0 = time.perf_counter()
@@ -276,11 +281,11 @@ def cpu_step_time(state, step_idx, nsteps=1):
 
 def _replica_worker(args_tuple):
     """one replica's step; replica 0 also returns the advanced state"""
-    state, step_idx, keep = args_tuple
+    state, step_idx, keep, prm = args_tuple
     from coupled_codefort_2d_b200.layout import Grid
     from oracle import oracle
 
-    o = oracle.Oracle(Grid(N, N), case_params())
+    o = oracle.Oracle(Grid(N, N), prm)
     st = {k: a.copy(order="F") for k, a in state.items()}
     t0 = time.perf_counter()
     o.step(st, DT, step_idx, use_bicgstab2=True)
@@ -298,7 +303,7 @@ def reference_arm(args, rank, world):
 
     oracle.build()
     g = Grid(N, N)
-    prm = case_params()
+    prm = case_params(INNER[args.inner])
     st = initial_state(g, prm)
     o = oracle.Oracle(g, prm)
     o.densities(st["c_field"], st["rho_c"], st["rho_u"], st["rho_v"])
@@ -313,7 +318,7 @@ def reference_arm(args, rank, world):
     with ctx.Pool(cores) as pool:
         for s in range(args.warmup + 1, args.warmup + args.steps + 1):
             t0 = time.perf_counter()
-            res = pool.map(_replica_worker, [(st, s, i == 0) for i in range(cores)])
+            res = pool.map(_replica_worker, [(st, s, i == 0, prm) for i in range(cores)])
             per_step.append(time.perf_counter() - t0)
             st = res[0][1]
     ms = 1000.0 * float(np.mean(per_step))
@@ -322,7 +327,7 @@ def reference_arm(args, rank, world):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / cores, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(
-            "FP64 defect correction around BiCGStab(2)+PCD (oracle port of the reference modules)"),
+            f"FP64 defect correction around {INNER_NAME[prm.refine]}+PCD (oracle port of the reference modules)"),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{cores} independent replicas x 1 thread, whole steps of the {N}^2 droplet"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -367,6 +372,8 @@ def main():
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
     ap.add_argument("--quick", action="store_true", help="skip the secondary arms")
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--inner", default="fgmres", choices=sorted(INNER),
+                    help="inner solve of the FP64 defect correction")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -409,7 +416,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 outer",
         "data": "synthetic (droplet case fully determined by its parameters)",
-        "config": workload_config("FP64 defect correction around FP32 BiCGStab(2)+PCD (inner tol 1e-2)"),
+        "config": workload_config(f"FP64 defect correction around FP32 {INNER_NAME[INNER[args.inner]]}+PCD "
+                                  "(inner tol 1e-2)"),
         "max_true_residual": max(r["res"] for r in s_m),
         "per_step": {"outer": [r["outer"] for r in s_m], "inner_iters": [r["iter"] for r in s_m],
                      "pcg_calls": [r["pcg_calls"] for r in s_m], "pcg_iters": [r["pcg_iters"] for r in s_m]},
@@ -421,7 +429,7 @@ def main():
         s64 = out["s_fp64"][args.warmup:]
         line["fp64"] = {"value": 1000.0 * len(out["t_fp64"]) / float(np.sum(out["t_fp64"])), "unit": UNIT,
                         "max_true_residual": max(r["res"] for r in s64),
-                        "solver": "FP64 defect correction around FP64 BiCGStab(2)+PCD"}
+                        "solver": f"FP64 defect correction around FP64 {INNER_NAME[INNER[args.inner]]}+PCD"}
         line["mixed_over_fp64"] = value / world / line["fp64"]["value"]
         sref = out["s_ref"][1:]
         line["reference_algorithm_fp64"] = {
@@ -433,11 +441,11 @@ def main():
         line["e2e"] = out["e2e"]
     if not args.no_cpu and "state_w" in out:
         nxt = args.warmup + args.steps + 1
-        dt_cpu, st_cpu = cpu_step_time(out["state_w"], nxt)
+        dt_cpu, st_cpu = cpu_step_time(out["state_w"], nxt, case_params(INNER[args.inner]))
         line["cpu_baseline"] = {
             "value": 1.0 / dt_cpu, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"1 coupled step (step {nxt}) of the same workload from the GPU run's state, "
-                      "oracle C port, FP64 defect correction around BiCGStab(2)+PCD, 1 thread",
+                      f"oracle C port, FP64 defect correction around {INNER_NAME[INNER[args.inner]]}+PCD, 1 thread",
             "true_residual": st_cpu[0].res}
     print(json.dumps(line), flush=True)
 

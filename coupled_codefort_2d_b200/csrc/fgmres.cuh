@@ -1,0 +1,191 @@
+// fgmres.cuh -- flexible GMRES(m) with right PCD preconditioning (extension,
+// not in the reference): the inner solve of the FP64 defect correction when
+// refine = 2.  The reference's BiCGStab(l) needs a fixed preconditioner; PCD
+// around a truncated PCG is not one, and BiCGStab(2) diverges on high
+// density-ratio bubbles, while flexible GMRES keeps Z_j = M^{-1} V_j and
+// minimises the true residual over span(Z).
+//
+// Device pieces: a multi-vector coupled dot (all projections of one
+// Gram-Schmidt pass in one launch), a multi-vector axpy, the scale of a new
+// basis vector, and the scalar steps (projections into H, Givens rotations,
+// the small triangular solve), which run in the last CTA of the reductions
+// like the BiCGStab recurrences do.
+#pragma once
+
+#include "scalars.cuh"
+
+namespace fugu {
+
+// device-resident scalars of one FGMRES cycle (doubles)
+struct FgLayout {
+  int m;  // Arnoldi steps of the cycle
+  __host__ __device__ int H(int i, int j) const { return i + j * (m + 1); }  // (m+1) x m, column-major
+  __host__ __device__ int cs() const { return (m + 1) * m; }
+  __host__ __device__ int sn() const { return cs() + m; }
+  __host__ __device__ int g() const { return sn() + m; }
+  __host__ __device__ int y() const { return g() + m + 1; }
+  __host__ __device__ int h() const { return y() + m; }  // projections of the current pass
+  __host__ __device__ int beta() const { return h() + m + 1; }
+  __host__ __device__ int inv() const { return beta() + 1; }  // scale of the next basis vector
+  __host__ __device__ int rel() const { return beta() + 2; }
+  __host__ __device__ int size() const { return beta() + 3; }
+};
+
+enum FgOp {
+  FG_BETA = 0,  // beta = |B|; V_0 scale; g[0] = beta; exit when beta == 0
+  FG_PROJ1,     // first Gram-Schmidt pass: h = d, H[0..j, j] = 0 + d
+  FG_PROJ2,     // second pass: h = d, H[0..j, j] += d
+  FG_ROTATE,    // H[j+1, j] = |w|, Givens rotations, g, rel, exit test
+};
+
+__device__ inline void fg_op(int op, const double* d, int j, double tol, const FgLayout L, double* st, KState* ks) {
+  switch (op) {
+    case FG_BETA: {
+      const double beta = sqrt(d[0]);
+      st[L.beta()] = beta;
+      st[L.g()] = beta;
+      st[L.inv()] = beta > 0.0 ? 1.0 / beta : 0.0;
+      st[L.rel()] = beta > 0.0 ? 1.0 : 0.0;
+      if (isnan(beta)) ks->nan = 1;
+      if (!(beta > 0.0)) kexit(ks, 0);
+      break;
+    }
+    case FG_PROJ1:
+    case FG_PROJ2:
+      for (int i = 0; i <= j; ++i) {
+        st[L.h() + i] = d[i];
+        if (op == FG_PROJ1) st[L.H(i, j)] = 0.0;
+        st[L.H(i, j)] += d[i];
+      }
+      break;
+    case FG_ROTATE: {
+      const double hn = sqrt(d[0]);
+      double* col = st + L.H(0, j);
+      double* cs = st + L.cs();
+      double* sn = st + L.sn();
+      double* g = st + L.g();
+      col[j + 1] = hn;
+      for (int i = 0; i < j; ++i) {
+        const double a = col[i], b = col[i + 1];
+        col[i] = cs[i] * a + sn[i] * b;
+        col[i + 1] = -sn[i] * a + cs[i] * b;
+      }
+      const double a = col[j], b = col[j + 1];
+      const double rr = sqrt(a * a + b * b);
+      cs[j] = rr > 0.0 ? a / rr : 1.0;
+      sn[j] = rr > 0.0 ? b / rr : 0.0;
+      col[j] = rr;
+      col[j + 1] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      const double rel = fabs(g[j + 1]) / st[L.beta()];
+      st[L.rel()] = rel;
+      st[L.inv()] = hn > 0.0 ? 1.0 / hn : 0.0;
+      if (isnan(rel)) ks->nan = 1;
+      if (rel < tol || hn == 0.0 || j + 1 == L.m || isnan(rel)) kexit(ks, j + 1);
+      break;
+    }
+  }
+}
+
+// coupled dots of w with nvec vectors V_i = V0 + i * stride: grid (S, nvec),
+// one DD partial per CTA and vector, the last CTA reduces and runs fg_op
+template <typename T>
+struct MdotArgs {
+  Geo g;
+  long n;  // elements of one component buffer
+  const T* w;
+  const T* V0;
+  long stride;
+  int nvec;
+  double vol;
+  double* part;  // >= 2 * nvec * gridDim.x
+  double* st;
+  KState* ks;
+  FgLayout L;
+  int op, j;
+  double tol;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_mdot(MdotArgs<T> a) {
+  if (!a.ks->active) return;
+  __shared__ DD sh[32];
+  __shared__ bool last;
+  __shared__ double dsum[128];
+  const Geo g = a.g;
+  const int i = blockIdx.y;
+  const T* V = a.V0 + i * a.stride;
+  const int nx = g.nx, ny = g.ny, imax = g.imax(), jmax = g.jmax();
+  const long nu = (long)imax * ny, nv = (long)nx * jmax, np = (long)nx * ny;
+  DD acc{0.0, 0.0};
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nu + nv + np; q += (long)gridDim.x * blockDim.x) {
+    long e;
+    if (q < nu) {
+      e = g.at(1 + (int)(q % imax), 1 + (int)(q / imax));
+    } else if (q < nu + nv) {
+      const long r = q - nu;
+      e = a.n + g.at(1 + (int)(r % nx), 1 + (int)(r / nx));
+    } else {
+      const long r = q - nu - nv;
+      e = 2 * a.n + g.at(1 + (int)(r % nx), 1 + (int)(r / nx));
+    }
+    dd_add(acc, (double(a.w[e]) * double(V[e])) * a.vol);
+  }
+  const DD s = block_sum_dd(acc, sh);
+  if (threadIdx.x == 0) {
+    put_partial(a.part + 2L * i * gridDim.x, blockIdx.x, s);
+    __threadfence();
+    const unsigned int t = atomicAdd(&a.ks->ticket, 1u);
+    last = (t == gridDim.x * gridDim.y - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  for (int v = 0; v < a.nvec; ++v) {
+    const double d = sum_partials_dd(a.part + 2L * v * gridDim.x, gridDim.x);
+    if (threadIdx.x == 0) dsum[v] = d;
+  }
+  if (threadIdx.x == 0) {
+    a.ks->ticket = 0;
+    fg_op(a.op, dsum, a.j, a.tol, a.L, a.st, a.ks);
+  }
+}
+
+// w = (...((w + s_0 V_0) + s_1 V_1) ...) + s_{nvec-1} V_{nvec-1}, s_i = sign * coef[i],
+// over every element of the triple (whole-array, as the reference's array
+// expressions)
+template <typename T>
+__global__ void k_maxpy(long n3, T* w, const T* V0, long stride, const double* coef, int nvec, double sign,
+                        const int* active) {
+  if (active && !*active) return;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n3; q += (long)gridDim.x * blockDim.x) {
+    T x = w[q];
+    for (int i = 0; i < nvec; ++i) x = x + T(sign * coef[i]) * V0[i * stride + q];
+    w[q] = x;
+  }
+}
+
+// dst = 0 + s * src (the reference-style array expression of a fresh vector)
+template <typename T>
+__global__ void k_fg_scale(long n3, T* dst, const T* src, const double* s, const int* active) {
+  if (active && !*active) return;
+  const T f = T(*s);
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n3; q += (long)gridDim.x * blockDim.x)
+    dst[q] = T(0) + f * src[q];
+}
+
+// back substitution R y = g over the k columns used
+__global__ void k_fg_solve(double* st, FgLayout L, int k) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double* g = st + L.g();
+  double* y = st + L.y();
+  for (int i = k - 1; i >= 0; --i) {
+    double s = g[i];
+    for (int q = i + 1; q < k; ++q) s -= st[L.H(i, q)] * y[q];
+    const double hii = st[L.H(i, i)];
+    y[i] = hii != 0.0 ? s / hii : 0.0;
+  }
+}
+
+}  // namespace fugu

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "fugu_gpu.h"
+#include "fgmres.cuh"
 #include "kernels.cuh"
 #include "pcg_cluster.cuh"
 #include "persistent.cuh"
@@ -98,6 +99,15 @@ struct KrylovWork {
   CoefBufs<T> cf;  // converted coefficients (FP32 only; FP64 points at the originals)
 };
 
+// flexible GMRES basis: V_0..V_m and Z_0..Z_{m-1}, contiguous triples
+template <typename T>
+struct FgWork {
+  T* V = nullptr;
+  T* Z = nullptr;
+  double* st = nullptr;  // FgLayout scalars
+  int cap = 0;           // m the buffers hold
+};
+
 }  // namespace
 
 struct fugu_ctx {
@@ -118,6 +128,8 @@ struct fugu_ctx {
   KrylovWork<double> w64;
   KrylovWork<float> w32;
   bool w32_ready = false;
+  FgWork<double> fg64;
+  FgWork<float> fg32;
   // routine-level scratch
   double* scratch[20] = {};
   // device scalars / state
@@ -694,10 +706,122 @@ KrylovResult bicgstab2(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, con
 }
 
 template <typename T>
+FgWork<T>& fg_work(fugu_ctx* c);
+template <>
+FgWork<double>& fg_work<double>(fugu_ctx* c) { return c->fg64; }
+template <>
+FgWork<float>& fg_work<float>(fugu_ctx* c) { return c->fg32; }
+
+template <typename T>
+FgWork<T>& ensure_fg(fugu_ctx* c, int m) {
+  FgWork<T>& f = fg_work<T>(c);
+  if (f.cap < m) {
+    f.V = dalloc<T>(c, (long)(m + 1) * 3 * c->n);
+    f.Z = dalloc<T>(c, (long)m * 3 * c->n);
+    f.st = dalloc<double>(c, FgLayout{m}.size());
+    f.cap = m;
+  }
+  return f;
+}
+
+template <typename T>
+Trip<T> trip_at(T* base, int i, long n) {
+  Trip<T> t;
+  t.base = base + (long)i * 3 * n;
+  t.u = t.base;
+  t.v = t.base + n;
+  t.p = t.base + 2 * n;
+  return t;
+}
+
+template <typename T>
+void mdot(fugu_ctx* c, const T* w, const T* V0, int nvec, int op, int j, double tol, FgLayout L, double* st) {
+  MdotArgs<T> a;
+  a.g = c->g;
+  a.n = c->n;
+  a.w = w;
+  a.V0 = V0;
+  a.stride = 3 * c->n;
+  a.nvec = nvec;
+  a.vol = c->g.dx * c->g.dy;
+  a.part = c->part;
+  a.st = st;
+  a.ks = c->ks;
+  a.L = L;
+  a.op = op;
+  a.j = j;
+  a.tol = tol;
+  int S = (2 * c->nsm + nvec - 1) / nvec;
+  if (S < 2) S = 2;
+  if (2L * nvec * S > c->part_len) S = (int)(c->part_len / (2L * nvec));
+  k_mdot<T><<<dim3(S, nvec), DOT_TPB, 0, c->s>>>(a);
+  CKL("k_mdot");
+}
+
+// flexible GMRES(m), right PCD preconditioning, one cycle from X = 0
+// (extension; the inner solve of refine_solve when refine = 2)
+template <typename T>
+KrylovResult fgmres(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const SolveOpt& o, Trip<T> X, Trip<T> B,
+                    double dt, double tol, int m) {
+  FgWork<T>& f = ensure_fg<T>(c, m);
+  const FgLayout L{m};
+  const long n3 = 3 * c->n;
+  const int g1 = grid1d(c, n3);
+  Trip<T>& wv = w.t[0];
+  const int* act = &c->ks->active;
+  reset_ks(c);
+  CK(cudaMemsetAsync(f.st, 0, sizeof(double) * L.size(), c->s));
+  mdot<T>(c, B.base, B.base, 1, FG_BETA, 0, tol, L, f.st);
+  k_fg_scale<T><<<g1, 256, 0, c->s>>>(n3, f.V, B.base, f.st + L.inv(), act);
+  CKL("k_fg_scale");
+  KState ks = read_ks(c);
+  for (int j = 0; j < m && ks.active; ++j) {
+    Trip<T> Vj = trip_at(f.V, j, c->n), Zj = trip_at(f.Z, j, c->n);
+    pcd<T>(c, w, cb, o, Vj, Zj, dt, act);
+    vbcs(c, Zj.u, Zj.v, 0.0, act);
+    matvec<T>(c, cb, o, Zj, wv, dt, act);
+    // classical Gram-Schmidt, twice
+    mdot<T>(c, wv.base, f.V, j + 1, FG_PROJ1, j, tol, L, f.st);
+    k_maxpy<T><<<g1, 256, 0, c->s>>>(n3, wv.base, f.V, n3, f.st + L.h(), j + 1, -1.0, act);
+    CKL("k_maxpy");
+    mdot<T>(c, wv.base, f.V, j + 1, FG_PROJ2, j, tol, L, f.st);
+    k_maxpy<T><<<g1, 256, 0, c->s>>>(n3, wv.base, f.V, n3, f.st + L.h(), j + 1, -1.0, act);
+    CKL("k_maxpy");
+    mdot<T>(c, wv.base, wv.base, 1, FG_ROTATE, j, tol, L, f.st);
+    k_fg_scale<T><<<g1, 256, 0, c->s>>>(n3, f.V + (long)(j + 1) * n3, wv.base, f.st + L.inv(), act);
+    CKL("k_fg_scale");
+    ks = read_ks(c);
+  }
+  const int k = ks.active ? m : ks.exit_iter;
+  KrylovResult res;
+  if (k > 0) {
+    k_fg_solve<<<1, 32, 0, c->s>>>(f.st, L, k);
+    CKL("k_fg_solve");
+    k_maxpy<T><<<g1, 256, 0, c->s>>>(n3, X.base, f.Z, n3, f.st + L.y(), k, 1.0, nullptr);
+    CKL("k_maxpy");
+  }
+  CK(cudaMemcpyAsync(c->h_sc, f.st + L.rel(), sizeof(double), cudaMemcpyDeviceToHost, c->s));
+  sync(c);
+  res.iter = k;
+  res.res = c->h_sc[0];
+  res.status = ks.nan ? FUGU_NAN : (res.res < tol ? FUGU_CONVERGED : FUGU_MAXITER);
+  return res;
+}
+
+template <typename T>
 KrylovResult krylov_inner(fugu_ctx* c, int solver, KrylovWork<T>& w, const CoefBufs<T>& cb, const SolveOpt& o,
                           Trip<T> X, Trip<T> B, double dt, double tol, int max_iter, bool has_lid, double lid) {
   if (solver == 2) return bicgstab2<T>(c, w, cb, o, X, B, dt, tol, max_iter, has_lid, lid);
   return bicgstab1<T>(c, w, cb, o, X, B, dt, tol, max_iter, has_lid, lid);
+}
+
+// inner solve of the defect correction: flexible GMRES when refine = 2,
+// else the step's BiCGStab(l)
+template <typename T>
+KrylovResult refine_inner(fugu_ctx* c, int solver, KrylovWork<T>& w, const CoefBufs<T>& cb, const SolveOpt& o,
+                          Trip<T> X, Trip<T> B, double dt) {
+  if (c->prm.refine == 2) return fgmres<T>(c, w, cb, o, X, B, dt, c->prm.refine_inner_tol, c->prm.refine_max_inner);
+  return krylov_inner<T>(c, solver, w, cb, o, X, B, dt, c->prm.refine_inner_tol, c->prm.refine_max_inner, false, 0.0);
 }
 
 void ensure_w32(fugu_ctx* c) {
@@ -766,14 +890,12 @@ KrylovResult refine_solve(fugu_ctx* c, int solver, const CoefBufs<double>& cb64,
       k_convert_scaled<float><<<grid1d(c, n3), 256, 0, c->s>>>(n3, r32.base, r.base, c->sc + S_INVRNORM);
       CKL("k_convert_scaled");
       zero_trip(c, d32);
-      ir = krylov_inner<float>(c, solver, w32, w32.cf, o, d32, r32, dt, c->prm.refine_inner_tol,
-                               c->prm.refine_max_inner, false, 0.0);
+      ir = refine_inner<float>(c, solver, w32, w32.cf, o, d32, r32, dt);
       k_accumulate<float><<<grid1d(c, n3), 256, 0, c->s>>>(n3, X.base, d32.base, c->sc + S_RNORM);
       CKL("k_accumulate");
     } else {
       zero_trip(c, d);
-      ir = krylov_inner<double>(c, solver, w, cb64, o, d, r, dt, c->prm.refine_inner_tol, c->prm.refine_max_inner,
-                                false, 0.0);
+      ir = refine_inner<double>(c, solver, w, cb64, o, d, r, dt);
       lin<double>(c, X, X, 1.0, c->sc + S_ONE, d);
     }
     inner_total += ir.iter;
@@ -1005,6 +1127,9 @@ int check_params(const fugu_params* p) {
   if (!(p->dx > 0.0) || !(p->dy > 0.0)) return FUGU_EINVAL;
   if (p->pcg_max_iter < 0 || p->pcd_sweeps < 0 || p->svof_max_iter < 0) return FUGU_EINVAL;
   if (p->precision == FUGU_MIXED && !p->refine) return FUGU_EINVAL;
+  if (p->refine < 0 || p->refine > 2) return FUGU_EINVAL;
+  // flexible GMRES keeps one projection per basis vector in shared memory
+  if (p->refine == 2 && (p->refine_max_inner < 1 || p->refine_max_inner > 127)) return FUGU_EINVAL;
   if (p->precision != FUGU_FP64 && p->precision != FUGU_MIXED) return FUGU_EINVAL;
   return FUGU_OK;
 }

@@ -40,7 +40,8 @@ class Params:
     limiter: int = 0  # 0 van Leer (mod_vof.f90:25-33), 1 Superbee
     free_slip_x: int = 0  # 1: side walls free-slip
     krylov_bc_fix: int = 0  # 1: BiCGStab(2) applies wall BCs to r before A*r
-    # FP64 defect-correction outer loop (0 = reference Krylov stopping rule)
+    # FP64 defect-correction outer loop (0 = reference Krylov stopping rule;
+    # 1 = inner BiCGStab(l) of the step, 2 = inner flexible GMRES)
     refine: int = 0
     refine_inner_tol: float = 1.0e-2
     refine_max_inner: int = 20

@@ -74,11 +74,14 @@ typedef struct {
   int krylov_bc_fix;          /* 1: BiCGStab(2) applies wall BCs to r before
                                  A*r (mod_bicgstab2.f90:430 does not)       */
   int refine;                 /* 1: FP64 defect-correction outer loop on the
-                                 true residual |B-AX|/|B| < tol             */
+                                 true residual |B-AX|/|B| < tol, inner solve
+                                 the step's BiCGStab(l); 2: the same loop
+                                 around flexible GMRES(refine_max_inner <= 127)
+                                 with right PCD preconditioning              */
   double refine_inner_tol;
   int refine_max_inner;
   int refine_max_outer;
-  int precision;              /* FUGU_FP64 or FUGU_MIXED (needs refine = 1) */
+  int precision;              /* FUGU_FP64 or FUGU_MIXED (needs refine >= 1) */
 } fugu_params;
 
 /* Optional arguments of advance_coupled_step (src/mod_solver_coupled.f90:137-160):

@@ -912,6 +912,89 @@ static void bicgstab2(const kctx* c, trip X, trip B, double tol, int max_iter, i
   trip_free(ss); trip_free(tt); trip_free(z); trip_free(q);
 }
 
+/* Flexible GMRES with right PCD preconditioning (extension, not in the
+ * reference; the inner solve of refine_solve when refine == 2).  One cycle
+ * of at most max_iter Arnoldi steps from X = 0: the outer defect correction
+ * restarts it.  Z_j = M^{-1} V_j is kept because M (PCD around a truncated
+ * PCG) differs from one application to the next; wall BCs are applied to
+ * Z_j before A, as the Krylov solvers do.  Classical Gram-Schmidt applied
+ * twice (all projections of a pass are independent dot products); Givens
+ * rotations on the Hessenberg column.  Stops when |g_{j+1}| / |B| < tol,
+ * which for right preconditioning is the residual of the unpreconditioned
+ * system in exact arithmetic. */
+static void fgmres(const kctx* c, trip X, trip B, double tol, int max_iter, int* iter_out, double* res_out) {
+  const fo_model* m = c->m;
+  const int mr = max_iter < 1 ? 1 : max_iter;
+  trip* V = (trip*)calloc((size_t)mr + 1, sizeof(trip));
+  trip* Z = (trip*)calloc((size_t)mr, sizeof(trip));
+  double* H = (double*)calloc((size_t)(mr + 1) * mr, sizeof(double)); /* H[i + j*(mr+1)] */
+  double *cs = (double*)calloc(mr, sizeof(double)), *sn = (double*)calloc(mr, sizeof(double));
+  double *g = (double*)calloc((size_t)mr + 1, sizeof(double)), *y = (double*)calloc(mr, sizeof(double));
+  double* h = (double*)calloc((size_t)mr + 1, sizeof(double));
+  trip w = trip_new(m);
+  int k = 0;
+  const double beta = sqrt(cdot(m, B, B));
+  double rel = 0.0;
+  if (beta > 0.0) {
+    V[0] = trip_new(m);
+    lin2(m, V[0], V[0], 1.0 / beta, B); /* V0 = 0 + B/beta */
+    g[0] = beta;
+    rel = 1.0;
+    for (int j = 0; j < mr; ++j) {
+      Z[j] = trip_new(m);
+      kc_precond(c, V[j], Z[j]);
+      fo_apply_velocity_bcs(m, Z[j].u, Z[j].v, 0, 0.0);
+      kc_matvec(c, Z[j], w);
+      for (int i = 0; i <= j + 1; ++i) H[i + (size_t)j * (mr + 1)] = 0.0;
+      for (int pass = 0; pass < 2; ++pass) {
+        for (int i = 0; i <= j; ++i) h[i] = cdot(m, w, V[i]);
+        for (int i = 0; i <= j; ++i) {
+          lin2(m, w, w, -h[i], V[i]);
+          H[i + (size_t)j * (mr + 1)] += h[i];
+        }
+      }
+      const double hn = sqrt(cdot(m, w, w));
+      H[j + 1 + (size_t)j * (mr + 1)] = hn;
+      k = j + 1;
+      /* apply the previous rotations, then a new one zeroing H[j+1, j] */
+      double* col = &H[(size_t)j * (mr + 1)];
+      for (int i = 0; i < j; ++i) {
+        const double a = col[i], b = col[i + 1];
+        col[i] = cs[i] * a + sn[i] * b;
+        col[i + 1] = -sn[i] * a + cs[i] * b;
+      }
+      const double a = col[j], b = col[j + 1];
+      const double rr = sqrt(a * a + b * b);
+      cs[j] = rr > 0.0 ? a / rr : 1.0;
+      sn[j] = rr > 0.0 ? b / rr : 0.0;
+      col[j] = rr;
+      col[j + 1] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      rel = fabs(g[j + 1]) / beta;
+      if (g_verbose) fprintf(stderr, "fgmres k=%d rel=%.6e\n", k, rel);
+      if (rel < tol || hn == 0.0 || j + 1 == mr) break;
+      V[j + 1] = trip_new(m);
+      lin2(m, V[j + 1], V[j + 1], 1.0 / hn, w);
+    }
+    /* back substitution R y = g, then X += sum_j y_j Z_j */
+    for (int i = k - 1; i >= 0; --i) {
+      double s = g[i];
+      for (int q = i + 1; q < k; ++q) s -= H[i + (size_t)q * (mr + 1)] * y[q];
+      y[i] = H[i + (size_t)i * (mr + 1)] != 0.0 ? s / H[i + (size_t)i * (mr + 1)] : 0.0;
+    }
+    for (int i = 0; i < k; ++i) lin2(m, X, X, y[i], Z[i]);
+  }
+  if (iter_out) *iter_out = k;
+  if (res_out) *res_out = rel;
+  for (int i = 0; i <= mr; ++i)
+    if (V[i].u) trip_free(V[i]);
+  for (int i = 0; i < mr; ++i)
+    if (Z[i].u) trip_free(Z[i]);
+  trip_free(w);
+  free(V); free(Z); free(H); free(cs); free(sn); free(g); free(y); free(h);
+}
+
 /* FP64 defect correction around an inner BiCGStab(l)+PCD solve (extension,
  * not in the reference): the true residual B - A X is formed with the
  * homogeneous wall BCs applied to X, so the operator is the same linear map
@@ -936,7 +1019,8 @@ static void refine_solve(const kctx* c, int solver, trip X, trip B, double tol, 
     memset(d.p, 0, n_cell(m) * sizeof(double));
     int it = 0;
     double ires = 0.0;
-    if (solver == 2) bicgstab2(c, d, r, m->refine_inner_tol, m->refine_max_inner, 0, 0.0, &it, &ires);
+    if (m->refine == 2) fgmres(c, d, r, m->refine_inner_tol, m->refine_max_inner, &it, &ires);
+    else if (solver == 2) bicgstab2(c, d, r, m->refine_inner_tol, m->refine_max_inner, 0, 0.0, &it, &ires);
     else bicgstab1(c, d, r, m->refine_inner_tol, m->refine_max_inner, 0, 0.0, &it, &ires);
     inner_total += it;
     lin2(m, X, X, 1.0, d);

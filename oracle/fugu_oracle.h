@@ -60,7 +60,9 @@ typedef struct {
   int krylov_bc_fix;        /* 1: BiCGStab(2) applies the wall BCs to r before
                                A*r (the reference does not, mod_bicgstab2.f90:430) */
   /* FP64 defect-correction outer loop (extension; refine = 0 is the reference):
-   * X += inner_solve(B - A X) until |B - A X| / |B| < tol (coupled_dot norm) */
+   * X += inner_solve(B - A X) until |B - A X| / |B| < tol (coupled_dot norm);
+   * the inner solve is the step's BiCGStab(l) when refine = 1, flexible GMRES
+   * (right PCD preconditioning) when refine = 2 */
   int refine;
   double refine_inner_tol;
   int refine_max_inner;

@@ -121,24 +121,32 @@ def test_step_parity_grid_wide_pcg(gpu, oracle_mod, name, monkeypatch):
         np.testing.assert_array_equal(st_g[k], st_o[k], err_msg=k)
 
 
-def test_refine_fp64_parity(gpu, oracle_mod):
-    over = dict(refine=1, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=30, krylov_bc_fix=1,
+@pytest.mark.parametrize("name,refine", [("droplet", 1), ("droplet", 2), ("bubble_freeslip", 2)])
+def test_refine_fp64_parity(gpu, oracle_mod, name, refine):
+    """FP64 defect correction around BiCGStab (refine 1) or flexible GMRES
+    (refine 2): same outer and inner iteration counts as the oracle, and the
+    same bits."""
+    over = dict(refine=refine, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=30, krylov_bc_fix=1,
                 tol_bicgstab2=1e-9)
-    g, st_o, st_g, hist = run_pair(oracle_mod, "droplet", over)
+    g, st_o, st_g, hist = run_pair(oracle_mod, name, over)
     for so, sg in hist:
         assert sg["res"] < 1e-9 and so.res < 1e-9
-        assert sg["outer"] == so.outer
+        assert sg["outer"] == so.outer and sg["iter"] == so.iter
+        assert sg["pcg_calls"] == so.pcg_calls
     for k in ("u_vel", "v_vel", "p_field"):
         assert rel(st_g[k], st_o[k]) <= 1e-8, (k, rel(st_g[k], st_o[k]))
+    for k in STATE:
+        np.testing.assert_array_equal(st_g[k], st_o[k], err_msg=k)
 
 
+@pytest.mark.parametrize("refine", [1, 2])
 @pytest.mark.parametrize("name", ["cavity", "droplet", "bubble_amp", "bubble_freeslip"])
-def test_mixed_precision_error_vs_fp64_oracle(gpu, oracle_mod, name):
+def test_mixed_precision_error_vs_fp64_oracle(gpu, oracle_mod, name, refine):
     """FP32 inner Krylov+PCD inside FP64 defect correction: every step reaches
     the FP64 true residual tolerance (1e-9 relative), and the coupled state
     (u, v, p) stays within 1e-6 relative L2 of the FP64 oracle solving the
     same steps to the same tolerance; per-field errors are reported."""
-    over = dict(refine=1, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=40, krylov_bc_fix=1,
+    over = dict(refine=refine, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=40, krylov_bc_fix=1,
                 tol_bicgstab2=1e-9)
     g, st_o, st_g, hist = run_pair(oracle_mod, name, over, precision=1)
     for so, sg in hist:
