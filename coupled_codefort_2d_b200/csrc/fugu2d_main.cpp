@@ -9,7 +9,7 @@
 // checkpoints every chk_freq steps (mod_io.f90:169-187 byte format).
 //
 // Extra namelist keys (this build): use_gpu (accepted, the path is the GPU),
-// precision ('fp64' | 'mixed'), refine, refine_inner_tol, refine_max_inner,
+// precision ('fp64' | 'mixed'), refine (logical or 0 / 1 / 2), refine_inner_tol, refine_max_inner,
 // refine_max_outer, krylov_bc_fix, limiter ('vanleer' | 'superbee'),
 // free_slip_x, device.
 //
@@ -194,7 +194,12 @@ bool apply(Settings& st, const std::map<std::string, std::string>& kv, std::stri
     else if (k == "use_gpu") st.use_gpu = flog(v);
     else if (k == "precision") st.precision = lower(fstr(v));
     else if (k == "limiter") st.limiter = lower(fstr(v));
-    else if (k == "refine") st.refine = flog(v) ? 1 : 0;
+    else if (k == "refine") {
+      // logical (.true. = defect correction around the step's BiCGStab) or
+      // 0 / 1 / 2 (2 = around flexible GMRES)
+      const std::string t = trim(v);
+      st.refine = (!t.empty() && std::isdigit((unsigned char)t[0])) ? (int)fnum(t) : (flog(v) ? 1 : 0);
+    }
     else if (k == "refine_inner_tol") st.refine_inner_tol = fnum(v);
     else if (k == "refine_max_inner") st.refine_max_inner = (int)fnum(v);
     else if (k == "refine_max_outer") st.refine_max_outer = (int)fnum(v);
@@ -349,7 +354,9 @@ int main(int argc, char** argv) {
   p.gx = st.gx; p.gy = st.gy; p.cfl_target = st.cfl_target; p.alpha_penalty = st.alpha_penalty;
   p.time_order = st.time_order; p.tol_bicgstab2 = st.tol_bicgstab2; p.max_iter_bicgstab2 = st.max_iter_bicgstab2;
   p.limiter = st.limiter == "superbee" ? 1 : 0; p.free_slip_x = st.free_slip_x; p.krylov_bc_fix = st.krylov_bc_fix;
-  p.refine = st.refine || st.precision == "mixed"; p.refine_inner_tol = st.refine_inner_tol;
+  // mixed precision needs the defect correction; flexible GMRES is its default inner solve
+  p.refine = st.refine ? st.refine : (st.precision == "mixed" ? 2 : 0);
+  p.refine_inner_tol = st.refine_inner_tol;
   p.refine_max_inner = st.refine_max_inner; p.refine_max_outer = st.refine_max_outer;
   p.precision = st.precision == "mixed" ? FUGU_MIXED : FUGU_FP64;
   fugu_ctx* ctx = nullptr;
