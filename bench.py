@@ -358,7 +358,7 @@ def roofline(prof, peaks):
             traffic = t.get("dram_bytes_per_launch")
         except Exception:
             traffic = None
-    return {"kernel": "k_pcg<float> (persistent Jacobi-PCG of the PCD pressure step)", "bound": "hbm",
+    return {"kernel": "k_pcg_cluster<float> (cluster-resident Jacobi-PCG of the PCD pressure step)", "bound": "hbm",
             "achieved": achieved, "peak": peak, "peak_source": src, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "bytes_per_launch": bytes_per_launch, "ms_per_launch": ms_per_launch,
             "iters_per_launch": prof["pcg_iters"] / prof["pcg_launches"]}
