@@ -130,6 +130,8 @@ struct fugu_ctx {
   bool w32_ready = false;
   FgWork<double> fg64;
   FgWork<float> fg32;
+  int pcg_cap_cur = 0;    // PCG cap of the PCD during an adaptive solve (0: pcg_max_iter)
+  int pcg_cap_state = 0;  // cap the last adaptive solve ended with (carried to the next)
   // routine-level scratch
   double* scratch[20] = {};
   // device scalars / state
@@ -543,7 +545,8 @@ void pcd(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const SolveOpt& o
   // even after an exit; the output of an exited iteration is never read.
   CK(cudaMemsetAsync(r.base, 0, sizeof(T) * 3 * c->n, c->s));
   CK(cudaMemsetAsync(pw.phi, 0, sizeof(T) * c->n, c->s));
-  pcg<T>(c, w.pcg, pw.phi, z.p, c->prm.pcg_tol, c->prm.pcg_max_iter, true, active);
+  pcg<T>(c, w.pcg, pw.phi, z.p, c->prm.pcg_tol, c->pcg_cap_cur > 0 ? c->pcg_cap_cur : c->prm.pcg_max_iter, true,
+         active);
   halo(c, pw.phi, K_CELL, active);
   k_pcd_schur<T><<<b.grid, b.block, 0, c->s>>>(c->g, pw.phi, cb.u_adv, cb.v_adv, r.p, T(1.0 / dt), active);
   CKL("k_pcd_schur");
@@ -872,6 +875,17 @@ KrylovResult refine_solve(fugu_ctx* c, int solver, const CoefBufs<double>& cb64,
   KrylovResult res;
   int outer = 0, inner_total = 0;
   double rel = 0.0;
+  // adaptive PCG cap of the PCD (refine = 2 with pcg_cap_start > 0): start
+  // from the cap the previous solve ended with (at least pcg_cap_start),
+  // double it after a pass whose inner solve missed its tolerance; the guard
+  // restores the fixed cap however the solve ends
+  const bool adapt = c->prm.refine == 2 && c->prm.pcg_cap_start > 0;
+  struct CapGuard {
+    fugu_ctx* c;
+    ~CapGuard() { c->pcg_cap_cur = 0; }
+  } cap_guard{c};
+  if (adapt)
+    c->pcg_cap_cur = std::min(std::max(c->prm.pcg_cap_start, c->pcg_cap_state), c->prm.pcg_max_iter);
   for (;; ++outer) {
     matvec<double>(c, cb64, o, X, ax, dt, nullptr);
     lin<double>(c, r, B, -1.0, c->sc + S_ONE, ax);
@@ -899,10 +913,13 @@ KrylovResult refine_solve(fugu_ctx* c, int solver, const CoefBufs<double>& cb64,
       lin<double>(c, X, X, 1.0, c->sc + S_ONE, d);
     }
     inner_total += ir.iter;
+    if (adapt && !(ir.res < c->prm.refine_inner_tol) && c->pcg_cap_cur < c->prm.pcg_max_iter)
+      c->pcg_cap_cur = std::min(2 * c->pcg_cap_cur, c->prm.pcg_max_iter);
     reset_ks(c);
     vbcs(c, X.u, X.v, 0.0);
   }
   if (has_lid) vbcs(c, X.u, X.v, lid);
+  if (adapt) c->pcg_cap_state = c->pcg_cap_cur;
   res.iter = inner_total;
   res.res = rel;
   if (outer_out) *outer_out = outer;
@@ -1125,7 +1142,7 @@ int check_params(const fugu_params* p) {
   if (!p) return FUGU_EINVAL;
   if (p->nx < 4 || p->ny < 4 || p->nx > 65536 || p->ny > 65536) return FUGU_EINVAL;
   if (!(p->dx > 0.0) || !(p->dy > 0.0)) return FUGU_EINVAL;
-  if (p->pcg_max_iter < 0 || p->pcd_sweeps < 0 || p->svof_max_iter < 0) return FUGU_EINVAL;
+  if (p->pcg_max_iter < 0 || p->pcd_sweeps < 0 || p->svof_max_iter < 0 || p->pcg_cap_start < 0) return FUGU_EINVAL;
   if (p->precision == FUGU_MIXED && !p->refine) return FUGU_EINVAL;
   if (p->refine < 0 || p->refine > 2) return FUGU_EINVAL;
   // flexible GMRES keeps one projection per basis vector in shared memory
@@ -1307,6 +1324,7 @@ int fugu_set_params(fugu_ctx* c, const fugu_params* p) {
   }
   c->prm = *p;
   c->g = make_geo(*p);
+  c->pcg_cap_state = 0;  // the adaptive PCG cap restarts from pcg_cap_start
   return FUGU_OK;
 }
 

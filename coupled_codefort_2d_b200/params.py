@@ -46,6 +46,9 @@ class Params:
     refine_inner_tol: float = 1.0e-2
     refine_max_inner: int = 20
     refine_max_outer: int = 30
+    # refine = 2: PCD's PCG starts at this cap and doubles it up to pcg_max_iter
+    # after an outer pass whose inner solve missed refine_inner_tol (0 = off)
+    pcg_cap_start: int = 0
 
     def with_(self, **kw) -> "Params":
         return replace(self, **kw)

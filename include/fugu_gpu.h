@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define FUGU_ABI_VERSION 1
+#define FUGU_ABI_VERSION 2
 
 /* return codes */
 #define FUGU_OK 0
@@ -82,6 +82,11 @@ typedef struct {
   int refine_max_inner;
   int refine_max_outer;
   int precision;              /* FUGU_FP64 or FUGU_MIXED (needs refine >= 1) */
+  int pcg_cap_start;          /* refine = 2 only; 0 keeps the cap pcg_max_iter.
+                                 > 0: each defect correction starts the PCD's
+                                 PCG at this many iterations and doubles it (up
+                                 to pcg_max_iter) after every outer pass whose
+                                 flexible GMRES missed refine_inner_tol       */
 } fugu_params;
 
 /* Optional arguments of advance_coupled_step (src/mod_solver_coupled.f90:137-160):

@@ -1005,6 +1005,10 @@ static void refine_solve(const kctx* c, int solver, trip X, trip B, double tol, 
   trip r = trip_new(m), d = trip_new(m), ax = trip_new(m);
   int inner_total = 0, outer;
   double rel = 0.0;
+  /* adaptive PCG cap of the PCD (refine = 2 with pcg_cap_start > 0) */
+  const int adapt = m->refine == 2 && m->pcg_cap_start > 0;
+  int cap = adapt && m->pcg_cap_start < m->pcg_max_iter ? m->pcg_cap_start : m->pcg_max_iter;
+  if (adapt && c->st && c->st->pcg_cap > cap) cap = c->st->pcg_cap < m->pcg_max_iter ? c->st->pcg_cap : m->pcg_max_iter;
   fo_apply_velocity_bcs(m, X.u, X.v, 0, 0.0);
   double nb = sqrt(cdot(m, B, B));
   if (nb < 1.0e-300) nb = 1.0;
@@ -1019,14 +1023,27 @@ static void refine_solve(const kctx* c, int solver, trip X, trip B, double tol, 
     memset(d.p, 0, n_cell(m) * sizeof(double));
     int it = 0;
     double ires = 0.0;
-    if (m->refine == 2) fgmres(c, d, r, m->refine_inner_tol, m->refine_max_inner, &it, &ires);
-    else if (solver == 2) bicgstab2(c, d, r, m->refine_inner_tol, m->refine_max_inner, 0, 0.0, &it, &ires);
-    else bicgstab1(c, d, r, m->refine_inner_tol, m->refine_max_inner, 0, 0.0, &it, &ires);
+    if (m->refine == 2) {
+      /* the PCD of this pass runs its PCG at the current cap */
+      fo_model mm = *m;
+      mm.pcg_max_iter = cap;
+      kctx cc = *c;
+      cc.m = &mm;
+      fgmres(&cc, d, r, m->refine_inner_tol, m->refine_max_inner, &it, &ires);
+      /* a pass whose inner solve missed its tolerance doubles the cap */
+      if (adapt && !(ires < m->refine_inner_tol) && cap < m->pcg_max_iter)
+        cap = 2 * cap < m->pcg_max_iter ? 2 * cap : m->pcg_max_iter;
+    } else if (solver == 2) {
+      bicgstab2(c, d, r, m->refine_inner_tol, m->refine_max_inner, 0, 0.0, &it, &ires);
+    } else {
+      bicgstab1(c, d, r, m->refine_inner_tol, m->refine_max_inner, 0, 0.0, &it, &ires);
+    }
     inner_total += it;
     lin2(m, X, X, 1.0, d);
     fo_apply_velocity_bcs(m, X.u, X.v, 0, 0.0);
   }
   if (c->st) c->st->outer += outer;
+  if (adapt && c->st) c->st->pcg_cap = cap;
   if (has_lid) fo_apply_velocity_bcs(m, X.u, X.v, 1, u_lid);
   if (iter_out) *iter_out = inner_total;
   if (res_out) *res_out = rel;

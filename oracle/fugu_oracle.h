@@ -67,6 +67,10 @@ typedef struct {
   double refine_inner_tol;
   int refine_max_inner;
   int refine_max_outer;
+  /* refine = 2: the PCD's PCG starts each defect correction capped at
+   * pcg_cap_start iterations and doubles the cap (up to pcg_max_iter) after
+   * each outer pass whose flexible GMRES missed refine_inner_tol; 0 = off */
+  int pcg_cap_start;
 } fo_model;
 
 void fo_model_defaults(fo_model* m);
@@ -95,6 +99,10 @@ typedef struct {
   int svof_iters;
   int matvecs;
   int outer;                /* defect-correction outer iterations (refine) */
+  int pcg_cap;              /* in/out, adaptive PCG cap (refine = 2,
+                               pcg_cap_start > 0): the cap a solve starts
+                               from (0: pcg_cap_start) and ends with; the
+                               caller carries it from step to step         */
 } fo_stats;
 
 /* --- mod_mpi single-rank halo semantics (mod_mpi.f90:113-245) ---------- */

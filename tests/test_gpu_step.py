@@ -121,13 +121,15 @@ def test_step_parity_grid_wide_pcg(gpu, oracle_mod, name, monkeypatch):
         np.testing.assert_array_equal(st_g[k], st_o[k], err_msg=k)
 
 
-@pytest.mark.parametrize("name,refine", [("droplet", 1), ("droplet", 2), ("bubble_freeslip", 2)])
-def test_refine_fp64_parity(gpu, oracle_mod, name, refine):
+@pytest.mark.parametrize("name,refine,cap0", [("droplet", 1, 0), ("droplet", 2, 0), ("bubble_freeslip", 2, 0),
+                                              ("droplet", 2, 3), ("bubble_freeslip", 2, 2)])
+def test_refine_fp64_parity(gpu, oracle_mod, name, refine, cap0):
     """FP64 defect correction around BiCGStab (refine 1) or flexible GMRES
     (refine 2): same outer and inner iteration counts as the oracle, and the
-    same bits."""
+    same bits.  cap0 > 0 runs the adaptive PCG cap from a start so low that
+    it must grow, and carries it across the steps on both sides."""
     over = dict(refine=refine, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=30, krylov_bc_fix=1,
-                tol_bicgstab2=1e-9)
+                tol_bicgstab2=1e-9, pcg_cap_start=cap0)
     g, st_o, st_g, hist = run_pair(oracle_mod, name, over)
     for so, sg in hist:
         assert sg["res"] < 1e-9 and so.res < 1e-9
