@@ -203,6 +203,9 @@ def gpu_arm(args, rank, world, local_rank):
         total_ms = float(tt.item())
     out = {"t_mixed": t_mixed, "s_mixed": s_mixed, "prof": prof, "total_ms": total_ms, "clocks": sampler.summary()}
 
+    if not args.quick:  # every rank: the ensemble is sharded over the ranks
+        out["batched"] = batched_arm(world, rank, local_rank)
+
     if rank == 0 and not args.quick:
         # FP64 inner form of the same solver, same steps
         t64, s64, _, _ = run_form(FP64, args.steps, args.warmup)
@@ -214,6 +217,57 @@ def gpu_arm(args, rank, world, local_rank):
         out["e2e"] = e2e_arm(args, g, prm, st0, local_rank)
         out["state_w"] = state_w
     return out
+
+
+BATCH_CASES_PER_GPU = 32
+BATCH_STEPS = 2
+
+
+def batched_arm(world, rank, local_rank):
+    """The batched form on the rising-bubble ensemble (first 32 x N cases of
+    the seeded ensemble, grids 64x128 .. 256x512, density ratios 10-1000),
+    sharded over the N ranks, mixed precision; beside it, on rank 0, the
+    plain FP64 single-case form on the first cases, one context at a time."""
+    import torch
+
+    from coupled_codefort_2d_b200 import cases, ensemble
+    from coupled_codefort_2d_b200._lib import FP64
+    from coupled_codefort_2d_b200.batch import ensemble_params, initial_bubble_state
+    from coupled_codefort_2d_b200.context import Context
+
+    specs = cases.bubble_ensemble(BATCH_CASES_PER_GPU * world)
+    if world > 1:
+        barrier, max_reduce, gather = ensemble._dist_ops()
+    else:
+        barrier, max_reduce, gather = (lambda: None), (lambda x: x), (lambda o: [o])
+    res = ensemble.run_ensemble(
+        specs, BATCH_STEPS, rank, world,
+        lambda idx: ensemble.run_shard_gpu(specs, idx, BATCH_STEPS, local_rank, nthreads=8, warmup=1),
+        barrier, max_reduce, gather)
+    if rank != 0:
+        return None
+    rows = res.pop("rows")
+    # plain FP64 form, single case at a time, on the first cases (1 warm-up + 1 timed step each)
+    n64, t64 = 0, 0.0
+    for s in specs[:8]:
+        with Context(s["grid"], ensemble_params(s, **ensemble.SOLVER), device=local_rank, precision=FP64) as ctx:
+            initial_bubble_state(ctx, s)
+            o = ctx.step_opts(use_bicgstab2=True)
+            ctx.step(ensemble.DT, 1, o)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            ctx.step(ensemble.DT, 2, o)
+            torch.cuda.synchronize()
+            t64 += time.perf_counter() - t0
+            n64 += 1
+    fp64_single = n64 / t64
+    return {"workload": f"rising_bubble_ensemble_{len(specs)} (seed {cases.ENSEMBLE_SEED}, first cases)",
+            "value": res["case_steps_per_s"], "unit": "case-steps/s", "steps": BATCH_STEPS, "warmup": 1,
+            "seconds": res["seconds"], "dtype": "f32 inner / f64 outer", "max_true_residual":
+            max(r["max_res"] for r in rows), "failed_cases": [r["case"] for r in rows if r["status"] != 0],
+            "fp64_single_case": {"value": fp64_single, "unit": "case-steps/s", "cases": n64},
+            "batched_mixed_over_fp64_single": res["case_steps_per_s"] / world / fp64_single,
+            "timing": "host wall clock around the batch run, CUDA-synchronised, max over ranks"}
 
 
 class _Null:
@@ -445,6 +499,8 @@ def main():
             "solver": "bicgstab_solve + PCD exactly as the reference (tol 1e-8 on the preconditioned residual)"}
     if "e2e" in out:
         line["e2e"] = out["e2e"]
+    if out.get("batched"):
+        line["batched"] = out["batched"]
     if not args.no_cpu and "state_w" in out:
         nxt = args.warmup + args.steps + 1
         dt_cpu, st_cpu = cpu_step_time(out["state_w"], nxt, case_params(INNER[args.inner]))

@@ -1,0 +1,177 @@
+"""The batched ensemble across GPUs: independent cases sharded over ranks.
+
+One process per GPU (``torchrun``); every rank advances its own shard of the
+cases with a :class:`~coupled_codefort_2d_b200.batch.Batch` on its GPU.
+Cases never exchange data, so the data path has no collective: the ranks
+meet only at the barriers around the timed region, in one max-reduction of
+the elapsed time, and in a final gather of per-case scalars (status,
+largest residual, iterations, bubble centroid) to rank 0.  The reference
+runs one case per ``mpirun`` and has no counterpart.
+
+    torchrun --nproc-per-node 8 --master-addr 127.0.0.1 -m coupled_codefort_2d_b200.ensemble \
+        --cases 256 --steps 200
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import cases
+
+SOLVER = dict(tol_bicgstab2=1e-8, max_iter_bicgstab2=500, refine=2, refine_inner_tol=1e-2, refine_max_inner=30,
+              refine_max_outer=60, krylov_bc_fix=1, pcg_cap_start=40)
+DT = 5e-4
+
+
+def partition(costs, world: int) -> list[list[int]]:
+    """Greedy longest-processing-time split of case indices over ``world``
+    ranks: cases in decreasing cost (ties by index) go to the least-loaded
+    rank (ties by rank).  Deterministic, so every rank computes the same
+    split without communicating."""
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    shards = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        shards[r].append(i)
+        load[r] += costs[i]
+    return [sorted(s) for s in shards]
+
+
+def case_cost(spec: dict) -> float:
+    """Cost model of a case: its cell count (the work of every kernel of a
+    step scales with it)."""
+    return float(spec["grid"].ncells)
+
+
+def run_shard_gpu(specs, idx, nsteps, device, nthreads=0, precision=None, warmup=0):
+    """Advance the cases ``idx`` on ``device`` and return their per-case
+    scalars and the elapsed seconds of the stepping (barrier-free; the caller
+    brackets it).  ``warmup`` untimed steps come first (work space
+    allocation, the adaptive PCG cap settling)."""
+    import torch
+
+    from ._lib import MIXED
+    from .batch import Batch, ensemble_params, initial_bubble_state
+
+    prec = MIXED if precision is None else precision
+    sub = [specs[i] for i in idx]
+    if not sub:  # more ranks than cases: this rank only takes part in the collectives
+        yield "ready", None
+        yield "done", ([], 0.0)
+        return
+    with Batch([(s["grid"], ensemble_params(s, **SOLVER), prec) for s in sub], device=device,
+               nthreads=nthreads) as b:
+        for k, s in enumerate(sub):
+            initial_bubble_state(b.case(k), s)
+        opts = b.case(0).step_opts(use_bicgstab2=True)
+        if warmup:
+            b.run(warmup, DT, 1, opts)
+        torch.cuda.synchronize(device)
+        yield "ready", None
+        t0 = time.perf_counter()
+        out = b.run(nsteps, DT, warmup + 1, opts)
+        torch.cuda.synchronize(device)
+        elapsed = time.perf_counter() - t0
+        rows = []
+        for k, s in enumerate(sub):
+            st = b.case(k).download_state(["c_field", "v_vel"])
+            ycm, vr = cases.bubble_centroid_velocity(s["grid"], st["c_field"], st["v_vel"])
+            rows.append({"case": s["case"], "status": out["status"][k], "max_res": out["max_res"][k],
+                         "last_iter": out["last"][k]["iter"], "y_centroid": ycm, "rise_velocity": vr})
+        yield "done", (rows, elapsed)
+
+
+def run_ensemble(specs, nsteps, rank, world, runner, barrier, max_reduce, gather):
+    """Shard, run, time and gather.  ``runner(idx)`` is a generator that
+    yields ("ready", None) once its cases are set up and ("done", (rows,
+    seconds)) after stepping them; ``barrier``, ``max_reduce(x)`` and
+    ``gather(obj) -> list | None`` are the process-group operations (rank 0
+    receives the list).  Every rank takes the same collective steps in the
+    same order, whatever its shard holds."""
+    shards = partition([case_cost(s) for s in specs], world)
+    mine = shards[rank]
+    it = runner(mine)
+    tag, _ = next(it)
+    assert tag == "ready"
+    barrier()
+    tag, (rows, elapsed) = next(it)
+    assert tag == "done"
+    it.close()  # releases the shard's batch before the collectives
+    barrier()
+    slowest = max_reduce(elapsed)
+    all_rows = gather(rows)
+    if rank != 0:
+        return None
+    merged = sorted((r for part in all_rows for r in part), key=lambda r: r["case"])
+    return {"cases": len(specs), "steps": nsteps, "world": world, "seconds": slowest,
+            "case_steps_per_s": len(specs) * nsteps / slowest if slowest > 0 else float("inf"),
+            "shard_cells": [sum(specs[i]["grid"].ncells for i in s) for s in shards], "rows": merged}
+
+
+def _dist_ops():
+    import torch
+    import torch.distributed as dist
+
+    def barrier():
+        dist.barrier()
+
+    def max_reduce(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def gather(obj):
+        out = [None] * dist.get_world_size()
+        dist.all_gather_object(out, obj)
+        return out
+
+    return barrier, max_reduce, gather
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--cases", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--seed", type=int, default=cases.ENSEMBLE_SEED)
+    ap.add_argument("--threads", type=int, default=8, help="host threads per rank")
+    ap.add_argument("--out", default=None, help="write the per-case table (JSON) here")
+    args = ap.parse_args(argv)
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        barrier, max_reduce, gather = _dist_ops()
+    else:
+        barrier, max_reduce, gather = (lambda: None), (lambda x: x), (lambda o: [o])
+    specs = cases.bubble_ensemble(args.cases, seed=args.seed)
+    res = run_ensemble(specs, args.steps, rank, world,
+                       lambda idx: run_shard_gpu(specs, idx, args.steps, local, args.threads),
+                       barrier, max_reduce, gather)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        rows = res.pop("rows")
+        res["failed"] = [r["case"] for r in rows if r["status"] != 0]
+        res["max_res"] = max(r["max_res"] for r in rows)
+        print(json.dumps(res), flush=True)
+        if args.out:
+            with open(args.out, "w") as f:
+                json.dump(rows, f, indent=1)
+
+
+if __name__ == "__main__":
+    main()

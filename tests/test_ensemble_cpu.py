@@ -1,0 +1,82 @@
+"""Sharding the batched ensemble over ranks, without a GPU: the partition
+covers every case exactly once and balances cells, and a world-size-2 gloo
+run of the host logic (shard, barrier, max-reduce of the time, gather of
+per-case rows to rank 0) reassembles the whole ensemble.  The GPU stepping
+is replaced by a runner that returns per-case rows."""
+import json
+import os
+import socket
+import time
+
+import pytest
+import torch.multiprocessing as mp
+
+from coupled_codefort_2d_b200 import cases
+from coupled_codefort_2d_b200.ensemble import case_cost, partition, run_ensemble
+
+
+def test_partition_covers_every_case_once_and_balances():
+    specs = cases.bubble_ensemble(256)
+    costs = [case_cost(s) for s in specs]
+    for world in (1, 2, 3, 4, 8):
+        shards = partition(costs, world)
+        assert len(shards) == world
+        flat = sorted(i for s in shards for i in s)
+        assert flat == list(range(256))
+        loads = [sum(costs[i] for i in s) for s in shards]
+        # greedy LPT: max load <= mean + the largest single case
+        assert max(loads) <= sum(costs) / world + max(costs)
+    assert partition(costs, 4) == partition(costs, 4)  # deterministic: no exchange needed
+
+
+def test_partition_more_ranks_than_cases():
+    shards = partition([3.0, 1.0], 4)
+    assert sorted(i for s in shards for i in s) == [0, 1]
+    assert sum(1 for s in shards if not s) == 2
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, out_path, ncases):
+    import datetime
+
+    import torch.distributed as dist
+
+    from coupled_codefort_2d_b200.ensemble import _dist_ops
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    barrier, max_reduce, gather = _dist_ops()
+    specs = cases.bubble_ensemble(ncases)
+
+    def runner(idx):
+        yield "ready", None
+        t0 = time.perf_counter()
+        time.sleep(0.05 * (rank + 1))  # ranks finish at different times
+        rows = [{"case": specs[i]["case"], "status": 0, "max_res": 1e-9, "rank": rank} for i in idx]
+        yield "done", (rows, time.perf_counter() - t0)
+
+    res = run_ensemble(specs, 5, rank, world, runner, barrier, max_reduce, gather)
+    dist.destroy_process_group()
+    if rank == 0:
+        with open(out_path, "w") as f:
+            json.dump(res, f)
+    else:
+        assert res is None
+
+
+@pytest.mark.timeout(120)
+def test_gloo_two_ranks_reassemble_the_ensemble(tmp_path):
+    out = tmp_path / "res.json"
+    mp.start_processes(_worker, args=(2, _free_port(), str(out), 12), nprocs=2, join=True, start_method="spawn")
+    res = json.loads(out.read_text())
+    assert res["world"] == 2 and res["cases"] == 12 and res["steps"] == 5
+    assert [r["case"] for r in res["rows"]] == list(range(12))
+    assert {r["rank"] for r in res["rows"]} == {0, 1}
+    # the timed region is the slower rank's (max over ranks)
+    assert res["seconds"] >= 0.1
+    assert res["case_steps_per_s"] == pytest.approx(12 * 5 / res["seconds"])
