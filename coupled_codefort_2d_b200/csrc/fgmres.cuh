@@ -88,8 +88,17 @@ __device__ inline void fg_op(int op, const double* d, int j, double tol, const F
   }
 }
 
-// coupled dots of w with nvec vectors V_i = V0 + i * stride: grid (S, nvec),
-// one DD partial per CTA and vector, the last CTA reduces and runs fg_op
+// coupled dots of w with nvec vectors V_i = V0 + i * stride.  The work items
+// are chunks of MDOT_CHUNK consecutive unknowns of one grid row of one
+// component (u, v or p rows of the owned interior), so a warp reads contiguous
+// memory and maps an item to its row once.  Each CTA keeps one DD partial for
+// its vector; the last CTA merges the partials of each vector with one warp per
+// vector and runs fg_op.  Launch: grid (Gx, nvec) of MDOT_TPB threads, grid
+// row y computing the dot with V_y.
+constexpr int MDOT_TPB = 256;
+constexpr int MDOT_CHUNK = 128;
+constexpr int MDOT_MAXV = 128;
+
 template <typename T>
 struct MdotArgs {
   Geo g;
@@ -97,7 +106,7 @@ struct MdotArgs {
   const T* w;
   const T* V0;
   long stride;
-  int nvec;
+  int nvec;      // <= MDOT_MAXV
   double vol;
   double* part;  // >= 2 * nvec * gridDim.x
   double* st;
@@ -107,34 +116,58 @@ struct MdotArgs {
   double tol;
 };
 
+// number of work items of a grid (u rows, v rows, p rows in MDOT_CHUNK pieces)
+__host__ __device__ inline long mdot_items(const Geo& g) {
+  const long cu = (g.imax() + MDOT_CHUNK - 1) / MDOT_CHUNK, cv = (g.nx + MDOT_CHUNK - 1) / MDOT_CHUNK;
+  return (long)g.ny * cu + (long)g.jmax() * cv + (long)g.ny * cv;
+}
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_mdot(MdotArgs<T> a) {
+__global__ void __launch_bounds__(MDOT_TPB) k_mdot(MdotArgs<T> a) {
   if (!a.ks->active) return;
-  __shared__ DD sh[32];
+  constexpr int NW = MDOT_TPB / 32;
+  __shared__ DD wsum[NW];
+  __shared__ double dsum[MDOT_MAXV];
   __shared__ bool last;
-  __shared__ double dsum[128];
   const Geo g = a.g;
-  const int i = blockIdx.y;
-  const T* V = a.V0 + i * a.stride;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nx = g.nx, ny = g.ny, imax = g.imax(), jmax = g.jmax();
-  const long nu = (long)imax * ny, nv = (long)nx * jmax, np = (long)nx * ny;
+  const int cu = (imax + MDOT_CHUNK - 1) / MDOT_CHUNK, cv = (nx + MDOT_CHUNK - 1) / MDOT_CHUNK;
+  const long iu = (long)ny * cu, iv = (long)jmax * cv, ip = (long)ny * cv;
+  const long items = iu + iv + ip;
+  const T* V = a.V0 + blockIdx.y * a.stride;  // this grid row's vector
   DD acc{0.0, 0.0};
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nu + nv + np; q += (long)gridDim.x * blockDim.x) {
-    long e;
-    if (q < nu) {
-      e = g.at(1 + (int)(q % imax), 1 + (int)(q / imax));
-    } else if (q < nu + nv) {
-      const long r = q - nu;
-      e = a.n + g.at(1 + (int)(r % nx), 1 + (int)(r / nx));
+  for (long it = (long)blockIdx.x * NW + warp; it < items; it += (long)gridDim.x * NW) {
+    long base;
+    int len, c;
+    if (it < iu) {
+      c = (int)(it % cu);
+      base = g.at(1, 1 + (int)(it / cu));
+      len = imax;
+    } else if (it < iu + iv) {
+      const long r = it - iu;
+      c = (int)(r % cv);
+      base = a.n + g.at(1, 1 + (int)(r / cv));
+      len = nx;
     } else {
-      const long r = q - nu - nv;
-      e = 2 * a.n + g.at(1 + (int)(r % nx), 1 + (int)(r / nx));
+      const long r = it - iu - iv;
+      c = (int)(r % cv);
+      base = 2 * a.n + g.at(1, 1 + (int)(r / cv));
+      len = nx;
     }
-    dd_add(acc, (double(a.w[e]) * double(V[e])) * a.vol);
+    const int i1 = min(len, (c + 1) * MDOT_CHUNK);
+    for (int i = c * MDOT_CHUNK + lane; i < i1; i += 32) {
+      const long e = base + i;
+      dd_add(acc, (double(a.w[e]) * double(V[e])) * a.vol);
+    }
   }
-  const DD s = block_sum_dd(acc, sh);
+  for (int o = 16; o > 0; o >>= 1) acc = dd_merge(acc, dd_shfl_down(acc, o));
+  if (lane == 0) wsum[warp] = acc;
+  __syncthreads();
   if (threadIdx.x == 0) {
-    put_partial(a.part + 2L * i * gridDim.x, blockIdx.x, s);
+    DD s = wsum[0];
+    for (int k = 1; k < NW; ++k) s = dd_merge(s, wsum[k]);
+    put_partial(a.part + 2L * blockIdx.y * gridDim.x, blockIdx.x, s);
     __threadfence();
     const unsigned int t = atomicAdd(&a.ks->ticket, 1u);
     last = (t == gridDim.x * gridDim.y - 1);
@@ -142,10 +175,19 @@ __global__ void __launch_bounds__(256) k_mdot(MdotArgs<T> a) {
   __syncthreads();
   if (!last) return;
   __threadfence();
-  for (int v = 0; v < a.nvec; ++v) {
-    const double d = sum_partials_dd(a.part + 2L * v * gridDim.x, gridDim.x);
-    if (threadIdx.x == 0) dsum[v] = d;
+  for (int v = warp; v < a.nvec; v += NW) {
+    const double* pv = a.part + 2L * v * gridDim.x;
+    DD s{0.0, 0.0};
+    for (int k = lane; k < (int)gridDim.x; k += 32) {
+      DD q;
+      q.hi = __ldcg(pv + 2 * k);
+      q.lo = __ldcg(pv + 2 * k + 1);
+      s = dd_merge(s, q);
+    }
+    for (int o = 16; o > 0; o >>= 1) s = dd_merge(s, dd_shfl_down(s, o));
+    if (lane == 0) dsum[v] = s.hi + s.lo;
   }
+  __syncthreads();
   if (threadIdx.x == 0) {
     a.ks->ticket = 0;
     fg_op(a.op, dsum, a.j, a.tol, a.L, a.st, a.ks);
@@ -159,9 +201,12 @@ template <typename T>
 __global__ void k_maxpy(long n3, T* w, const T* V0, long stride, const double* coef, int nvec, double sign,
                         const int* active) {
   if (active && !*active) return;
+  __shared__ T s[MDOT_MAXV];  // the coefficients, converted once per CTA
+  for (int i = threadIdx.x; i < nvec; i += blockDim.x) s[i] = T(sign * coef[i]);
+  __syncthreads();
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n3; q += (long)gridDim.x * blockDim.x) {
     T x = w[q];
-    for (int i = 0; i < nvec; ++i) x = x + T(sign * coef[i]) * V0[i * stride + q];
+    for (int i = 0; i < nvec; ++i) x = x + s[i] * V0[i * stride + q];
     w[q] = x;
   }
 }

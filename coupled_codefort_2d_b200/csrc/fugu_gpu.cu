@@ -754,10 +754,14 @@ void mdot(fugu_ctx* c, const T* w, const T* V0, int nvec, int op, int j, double 
   a.op = op;
   a.j = j;
   a.tol = tol;
-  int S = (2 * c->nsm + nvec - 1) / nvec;
-  if (S < 2) S = 2;
-  if (2L * nvec * S > c->part_len) S = (int)(c->part_len / (2L * nvec));
-  k_mdot<T><<<dim3(S, nvec), DOT_TPB, 0, c->s>>>(a);
+  // about two CTAs per SM over all vectors, each with a work item per warp
+  const long per_cta = MDOT_TPB / 32;
+  long G = (2L * c->nsm + nvec - 1) / nvec;
+  const long gmax = (mdot_items(c->g) + per_cta - 1) / per_cta;
+  if (G > gmax) G = gmax;
+  if (G < 1) G = 1;
+  if (nvec > MDOT_MAXV || 2L * nvec * G > c->part_len) throw ApiError{FUGU_EINVAL, "k_mdot: too many vectors"};
+  k_mdot<T><<<dim3((unsigned)G, (unsigned)nvec), MDOT_TPB, 0, c->s>>>(a);
   CKL("k_mdot");
 }
 
@@ -1206,7 +1210,8 @@ void create(fugu_ctx* c) {
   if (env && std::strcmp(env, "cluster") == 0 && !(c->pcgc[0].ok && c->pcgc[1].ok))
     throw ApiError{FUGU_EINVAL, "FUGU_PCG=cluster but this grid does not fit a thread-block cluster"};
   c->dot_grid = c->nsm * 2;
-  c->part_len = 8L * (c->nsm * 8 + 64);
+  // CTA partials: the reductions' 8 per CTA, or k_mdot's 2 per vector and CTA
+  c->part_len = std::max(8L * (c->nsm * 8 + 64), 2L * MDOT_MAXV * c->nsm);
   c->part = dalloc<double>(c, c->part_len);
   c->gs = dalloc<GridSync>(c, 1);
   c->pcg_out = dalloc<PcgOut>(c, 1);
