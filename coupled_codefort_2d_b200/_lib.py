@@ -124,6 +124,8 @@ SIGNATURES = {
     "fugu_batch_size": (_i, [_vp]),
     "fugu_batch_case": (_i, [_vp, _i, _vp]),
     "fugu_batch_run": (_i, [_vp, _i] + [_vp] * 6),
+    "fugu_matvec_coupled_t": (_i, [_vp] * 15 + [_d] + [_vp] * 4),
+    "fugu_adjoint_solve": (_i, [_vp] * 15 + [_d, _d] + [_vp] * 5),
 }
 
 

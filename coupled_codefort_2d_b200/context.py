@@ -277,6 +277,30 @@ class Context:
             C.byref(st)))
         return st.as_dict()
 
+    # ------------------------------------------------------ discrete adjoint
+    def matvec_coupled_t(self, Y_u, Y_v, Y_p, X_u, X_v, X_p, u_adv, v_adv, rho_c, rho_u, rho_v, kappa, zeta, eta,
+                         dt_step, penalty_u=None, penalty_v=None, mdot_u_cons=None, mdot_v_cons=None):
+        """X = A^T Y for the solvers' operator A: x -> matvec_coupled(BC(x)) on
+        the owned unknowns (no counterpart in the reference)."""
+        self._ck(self.L.fugu_matvec_coupled_t(
+            self.h, self._f(Y_u, "u"), self._f(Y_v, "v"), self._f(Y_p, "cell"), self._f(X_u, "u"),
+            self._f(X_v, "v"), self._f(X_p, "cell"), self._f(u_adv, "u"), self._f(v_adv, "v"),
+            self._f(rho_c, "cell"), self._f(rho_u, "u"), self._f(rho_v, "v"), self._f(kappa, "cell"),
+            self._f(zeta, "vert"), self._f(eta, "vert"), float(dt_step), self._o(penalty_u, "u"),
+            self._o(penalty_v, "v"), self._o(mdot_u_cons, "u"), self._o(mdot_v_cons, "v")))
+
+    def adjoint_solve(self, g_u, g_v, g_p, lam_u, lam_v, lam_p, u_adv, v_adv, rho_c, rho_u, rho_v, kappa, zeta, eta,
+                      dt_step, tol=1e-10, penalty_u=None, penalty_v=None, mdot_u_cons=None, mdot_v_cons=None) -> dict:
+        """Solve A^T lambda = g (no counterpart in the reference)."""
+        st = FuguStats()
+        self._ck(self.L.fugu_adjoint_solve(
+            self.h, self._f(g_u, "u"), self._f(g_v, "v"), self._f(g_p, "cell"), self._f(lam_u, "u"),
+            self._f(lam_v, "v"), self._f(lam_p, "cell"), self._f(u_adv, "u"), self._f(v_adv, "v"),
+            self._f(rho_c, "cell"), self._f(rho_u, "u"), self._f(rho_v, "v"), self._f(kappa, "cell"),
+            self._f(zeta, "vert"), self._f(eta, "vert"), float(dt_step), float(tol), self._o(penalty_u, "u"),
+            self._o(penalty_v, "v"), self._o(mdot_u_cons, "u"), self._o(mdot_v_cons, "v"), C.byref(st)))
+        return st.as_dict()
+
     def bicgstab_solve(self, *a, **kw) -> dict:
         """``bicgstab_solve`` (mod_bicgstab2.f90:77-264); returns stats with
         iter (iter_out) and res (res_out)."""

@@ -22,9 +22,11 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "fugu_gpu.h"
+#include "adjoint.cuh"
 #include "fgmres.cuh"
 #include "kernels.cuh"
 #include "pcg_cluster.cuh"
@@ -132,6 +134,11 @@ struct fugu_ctx {
   FgWork<float> fg32;
   int pcg_cap_cur = 0;    // PCG cap of the PCD during an adaptive solve (0: pcg_max_iter)
   int pcg_cap_state = 0;  // cap the last adaptive solve ended with (carried to the next)
+  // adjoint: the probed stencil of the coupled operator; while adj_on, the
+  // solvers' operator is S A^T S instead of A
+  double* adj_val = nullptr;
+  unsigned int* adj_err = nullptr;
+  bool adj_on = false;
   // routine-level scratch
   double* scratch[20] = {};
   // device scalars / state
@@ -284,6 +291,17 @@ Coefs<T> coefs_of(const CoefBufs<T>& b, const SolveOpt& o) {
 template <typename T>
 void matvec(fugu_ctx* c, const CoefBufs<T>& cb, const SolveOpt& o, Trip<T> X, Trip<T> Y, double dt,
             const int* active) {
+  if (c->adj_on) {  // adjoint solve: the sign-conjugated transpose from the probed stencil
+    if constexpr (std::is_same<T, double>::value) {
+      Box b = box_launch(c->g);
+      k_adj_apply_t<<<b.grid, b.block, 0, c->s>>>(c->g, c->n, c->adj_val, X.base, Y.base, -1.0, active,
+                                                   &c->ks->matvecs);
+      CKL("k_adj_apply_t");
+      return;
+    } else {
+      throw ApiError{FUGU_EINVAL, "the adjoint solve runs in FP64"};
+    }
+  }
   halo(c, X.u, K_U, active);
   halo(c, X.v, K_V, active);
   halo(c, X.p, K_CELL, active);
@@ -1592,6 +1610,52 @@ void down_trip(fugu_ctx* c, Trip<double> t, double* u, double* v, double* p) {
   if (p) down(c, p, t.p, K_CELL);
 }
 
+// colour period of the stencil probe along one direction: 5 on a wall-bounded
+// extent; on a periodic one the smallest divisor >= 5 of the extent, so
+// colours stay 5 apart across the wrap
+int probe_period(int len, bool periodic) {
+  if (!periodic) return 5;
+  if (len < 5) throw ApiError{FUGU_EINVAL, "the adjoint needs at least 5 cells along a periodic direction"};
+  for (int q = 5; q < len; ++q)
+    if (len % q == 0) return q;
+  return len;
+}
+
+// Probe the coupled operator x_owned -> (A . BC(x))_owned (BC: the homogeneous
+// wall BCs the Krylov solvers apply before each product) with coloured unit
+// vectors and store its stencil in c->adj_val.
+void adj_assemble(fugu_ctx* c, const CoefBufs<double>& cb, const SolveOpt& o, double dt) {
+  if (!c->adj_val) {
+    c->adj_val = dalloc<double>(c, (long)ADJ_SLOTS * c->n);
+    c->adj_err = dalloc<unsigned int>(c, 1);
+  }
+  CK(cudaMemsetAsync(c->adj_val, 0, sizeof(double) * ADJ_SLOTS * c->n, c->s));
+  CK(cudaMemsetAsync(c->adj_err, 0, sizeof(unsigned int), c->s));
+  const int qx = probe_period(c->g.nx, c->g.px), qy = probe_period(c->g.ny, c->g.py);
+  Trip<double> X = ST(c, 16), Y = ST(c, 17);
+  Box b = box_launch(c->g);
+  const bool was_on = c->adj_on;
+  c->adj_on = false;
+  for (int cc = 0; cc < 3; ++cc)
+    for (int a = 0; a < qx; ++a)
+      for (int bb = 0; bb < qy; ++bb) {
+        CK(cudaMemsetAsync(X.base, 0, sizeof(double) * 3 * c->n, c->s));
+        k_adj_probe_set<<<b.grid, b.block, 0, c->s>>>(c->g, X.base, c->n, cc, qx, qy, a, bb);
+        CKL("k_adj_probe_set");
+        vbcs(c, X.u, X.v, 0.0);
+        matvec<double>(c, cb, o, X, Y, dt, nullptr);
+        k_adj_probe_collect<<<b.grid, b.block, 0, c->s>>>(c->g, Y.base, c->n, cc, qx, qy, a, bb, c->adj_val,
+                                                          c->adj_err);
+        CKL("k_adj_probe_collect");
+      }
+  c->adj_on = was_on;
+  unsigned int err = 0;
+  CK(cudaMemcpyAsync(&err, c->adj_err, sizeof(err), cudaMemcpyDeviceToHost, c->s));
+  sync(c);
+  if (err) throw ApiError{FUGU_ECUDA, "adjoint stencil probe: " + std::to_string(err) +
+                                          " operator entries beyond a 2-cell reach"};
+}
+
 }  // namespace
 
 extern "C" {
@@ -1743,6 +1807,80 @@ int fugu_krylov_solve(fugu_ctx* c, int solver, double* X_u, double* X_v, double*
       st->matvecs = (int)ks.matvecs;
     }
     down_trip(c, X, X_u, X_v, X_p);
+    sync(c);
+  });
+}
+
+int fugu_matvec_coupled_t(fugu_ctx* c, const double* Y_u, const double* Y_v, const double* Y_p, double* X_u,
+                          double* X_v, double* X_p, const double* u_adv, const double* v_adv, const double* rho_c,
+                          const double* rho_u, const double* rho_v, const double* kappa, const double* zeta,
+                          const double* eta, double dt, const double* penalty_u, const double* penalty_v,
+                          const double* mdot_u, const double* mdot_v) {
+  return guard(c, [&] {
+    CoefBufs<double> cb = up_coefs(c, u_adv, v_adv, rho_c, rho_u, rho_v, kappa, zeta, eta, penalty_u,
+                                   penalty_v, mdot_u, mdot_v);
+    SolveOpt o;
+    o.pen = penalty_u && penalty_v;
+    o.amp = mdot_u && mdot_v;
+    adj_assemble(c, cb, o, dt);
+    Trip<double> Y = ST(c, 0), X = ST(c, 1);
+    up_trip(c, Y, Y_u, Y_v, Y_p);
+    Box b = box_launch(c->g);
+    k_adj_apply_t<<<b.grid, b.block, 0, c->s>>>(c->g, c->n, c->adj_val, Y.base, X.base, 1.0, nullptr, nullptr);
+    CKL("k_adj_apply_t");
+    down_trip(c, X, X_u, X_v, X_p);
+    sync(c);
+  });
+}
+
+int fugu_adjoint_solve(fugu_ctx* c, const double* g_u, const double* g_v, const double* g_p, double* lam_u,
+                       double* lam_v, double* lam_p, const double* u_adv, const double* v_adv, const double* rho_c,
+                       const double* rho_u, const double* rho_v, const double* kappa, const double* zeta,
+                       const double* eta, double dt, double tol, const double* penalty_u, const double* penalty_v,
+                       const double* mdot_u, const double* mdot_v, fugu_stats* st) {
+  // the solve below runs the FP64 defect correction around flexible GMRES on
+  // S A^T S; the context's own settings come back however it ends
+  struct Restore {
+    fugu_ctx* c;
+    fugu_params prm;
+    ~Restore() {
+      c->prm = prm;
+      c->adj_on = false;
+    }
+  };
+  return guard(c, [&] {
+    Restore restore{c, c->prm};
+    CoefBufs<double> cb = up_coefs(c, u_adv, v_adv, rho_c, rho_u, rho_v, kappa, zeta, eta, penalty_u,
+                                   penalty_v, mdot_u, mdot_v);
+    SolveOpt o;
+    o.pen = penalty_u && penalty_v;
+    o.amp = mdot_u && mdot_v;
+    adj_assemble(c, cb, o, dt);
+    Trip<double> X = ST(c, 0), B = ST(c, 1);
+    zero_trip(c, X);
+    up_trip(c, B, g_u, g_v, g_p);
+    const int g1 = grid1d(c, c->n);
+    k_adj_flip_p<<<g1, 256, 0, c->s>>>(c->n, B.base);  // S g
+    CKL("k_adj_flip_p");
+    c->prm.refine = 2;
+    c->prm.precision = FUGU_FP64;
+    if (c->prm.refine_max_inner < 1 || c->prm.refine_max_inner > 127) c->prm.refine_max_inner = 30;
+    c->adj_on = true;
+    reset_counters(c);
+    int outer = 0;
+    KrylovResult kr = solve(c, 2, cb, o, X, B, dt, tol, 0, false, 0.0, &outer);
+    c->adj_on = false;
+    k_adj_flip_p<<<g1, 256, 0, c->s>>>(c->n, X.base);  // lambda = S mu
+    CKL("k_adj_flip_p");
+    if (st) std::memset(st, 0, sizeof(*st));
+    collect(c, st);
+    if (st) {
+      st->iter = kr.iter;
+      st->res = kr.res;
+      st->outer = outer;
+      st->status = kr.status;
+    }
+    down_trip(c, X, lam_u, lam_v, lam_p);
     sync(c);
   });
 }

@@ -258,6 +258,38 @@ int fugu_krylov_solve(fugu_ctx* ctx, int solver,
                       const double* penalty_u, const double* penalty_v,
                       const double* mdot_u, const double* mdot_v, fugu_stats* st);
 
+/* ------------------------------------------------ discrete adjoint
+ * No counterpart in the reference.  The linear map the Krylov solvers see is
+ * A: x -> (matvec_coupled(BC(x)))_owned (mod_operators.f90:341-443 after the
+ * homogeneous wall BCs, :254-333), on the owned unknowns (the coupled_dot set:
+ * interior u faces, v faces and cells).  Its stencil is measured on the
+ * device by probing with coloured unit vectors (about 75-200 products), then
+ * applied transposed by a gather kernel.  Arrays are reference-layout host
+ * arrays; entries outside the owned set are ignored on input and zero on
+ * output.  The coefficient arguments are matvec_coupled's (advection always
+ * included, as in the solvers). */
+/* X = A^T Y */
+int fugu_matvec_coupled_t(fugu_ctx* ctx, const double* Y_u, const double* Y_v, const double* Y_p,
+                          double* X_u, double* X_v, double* X_p,
+                          const double* u_adv, const double* v_adv,
+                          const double* rho_c, const double* rho_u, const double* rho_v,
+                          const double* kappa, const double* zeta, const double* eta, double dt,
+                          const double* penalty_u, const double* penalty_v,
+                          const double* mdot_u, const double* mdot_v);
+/* Solve A^T lambda = g to true relative residual tol: the FP64 defect
+ * correction around flexible GMRES on S A^T S (S flips the pressure block,
+ * which turns A^T back into A's block structure with the velocity block
+ * transposed) with the step's PCD as right preconditioner.  st reports the
+ * iterations; lambda's pressure block is defined up to the null space of
+ * A^T (a constant in a closed or periodic box). */
+int fugu_adjoint_solve(fugu_ctx* ctx, const double* g_u, const double* g_v, const double* g_p,
+                       double* lambda_u, double* lambda_v, double* lambda_p,
+                       const double* u_adv, const double* v_adv,
+                       const double* rho_c, const double* rho_u, const double* rho_v,
+                       const double* kappa, const double* zeta, const double* eta, double dt, double tol,
+                       const double* penalty_u, const double* penalty_v,
+                       const double* mdot_u, const double* mdot_v, fugu_stats* st);
+
 /* mod_vof.f90:38-140 (flux_x/flux_y may be NULL), :145-194 */
 int fugu_vof_advection_tvd(fugu_ctx* ctx, const double* c_in, double* c_out,
                            const double* u, const double* v, double dt,
