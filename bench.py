@@ -48,20 +48,24 @@ TOL = 1e-8
 # inner solve of the FP64 defect correction: flexible GMRES (refine 2) or the
 # step's BiCGStab(2) (refine 1); both around the same PCD preconditioner.
 # With flexible GMRES the PCG inside PCD starts capped at 40 iterations and
-# doubles its cap (up to the reference's 150) when an inner solve misses
-# its tolerance; BiCGStab keeps the fixed cap it needs.
+# the velocity smoothing at 6 Jacobi sweeps; an inner solve that misses its
+# tolerance doubles the cap (up to the reference's 150), then the sweeps (up
+# to 24).  BiCGStab keeps the reference's fixed preconditioner.
 INNER = {"fgmres": 2, "bicgstab2": 1}
 INNER_NAME = {2: "flexible GMRES(30)", 1: "BiCGStab(2)"}
 PCG_CAP_START = 40
+PCD_SWEEPS, PCD_SWEEPS_MAX = 6, 24
 
 
 def case_params(refine=2):
     from coupled_codefort_2d_b200.params import Params
 
+    fg = refine == 2
     return Params(rho1=1.0, rho2=0.1, mu1=0.1, mu2=0.01, sigma=1.0, gx=0.0, gy=0.0, time_order=2,
                   tol_bicgstab2=TOL, max_iter_bicgstab2=500, refine=refine, refine_inner_tol=1e-2,
                   refine_max_inner=30, refine_max_outer=60, krylov_bc_fix=1,
-                  pcg_cap_start=PCG_CAP_START if refine == 2 else 0)
+                  pcg_cap_start=PCG_CAP_START if fg else 0, pcd_sweeps=PCD_SWEEPS if fg else 3,
+                  pcd_sweeps_max=PCD_SWEEPS_MAX if fg else 0)
 
 
 def initial_state(g, prm):
@@ -476,7 +480,8 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 outer",
         "data": "synthetic (droplet case fully determined by its parameters)",
         "config": workload_config(f"FP64 defect correction around FP32 {INNER_NAME[INNER[args.inner]]}+PCD "
-                                  "(inner tol 1e-2" + (f", PCD PCG cap adaptive from {PCG_CAP_START} to 150)"
+                                  "(inner tol 1e-2" + (f", PCD PCG cap adaptive {PCG_CAP_START}-150, sweeps "
+                                                       f"{PCD_SWEEPS}-{PCD_SWEEPS_MAX})"
                                                        if INNER[args.inner] == 2 else ")")),
         "max_true_residual": max(r["res"] for r in s_m),
         "per_step": {"outer": [r["outer"] for r in s_m], "inner_iters": [r["iter"] for r in s_m],

@@ -134,6 +134,8 @@ struct fugu_ctx {
   FgWork<float> fg32;
   int pcg_cap_cur = 0;    // PCG cap of the PCD during an adaptive solve (0: pcg_max_iter)
   int pcg_cap_state = 0;  // cap the last adaptive solve ended with (carried to the next)
+  int pcd_sweeps_cur = 0;    // PCD Jacobi sweeps during an adaptive solve (0: pcd_sweeps)
+  int pcd_sweeps_state = 0;  // sweeps the last adaptive solve ended with
   // adjoint: the probed stencil of the coupled operator; while adj_on, the
   // solvers' operator is S A^T S instead of A
   double* adj_val = nullptr;
@@ -571,11 +573,12 @@ void pcd(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const SolveOpt& o
   halo(c, r.p, K_CELL, active);
   k_pcd_zwork<T><<<b.grid, b.block, 0, c->s>>>(c->g, z.u, z.v, r.p, pw.zuw, pw.zvw, active);
   CKL("k_pcd_zwork");
-  helmholtz<T>(c, false, r.v, pw.tmp, pw.zvw, cb, o, dt, c->prm.pcd_sweeps, active);
+  const int sweeps = c->pcd_sweeps_cur > 0 ? c->pcd_sweeps_cur : c->prm.pcd_sweeps;
+  helmholtz<T>(c, false, r.v, pw.tmp, pw.zvw, cb, o, dt, sweeps, active);
   halo(c, r.v, K_V, active);
   k_pcd_cross<T><<<b.grid, b.block, 0, c->s>>>(c->g, cb.eta, r.v, pw.zuw, active);
   CKL("k_pcd_cross");
-  helmholtz<T>(c, true, r.u, pw.tmp, pw.zuw, cb, o, dt, c->prm.pcd_sweeps, active);
+  helmholtz<T>(c, true, r.u, pw.tmp, pw.zuw, cb, o, dt, sweeps, active);
   halo(c, r.u, K_U, active);
 }
 
@@ -902,12 +905,19 @@ KrylovResult refine_solve(fugu_ctx* c, int solver, const CoefBufs<double>& cb64,
   // double it after a pass whose inner solve missed its tolerance; the guard
   // restores the fixed cap however the solve ends
   const bool adapt = c->prm.refine == 2 && c->prm.pcg_cap_start > 0;
+  // likewise the PCD's Jacobi sweeps once the cap cannot grow
+  const bool adapt_sw = c->prm.refine == 2 && c->prm.pcd_sweeps_max > c->prm.pcd_sweeps;
   struct CapGuard {
     fugu_ctx* c;
-    ~CapGuard() { c->pcg_cap_cur = 0; }
+    ~CapGuard() {
+      c->pcg_cap_cur = 0;
+      c->pcd_sweeps_cur = 0;
+    }
   } cap_guard{c};
   if (adapt)
     c->pcg_cap_cur = std::min(std::max(c->prm.pcg_cap_start, c->pcg_cap_state), c->prm.pcg_max_iter);
+  if (adapt_sw)
+    c->pcd_sweeps_cur = std::min(std::max(c->prm.pcd_sweeps, c->pcd_sweeps_state), c->prm.pcd_sweeps_max);
   for (;; ++outer) {
     matvec<double>(c, cb64, o, X, ax, dt, nullptr);
     lin<double>(c, r, B, -1.0, c->sc + S_ONE, ax);
@@ -935,13 +945,18 @@ KrylovResult refine_solve(fugu_ctx* c, int solver, const CoefBufs<double>& cb64,
       lin<double>(c, X, X, 1.0, c->sc + S_ONE, d);
     }
     inner_total += ir.iter;
-    if (adapt && !(ir.res < c->prm.refine_inner_tol) && c->pcg_cap_cur < c->prm.pcg_max_iter)
-      c->pcg_cap_cur = std::min(2 * c->pcg_cap_cur, c->prm.pcg_max_iter);
+    if (!(ir.res < c->prm.refine_inner_tol)) {
+      if (adapt && c->pcg_cap_cur < c->prm.pcg_max_iter)
+        c->pcg_cap_cur = std::min(2 * c->pcg_cap_cur, c->prm.pcg_max_iter);
+      else if (adapt_sw && c->pcd_sweeps_cur < c->prm.pcd_sweeps_max)
+        c->pcd_sweeps_cur = std::min(2 * c->pcd_sweeps_cur, c->prm.pcd_sweeps_max);
+    }
     reset_ks(c);
     vbcs(c, X.u, X.v, 0.0);
   }
   if (has_lid) vbcs(c, X.u, X.v, lid);
   if (adapt) c->pcg_cap_state = c->pcg_cap_cur;
+  if (adapt_sw) c->pcd_sweeps_state = c->pcd_sweeps_cur;
   res.iter = inner_total;
   res.res = rel;
   if (outer_out) *outer_out = outer;
@@ -1165,6 +1180,9 @@ int check_params(const fugu_params* p) {
   if (p->nx < 4 || p->ny < 4 || p->nx > 65536 || p->ny > 65536) return FUGU_EINVAL;
   if (!(p->dx > 0.0) || !(p->dy > 0.0)) return FUGU_EINVAL;
   if (p->pcg_max_iter < 0 || p->pcd_sweeps < 0 || p->svof_max_iter < 0 || p->pcg_cap_start < 0) return FUGU_EINVAL;
+  if (p->pcd_sweeps_max < 0 || p->pcd_sweeps_max > 1024) return FUGU_EINVAL;
+  // the sweeps double from pcd_sweeps, which must be > 0 for that
+  if (p->refine == 2 && p->pcd_sweeps_max > p->pcd_sweeps && p->pcd_sweeps < 1) return FUGU_EINVAL;
   if (p->precision == FUGU_MIXED && !p->refine) return FUGU_EINVAL;
   if (p->refine < 0 || p->refine > 2) return FUGU_EINVAL;
   // flexible GMRES keeps one projection per basis vector in shared memory
@@ -1347,7 +1365,8 @@ int fugu_set_params(fugu_ctx* c, const fugu_params* p) {
   }
   c->prm = *p;
   c->g = make_geo(*p);
-  c->pcg_cap_state = 0;  // the adaptive PCG cap restarts from pcg_cap_start
+  c->pcg_cap_state = 0;  // the adaptive PCG cap and sweeps restart from their starts
+  c->pcd_sweeps_state = 0;
   return FUGU_OK;
 }
 

@@ -23,7 +23,7 @@ import numpy as np
 from . import cases
 
 SOLVER = dict(tol_bicgstab2=1e-8, max_iter_bicgstab2=500, refine=2, refine_inner_tol=1e-2, refine_max_inner=30,
-              refine_max_outer=60, krylov_bc_fix=1, pcg_cap_start=40)
+              refine_max_outer=60, krylov_bc_fix=1, pcg_cap_start=40, pcd_sweeps=6, pcd_sweeps_max=24)
 DT = 5e-4
 
 

@@ -49,6 +49,9 @@ class Params:
     # refine = 2: PCD's PCG starts at this cap and doubles it up to pcg_max_iter
     # after an outer pass whose inner solve missed refine_inner_tol (0 = off)
     pcg_cap_start: int = 0
+    # refine = 2: when the PCG cap cannot grow, a missed inner tolerance doubles
+    # the PCD's Jacobi sweeps up to this many (<= pcd_sweeps: off)
+    pcd_sweeps_max: int = 0
 
     def with_(self, **kw) -> "Params":
         return replace(self, **kw)

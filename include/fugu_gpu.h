@@ -87,6 +87,11 @@ typedef struct {
                                  PCG at this many iterations and doubles it (up
                                  to pcg_max_iter) after every outer pass whose
                                  flexible GMRES missed refine_inner_tol       */
+  int pcd_sweeps_max;         /* refine = 2 only; > pcd_sweeps: once the PCG
+                                 cap is at pcg_max_iter (or fixed), a missed
+                                 refine_inner_tol doubles the PCD's Jacobi
+                                 sweeps instead, up to this many; carried
+                                 from step to step like the cap              */
 } fugu_params;
 
 /* Optional arguments of advance_coupled_step (src/mod_solver_coupled.f90:137-160):

@@ -1009,6 +1009,11 @@ static void refine_solve(const kctx* c, int solver, trip X, trip B, double tol, 
   const int adapt = m->refine == 2 && m->pcg_cap_start > 0;
   int cap = adapt && m->pcg_cap_start < m->pcg_max_iter ? m->pcg_cap_start : m->pcg_max_iter;
   if (adapt && c->st && c->st->pcg_cap > cap) cap = c->st->pcg_cap < m->pcg_max_iter ? c->st->pcg_cap : m->pcg_max_iter;
+  /* adaptive PCD sweeps (refine = 2 with pcd_sweeps_max > pcd_sweeps) */
+  const int adapt_sw = m->refine == 2 && m->pcd_sweeps_max > m->pcd_sweeps;
+  int sweeps = m->pcd_sweeps;
+  if (adapt_sw && c->st && c->st->pcd_sweeps > sweeps)
+    sweeps = c->st->pcd_sweeps < m->pcd_sweeps_max ? c->st->pcd_sweeps : m->pcd_sweeps_max;
   fo_apply_velocity_bcs(m, X.u, X.v, 0, 0.0);
   double nb = sqrt(cdot(m, B, B));
   if (nb < 1.0e-300) nb = 1.0;
@@ -1027,12 +1032,18 @@ static void refine_solve(const kctx* c, int solver, trip X, trip B, double tol, 
       /* the PCD of this pass runs its PCG at the current cap */
       fo_model mm = *m;
       mm.pcg_max_iter = cap;
+      mm.pcd_sweeps = sweeps;
       kctx cc = *c;
       cc.m = &mm;
       fgmres(&cc, d, r, m->refine_inner_tol, m->refine_max_inner, &it, &ires);
-      /* a pass whose inner solve missed its tolerance doubles the cap */
-      if (adapt && !(ires < m->refine_inner_tol) && cap < m->pcg_max_iter)
-        cap = 2 * cap < m->pcg_max_iter ? 2 * cap : m->pcg_max_iter;
+      /* a pass whose inner solve missed its tolerance doubles the cap, or,
+       * once the cap cannot grow, the PCD sweeps */
+      if (!(ires < m->refine_inner_tol)) {
+        if (adapt && cap < m->pcg_max_iter)
+          cap = 2 * cap < m->pcg_max_iter ? 2 * cap : m->pcg_max_iter;
+        else if (adapt_sw && sweeps < m->pcd_sweeps_max)
+          sweeps = 2 * sweeps < m->pcd_sweeps_max ? 2 * sweeps : m->pcd_sweeps_max;
+      }
     } else if (solver == 2) {
       bicgstab2(c, d, r, m->refine_inner_tol, m->refine_max_inner, 0, 0.0, &it, &ires);
     } else {
@@ -1044,6 +1055,7 @@ static void refine_solve(const kctx* c, int solver, trip X, trip B, double tol, 
   }
   if (c->st) c->st->outer += outer;
   if (adapt && c->st) c->st->pcg_cap = cap;
+  if (adapt_sw && c->st) c->st->pcd_sweeps = sweeps;
   if (has_lid) fo_apply_velocity_bcs(m, X.u, X.v, 1, u_lid);
   if (iter_out) *iter_out = inner_total;
   if (res_out) *res_out = rel;

@@ -71,6 +71,9 @@ typedef struct {
    * pcg_cap_start iterations and doubles the cap (up to pcg_max_iter) after
    * each outer pass whose flexible GMRES missed refine_inner_tol; 0 = off */
   int pcg_cap_start;
+  /* refine = 2: once the cap cannot grow, a missed inner tolerance doubles
+   * the PCD's Jacobi sweeps up to pcd_sweeps_max (<= pcd_sweeps: off) */
+  int pcd_sweeps_max;
 } fo_model;
 
 void fo_model_defaults(fo_model* m);
@@ -103,6 +106,7 @@ typedef struct {
                                pcg_cap_start > 0): the cap a solve starts
                                from (0: pcg_cap_start) and ends with; the
                                caller carries it from step to step         */
+  int pcd_sweeps;           /* in/out, adaptive PCD sweeps, as pcg_cap     */
 } fo_stats;
 
 /* --- mod_mpi single-rank halo semantics (mod_mpi.f90:113-245) ---------- */

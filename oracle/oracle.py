@@ -32,6 +32,7 @@ class FoModel(C.Structure):
         ("svof_tol", C.c_double), ("limiter", C.c_int), ("free_slip_x", C.c_int),
         ("krylov_bc_fix", C.c_int), ("refine", C.c_int), ("refine_inner_tol", C.c_double),
         ("refine_max_inner", C.c_int), ("refine_max_outer", C.c_int), ("pcg_cap_start", C.c_int),
+        ("pcd_sweeps_max", C.c_int),
     ]
 
 
@@ -49,6 +50,7 @@ class FoStats(C.Structure):
     _fields_ = [
         ("iter", C.c_int), ("res", C.c_double), ("pcg_iters", C.c_long), ("pcg_calls", C.c_int),
         ("svof_iters", C.c_int), ("matvecs", C.c_int), ("outer", C.c_int), ("pcg_cap", C.c_int),
+        ("pcd_sweeps", C.c_int),
     ]
 
 
@@ -102,6 +104,7 @@ class Oracle:
         self.m = model(g, prm)
         self.L = lib()
         self.pcg_cap = 0  # adaptive PCG cap carried from solve to solve (refine = 2)
+        self.pcd_sweeps = 0  # adaptive PCD sweeps, likewise
 
     def halo(self, kind, a):
         fn = {"cell": self.L.fo_halo_scalar, "u": self.L.fo_halo_u, "v": self.L.fo_halo_v}[kind]
@@ -176,6 +179,7 @@ class Oracle:
         res = C.c_double(0.0)
         st = FoStats()
         st.pcg_cap = self.pcg_cap
+        st.pcd_sweeps = self.pcd_sweeps
         self.L.fo_krylov_solve(C.byref(self.m), int(solver), P(X[0]), P(X[1]), P(X[2]),
                                P(B[0]), P(B[1]), P(B[2]), P(uadv), P(vadv), P(pr["rho_c"]),
                                P(pr["rho_u"]), P(pr["rho_v"]), P(pr["kappa"]), P(pr["zeta"]),
@@ -183,6 +187,7 @@ class Oracle:
                                D(0.0 if u_lid is None else u_lid), P(pen_u), P(pen_v), P(mdu), P(mdv),
                                C.byref(it), C.byref(res), C.byref(st))
         self.pcg_cap = st.pcg_cap
+        self.pcd_sweeps = st.pcd_sweeps
         return it.value, res.value, st
 
     def vof(self, c_in, c_out, u, v, dt, fx=None, fy=None):
@@ -227,12 +232,14 @@ class Oracle:
         o.v_solid = 0.0 if v_solid is None else v_solid
         stats = FoStats()
         stats.pcg_cap = self.pcg_cap
+        stats.pcd_sweeps = self.pcd_sweeps
         self.L.fo_advance_coupled_step(
             C.byref(self.m), P(st["u_vel"]), P(st["v_vel"]), P(st["p_field"]), P(st["c_field"]),
             P(st["u_prev"]), P(st["v_prev"]), P(st["rho_c"]), P(st["rho_u"]), P(st["rho_v"]),
             P(st["kappa"]), P(st["zeta"]), P(st["eta"]), P(st["kappa_curv"]), P(st["f_sigma_u"]),
             P(st["f_sigma_v"]), D(dt), int(step_idx), C.byref(o), C.byref(stats))
         self.pcg_cap = stats.pcg_cap
+        self.pcd_sweeps = stats.pcd_sweeps
         return stats
 
     def write_checkpoint(self, path, step, t, st):

@@ -121,15 +121,19 @@ def test_step_parity_grid_wide_pcg(gpu, oracle_mod, name, monkeypatch):
         np.testing.assert_array_equal(st_g[k], st_o[k], err_msg=k)
 
 
-@pytest.mark.parametrize("name,refine,cap0", [("droplet", 1, 0), ("droplet", 2, 0), ("bubble_freeslip", 2, 0),
-                                              ("droplet", 2, 3), ("bubble_freeslip", 2, 2)])
-def test_refine_fp64_parity(gpu, oracle_mod, name, refine, cap0):
+@pytest.mark.parametrize("name,refine,cap0,swmax", [("droplet", 1, 0, 0), ("droplet", 2, 0, 0),
+                                                    ("bubble_freeslip", 2, 0, 0), ("droplet", 2, 3, 0),
+                                                    ("bubble_freeslip", 2, 2, 0), ("bubble_freeslip", 2, 2, 8)])
+def test_refine_fp64_parity(gpu, oracle_mod, name, refine, cap0, swmax):
     """FP64 defect correction around BiCGStab (refine 1) or flexible GMRES
     (refine 2): same outer and inner iteration counts as the oracle, and the
     same bits.  cap0 > 0 runs the adaptive PCG cap from a start so low that
-    it must grow, and carries it across the steps on both sides."""
+    it must grow, swmax > 0 then also the PCD sweeps from 1; both carry
+    across the steps on both sides."""
     over = dict(refine=refine, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=30, krylov_bc_fix=1,
                 tol_bicgstab2=1e-9, pcg_cap_start=cap0)
+    if swmax:  # a low PCG ceiling, so that the sweeps must grow too
+        over.update(pcd_sweeps=1, pcd_sweeps_max=swmax, pcg_max_iter=8)
     g, st_o, st_g, hist = run_pair(oracle_mod, name, over)
     for so, sg in hist:
         assert sg["res"] < 1e-9 and so.res < 1e-9
