@@ -185,3 +185,145 @@ def torch_flux_function(problem: SteadyPoiseuille):
             return gout * grads
 
     return SteadyFlux.apply
+
+
+class StartupPoiseuille(SteadyPoiseuille):
+    """The two-phase Poiseuille channel started from rest: N steps of
+    advance_coupled_step's time discretisation (BDF1 first, then BDF2:
+    ``mod_solver_coupled.f90:196-201, 268-303``), J = g . u^N (the mean
+    velocity after N steps), and its gradient by the multi-step discrete
+    adjoint with checkpointing.
+
+    Step s solves A_s X^s = B_s with B_s = M (c1 u^(s-1) + c0 u^(s-2)) + rho g
+    (M = rho/dt on the velocity rows; c1, c0 = 1, 0 for BDF1 and 2, -1/2 for
+    BDF2) and A_s the coupled operator at dt_eff (dt, then dt/1.5), its
+    advecting velocity the AB extrapolation 2u^(s-1) - u^(s-2).  The adjoint
+    runs backwards:
+
+        A_s^T lam^s = [s = N] g + M (c1_(s+1) lam^(s+1) + c0_(s+2) lam^(s+2)),
+        dJ/dtheta   = -sum_s lam^s . (dA_s/dtheta) X^s.
+
+    The coefficient fields (colour, densities, viscosities, advecting
+    velocity) are held at their forward values: exact here, where the flow
+    stays parallel to the layers, so C does not move and the advection terms
+    vanish along every sensitivity (checked against ``fugu_step`` and finite
+    differences in the tests).  States X^s are kept every ``checkpoint``
+    steps and recomputed in between during the backward sweep.
+    """
+
+    def __init__(self, nx=16, ny=32, nsteps=20, dt=0.05, checkpoint=5, **kw):
+        super().__init__(nx=nx, ny=ny, **kw)
+        self.nsteps, self.dt, self.checkpoint = nsteps, dt, checkpoint
+        self.recomputed_steps = 0
+
+    def params(self, mu1, mu2) -> Params:
+        return super().params(mu1, mu2).with_(time_order=2)
+
+    def _coeffs(self, s):
+        bdf2 = s >= 2
+        return (2.0, -0.5, self.dt / 1.5) if bdf2 else (1.0, 0.0, self.dt)
+
+    def _step(self, pr, s, u1, u2):
+        """X^s from u^(s-1) (u1) and u^(s-2) (u2), triples of host arrays."""
+        g = self.g
+        c1, c0, dt_eff = self._coeffs(s)
+        mu_, mv_, _ = owned_masks(g)
+        B = [g.zeros("u"), g.zeros("v"), g.zeros("cell")]
+        B[0][mu_] = ((pr["rho_u"] / self.dt) * (c1 * u1[0] + c0 * u2[0]) + pr["rho_u"] * self.gx)[mu_]
+        B[1][mv_] = ((pr["rho_v"] / self.dt) * (c1 * u1[1] + c0 * u2[1]))[mv_]
+        ua = u1[0] if s == 1 else 2.0 * u1[0] - u2[0]
+        va = u1[1] if s == 1 else 2.0 * u1[1] - u2[1]
+        X = [a.copy(order="F") for a in u1]  # the previous step's state is the initial guess
+        self.ctx.bicgstab2_solve(*X, *B, np.asfortranarray(ua), np.asfortranarray(va), pr["rho_c"], pr["rho_u"],
+                                 pr["rho_v"], pr["kappa"], pr["zeta"], pr["eta"], dt_eff, tol_in=self.tol,
+                                 max_iter_in=500)
+        self.ctx.apply_velocity_bcs(X[0], X[1], None)
+        return X, (np.asfortranarray(ua), np.asfortranarray(va), dt_eff)
+
+    def _run(self, pr, s0, X_prev, X_prev2, s1, keep=None):
+        """States from step s0 to s1 (inclusive) given X^(s0-1), X^(s0-2)."""
+        out = {}
+        for s in range(s0, s1 + 1):
+            X, _ = self._step(pr, s, X_prev, X_prev2)
+            if keep is None or s in keep:
+                out[s] = X
+            X_prev2, X_prev = X_prev, X
+        return out, X_prev, X_prev2
+
+    def trajectory_value(self, mu1, mu2):
+        g = self.g
+        pr, _ = self._setup(mu1, mu2)
+        zero = [g.zeros("u"), g.zeros("v"), g.zeros("cell")]
+        _, XN, _ = self._run(pr, 1, zero, zero, self.nsteps, keep=set())
+        return owned_dot(g, self.functional(), XN), XN
+
+    def value(self, mu1, mu2) -> float:
+        return self.trajectory_value(mu1, mu2)[0]
+
+    def value_and_grad(self, mu1, mu2):
+        g = self.g
+        N, K = self.nsteps, self.checkpoint
+        pr, _ = self._setup(mu1, mu2)
+        zero = [g.zeros("u"), g.zeros("v"), g.zeros("cell")]
+        # forward sweep: keep every K-th state and the one before it (BDF2
+        # restarts from the pair)
+        keep = {s for s in range(1, N + 1) if s % K == 0 or s % K == K - 1}
+        ck, XN, _ = self._run(pr, 1, zero, zero, N, keep=keep)
+        ck[0] = ck[-1] = zero
+        self.kept_states = len(keep)
+        gJ = self.functional()
+        J = owned_dot(g, gJ, XN)
+        dk = [mixture_derivatives(pr["kappa"], mu1, mu2, 2.0)[w] for w in (0, 1)]
+        dz = [mixture_derivatives(pr["zeta"], mu1, mu2, 2.0)[w] for w in (0, 1)]
+        de = [mixture_derivatives(pr["eta"], mu1, mu2, 1.0)[w] for w in (0, 1)]
+        grads = [0.0, 0.0]
+        lam_next, lam_next2 = None, None  # lambda^(s+1), lambda^(s+2)
+        segment = {0: zero, -1: zero}
+        self.recomputed_steps = 0
+        for s in range(N, 0, -1):
+            if any(k not in segment for k in (s, s - 1, s - 2) if k >= 1):
+                # recompute the checkpoint segment that ends at s from its stored pair
+                start = (s - 1) // K * K
+                if start >= 1 and s - 2 < start:  # X^(s-2) lies in the segment before
+                    start = (start - 1) // K * K
+                base1, base2 = ck[start], ck[start - 1]
+                segment, _, _ = self._run(pr, start + 1, base1, base2, s)
+                self.recomputed_steps += s - start
+                segment.update({start: base1, start - 1: base2, 0: zero, -1: zero})
+            X, X1, X2 = segment[s], segment[s - 1], segment[s - 2]
+            ua = X1[0] if s == 1 else 2.0 * X1[0] - X2[0]
+            va = X1[1] if s == 1 else 2.0 * X1[1] - X2[1]
+            _, _, dt_eff = self._coeffs(s)
+            rhs = [a.copy(order="F") for a in (gJ if s == N else zero)]
+            for lam, sp in ((lam_next, s + 1), (lam_next2, s + 2)):
+                if lam is None or sp > N:
+                    continue
+                c1, c0, _ = self._coeffs(sp)
+                c = c1 if sp == s + 1 else c0
+                rhs[0] = rhs[0] + c * (pr["rho_u"] / self.dt) * lam[0]
+                rhs[1] = rhs[1] + c * (pr["rho_v"] / self.dt) * lam[1]
+            mu_, mv_, mp_ = owned_masks(g)
+            rhs = [np.asfortranarray(np.where(m, a, 0.0)) for a, m in zip(rhs, (mu_, mv_, mp_))]
+            lam = [g.zeros("u"), g.zeros("v"), g.zeros("cell")]
+            co = (np.asfortranarray(ua), np.asfortranarray(va), pr["rho_c"], pr["rho_u"], pr["rho_v"], pr["kappa"],
+                  pr["zeta"], pr["eta"])
+            self.ctx.adjoint_solve(*rhs, *lam, *co, dt_eff, tol=self.tol)
+            for w in (0, 1):
+                grads[w] -= owned_dot(g, lam, self._dA_X_dt(X, co, dk[w], dz[w], de[w], dt_eff))
+            lam_next2, lam_next = lam_next, lam
+        return J, grads, {}
+
+    def _dA_X_dt(self, X, co, dk, dz, de, dt_eff):
+        g = self.g
+        Xb = [a.copy(order="F") for a in X]
+        self.ctx.apply_velocity_bcs(Xb[0], Xb[1], None)
+
+        def mv(k, z, e):
+            Y = [g.zeros("u"), g.zeros("v"), g.zeros("cell")]
+            Xc = [a.copy(order="F") for a in Xb]
+            self.ctx.matvec_coupled(*Xc, *Y, co[0], co[1], co[2], co[3], co[4], k, z, e, dt_eff)
+            return Y
+
+        Y1 = mv(dk, dz, de)
+        Y0 = mv(g.zeros("cell"), g.zeros("vert"), g.zeros("vert"))
+        return [a - b for a, b in zip(Y1, Y0)]

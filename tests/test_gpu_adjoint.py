@@ -11,6 +11,10 @@
    (h = 1e-5 relative) to 1e-6, and the analytic derivative of the two-layer
    profile to the discretisation error (2 %), also through the
    torch.autograd.Function harness.
+4. The start-up of the same channel over 12 BDF steps: the harness's time
+   stepping equals fugu_step on the device state, and the multi-step adjoint
+   with checkpointing (every 4th state kept, the rest recomputed) equals
+   central finite differences to 1e-6.
 """
 import numpy as np
 import pytest
@@ -145,3 +149,47 @@ def test_torch_autograd_harness(poiseuille):
     (2.0 * J).backward()
     _, grads, _ = poiseuille.value_and_grad(1.0, 0.1)
     np.testing.assert_allclose(mu.grad.numpy(), 2.0 * np.array(grads), rtol=1e-12)
+
+
+@pytest.fixture(scope="module")
+def startup(gpu):
+    p = adjoint.StartupPoiseuille(nx=16, ny=32, nsteps=12, dt=0.05, checkpoint=4)
+    yield p
+    p.close()
+
+
+def test_startup_forward_is_the_device_step(startup):
+    """The multi-step harness's time stepping equals advance_coupled_step on
+    the device-resident state (fugu_step): the coefficients it holds fixed do
+    not move in this flow."""
+    from coupled_codefort_2d_b200 import cases
+    from oracle import oracle as O
+
+    mu1, mu2 = 1.0, 0.1
+    J, XN = startup.trajectory_value(mu1, mu2)
+    g = startup.g
+    p = startup.params(mu1, mu2)
+    st = O.new_state(g, cases.initial_colour(g, "poiseuille"), p)
+    with Context(g, p) as ctx:
+        ctx.upload_state(st)
+        opts = ctx.step_opts(use_bicgstab2=True)
+        for s in range(1, startup.nsteps + 1):
+            ctx.step(startup.dt, s, opts)
+        u = ctx.download("u_vel")
+        c = ctx.download("c_field")
+    mu_, _, _ = adjoint.owned_masks(g)
+    assert np.linalg.norm(u[mu_] - XN[0][mu_]) <= 1e-9 * np.linalg.norm(XN[0][mu_])
+    np.testing.assert_allclose(c, st["c_field"], rtol=0, atol=1e-12)  # the layers do not move
+
+
+def test_startup_gradient_with_checkpointing_matches_fd(startup):
+    mu1, mu2 = 1.0, 0.1
+    J, grads, _ = startup.value_and_grad(mu1, mu2)
+    assert startup.kept_states < startup.nsteps and startup.recomputed_steps > 0
+    h1, h2 = 1e-5 * mu1, 1e-5 * mu2
+    fd1 = (startup.value(mu1 + h1, mu2) - startup.value(mu1 - h1, mu2)) / (2 * h1)
+    fd2 = (startup.value(mu1, mu2 + h2) - startup.value(mu1, mu2 - h2)) / (2 * h2)
+    assert abs(grads[0] - fd1) <= 1e-6 * abs(fd1), (grads[0], fd1)
+    assert abs(grads[1] - fd2) <= 1e-6 * abs(fd2), (grads[1], fd2)
+    # the start-up is still far from the steady profile: the gradient differs from the steady one
+    assert J < adjoint.analytic_mean_velocity(mu1, mu2)
