@@ -1,0 +1,164 @@
+"""Run the benchmark configurations and print their reports (one JSON object
+per configuration).
+
+    python -m coupled_codefort_2d_b200.configs c1            # lid-driven cavity, 128^2, 200 steps
+    python -m coupled_codefort_2d_b200.configs c2            # static droplet, 256^2, 500 steps
+    python -m coupled_codefort_2d_b200.configs c3 --steps N  # rising bubble, 320x640 (6000 steps to t = 3)
+
+c1: cavity on the unit square, rho = 1, mu = 1e-3 (Re = 1000), lid u = 1, BDF1,
+dt = 1e-2, tolerance 1e-10, zero initial fields.  The reference's own solver
+cannot reach 1e-10 (its BiCGStab(2) diverges on this case), so the plain FP64
+form here is the FP64 defect correction around flexible GMRES with the
+reference's PCD.  Reports the centreline extremes and the divergence.
+
+c2: static droplet (R = 0.25, rho 1 / 0.1, mu 0.1 / 0.01, sigma = 1, no
+gravity), area fractions by 16 x 16 sub-sampling, BDF2, dt = 1e-4, 500 steps,
+mixed precision and FP64.  Reports the spurious-current max |u|, the pressure
+jump against sigma / R (``tests/test_laplace_coupled.f90:129-159``) and mass.
+
+c3: rising bubble in a 1 x 2 box (R = 0.25 at (0.5, 0.5); outer rho 1000,
+mu 10; bubble rho 100, mu 1; sigma 24.5; g = 0.98), no-slip top and bottom,
+free-slip sides, BDF2, dt = 5e-4; the high-contrast variant has bubble rho 1,
+mu 0.1, sigma 1.96.  Mixed precision against FP64: centroid height, rise
+velocity (``tests/test_rising_bubble.f90:134-155``) and circularity, and their
+differences.
+
+Every run is synthetic: the fields are fully determined by the parameters.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import cases
+from ._lib import FIELD_KIND, FP64, MIXED
+from .context import Context
+from .layout import Grid, at
+from .params import Params
+
+SOLVER = dict(refine=2, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=60, krylov_bc_fix=1,
+              pcg_cap_start=40, pcd_sweeps=6, pcd_sweeps_max=24)
+STATE = ("u_vel", "v_vel", "p_field", "c_field", "u_prev", "v_prev", "rho_c", "rho_u", "rho_v", "kappa", "zeta",
+         "eta", "kappa_curv", "f_sigma_u", "f_sigma_v")
+
+
+def _run(g, prm, c0, precision, nsteps, dt, lid=None, every=None, device=0):
+    """Advance nsteps from rest; returns the final state, per-step stats and
+    seconds of stepping (CUDA-synchronised wall clock)."""
+    import torch
+
+    st = {k: g.zeros(FIELD_KIND[k]) for k in STATE}
+    st["c_field"][...] = c0
+    with Context(g, prm, device=device, precision=precision) as ctx:
+        ctx.compute_mixture_densities(st["c_field"], st["rho_c"], st["rho_u"], st["rho_v"])
+        ctx.compute_mixture_viscosities(st["c_field"], st["kappa"], st["zeta"], st["eta"])
+        ctx.upload_state(st)
+        opts = ctx.step_opts(use_bicgstab2=True, u_top_lid=lid)
+        stats, hist = [], []
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s in range(1, nsteps + 1):
+            stats.append(ctx.step(dt, s, opts))
+            if every and s % every == 0:
+                hist.append((s, ctx.download_state(["c_field", "v_vel"])))
+        torch.cuda.synchronize()
+        secs = time.perf_counter() - t0
+        out = ctx.download_state(list(STATE))
+    return out, stats, secs, hist
+
+
+def _summary(stats, secs):
+    return {"steps_per_s": len(stats) / secs, "max_true_residual": max(s["res"] for s in stats),
+            "failed_steps": sum(1 for s in stats if s["status"] != 0),
+            "mean_inner_iterations": float(np.mean([s["iter"] for s in stats]))}
+
+
+def config_c1(args):
+    n = 128
+    g = Grid(n, n)
+    prm = Params(rho1=1.0, rho2=1.0, mu1=1e-3, mu2=1e-3, sigma=0.0, gx=0.0, gy=0.0, time_order=1,
+                 tol_bicgstab2=1e-10, max_iter_bicgstab2=500, **SOLVER)
+    steps = args.steps or 200
+    st, stats, secs, _ = _run(g, prm, g.full("cell", 1.0), FP64, steps, 1e-2, lid=1.0, device=args.device)
+    u = st["u_vel"]
+    v = st["v_vel"]
+    # vertical centreline u(x = 0.5, y) and horizontal centreline v(x, y = 0.5)
+    uc = at(u, "u", n // 2, slice(1, n))  # u faces at x = 0.5
+    vc = at(v, "v", slice(1, n), n // 2)  # v faces at y = 0.5
+    return {"config": "c1", "workload": f"lid_driven_cavity_{n}x{n}_Re1000", "steps": steps, "dtype": "f64",
+            **_summary(stats, secs), "u_min_vertical_centreline": float(uc.min()),
+            "v_min_horizontal_centreline": float(vc.min()), "v_max_horizontal_centreline": float(vc.max()),
+            "max_divergence": cases.max_divergence(g, u, v)}
+
+
+def config_c2(args):
+    n = 256
+    g = Grid(n, n)
+    prm = Params(rho1=1.0, rho2=0.1, mu1=0.1, mu2=0.01, sigma=1.0, gx=0.0, gy=0.0, time_order=2,
+                 tol_bicgstab2=1e-8, max_iter_bicgstab2=500, **SOLVER)
+    steps = args.steps or 500
+    c0 = cases.circle_fraction(g, 0.5, 0.5, 0.25, inside=1.0, ns=16)
+    vol0 = cases.fluid1_volume(g, c0)
+    rep = {"config": "c2", "workload": f"static_droplet_{n}x{n}", "steps": steps, "sigma_over_R": 1.0 / 0.25}
+    finals = {}
+    for name, prec in (("mixed", MIXED), ("fp64", FP64)):
+        st, stats, secs, _ = _run(g, prm, c0, prec, steps, 1e-4, device=args.device)
+        umax = float(max(np.abs(at(st["u_vel"], "u", slice(1, n - 1), slice(1, n))).max(),
+                         np.abs(at(st["v_vel"], "v", slice(1, n), slice(1, n - 1))).max()))
+        dp = cases.laplace_jump(g, st["p_field"], 0.25)
+        rep[name] = {**_summary(stats, secs), "spurious_max_u": umax, "pressure_jump": dp,
+                     "pressure_jump_rel_error": abs(dp - 4.0) / 4.0,
+                     "mass_rel_change": abs(cases.fluid1_volume(g, st["c_field"]) - vol0) / vol0}
+        finals[name] = st
+    rep["mixed_vs_fp64"] = {k: float(np.linalg.norm(finals["mixed"][k] - finals["fp64"][k]) /
+                                     max(np.linalg.norm(finals["fp64"][k]), 1e-300)) for k in ("u_vel", "v_vel")}
+    return rep
+
+
+def config_c3(args):
+    g = Grid(320, 640, 1.0, 2.0)
+    if args.variant == "high_contrast":
+        phys = dict(rho1=1000.0, rho2=1.0, mu1=10.0, mu2=0.1, sigma=1.96)
+    else:
+        phys = dict(rho1=1000.0, rho2=100.0, mu1=10.0, mu2=1.0, sigma=24.5)
+    prm = Params(gx=0.0, gy=-0.98, time_order=2, tol_bicgstab2=1e-8, max_iter_bicgstab2=500, free_slip_x=1,
+                 **phys, **SOLVER)
+    steps = args.steps or 6000
+    dt = 5e-4
+    c0 = cases.binary_circle(g, 0.5, 0.5, 0.25, inside=0.0)
+    every = max(1, steps // 4)
+    rep = {"config": "c3", "workload": f"rising_bubble_320x640_{args.variant}", "steps": steps, "t": steps * dt}
+    hists = {}
+    for name, prec in (("mixed", MIXED), ("fp64", FP64)):
+        st, stats, secs, hist = _run(g, prm, c0, prec, steps, dt, every=every, device=args.device)
+        ycm, vr = cases.bubble_centroid_velocity(g, st["c_field"], st["v_vel"])
+        rep[name] = {**_summary(stats, secs), "y_centroid": ycm, "rise_velocity": vr,
+                     "circularity": cases.circularity(g, st["c_field"]),
+                     "bubble_volume": cases.bubble_volume(g, st["c_field"])}
+        hists[name] = [(s, cases.bubble_centroid_velocity(g, h["c_field"], h["v_vel"])) for s, h in hist]
+    m, f = rep["mixed"], rep["fp64"]
+    rep["mixed_vs_fp64"] = {"y_centroid_abs": abs(m["y_centroid"] - f["y_centroid"]),
+                            "rise_velocity_rel": abs(m["rise_velocity"] - f["rise_velocity"]) /
+                            max(abs(f["rise_velocity"]), 1e-300),
+                            "circularity_abs": abs(m["circularity"] - f["circularity"]),
+                            "history": [{"step": s, "y_mixed": a[0], "y_fp64": b[0], "v_mixed": a[1], "v_fp64": b[1]}
+                                        for (s, a), (_, b) in zip(hists["mixed"], hists["fp64"])]}
+    return rep
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description="run a benchmark configuration and print its report")
+    ap.add_argument("config", choices=["c1", "c2", "c3"])
+    ap.add_argument("--steps", type=int, default=0, help="override the configuration's step count")
+    ap.add_argument("--variant", default="standard", choices=["standard", "high_contrast"], help="c3 only")
+    ap.add_argument("--device", type=int, default=0)
+    args = ap.parse_args(argv)
+    rep = {"c1": config_c1, "c2": config_c2, "c3": config_c3}[args.config](args)
+    print(json.dumps(rep), flush=True)
+
+
+if __name__ == "__main__":
+    main()
