@@ -382,10 +382,10 @@ __global__ void k_poisson_coefs(Geo g, const double* rho_u, const double* rho_v,
 
 // PCD Schur step r_p = -((1/dt) phi + u.grad phi) (mod_pcd_precond.f90:54-62);
 // r_p is zero outside the interior (as after r_p = zero).
+// Each PCD step is an element function plus a thin whole-box kernel around it.
 template <typename T>
-__global__ void k_pcd_schur(Geo g, const T* phi, const T* ua, const T* va, T* rp, T inv_dt, const int* active) {
-  if (active && !*active) return;
-  FUGU_BOX_IJ
+__device__ __forceinline__ T pcd_schur_at(const Geo& g, int k, int i, int j, const T* phi, const T* ua,
+                                          const T* va, T inv_dt) {
   T r = T(0);
   if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny) {
     const T h = T(0.5);
@@ -395,14 +395,19 @@ __global__ void k_pcd_schur(Geo g, const T* phi, const T* ua, const T* va, T* rp
                    vavg * (phi[g.at(i, j + 1)] - phi[g.at(i, j - 1)]) * (h * T(g.idy));
     r = -(inv_dt * phi[k] + conv);
   }
-  rp[k] = r;
+  return r;
+}
+template <typename T>
+__global__ void k_pcd_schur(Geo g, const T* phi, const T* ua, const T* va, T* rp, T inv_dt, const int* active) {
+  if (active && !*active) return;
+  FUGU_BOX_IJ
+  rp[k] = pcd_schur_at<T>(g, k, i, j, phi, ua, va, inv_dt);
 }
 
 // velocity residual update z - B_p^T r_p (mod_pcd_precond.f90:66-84)
 template <typename T>
-__global__ void k_pcd_zwork(Geo g, const T* zu, const T* zv, const T* rp, T* zuw, T* zvw, const int* active) {
-  if (active && !*active) return;
-  FUGU_BOX_IJ
+__device__ __forceinline__ void pcd_zwork_at(const Geo& g, int k, int i, int j, const T* zu, const T* zv,
+                                             const T* rp, T* zuw, T* zvw) {
   const int nx = g.nx, ny = g.ny;
   T a = T(0), b = T(0);
   if (j >= 1 && j <= ny) {
@@ -416,12 +421,17 @@ __global__ void k_pcd_zwork(Geo g, const T* zu, const T* zv, const T* rp, T* zuw
   zuw[k] = a;
   zvw[k] = b;
 }
+template <typename T>
+__global__ void k_pcd_zwork(Geo g, const T* zu, const T* zv, const T* rp, T* zuw, T* zvw, const int* active) {
+  if (active && !*active) return;
+  FUGU_BOX_IJ
+  pcd_zwork_at<T>(g, k, i, j, zu, zv, rp, zuw, zvw);
+}
 
 // cross term from r_v into the u residual (mod_pcd_precond.f90:91-98)
 template <typename T>
-__global__ void k_pcd_cross(Geo g, const T* eta, const T* rv, T* zuw, const int* active) {
-  if (active && !*active) return;
-  FUGU_BOX_IJ
+__device__ __forceinline__ void pcd_cross_at(const Geo& g, int k, int i, int j, const T* eta, const T* rv,
+                                             T* zuw) {
   if (j >= 1 && j <= g.ny && i >= 1 && i <= g.nx - 1) {
     const T idx = T(g.idx), idy = T(g.idy);
     const T cross = -idy * (eta[k] * (rv[g.at(i + 1, j)] - rv[k]) * idx -
@@ -429,15 +439,20 @@ __global__ void k_pcd_cross(Geo g, const T* eta, const T* rv, T* zuw, const int*
     zuw[k] = zuw[k] - cross;
   }
 }
+template <typename T>
+__global__ void k_pcd_cross(Geo g, const T* eta, const T* rv, T* zuw, const int* active) {
+  if (active && !*active) return;
+  FUGU_BOX_IJ
+  pcd_cross_at<T>(g, k, i, j, eta, rv, zuw);
+}
 
 // One damped-Jacobi sweep of solve_helmholtz_u (mod_subsolvers.f90:284-306):
 // un = Jacobi(uo) on owned faces, rhs on wall faces, uo elsewhere (the
 // reference's u_old = u_sol copy).
 template <typename T>
-__global__ void k_jacobi_u(Geo g, const T* uo, T* un, const T* rhs, const T* rho_u, const T* kap,
-                           const T* zeta, const T* eta, const T* pen, T dt, T om, const int* active) {
-  if (active && !*active) return;
-  FUGU_BOX_IJ
+__device__ __forceinline__ T jacobi_u_at(const Geo& g, int k, int i, int j, const T* uo, const T* rhs,
+                                         const T* rho_u, const T* kap, const T* zeta, const T* eta, const T* pen,
+                                         T dt, T om) {
   const int nx = g.nx, ny = g.ny;
   T val = uo[k];
   if (j >= 1 && j <= ny) {
@@ -456,15 +471,21 @@ __global__ void k_jacobi_u(Geo g, const T* uo, T* un, const T* rhs, const T* rho
       val = rhs[k];
     }
   }
-  un[k] = val;
+  return val;
+}
+template <typename T>
+__global__ void k_jacobi_u(Geo g, const T* uo, T* un, const T* rhs, const T* rho_u, const T* kap,
+                           const T* zeta, const T* eta, const T* pen, T dt, T om, const int* active) {
+  if (active && !*active) return;
+  FUGU_BOX_IJ
+  un[k] = jacobi_u_at<T>(g, k, i, j, uo, rhs, rho_u, kap, zeta, eta, pen, dt, om);
 }
 
 // One damped-Jacobi sweep of solve_helmholtz_v (mod_subsolvers.f90:346-369)
 template <typename T>
-__global__ void k_jacobi_v(Geo g, const T* vo, T* vn, const T* rhs, const T* rho_v, const T* kap,
-                           const T* zeta, const T* eta, const T* pen, T dt, T om, const int* active) {
-  if (active && !*active) return;
-  FUGU_BOX_IJ
+__device__ __forceinline__ T jacobi_v_at(const Geo& g, int k, int i, int j, const T* vo, const T* rhs,
+                                         const T* rho_v, const T* kap, const T* zeta, const T* eta, const T* pen,
+                                         T dt, T om) {
   const int nx = g.nx, ny = g.ny;
   T val = vo[k];
   if (i >= 1 && i <= nx) {
@@ -483,7 +504,14 @@ __global__ void k_jacobi_v(Geo g, const T* vo, T* vn, const T* rhs, const T* rho
       val = rhs[k];
     }
   }
-  vn[k] = val;
+  return val;
+}
+template <typename T>
+__global__ void k_jacobi_v(Geo g, const T* vo, T* vn, const T* rhs, const T* rho_v, const T* kap,
+                           const T* zeta, const T* eta, const T* pen, T dt, T om, const int* active) {
+  if (active && !*active) return;
+  FUGU_BOX_IJ
+  vn[k] = jacobi_v_at<T>(g, k, i, j, vo, rhs, rho_v, kap, zeta, eta, pen, dt, om);
 }
 
 // ------------------------------------------------------------ Krylov vectors

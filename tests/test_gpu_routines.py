@@ -245,17 +245,22 @@ def test_poisson_pcg(gpu, oracle_mod, grid, zero_init, pcg_variant):
     exact(pg, po)
 
 
-def test_pcd_precond(gpu, oracle_mod, grid, pcg_variant):
+@pytest.mark.parametrize("sweeps,penalty", [(3, False), (4, True)])
+def test_pcd_precond(gpu, oracle_mod, grid, pcg_variant, sweeps, penalty):
+    """apply_pcd_precond: 3 sweeps (odd: the Jacobi result is copied back) and
+    4 sweeps with the Darcy penalty diagonal."""
     rng = np.random.default_rng(11)
-    prm = two_phase_params()
+    prm = two_phase_params(pcd_sweeps=sweeps)
     o = oracle_mod.Oracle(grid, prm)
     c, pr = props(o, grid, rng, prm)
     z = [rfield(rng, grid, k) for k in ("u", "v", "cell")]
     ua, va = rfield(rng, grid, "u"), rfield(rng, grid, "v")
+    pen = (np.abs(rfield(rng, grid, "u")) * 1e3, np.abs(rfield(rng, grid, "v")) * 1e3) if penalty else (None, None)
     rg = [grid.zeros(k) for k in ("u", "v", "cell")]
     ro = [grid.zeros(k) for k in ("u", "v", "cell")]
     with Context(grid, prm) as ctx:
-        ctx.apply_pcd_precond(*z, *rg, ua, va, pr["rho_u"], pr["rho_v"], pr["kappa"], pr["zeta"], pr["eta"], 2e-3)
-    o.pcd(*z, *ro, ua, va, pr, 2e-3)
+        ctx.apply_pcd_precond(*z, *rg, ua, va, pr["rho_u"], pr["rho_v"], pr["kappa"], pr["zeta"], pr["eta"], 2e-3,
+                              *pen)
+    o.pcd(*z, *ro, ua, va, pr, 2e-3, *pen)
     for a, b in zip(rg, ro):
         exact(a, b)
