@@ -116,13 +116,17 @@ __device__ __forceinline__ bool grid_sync(GridSync* gs, unsigned int nblocks, un
 }
 
 // --------------------------------------------------------------------------
-// Order-independent sums.  Every sum of the hot path (coupled_dot, the PCG
-// scalars, the zero-mean projections) is accumulated as an unevaluated pair
-// hi + lo with error-free transformations (Knuth's TwoSum), then rounded once.
-// The result is the correctly rounded exact sum except when that sum lies
-// within ~1e-30 relative of a rounding boundary, so the GPU tree order and the
-// oracle's serial order give the same double; the reference's own sums depend
-// on its MPI rank count.  Needs IEEE add without contraction or reassociation
+// Nearly order-independent sums.  Every sum of the hot path (coupled_dot, the
+// PCG scalars, the zero-mean projections) is accumulated as an unevaluated
+// pair hi + lo: Knuth's TwoSum makes each hi addition error-free, lo adds the
+// error terms with ordinary rounding, and the pair is rounded once.  While the
+// terms' exponents span less than ~50 bits the lo additions are exact and the
+// result is the correctly rounded sum in any order.  Wider spans (~2e5 terms
+// of a Krylov vector at 256^2) leave lo an error near n * eps^2 * |partial
+// sums|, so the GPU's short per-thread pairs merged in a tree and the oracle's
+// one serial pair can round the last bit differently when the sum cancels.
+// The reference's own sums depend on its MPI rank count.  Needs IEEE add
+// without contraction or reassociation
 // (the FP64 build uses --fmad=false).
 // --------------------------------------------------------------------------
 struct DD {

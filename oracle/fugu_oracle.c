@@ -38,12 +38,16 @@ static double* zalloc(size_t n) {
   if (!p) { fprintf(stderr, "fugu_oracle: out of memory\n"); abort(); }
   return p;
 }
-/* Order-independent sums: the reference accumulates each reduction serially
- * per MPI rank and then MPI_Allreduce-s the rank partials, so its rounding
- * depends on the rank count.  The oracle (and the CUDA path) accumulate the
- * same terms as an unevaluated pair hi + lo with Knuth's TwoSum and round
- * once, which yields the correctly rounded exact sum except within ~1e-30
- * relative of a rounding boundary -- the same double in any order. */
+/* Nearly order-independent sums: the reference accumulates each reduction
+ * serially per MPI rank and then MPI_Allreduce-s the rank partials, so its
+ * rounding depends on the rank count.  The oracle (and the CUDA path)
+ * accumulate the same terms as an unevaluated pair hi + lo -- Knuth's TwoSum
+ * on hi, the error terms added into lo with ordinary rounding -- and round
+ * once.  When the terms' exponents span less than ~50 bits every lo addition
+ * is exact and the result is the correctly rounded sum in any order; over a
+ * wider span lo keeps an error near n * eps^2 * |partial sums|, and a sum that
+ * cancels can then round its last bit differently from the CUDA path's tree
+ * of short pairs. */
 typedef struct { double hi, lo; } dsum;
 static void ds_add(dsum* d, double x) {
   double s = d->hi + x;

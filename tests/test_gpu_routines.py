@@ -4,19 +4,26 @@ contents are part of the reference's operator semantics).
 
 Tolerance: BIT-EXACT for every routine.  Element-wise kernels are compiled
 without FMA contraction and keep the reference's operand order; reductions
-(coupled_dot, the PCG scalars) are accumulated error-free on both sides and
-rounded once, so their value does not depend on the summation order.
+(coupled_dot, the PCG scalars) accumulate a double-double on both sides and
+round once, which on these inputs gives the correctly rounded sum in any
+summation order.  The same routines are bit-exact at 256^2 and 320 x 640
+too; whole solves at those sizes are compared within tolerance in
+``test_gpu_configs.py``.
 """
 import numpy as np
 import pytest
 
 from conftest import GRIDS, colour, rfield, two_phase_params
 from coupled_codefort_2d_b200.context import Context
+from coupled_codefort_2d_b200.layout import Grid
 from coupled_codefort_2d_b200.params import Params
 
 pytestmark = pytest.mark.gpu
 
-GRID_IDS = list(GRIDS)
+# the small grids plus the droplet and rising-bubble sizes (256^2 takes the
+# cluster-resident PCG, 320 x 640 the grid-wide one)
+ROUTINE_GRIDS = {**GRIDS, "walls_256x256": Grid(256, 256), "walls_320x640": Grid(320, 640, 1.0, 2.0)}
+GRID_IDS = list(ROUTINE_GRIDS)
 
 
 def exact(a, b):
@@ -29,7 +36,7 @@ def rel(a, b):
 
 @pytest.fixture(params=GRID_IDS)
 def grid(request):
-    return GRIDS[request.param]
+    return ROUTINE_GRIDS[request.param]
 
 
 def props(o, g, rng, prm):
