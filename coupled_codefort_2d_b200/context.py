@@ -18,6 +18,9 @@ from ._lib import FIELD_ID, FIELD_KIND, FuguError, FuguParams, FuguStats, FuguSt
 from .layout import Grid, as_fortran
 from .params import Params
 
+# the state a step maps, in the order of fugu_step_vjp's arguments
+VJP_STATE = (("u_vel", "u"), ("v_vel", "v"), ("c_field", "cell"), ("u_prev", "u"), ("v_prev", "v"))
+
 
 def make_params(g: Grid, prm: Params, precision: int = _lib.FP64) -> FuguParams:
     p = FuguParams()
@@ -148,6 +151,25 @@ class Context:
         st = FuguStats()
         self._ck(self.L.fugu_step(self.h, float(dt), int(step_idx), C.byref(opts), C.byref(st)))
         return st.as_dict()
+
+    def step_vjp(self, dt: float, step_idx: int, opts: FuguStepOpts, bar_out: dict):
+        """Advance the device-resident state by one step, as ``step`` does, and
+        return the adjoints of the state before it from those of the state
+        after it (``fugu_step_vjp``; no counterpart in the reference).
+
+        bar_out maps u_vel, v_vel, c_field, u_prev, v_prev to adjoint arrays in
+        the reference layout (a missing key is zero).  Returns (bar_in with the
+        same keys, d/d(sigma, mu1, mu2, rho1, rho2) of the step, statistics of
+        the forward step with ``status`` the adjoint solve's)."""
+        g = self.g
+        bo = [g.zeros(kind) if bar_out.get(k) is None else as_fortran(bar_out[k], g, kind)
+              for k, kind in VJP_STATE]
+        bi = [g.zeros(kind) for _, kind in VJP_STATE]
+        theta = np.zeros(5)
+        st = FuguStats()
+        self._ck(self.L.fugu_step_vjp(self.h, float(dt), int(step_idx), C.byref(opts), *[ptr(a) for a in bo],
+                                      *[ptr(a) for a in bi], ptr(theta), C.byref(st)))
+        return {k: a for (k, _), a in zip(VJP_STATE, bi)}, theta, st.as_dict()
 
     # --------------------------------------------- mod_solver_coupled mirror
     def advance_coupled_step(self, u_vel, v_vel, p_field, c_field, u_prev, v_prev, rho_c, rho_u, rho_v,

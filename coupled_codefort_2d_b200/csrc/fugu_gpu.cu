@@ -32,6 +32,7 @@
 #include "pcg_cluster.cuh"
 #include "persistent.cuh"
 #include "scalars.cuh"
+#include "step_vjp.cuh"
 
 using namespace fugu;
 
@@ -110,6 +111,29 @@ struct FgWork {
   int cap = 0;           // m the buffers hold
 };
 
+// buffers of the step's vector-Jacobian product (allocated on first use)
+struct VjpWork {
+  bool ready = false;
+  // the state before the step: C^n, u^n, v^n, u^(n-1), v^(n-1)
+  double *c0 = nullptr, *u0 = nullptr, *v0 = nullptr, *up0 = nullptr, *vp0 = nullptr;
+  // adjoints after the step (inputs; b_c1 also collects C^(n+1)'s whole adjoint)
+  double *b_u1 = nullptr, *b_v1 = nullptr, *b_c1 = nullptr, *b_up1 = nullptr, *b_vp1 = nullptr;
+  // adjoints before the step (outputs) and of C_smooth
+  double *b_c0 = nullptr, *b_u0 = nullptr, *b_v0 = nullptr, *b_up0 = nullptr, *b_vp0 = nullptr;
+  double *b_cs = nullptr, *t1 = nullptr, *t2 = nullptr;
+  Trip<double> g, lam, resid;
+  int* svof_it = nullptr;
+  // duals: VOF stage (C^n, u^n, v^n -> C^(n+1))
+  ad::Dual *dc0 = nullptr, *du0 = nullptr, *dv0 = nullptr, *dc1o = nullptr;
+  // duals: inputs and intermediates of the solve's stage
+  ad::Dual *dc1 = nullptr, *dcs = nullptr, *dun = nullptr, *dvn = nullptr, *dunm1 = nullptr, *dvnm1 = nullptr;
+  ad::Dual *drc = nullptr, *dru = nullptr, *drv = nullptr, *dka = nullptr, *dze = nullptr, *det = nullptr;
+  ad::Dual *dkc = nullptr, *dfu = nullptr, *dfv = nullptr, *dua = nullptr, *dva = nullptr;
+  ad::Dual *dB[3] = {}, *dX[3] = {}, *dY[3] = {};
+  // duals: the final wall BCs of the step (owned velocity -> every entry)
+  ad::Dual *dgu = nullptr, *dgv = nullptr;
+};
+
 }  // namespace
 
 struct fugu_ctx {
@@ -141,6 +165,7 @@ struct fugu_ctx {
   double* adj_val = nullptr;
   unsigned int* adj_err = nullptr;
   bool adj_on = false;
+  VjpWork vjp;
   // routine-level scratch
   double* scratch[20] = {};
   // device scalars / state
@@ -1675,6 +1700,321 @@ void adj_assemble(fugu_ctx* c, const CoefBufs<double>& cb, const SolveOpt& o, do
                                           " operator entries beyond a 2-cell reach"};
 }
 
+// Solve A^T X = B on the device: the FP64 defect correction around flexible
+// GMRES on S A^T S (S flips the pressure block), then X = S X.  B is
+// overwritten.  The context's parameters and its adaptive PCG cap and sweeps
+// come back as they were, so the forward steps that follow are unaffected.
+KrylovResult adjoint_solve_dev(fugu_ctx* c, const CoefBufs<double>& cb, const SolveOpt& o, double dt, double tol,
+                               Trip<double> B, Trip<double> X, int* outer) {
+  struct Restore {
+    fugu_ctx* c;
+    fugu_params prm;
+    int cap, sweeps;
+    ~Restore() {
+      c->prm = prm;
+      c->adj_on = false;
+      c->pcg_cap_state = cap;
+      c->pcd_sweeps_state = sweeps;
+    }
+  } restore{c, c->prm, c->pcg_cap_state, c->pcd_sweeps_state};
+  adj_assemble(c, cb, o, dt);
+  zero_trip(c, X);
+  const int g1 = grid1d(c, c->n);
+  k_adj_flip_p<<<g1, 256, 0, c->s>>>(c->n, B.base);  // S g
+  CKL("k_adj_flip_p");
+  c->prm.refine = 2;
+  c->prm.precision = FUGU_FP64;
+  if (c->prm.refine_max_inner < 1 || c->prm.refine_max_inner > 127) c->prm.refine_max_inner = 30;
+  c->adj_on = true;
+  reset_counters(c);
+  KrylovResult kr = solve(c, 2, cb, o, X, B, dt, tol, 0, false, 0.0, outer);
+  c->adj_on = false;
+  k_adj_flip_p<<<g1, 256, 0, c->s>>>(c->n, X.base);  // lambda = S mu
+  CKL("k_adj_flip_p");
+  return kr;
+}
+
+// ------------------------------------------------ vector-Jacobian product of one step
+// Reach (cells, in i and j) of each local stage, which fixes the colour
+// period 2R + 1 of its probes: the VOF update reads C two cells away; the
+// solve's stage reads C_smooth three cells away (curvature then CSF) and the
+// coefficients two; the wall BCs mirror up to four cells (u(-2) = -u(2)).
+constexpr int VJP_RA = 2, VJP_RB = 4, VJP_RG = 4;
+
+void vjp_alloc(fugu_ctx* c) {
+  VjpWork& w = c->vjp;
+  if (w.ready) return;
+  auto F = [&] { return dalloc<double>(c, c->n); };
+  auto D = [&] { return dalloc<ad::Dual>(c, c->n); };
+  w.c0 = F(); w.u0 = F(); w.v0 = F(); w.up0 = F(); w.vp0 = F();
+  w.b_u1 = F(); w.b_v1 = F(); w.b_c1 = F(); w.b_up1 = F(); w.b_vp1 = F();
+  w.b_c0 = F(); w.b_u0 = F(); w.b_v0 = F(); w.b_up0 = F(); w.b_vp0 = F();
+  w.b_cs = F(); w.t1 = F(); w.t2 = F();
+  w.g = talloc<double>(c); w.lam = talloc<double>(c); w.resid = talloc<double>(c);
+  w.svof_it = dalloc<int>(c, 1);
+  w.dc0 = D(); w.du0 = D(); w.dv0 = D(); w.dc1o = D();
+  w.dc1 = D(); w.dcs = D(); w.dun = D(); w.dvn = D(); w.dunm1 = D(); w.dvnm1 = D();
+  w.drc = D(); w.dru = D(); w.drv = D(); w.dka = D(); w.dze = D(); w.det = D();
+  w.dkc = D(); w.dfu = D(); w.dfv = D(); w.dua = D(); w.dva = D();
+  for (int q = 0; q < 3; ++q) { w.dB[q] = D(); w.dX[q] = D(); w.dY[q] = D(); }
+  w.dgu = D(); w.dgv = D();
+  w.ready = true;
+}
+
+void vjp_pack(fugu_ctx* c, const double* x, ad::Dual* out, int mask, bool seeded, int s, int a, int b) {
+  Box bx = box_launch(c->g);
+  k_dual_pack<<<bx.grid, bx.block, 0, c->s>>>(c->g, x, out, mask, seeded ? 1 : 0, s, a, b);
+  CKL("k_dual_pack");
+}
+
+void vjp_gather(fugu_ctx* c, const VjpOut& o, int mask, int s, int a, int b, int R, double* xbar) {
+  const int ti = (c->g.P - a + s - 1) / s, tj = (c->g.R - b + s - 1) / s;
+  if (ti <= 0 || tj <= 0) return;
+  const dim3 blk(32, 4), grd((ti + 31) / 32, (tj + 3) / 4);
+  k_vjp_gather<<<grd, blk, 0, c->s>>>(c->g, o, mask, s, a, b, R, xbar);
+  CKL("k_vjp_gather");
+}
+
+// one input field of a probed stage: its values, its dual buffer, the
+// entries that are inputs, and where its adjoint accumulates
+struct VjpIn {
+  const double* x;
+  ad::Dual* d;
+  int mask;
+  double* bar;
+};
+
+// x_bar += J^T y_bar for every input of a stage: each input field in turn is
+// seeded colour by colour while the others carry zero derivatives
+template <typename Stage>
+void vjp_probe(fugu_ctx* c, VjpIn* in, int nin, const VjpOut& out, int R, Stage&& stage) {
+  const int s = 2 * R + 1;
+  for (int e = 0; e < nin; ++e) vjp_pack(c, in[e].x, in[e].d, in[e].mask, false, s, 0, 0);
+  for (int f = 0; f < nin; ++f) {
+    for (int a = 0; a < s; ++a)
+      for (int b = 0; b < s; ++b) {
+        vjp_pack(c, in[f].x, in[f].d, in[f].mask, true, s, a, b);
+        stage();
+        vjp_gather(c, out, in[f].mask, s, a, b, R, in[f].bar);
+      }
+    vjp_pack(c, in[f].x, in[f].d, in[f].mask, false, s, 0, 0);
+  }
+}
+
+// the VOF stage on duals: C^n, u^n, v^n -> C^(n+1) (vof() without AMP fluxes)
+void vjp_stage_vof(fugu_ctx* c, double dt) {
+  VjpWork& w = c->vjp;
+  Box bx = box_launch(c->g);
+  k_vof_update<ad::Dual><<<bx.grid, bx.block, 0, c->s>>>(c->g, c->prm.limiter, w.dc0, w.du0, w.dv0, dt, w.dc1o);
+  CKL("k_vof_update<Dual>");
+  halo(c, w.dc1o, K_CELL);
+}
+
+// the solve's stage on duals: C^(n+1), C_smooth, u^n, v^n, u^(n-1), v^(n-1)
+// and the parameters -> B and A X with X fixed at the step's solution
+// (properties, curvature, CSF, AB extrapolation, right-hand side, matvec)
+void vjp_stage_solve(fugu_ctx* c, double dt, double dt_eff, bool bdf2, bool first, const fugu_step_opts* o,
+                     const MixT<ad::Dual>& m, ad::Dual sigma) {
+  VjpWork& w = c->vjp;
+  const Geo& g = c->g;
+  const fugu_params& p = c->prm;
+  Box bx = box_launch(g);
+  k_properties<ad::Dual><<<bx.grid, bx.block, 0, c->s>>>(g, m, w.dc1, w.drc, w.dru, w.drv, w.dka, w.dze, w.det);
+  CKL("k_properties<Dual>");
+  if (p.sigma > 1.0e-14) {
+    k_fill_ghost_neumann<ad::Dual><<<bx.grid, bx.block, 0, c->s>>>(g, w.dcs);
+    k_curvature<ad::Dual><<<bx.grid, bx.block, 0, c->s>>>(g, w.dcs, w.dkc);
+    k_csf<ad::Dual><<<bx.grid, bx.block, 0, c->s>>>(g, sigma, w.dc1, w.dkc, w.dfu, w.dfv);
+    CKL("k_csf<Dual>");
+  } else {
+    vjp_pack(c, nullptr, w.dfu, VM_U, false, 1, 0, 0);
+    vjp_pack(c, nullptr, w.dfv, VM_V, false, 1, 0, 0);
+  }
+  const int g1 = grid1d(c, c->n);
+  k_adv_dual<<<g1, 256, 0, c->s>>>(c->n, w.dun, w.dunm1, w.dua, first ? 1 : 0);
+  k_adv_dual<<<g1, 256, 0, c->s>>>(c->n, w.dvn, w.dvnm1, w.dva, first ? 1 : 0);
+  CKL("k_adv_dual");
+  RhsArgsT<ad::Dual> ra{};
+  ra.rho_u = w.dru; ra.rho_v = w.drv;
+  ra.u_n = w.dun; ra.u_nm1 = w.dunm1; ra.v_n = w.dvn; ra.v_nm1 = w.dvnm1;
+  ra.fsu = w.dfu; ra.fsv = w.dfv;
+  ra.pen_u = nullptr; ra.pen_v = nullptr;
+  ra.zeta = w.dze; ra.eta = w.det;
+  ra.dt = dt; ra.gx = p.gx; ra.gy = p.gy;
+  ra.u_sol = o->has_u_solid ? o->u_solid : 0.0;
+  ra.v_sol = o->has_v_solid ? o->v_solid : 0.0;
+  ra.u_lid = o->has_lid ? o->u_top_lid : 0.0;
+  ra.bdf2 = bdf2 ? 1 : 0;
+  ra.has_lid = o->has_lid ? 1 : 0;
+  k_rhs<ad::Dual><<<bx.grid, bx.block, 0, c->s>>>(g, ra, w.dB[0], w.dB[1], w.dB[2]);
+  CKL("k_rhs<Dual>");
+  Coefs<ad::Dual> cf{};
+  cf.u_adv = w.dua; cf.v_adv = w.dva; cf.rho_c = w.drc; cf.rho_u = w.dru; cf.rho_v = w.drv;
+  cf.kappa = w.dka; cf.zeta = w.dze; cf.eta = w.det;
+  k_matvec<ad::Dual><<<bx.grid, bx.block, 0, c->s>>>(g, cf, w.dX[0], w.dX[1], w.dX[2], w.dY[0], w.dY[1], w.dY[2],
+                                                     ad::Dual(dt_eff), 1, nullptr, nullptr);
+  CKL("k_matvec<Dual>");
+}
+
+// the step's final BCs on duals: owned velocity -> every velocity entry
+void vjp_stage_bc(fugu_ctx* c) {
+  VjpWork& w = c->vjp;
+  halo(c, w.dgu, K_U);
+  halo(c, w.dgv, K_V);
+  vbcs(c, w.dgu, w.dgv, 0.0);
+}
+
+MixT<ad::Dual> vjp_mix(const fugu_params& p, int seed) {
+  // seed: 1 sigma (not here), 2 mu1, 3 mu2, 4 rho1, 5 rho2
+  return MixT<ad::Dual>{ad::Dual(p.rho1, seed == 4 ? 1.0 : 0.0), ad::Dual(p.rho2, seed == 5 ? 1.0 : 0.0),
+                        ad::Dual(p.mu1, seed == 2 ? 1.0 : 0.0), ad::Dual(p.mu2, seed == 3 ? 1.0 : 0.0)};
+}
+
+// The step as a map of the state (u, v, C, u_prev, v_prev) -> (u', v', C',
+// u_prev' = u, v_prev' = v) and its transpose applied to the adjoints of the
+// state after the step.  The context holds the state before the step and is
+// left holding the state after it.
+void step_vjp(fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o, const double* const* bar_out,
+              double* const* bar_in, double* bar_theta, fugu_stats* st_out) {
+  const fugu_params& p = c->prm;
+  const Geo& g = c->g;
+  if (g.px || g.py) throw ApiError{FUGU_EINVAL, "the step VJP supports wall-bounded boxes only"};
+  if (o->consistent_amp) throw ApiError{FUGU_EINVAL, "the step VJP does not support consistent_amp"};
+  if (o->has_penalty) throw ApiError{FUGU_EINVAL, "the step VJP does not support the Darcy penalty"};
+  for (int q = 0; q < 5; ++q)
+    if (!bar_out[q] || !bar_in[q]) throw ApiError{FUGU_EINVAL, "NULL adjoint array"};
+  vjp_alloc(c);
+  VjpWork& w = c->vjp;
+  double** f = c->f;
+  const long n = c->n;
+  const size_t nb = sizeof(double) * n;
+  CK(cudaMemcpyAsync(w.c0, f[FUGU_F_C_FIELD], nb, cudaMemcpyDeviceToDevice, c->s));
+  CK(cudaMemcpyAsync(w.u0, f[FUGU_F_U_VEL], nb, cudaMemcpyDeviceToDevice, c->s));
+  CK(cudaMemcpyAsync(w.v0, f[FUGU_F_V_VEL], nb, cudaMemcpyDeviceToDevice, c->s));
+  CK(cudaMemcpyAsync(w.up0, f[FUGU_F_U_PREV], nb, cudaMemcpyDeviceToDevice, c->s));
+  CK(cudaMemcpyAsync(w.vp0, f[FUGU_F_V_PREV], nb, cudaMemcpyDeviceToDevice, c->s));
+  // the forward step
+  fugu_stats fst;
+  std::memset(&fst, 0, sizeof(fst));
+  step(c, dt, step_idx, o, &fst);
+  const bool bdf2 = (p.time_order == 2 && step_idx >= 2);
+  const double dt_eff = bdf2 ? dt / 1.5 : dt;
+  const bool first = step_idx <= 1;
+  // adjoints after the step
+  double* accs[] = {w.b_u1, w.b_v1, w.b_c1, w.b_up1, w.b_vp1, w.b_c0, w.b_u0, w.b_v0, w.b_up0, w.b_vp0, w.b_cs};
+  for (double* a : accs) CK(cudaMemsetAsync(a, 0, nb, c->s));
+  up(c, w.b_u1, bar_out[0], K_U);
+  up(c, w.b_v1, bar_out[1], K_V);
+  up(c, w.b_c1, bar_out[2], K_CELL);
+  up(c, w.b_up1, bar_out[3], K_U);
+  up(c, w.b_vp1, bar_out[4], K_V);
+  // 1. the final BCs: fold the adjoints of u', v' onto the owned unknowns
+  zero_trip(c, w.g);
+  {
+    VjpIn in[2] = {{nullptr, w.dgu, VM_OWNED_U, w.g.u}, {nullptr, w.dgv, VM_OWNED_V, w.g.v}};
+    VjpOut out{};
+    out.y[0] = w.dgu; out.ybar[0] = w.b_u1;
+    out.y[1] = w.dgv; out.ybar[1] = w.b_v1;
+    out.n = 2;
+    vjp_probe(c, in, 2, out, VJP_RG, [&] { vjp_stage_bc(c); });
+  }
+  // 2. lambda = A^-T g (the step's operator at its coefficients and dt_eff)
+  SolveOpt so;
+  const double tol = o->has_tol ? o->tol : p.tol_bicgstab2;
+  int aouter = 0;
+  KrylovResult ak = adjoint_solve_dev(c, coef64(c, c->u_adv, c->v_adv), so, dt_eff, tol, w.g, w.lam, &aouter);
+  {
+    Box bx = box_launch(g);
+    k_keep_owned<<<bx.grid, bx.block, 0, c->s>>>(g, w.lam.base, n);
+    CKL("k_keep_owned");
+  }
+  // 3. the solve's stage: x_bar += (dB/dx - (dA/dx) X)^T lambda
+  vjp_pack(c, c->Xstate.u, w.dX[0], VM_U, false, 1, 0, 0);
+  vjp_pack(c, c->Xstate.v, w.dX[1], VM_V, false, 1, 0, 0);
+  vjp_pack(c, c->Xstate.p, w.dX[2], VM_CELL, false, 1, 0, 0);
+  const MixT<ad::Dual> m0 = vjp_mix(p, 0);
+  const ad::Dual sig0(p.sigma);
+  VjpOut out{};
+  for (int q = 0; q < 3; ++q) {
+    out.y[q] = w.dB[q];
+    out.ysub[q] = w.dY[q];
+  }
+  out.ybar[0] = w.lam.u; out.ybar[1] = w.lam.v; out.ybar[2] = w.lam.p;
+  out.n = 3;
+  {
+    VjpIn in[6] = {{f[FUGU_F_C_FIELD], w.dc1, VM_CELL, w.b_c1}, {c->c_s, w.dcs, VM_INTERIOR, w.b_cs},
+                   {w.u0, w.dun, VM_U, w.b_u0},                 {w.v0, w.dvn, VM_V, w.b_v0},
+                   {w.up0, w.dunm1, VM_U, w.b_up0},             {w.vp0, w.dvnm1, VM_V, w.b_vp0}};
+    vjp_probe(c, in, 6, out, VJP_RB,
+              [&] { vjp_stage_solve(c, dt, dt_eff, bdf2, first, o, m0, sig0); });
+    // parameters: theta_bar += (dB/dtheta - (dA/dtheta) X) . lambda
+    const double vol = g.dx * g.dy;
+    for (int q = 0; q < 5; ++q) {
+      const int seed = q + 1;
+      vjp_stage_solve(c, dt, dt_eff, bdf2, first, o, vjp_mix(p, seed), ad::Dual(p.sigma, seed == 1 ? 1.0 : 0.0));
+      Box bx = box_launch(g);
+      k_dual_resid<<<bx.grid, bx.block, 0, c->s>>>(g, w.dB[0], w.dB[1], w.dB[2], w.dY[0], w.dY[1], w.dY[2],
+                                                    w.resid.base, n);
+      CKL("k_dual_resid");
+      dot_op<double>(c, {{w.resid, w.lam}}, OpArgs{OP_STORE, 0, 0.0}, false);
+      if (bar_theta) bar_theta[q] += read_slot(c, S_D0) / vol;
+    }
+  }
+  // 4. SVOF: C_smooth = L C^(n+1) with L a polynomial of the symmetric Jacobi
+  // iteration matrix (K sweeps), so L^T = L: the same sweeps on C_smooth's adjoint
+  if (p.sigma > 1.0e-14 && fst.svof_iters > 0) {
+    const double delta = p.svof_delta_h * (g.dx < g.dy ? g.dx : g.dy);
+    SvofArgs a;
+    a.g = g;
+    a.craw = w.b_cs;
+    a.out = w.t1;
+    a.work = w.t2;
+    a.cx = (delta / g.dx) * (delta / g.dx);
+    a.cy = (delta / g.dy) * (delta / g.dy);
+    a.diag = 1.0 + 2.0 * (a.cx + a.cy);
+    a.max_iter = fst.svof_iters;
+    a.tol = -1.0;  // no early exit: exactly the forward's sweeps
+    a.part = c->part;
+    a.gs = c->gs;
+    a.iters = w.svof_it;
+    a.status = c->svof_status;
+    CK(cudaMemsetAsync(c->gs, 0, sizeof(GridSync), c->s));
+    void* args[] = {&a};
+    launch_coop(c, (const void*)k_svof, c->svof_grid, args);
+    ++c->launches;
+    Box bx = box_launch(g);
+    k_add_interior<<<bx.grid, bx.block, 0, c->s>>>(g, w.t1, w.b_c1);
+    CKL("k_add_interior");
+  }
+  // 5. the VOF stage: C^(n+1)'s whole adjoint back to C^n, u^n, v^n
+  {
+    VjpIn in[3] = {{w.c0, w.dc0, VM_CELL, w.b_c0}, {w.u0, w.du0, VM_U, w.b_u0}, {w.v0, w.dv0, VM_V, w.b_v0}};
+    VjpOut vo{};
+    vo.y[0] = w.dc1o;
+    vo.ybar[0] = w.b_c1;
+    vo.n = 1;
+    vjp_probe(c, in, 3, vo, VJP_RA, [&] { vjp_stage_vof(c, dt); });
+  }
+  // 6. u_prev' = u^n and v_prev' = v^n pass their adjoints through
+  const int g1 = grid1d(c, n);
+  k_axpby<<<g1, 256, 0, c->s>>>(n, w.b_u0, 1.0, w.b_u0, 1.0, w.b_up1);
+  k_axpby<<<g1, 256, 0, c->s>>>(n, w.b_v0, 1.0, w.b_v0, 1.0, w.b_vp1);
+  CKL("k_axpby");
+  down(c, bar_in[0], w.b_u0, K_U);
+  down(c, bar_in[1], w.b_v0, K_V);
+  down(c, bar_in[2], w.b_c0, K_CELL);
+  down(c, bar_in[3], w.b_up0, K_U);
+  down(c, bar_in[4], w.b_vp0, K_V);
+  collect(c, nullptr);  // the adjoint SVOF's barrier status
+  sync(c);
+  if (st_out) {
+    *st_out = fst;
+    // a converged forward step reports the adjoint solve's outcome
+    if (fst.status == FUGU_CONVERGED) st_out->status = ak.status;
+    st_out->outer = aouter;
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1857,40 +2197,16 @@ int fugu_adjoint_solve(fugu_ctx* c, const double* g_u, const double* g_v, const 
                        const double* rho_u, const double* rho_v, const double* kappa, const double* zeta,
                        const double* eta, double dt, double tol, const double* penalty_u, const double* penalty_v,
                        const double* mdot_u, const double* mdot_v, fugu_stats* st) {
-  // the solve below runs the FP64 defect correction around flexible GMRES on
-  // S A^T S; the context's own settings come back however it ends
-  struct Restore {
-    fugu_ctx* c;
-    fugu_params prm;
-    ~Restore() {
-      c->prm = prm;
-      c->adj_on = false;
-    }
-  };
   return guard(c, [&] {
-    Restore restore{c, c->prm};
     CoefBufs<double> cb = up_coefs(c, u_adv, v_adv, rho_c, rho_u, rho_v, kappa, zeta, eta, penalty_u,
                                    penalty_v, mdot_u, mdot_v);
     SolveOpt o;
     o.pen = penalty_u && penalty_v;
     o.amp = mdot_u && mdot_v;
-    adj_assemble(c, cb, o, dt);
     Trip<double> X = ST(c, 0), B = ST(c, 1);
-    zero_trip(c, X);
     up_trip(c, B, g_u, g_v, g_p);
-    const int g1 = grid1d(c, c->n);
-    k_adj_flip_p<<<g1, 256, 0, c->s>>>(c->n, B.base);  // S g
-    CKL("k_adj_flip_p");
-    c->prm.refine = 2;
-    c->prm.precision = FUGU_FP64;
-    if (c->prm.refine_max_inner < 1 || c->prm.refine_max_inner > 127) c->prm.refine_max_inner = 30;
-    c->adj_on = true;
-    reset_counters(c);
     int outer = 0;
-    KrylovResult kr = solve(c, 2, cb, o, X, B, dt, tol, 0, false, 0.0, &outer);
-    c->adj_on = false;
-    k_adj_flip_p<<<g1, 256, 0, c->s>>>(c->n, X.base);  // lambda = S mu
-    CKL("k_adj_flip_p");
+    KrylovResult kr = adjoint_solve_dev(c, cb, o, dt, tol, B, X, &outer);
     if (st) std::memset(st, 0, sizeof(*st));
     collect(c, st);
     if (st) {
@@ -1901,6 +2217,18 @@ int fugu_adjoint_solve(fugu_ctx* c, const double* g_u, const double* g_v, const 
     }
     down_trip(c, X, lam_u, lam_v, lam_p);
     sync(c);
+  });
+}
+
+int fugu_step_vjp(fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o, const double* bar_u_out,
+                  const double* bar_v_out, const double* bar_c_out, const double* bar_uprev_out,
+                  const double* bar_vprev_out, double* bar_u_in, double* bar_v_in, double* bar_c_in,
+                  double* bar_uprev_in, double* bar_vprev_in, double* bar_theta, fugu_stats* st) {
+  return guard(c, [&] {
+    if (!o) throw ApiError{FUGU_EINVAL, "NULL step options"};
+    const double* bo[5] = {bar_u_out, bar_v_out, bar_c_out, bar_uprev_out, bar_vprev_out};
+    double* bi[5] = {bar_u_in, bar_v_in, bar_c_in, bar_uprev_in, bar_vprev_in};
+    step_vjp(c, dt, step_idx, o, bo, bi, bar_theta, st);
   });
 }
 

@@ -128,28 +128,36 @@ __global__ void k_velocity_bcs(Geo g, T* u, T* v, T u_lid, const int* active) {
 }
 
 // ------------------------------------------------------------ properties
-struct Mix {
-  double rho1, rho2, mu1, mu2;
+// The explicit stages of the step (properties, VOF transport, curvature,
+// CSF, right-hand side) are templates on their scalar type S: double for the
+// step itself, ad::Dual for its tangent (the discrete adjoint).
+template <typename S>
+struct MixT {
+  S rho1, rho2, mu1, mu2;
 };
+using Mix = MixT<double>;
 
 // harmonic_viscosity, mod_viscosity.f90:28-46
-__device__ __forceinline__ double harmonic_mu(const Mix& m, double c) {
-  const double cc = clip01(c);
+template <typename S>
+__device__ __forceinline__ S harmonic_mu(const MixT<S>& m, S c) {
+  const S cc = clip01(c);
   if (fabs(m.mu1 - m.mu2) < 1.0e-14) return m.mu1;
-  const double den = m.mu2 * cc + m.mu1 * (1.0 - cc);
+  const S den = m.mu2 * cc + m.mu1 * (1.0 - cc);
   if (den > 1.0e-15) return (m.mu1 * m.mu2) / den;
   return fmin(m.mu1, m.mu2);
 }
-__device__ __forceinline__ double rho_of(const Mix& m, double c) {
-  const double cv = clip01(c);
+template <typename S>
+__device__ __forceinline__ S rho_of(const MixT<S>& m, S c) {
+  const S cv = clip01(c);
   return m.rho1 * cv + m.rho2 * (1.0 - cv);
 }
 
 // compute_mixture_densities + compute_mixture_viscosities
 // (mod_viscosity.f90:54-151) in one pass: every output element is computed
 // from C directly; the border copies of the reference become index clamps.
-__global__ void k_properties(Geo g, Mix m, const double* __restrict__ c, double* rho_c, double* rho_u,
-                             double* rho_v, double* kappa, double* zeta, double* eta) {
+template <typename S>
+__global__ void k_properties(Geo g, MixT<S> m, const S* __restrict__ c, S* rho_c, S* rho_u, S* rho_v, S* kappa,
+                             S* zeta, S* eta) {
   FUGU_BOX_IJ
   const int nx = g.nx, ny = g.ny;
   if (in_kind(g, K_CELL, i, j)) {
@@ -167,9 +175,8 @@ __global__ void k_properties(Geo g, Mix m, const double* __restrict__ c, double*
   {  // vertex extent is the whole box's kind range
     if (in_kind(g, K_VERT, i, j)) {
       const int ie = min(max(i, -1), nx + 1), je = min(max(j, -1), ny + 1);
-      const double cv = 0.25 * (c[g.at(ie, je)] + c[g.at(ie + 1, je)] + c[g.at(ie, je + 1)] +
-                                c[g.at(ie + 1, je + 1)]);
-      const double mu = harmonic_mu(m, cv);
+      const S cv = 0.25 * (c[g.at(ie, je)] + c[g.at(ie + 1, je)] + c[g.at(ie, je + 1)] + c[g.at(ie + 1, je + 1)]);
+      const S mu = harmonic_mu(m, cv);
       zeta[k] = 2.0 * mu;
       eta[k] = mu;
     }
@@ -556,61 +563,62 @@ __global__ void k_pupdate(long n3, T* p, const T* r, const T* v, const double* b
 }
 
 // ------------------------------------------------------------ VOF transport
-__device__ __forceinline__ double limiter_psi(int lim, double r) {
+template <typename S>
+__device__ __forceinline__ S limiter_psi(int lim, S r) {
   if (lim == 1) {  // Superbee (extension)
-    const double a = fmin(2.0 * r, 1.0), b = fmin(r, 2.0);
+    const S a = fmin(2.0 * r, 1.0), b = fmin(r, 2.0);
     return fmax(0.0, fmax(a, b));
   }
-  if (r <= 0.0) return 0.0;  // van_leer_limiter, mod_vof.f90:25-33
+  if (r <= 0.0) return S(0.0);  // van_leer_limiter, mod_vof.f90:25-33
   return (2.0 * r) / (1.0 + r);
 }
 // face fluxes of vof_advection_tvd (mod_vof.f90:59-114)
-__device__ __forceinline__ double flux_x_at(const Geo& g, int lim, const double* c, const double* u,
-                                            int i, int j, double dt) {
-  const double uf = u[g.at(i, j)];
-  double num, den, r, cfl, cf;
+template <typename S>
+__device__ __forceinline__ S flux_x_at(const Geo& g, int lim, const S* c, const S* u, int i, int j, double dt) {
+  const S uf = u[g.at(i, j)];
+  S num, den, r, cfl, cf;
   if (uf >= 0.0) {
     num = c[g.at(i, j)] - c[g.at(i - 1, j)];
     den = c[g.at(i + 1, j)] - c[g.at(i, j)];
-    r = fabs(den) > 1.0e-12 ? num / den : 0.0;
+    r = fabs(den) > 1.0e-12 ? num / den : S(0.0);
     cfl = fabs(uf) * dt * g.idx;
     cf = c[g.at(i, j)] + 0.5 * (1.0 - cfl) * limiter_psi(lim, r) * den;
   } else {
     num = c[g.at(i + 2, j)] - c[g.at(i + 1, j)];
     den = c[g.at(i + 1, j)] - c[g.at(i, j)];
-    r = fabs(den) > 1.0e-12 ? num / den : 0.0;
+    r = fabs(den) > 1.0e-12 ? num / den : S(0.0);
     cfl = fabs(uf) * dt * g.idx;
     cf = c[g.at(i + 1, j)] - 0.5 * (1.0 - cfl) * limiter_psi(lim, r) * den;
   }
   return uf * clip01(cf);
 }
-__device__ __forceinline__ double flux_y_at(const Geo& g, int lim, const double* c, const double* v,
-                                            int i, int j, double dt) {
-  const double vf = v[g.at(i, j)];
-  double num, den, r, cfl, cf;
+template <typename S>
+__device__ __forceinline__ S flux_y_at(const Geo& g, int lim, const S* c, const S* v, int i, int j, double dt) {
+  const S vf = v[g.at(i, j)];
+  S num, den, r, cfl, cf;
   if (vf >= 0.0) {
     num = c[g.at(i, j)] - c[g.at(i, j - 1)];
     den = c[g.at(i, j + 1)] - c[g.at(i, j)];
-    r = fabs(den) > 1.0e-12 ? num / den : 0.0;
+    r = fabs(den) > 1.0e-12 ? num / den : S(0.0);
     cfl = fabs(vf) * dt * g.idy;
     cf = c[g.at(i, j)] + 0.5 * (1.0 - cfl) * limiter_psi(lim, r) * den;
   } else {
     num = c[g.at(i, j + 2)] - c[g.at(i, j + 1)];
     den = c[g.at(i, j + 1)] - c[g.at(i, j)];
-    r = fabs(den) > 1.0e-12 ? num / den : 0.0;
+    r = fabs(den) > 1.0e-12 ? num / den : S(0.0);
     cfl = fabs(vf) * dt * g.idy;
     cf = c[g.at(i, j + 1)] - 0.5 * (1.0 - cfl) * limiter_psi(lim, r) * den;
   }
   return vf * clip01(cf);
 }
 // conservative update + clipping (mod_vof.f90:117-126); ghosts copied from C_in
-__global__ void k_vof_update(Geo g, int lim, const double* c, const double* u, const double* v,
-                             double dt, double* cout) {
+template <typename S>
+__global__ void k_vof_update(Geo g, int lim, const S* c, const S* u, const S* v, double dt, S* cout) {
   FUGU_BOX_IJ
-  double val = c[k];
+  S val = c[k];
   if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny) {
-    const double fe = flux_x_at(g, lim, c, u, i, j, dt), fw = flux_x_at(g, lim, c, u, i - 1, j, dt);
-    const double fn = flux_y_at(g, lim, c, v, i, j, dt), fs = flux_y_at(g, lim, c, v, i, j - 1, dt);
+    const S fe = flux_x_at(g, lim, c, u, i, j, dt), fw = flux_x_at(g, lim, c, u, i - 1, j, dt);
+    const S fn = flux_y_at(g, lim, c, v, i, j, dt), fs = flux_y_at(g, lim, c, v, i, j - 1, dt);
     val = clip01(c[k] - dt * ((fe - fw) * g.idx + (fn - fs) * g.idy));
   }
   cout[k] = val;
@@ -637,7 +645,8 @@ __device__ __forceinline__ int map_y(const Geo& g, int j) {
   return j < 1 ? 1 - j : 2 * g.ny + 1 - j;
 }
 // fill every ghost cell of a cell array from its interior (halo + Neumann)
-__global__ void k_fill_ghost_neumann(Geo g, double* a) {
+template <typename S>
+__global__ void k_fill_ghost_neumann(Geo g, S* a) {
   FUGU_BOX_IJ
   if (!in_kind(g, K_CELL, i, j)) return;
   if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny) return;
@@ -646,39 +655,43 @@ __global__ void k_fill_ghost_neumann(Geo g, double* a) {
 
 // compute_interface_curvature (mod_surface_tension.f90:25-72): face normals
 // on the fly, kappa = -div n at cells; ghosts 0 at walls or wrapped (halo).
-__device__ __forceinline__ double nx_face(const Geo& g, const double* cs, int i, int j) {
-  const double gx = (cs[g.at(i + 1, j)] - cs[g.at(i, j)]) * g.idx;
-  const double gy = 0.25 * (cs[g.at(i, j + 1)] + cs[g.at(i + 1, j + 1)] - cs[g.at(i, j - 1)] -
+template <typename S>
+__device__ __forceinline__ S nx_face(const Geo& g, const S* cs, int i, int j) {
+  const S gx = (cs[g.at(i + 1, j)] - cs[g.at(i, j)]) * g.idx;
+  const S gy = 0.25 * (cs[g.at(i, j + 1)] + cs[g.at(i + 1, j + 1)] - cs[g.at(i, j - 1)] -
                             cs[g.at(i + 1, j - 1)]) * g.idy;
   return gx / sqrt(gx * gx + gy * gy + 1.0e-12);
 }
-__device__ __forceinline__ double ny_face(const Geo& g, const double* cs, int i, int j) {
-  const double gx = 0.25 * (cs[g.at(i + 1, j)] + cs[g.at(i + 1, j + 1)] - cs[g.at(i - 1, j)] -
+template <typename S>
+__device__ __forceinline__ S ny_face(const Geo& g, const S* cs, int i, int j) {
+  const S gx = 0.25 * (cs[g.at(i + 1, j)] + cs[g.at(i + 1, j + 1)] - cs[g.at(i - 1, j)] -
                             cs[g.at(i - 1, j + 1)]) * g.idx;
-  const double gy = (cs[g.at(i, j + 1)] - cs[g.at(i, j)]) * g.idy;
+  const S gy = (cs[g.at(i, j + 1)] - cs[g.at(i, j)]) * g.idy;
   return gy / sqrt(gx * gx + gy * gy + 1.0e-12);
 }
-__global__ void k_curvature(Geo g, const double* cs, double* kc) {
+template <typename S>
+__global__ void k_curvature(Geo g, const S* cs, S* kc) {
   FUGU_BOX_IJ
-  if (!in_kind(g, K_CELL, i, j)) { kc[k] = 0.0; return; }
+  if (!in_kind(g, K_CELL, i, j)) { kc[k] = S(0.0); return; }
   int ci = i, cj = j;
   const bool gi = (i < 1 || i > g.nx), gj = (j < 1 || j > g.ny);
-  if ((gi && !g.px) || (gj && !g.py)) { kc[k] = 0.0; return; }
+  if ((gi && !g.px) || (gj && !g.py)) { kc[k] = S(0.0); return; }
   if (gi) ci = map_x(g, i);
   if (gj) cj = map_y(g, j);
   kc[k] = -((nx_face(g, cs, ci, cj) - nx_face(g, cs, ci - 1, cj)) * g.idx +
             (ny_face(g, cs, ci, cj) - ny_face(g, cs, ci, cj - 1)) * g.idy);
 }
 // compute_csf_force (mod_surface_tension.f90:78-109)
-__global__ void k_csf(Geo g, double sigma, const double* c, const double* kc, double* fu, double* fv) {
+template <typename S>
+__global__ void k_csf(Geo g, S sigma, const S* c, const S* kc, S* fu, S* fv) {
   FUGU_BOX_IJ
-  double a = 0.0, b = 0.0;
+  S a = S(0.0), b = S(0.0);
   if (j >= 1 && j <= g.ny && i >= 0 && i <= g.nx) {
-    const double kf = 0.5 * (kc[k] + kc[g.at(i + 1, j)]);
+    const S kf = 0.5 * (kc[k] + kc[g.at(i + 1, j)]);
     a = sigma * kf * (c[g.at(i + 1, j)] - c[k]) * g.idx;
   }
   if (i >= 1 && i <= g.nx && j >= 0 && j <= g.ny) {
-    const double kf = 0.5 * (kc[k] + kc[g.at(i, j + 1)]);
+    const S kf = 0.5 * (kc[k] + kc[g.at(i, j + 1)]);
     b = sigma * kf * (c[g.at(i, j + 1)] - c[k]) * g.idy;
   }
   fu[k] = a;
@@ -720,14 +733,17 @@ __global__ void k_accumulate(long n, double* x, const T* d, const double* scale)
 }
 
 // monolithic right-hand side (mod_solver_coupled.f90:261-303)
-struct RhsArgs {
-  const double *rho_u, *rho_v, *u_n, *u_nm1, *v_n, *v_nm1, *fsu, *fsv, *pen_u, *pen_v, *zeta, *eta;
+template <typename S>
+struct RhsArgsT {
+  const S *rho_u, *rho_v, *u_n, *u_nm1, *v_n, *v_nm1, *fsu, *fsv, *pen_u, *pen_v, *zeta, *eta;
   double dt, gx, gy, u_sol, v_sol, u_lid;
   int bdf2, has_lid;
 };
-__global__ void k_rhs(Geo g, RhsArgs a, double* Bu, double* Bv, double* Bp) {
+using RhsArgs = RhsArgsT<double>;
+template <typename S>
+__global__ void k_rhs(Geo g, RhsArgsT<S> a, S* Bu, S* Bv, S* Bp) {
   FUGU_BOX_IJ
-  double bu = 0.0, bv = 0.0;
+  S bu = S(0.0), bv = S(0.0);
   if (j >= 1 && j <= g.ny && i >= 1 && i <= g.imax()) {
     if (a.bdf2)
       bu = (a.rho_u[k] / a.dt) * (2.0 * a.u_n[k] - 0.5 * a.u_nm1[k]) + a.rho_u[k] * a.gx + a.fsu[k];
@@ -746,7 +762,7 @@ __global__ void k_rhs(Geo g, RhsArgs a, double* Bu, double* Bv, double* Bp) {
   }
   Bu[k] = bu;
   Bv[k] = bv;
-  Bp[k] = 0.0;
+  Bp[k] = S(0.0);
 }
 
 // max |u| over faces 0..nx x 1..ny and |v| over 1..nx x 0..ny

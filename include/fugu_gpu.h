@@ -295,6 +295,33 @@ int fugu_adjoint_solve(fugu_ctx* ctx, const double* g_u, const double* g_v, cons
                        const double* penalty_u, const double* penalty_v,
                        const double* mdot_u, const double* mdot_v, fugu_stats* st);
 
+/* Vector-Jacobian product of one whole step (no counterpart in the
+ * reference).  The step is the map of the state
+ *   (u_vel, v_vel, c_field, u_prev, v_prev)
+ *     -> (u_vel', v_vel', c_field', u_prev' = u_vel, v_prev' = v_vel)
+ * that fugu_step computes (mod_solver_coupled.f90:137-380): VOF transport,
+ * properties, SVOF, curvature, CSF, AB extrapolation, right-hand side and the
+ * coupled solve, taken as exact.  The context must hold the state before
+ * the step; the call runs the step (the context then holds the state after
+ * it, as after fugu_step) and applies the transpose of the step's Jacobian,
+ * for the branches the step took, to the adjoints of the state after it:
+ *   bar_*_out (adjoints of u_vel', v_vel', c_field', u_prev', v_prev';
+ *              reference-layout host arrays, every entry of the kind's extent)
+ *   -> bar_*_in (adjoints of the state before the step, same layout).
+ * p_field is only the solve's initial guess and has no adjoint.  bar_theta
+ * (may be NULL) accumulates += the derivatives with respect to
+ * {sigma, mu1, mu2, rho1, rho2}.  The step's own options apply (dt,
+ * step_idx, BDF order, lid, tolerance, which the adjoint solve also uses);
+ * wall-bounded boxes only, without consistent_amp or the Darcy penalty
+ * (FUGU_EINVAL otherwise).  st holds the forward step's statistics, with
+ * status the adjoint solve's when the forward step converged and outer its
+ * outer iterations. */
+int fugu_step_vjp(fugu_ctx* ctx, double dt, int step_idx, const fugu_step_opts* opts,
+                  const double* bar_u_out, const double* bar_v_out, const double* bar_c_out,
+                  const double* bar_uprev_out, const double* bar_vprev_out,
+                  double* bar_u_in, double* bar_v_in, double* bar_c_in,
+                  double* bar_uprev_in, double* bar_vprev_in, double* bar_theta, fugu_stats* st);
+
 /* mod_vof.f90:38-140 (flux_x/flux_y may be NULL), :145-194 */
 int fugu_vof_advection_tvd(fugu_ctx* ctx, const double* c_in, double* c_out,
                            const double* u, const double* v, double dt,

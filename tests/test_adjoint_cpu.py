@@ -1,8 +1,9 @@
 """Host side of the adjoint harness, no GPU: the closed-form mean velocity of
 the two-layer Poiseuille profile equals a quadrature of the profile the
 reference's test uses (tests/test_poiseuille_twophase.f90:307-323), its
-complex-step derivative equals central differences, and the mixture-law
-derivatives recover d mu / d mu_k."""
+complex-step derivative equals central differences, the mixture-law
+derivatives recover d mu / d mu_k, and the rising-bubble objective's seed
+dJ/dC equals central differences."""
 import numpy as np
 
 from coupled_codefort_2d_b200 import adjoint
@@ -37,3 +38,22 @@ def test_mixture_derivatives():
     h = 1e-7
     np.testing.assert_allclose(d1, 2.0 * (mu(C, mu1 + h, mu2) - mu(C, mu1 - h, mu2)) / (2 * h), rtol=1e-6, atol=1e-12)
     np.testing.assert_allclose(d2, 2.0 * (mu(C, mu1, mu2 + h) - mu(C, mu1, mu2 - h)) / (2 * h), rtol=1e-6, atol=1e-12)
+
+
+def test_centroid_objective_gradient():
+    """dJ/dC of the centroid height of fluid 2 (the rising-bubble adjoint's
+    seed) equals central differences, and is zero off the interior."""
+    pb = adjoint.RisingBubble(nx=12, ny=24, nsteps=1)
+    g = pb.g
+    rng = np.random.default_rng(0)
+    c = pb.c0 + 0.01 * rng.standard_normal(pb.c0.shape)
+    c = np.asfortranarray(c)
+    grad = pb.objective_grad(c)
+    for k in ((3, 4), (7, 20), (10, 13)):
+        cp, cm = c.copy(order="F"), c.copy(order="F")
+        cp[k] += 1e-6
+        cm[k] -= 1e-6
+        fd = (pb.objective(cp) - pb.objective(cm)) / 2e-6
+        assert abs(grad[k] - fd) <= 1e-8 * abs(fd)
+    assert not grad[0, :].any() and not grad[:, -1].any()
+    assert pb.params().svof_tol == 0.0 and abs(pb.dt - 1.0) < 1e-15

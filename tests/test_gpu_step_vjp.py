@@ -1,0 +1,184 @@
+"""The vector-Jacobian product of one coupled step (``fugu_step_vjp``) and the
+multi-step rising-bubble gradient built on it, against central differences
+of the GPU forward step.
+
+The step clips C to [0, 1] after transport, and a cell of pure fluid 1 sits
+on that clip: its new value is 1 - dt div(u), with div(u) at the solve's
+tolerance.  A perturbation of u that changes div(u) by more than that crosses
+the clip, so central differences along it mix two branches.  Velocity
+directions are therefore divergence-free (from a stream function that
+vanishes on the walls), as the solve's own responses are; the colour is
+perturbed on interface cells only.  The adjoint is the derivative of the
+branches the step took.
+
+Tolerances: relative 1e-5 for one step (h = 1e-5), 1e-5 for the gradient of
+the centroid height after 8 steps (h = 1e-4 relative; 1e-6 leaves the
+central difference with solver noise of the same size as the error sought).
+"""
+import numpy as np
+import pytest
+
+from coupled_codefort_2d_b200.adjoint import RisingBubble
+from coupled_codefort_2d_b200.context import VJP_STATE, Context
+from coupled_codefort_2d_b200._lib import FuguError
+from coupled_codefort_2d_b200.layout import Grid, at
+from coupled_codefort_2d_b200.params import Params
+
+pytestmark = pytest.mark.gpu
+
+DT = 2.5e-3
+
+
+def bubble(nsteps, checkpoint=3):
+    return RisingBubble(nx=24, ny=48, nsteps=nsteps, T=nsteps * DT, checkpoint=checkpoint, tol=1e-13)
+
+
+def divergence_free(rng, g):
+    """(u, v) = (d psi/dy, -d psi/dx) on the MAC faces, psi random at the
+    vertices and zero on the walls: the discrete divergence vanishes and so
+    do the wall faces."""
+    psi = np.zeros((g.nx + 1, g.ny + 1))
+    psi[1:-1, 1:-1] = rng.standard_normal((g.nx - 1, g.ny - 1))
+    du, dv = g.zeros("u"), g.zeros("v")
+    at(du, "u", slice(0, g.nx), slice(1, g.ny))[...] = (psi[:, 1:] - psi[:, :-1]) / g.dy
+    at(dv, "v", slice(1, g.nx), slice(0, g.ny))[...] = -(psi[1:, :] - psi[:-1, :]) / g.dx
+    s = max(np.abs(du).max(), np.abs(dv).max())  # unit entries: h d stays well below u
+    return du / s, dv / s
+
+
+def interface_cells(g, c, rng):
+    d = g.zeros("cell")
+    ci = at(c, "cell", slice(1, g.nx), slice(1, g.ny))
+    m = (ci > 0.02) & (ci < 0.98)
+    at(d, "cell", slice(1, g.nx), slice(1, g.ny))[...] = np.where(m, rng.standard_normal(ci.shape), 0.0)
+    return d
+
+
+@pytest.fixture(scope="module")
+def one_step(gpu):
+    """The state before step 4 of the small bubble, random adjoints of the
+    state after it, and the step's VJP."""
+    pb = bubble(3)
+    g = pb.g
+    rng = np.random.default_rng(3)
+    ctx = Context(g, pb.params())
+    opts = ctx.step_opts()
+    pb._put(ctx, pb._state0(None))
+    for s in range(1, 4):
+        ctx.step(DT, s, opts)
+    x = pb._get(ctx)
+    ybar = {k: np.asfortranarray(rng.standard_normal(g.shape(kind))) for k, kind in VJP_STATE}
+    pb._put(ctx, x)
+    bar, theta, st = ctx.step_vjp(DT, 4, opts, ybar)
+    yield pb, ctx, opts, x, ybar, bar, theta, st, rng
+    ctx.close()
+
+
+def phi(pb, ctx, opts, x, ybar):
+    pb._put(ctx, x)
+    st = ctx.step(DT, 4, opts)
+    assert st["status"] == 0
+    out = pb._get(ctx)
+    return sum(float(np.sum(ybar[k] * out[k])) for k, _ in VJP_STATE)
+
+
+def central(pb, ctx, opts, x, ybar, dirs, h=1e-5):
+    vals = []
+    for sgn in (1.0, -1.0):
+        xx = {k: a.copy(order="F") for k, a in x.items()}
+        for k, d in dirs.items():
+            xx[k] = xx[k] + sgn * h * d
+        vals.append(phi(pb, ctx, opts, xx, ybar))
+    return (vals[0] - vals[1]) / (2 * h)
+
+
+def test_step_vjp_converges(one_step):
+    *_, st, _ = one_step
+    assert st["status"] == 0 and st["res"] < 1e-13 and st["svof_iters"] == 150
+
+
+@pytest.mark.parametrize("which", ["velocity", "colour", "previous_velocity", "all"])
+def test_step_vjp_matches_central_differences(one_step, which):
+    pb, ctx, opts, x, ybar, bar, _, _, _ = one_step
+    g = pb.g
+    rng = np.random.default_rng({"velocity": 1, "colour": 2, "previous_velocity": 4, "all": 5}[which])
+    dirs = {}
+    if which in ("velocity", "all"):
+        dirs["u_vel"], dirs["v_vel"] = divergence_free(rng, g)
+    if which in ("colour", "all"):
+        dirs["c_field"] = interface_cells(g, x["c_field"], rng)
+    if which in ("previous_velocity", "all"):
+        dirs["u_prev"] = np.asfortranarray(rng.standard_normal(g.shape("u")))
+        dirs["v_prev"] = np.asfortranarray(rng.standard_normal(g.shape("v")))
+    ad = sum(float(np.sum(bar[k] * d)) for k, d in dirs.items())
+    fd = central(pb, ctx, opts, x, ybar, dirs)
+    assert abs(ad - fd) <= 1e-5 * abs(fd), (ad, fd)
+
+
+@pytest.mark.parametrize("q,name", list(enumerate(RisingBubble.PARAMS)))
+def test_step_vjp_parameters(one_step, q, name):
+    pb, ctx, opts, x, ybar, _, theta, _, _ = one_step
+    v0 = pb.phys[name]
+    h = 1e-5 * v0
+    vals = []
+    for sgn in (1.0, -1.0):
+        ctx.set_params(pb.params(**{name: v0 + sgn * h}))
+        vals.append(phi(pb, ctx, opts, x, ybar))
+    ctx.set_params(pb.params())
+    fd = (vals[0] - vals[1]) / (2 * h)
+    assert abs(theta[q] - fd) <= 1e-5 * abs(fd), (theta[q], fd)
+
+
+@pytest.fixture(scope="module")
+def gradient(gpu):
+    pb = bubble(8)
+    return pb, pb.value_and_grad()
+
+
+def test_bubble_value_matches_forward_run(gradient):
+    pb, (J, _, _) = gradient
+    assert J == pb.value()
+    assert 0.5 < J < 0.51  # the bubble has started to rise
+
+
+@pytest.mark.parametrize("name", ["sigma", "mu1"])
+def test_bubble_parameter_gradient(gradient, name):
+    pb, (_, grads, _) = gradient
+    v0 = pb.phys[name]
+    h = 1e-4 * v0
+    fd = (pb.value(**{name: v0 + h}) - pb.value(**{name: v0 - h})) / (2 * h)
+    assert abs(grads[name] - fd) <= 1e-5 * abs(fd), (grads[name], fd)
+
+
+def test_bubble_initial_colour_gradient(gradient):
+    pb, (_, _, dc0) = gradient
+    g = pb.g
+    ci = at(pb.c0, "cell", slice(1, g.nx), slice(1, g.ny))
+    cells = np.argwhere((ci > 0.1) & (ci < 0.9))[::7][:3]
+    for i0, j0 in cells:
+        k = (i0 + 2, j0 + 2)  # interior (i0 + 1, j0 + 1) in the cell array (lower bound -1)
+        h = 1e-4
+        cp, cm = pb.c0.copy(order="F"), pb.c0.copy(order="F")
+        cp[k] += h
+        cm[k] -= h
+        fd = (pb.value(c0=cp) - pb.value(c0=cm)) / (2 * h)
+        assert abs(dc0[k] - fd) <= 1e-6 * abs(fd), (k, dc0[k], fd)
+
+
+def test_bubble_gradient_independent_of_checkpointing(gradient):
+    pb, (J, grads, dc0) = gradient
+    J2, grads2, dc02 = bubble(8, checkpoint=8).value_and_grad()
+    assert J2 == J
+    assert grads2 == grads
+    np.testing.assert_array_equal(dc02, dc0)
+
+
+def test_step_vjp_rejects_unsupported_cases(gpu):
+    g = Grid(16, 16, periodic_x=True)
+    with Context(g, Params(sigma=1.0)) as ctx:
+        with pytest.raises(FuguError):
+            ctx.step_vjp(1e-3, 1, ctx.step_opts(), {})
+    g = Grid(16, 16)
+    with Context(g, Params(sigma=1.0)) as ctx:
+        with pytest.raises(FuguError):
+            ctx.step_vjp(1e-3, 1, ctx.step_opts(consistent_amp=True), {})
