@@ -4,6 +4,7 @@ per configuration).
     python -m coupled_codefort_2d_b200.configs c1            # lid-driven cavity, 128^2, 200 steps
     python -m coupled_codefort_2d_b200.configs c2            # static droplet, 256^2, 500 steps
     python -m coupled_codefort_2d_b200.configs c3 --steps N  # rising bubble, 320x640 (6000 steps to t = 3)
+    python -m coupled_codefort_2d_b200.configs c5            # adjoint gradients, 160x320, 400 steps
 
 c1: cavity on the unit square, rho = 1, mu = 1e-3 (Re = 1000), lid u = 1, BDF1,
 dt = 1e-2, tolerance 1e-10, zero initial fields.  The reference's own solver
@@ -22,6 +23,15 @@ free-slip sides, BDF2, dt = 5e-4; the high-contrast variant has bubble rho 1,
 mu 0.1, sigma 1.96.  Mixed precision against FP64: centroid height, rise
 velocity (``tests/test_rising_bubble.f90:134-155``) and circularity, and their
 differences.
+
+c5: the discrete adjoint.  Rising bubble (outer rho 1000, mu 10; bubble rho
+100, mu 1; sigma 24.5; g = 0.98; area-fraction disc) on 160 x 320, 400 BDF2
+steps of dt = 2.5e-3 in FP64 (T = 1), checkpoints every 20 steps; J = the
+centroid height at T.  dJ/dsigma, dJ/dmu1 (outer viscosity) and dJ/dC0 for
+two interface cells against central differences of the GPU forward run
+(h = 1e-6 relative, and 1e-4 for the parameters).  Second check: the steady
+two-phase Poiseuille channel, 64 x 128, mu ratio 10, body force 1, against
+the analytic derivative of the two-layer profile.
 
 Every run is synthetic: the fields are fully determined by the parameters.
 """
@@ -149,14 +159,77 @@ def config_c3(args):
     return rep
 
 
+def _fd_check(ad, fd):
+    return {"adjoint": float(ad), "central_difference": float(fd),
+            "rel_difference": float(abs(ad - fd) / max(abs(fd), 1e-300))}
+
+
+def config_c5(args):
+    from .adjoint import RisingBubble, SteadyPoiseuille, analytic_grad
+
+    steps = args.steps or 400
+    pb = RisingBubble(160, 320, nsteps=steps, T=steps * 2.5e-3, checkpoint=20, tol=1e-12, device=args.device)
+    g = pb.g
+    rep = {"config": "c5", "workload": f"rising_bubble_adjoint_160x320_{steps}_steps", "steps": steps,
+           "dt": pb.dt, "checkpoint_every": pb.checkpoint, "tolerance": pb.tol}
+    t0 = time.perf_counter()
+    J, grads, dc0 = pb.value_and_grad()
+    rep["gradient_seconds"] = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    J_fwd = pb.value()
+    rep["forward_seconds"] = time.perf_counter() - t0
+    rep["J_y_centroid"] = J
+    rep["J_equals_forward_run"] = J == J_fwd
+    rep["gradient"] = {k: float(v) for k, v in grads.items()}
+    checks = {}
+    for name in ("sigma", "mu1"):
+        v0 = pb.phys[name]
+        for hr in (1e-6, 1e-4):
+            h = hr * v0
+            fd = (pb.value(**{name: v0 + h}) - pb.value(**{name: v0 - h})) / (2 * h)
+            checks[f"d{name}_h{hr:g}"] = _fd_check(grads[name], fd)
+    ci = at(pb.c0, "cell", slice(1, g.nx), slice(1, g.ny))
+    di = at(dc0, "cell", slice(1, g.nx), slice(1, g.ny))
+    iface = (ci > 0.1) & (ci < 0.9)
+    big = np.unravel_index(np.argmax(np.where(iface, np.abs(di), 0.0)), ci.shape)
+    other = [tuple(t) for t in np.argwhere(iface)][len(np.argwhere(iface)) // 3]
+    for i0, j0 in (big, other):
+        k = (int(i0) + 2, int(j0) + 2)  # the cell array's lower bound is -1
+        h = 1e-6 * float(pb.c0[k])
+        cp, cm = pb.c0.copy(order="F"), pb.c0.copy(order="F")
+        cp[k] += h
+        cm[k] -= h
+        fd = (pb.value(c0=cp) - pb.value(c0=cm)) / (2 * h)
+        checks[f"dC0_cell_{int(i0) + 1}_{int(j0) + 1}_h1e-06"] = _fd_check(dc0[k], fd)
+    rep["bubble_checks"] = checks
+    # the second check: steady two-phase Poiseuille, 64 x 128, mu ratio 10,
+    # against the analytic derivative of the two-layer profile
+    pp = SteadyPoiseuille(nx=64, ny=128, device=args.device)
+    try:
+        mu1, mu2 = 1.0, 0.1
+        Jp, gp, _ = pp.value_and_grad(mu1, mu2)
+        a1, a2 = analytic_grad(mu1, mu2)
+        h = 1e-6
+        fd1 = (pp.value(mu1 + h * mu1, mu2) - pp.value(mu1 - h * mu1, mu2)) / (2 * h * mu1)
+        rep["poiseuille_64x128"] = {
+            "mean_velocity": Jp, "dmu1": _fd_check(gp[0], fd1),
+            # d/d(mu1/mu2) at fixed mu2 = mu2 d/dmu1
+            "d_ratio_adjoint": mu2 * gp[0], "d_ratio_analytic": mu2 * a1,
+            "d_ratio_rel_difference": abs(gp[0] - a1) / abs(a1),
+            "dmu2_adjoint": gp[1], "dmu2_analytic": a2}
+    finally:
+        pp.close()
+    return rep
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description="run a benchmark configuration and print its report")
-    ap.add_argument("config", choices=["c1", "c2", "c3"])
+    ap.add_argument("config", choices=["c1", "c2", "c3", "c5"])
     ap.add_argument("--steps", type=int, default=0, help="override the configuration's step count")
     ap.add_argument("--variant", default="standard", choices=["standard", "high_contrast"], help="c3 only")
     ap.add_argument("--device", type=int, default=0)
     args = ap.parse_args(argv)
-    rep = {"c1": config_c1, "c2": config_c2, "c3": config_c3}[args.config](args)
+    rep = {"c1": config_c1, "c2": config_c2, "c3": config_c3, "c5": config_c5}[args.config](args)
     print(json.dumps(rep), flush=True)
 
 
