@@ -5,6 +5,7 @@ per configuration).
     python -m coupled_codefort_2d_b200.configs c2            # static droplet, 256^2, 500 steps
     python -m coupled_codefort_2d_b200.configs c3 --steps N  # rising bubble, 320x640 (6000 steps to t = 3)
     python -m coupled_codefort_2d_b200.configs c5            # adjoint gradients, 160x320, 400 steps
+    python -m coupled_codefort_2d_b200.configs scale --n 2048 --steps 1   # droplet at n x n (HBM-bound)
 
 c1: cavity on the unit square, rho = 1, mu = 1e-3 (Re = 1000), lid u = 1, BDF1,
 dt = 1e-2, tolerance 1e-10, zero initial fields.  The reference's own solver
@@ -33,6 +34,12 @@ two interface cells against central differences of the GPU forward run
 two-phase Poiseuille channel, 64 x 128, mu ratio 10, body force 1, against
 the analytic derivative of the two-layer profile.
 
+scale: the c2 droplet (BDF2, dt = 1e-4, the bench's solver) on an n x n grid
+with n large enough that every field is far larger than the 126 MB L2 (2048^2:
+34 MB per FP64 field), so that each kernel of the step streams HBM.  It is the
+workload of the per-kernel HBM roofline (ncu launch list of its first step);
+colour by 4 x 4 sub-sampling.  Reports steps/s and the device memory held.
+
 Every run is synthetic: the fields are fully determined by the parameters.
 """
 from __future__ import annotations
@@ -55,7 +62,7 @@ STATE = ("u_vel", "v_vel", "p_field", "c_field", "u_prev", "v_prev", "rho_c", "r
          "eta", "kappa_curv", "f_sigma_u", "f_sigma_v")
 
 
-def _run(g, prm, c0, precision, nsteps, dt, lid=None, every=None, device=0):
+def _run(g, prm, c0, precision, nsteps, dt, lid=None, every=None, device=0, on_step=None):
     """Advance nsteps from rest; returns the final state, per-step stats and
     seconds of stepping (CUDA-synchronised wall clock)."""
     import torch
@@ -74,6 +81,8 @@ def _run(g, prm, c0, precision, nsteps, dt, lid=None, every=None, device=0):
             stats.append(ctx.step(dt, s, opts))
             if every and s % every == 0:
                 hist.append((s, ctx.download_state(["c_field", "v_vel"])))
+            if on_step:
+                on_step(s, ctx)
         torch.cuda.synchronize()
         secs = time.perf_counter() - t0
         out = ctx.download_state(list(STATE))
@@ -222,14 +231,39 @@ def config_c5(args):
     return rep
 
 
+def config_scale(args):
+    import torch
+
+    n = args.n
+    g = Grid(n, n)
+    prm = Params(rho1=1.0, rho2=0.1, mu1=0.1, mu2=0.01, sigma=1.0, gx=0.0, gy=0.0, time_order=2,
+                 tol_bicgstab2=1e-8, max_iter_bicgstab2=500, **SOLVER)
+    steps = args.steps or 1
+    c0 = cases.circle_fraction(g, 0.5, 0.5, 0.25, inside=1.0, ns=4)
+    prec = {"mixed": MIXED, "fp64": FP64}[args.precision]
+    free0, total = torch.cuda.mem_get_info(args.device)
+    peak = [0]
+
+    def probe(_s, _ctx):
+        peak[0] = max(peak[0], free0 - torch.cuda.mem_get_info(args.device)[0])
+
+    _, stats, secs, _ = _run(g, prm, c0, prec, steps, 1e-4, device=args.device, on_step=probe)
+    return {"config": "scale", "workload": f"static_droplet_{n}x{n}", "steps": steps, "precision": args.precision,
+            **_summary(stats, secs), **{k: [s[k] for s in stats] for k in ("outer", "iter", "pcg_calls", "pcg_iters",
+                                                                                "svof_iters")},
+            "device_bytes_held": peak[0], "device_bytes_total": total}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description="run a benchmark configuration and print its report")
-    ap.add_argument("config", choices=["c1", "c2", "c3", "c5"])
+    ap.add_argument("config", choices=["c1", "c2", "c3", "c5", "scale"])
     ap.add_argument("--steps", type=int, default=0, help="override the configuration's step count")
     ap.add_argument("--variant", default="standard", choices=["standard", "high_contrast"], help="c3 only")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--n", type=int, default=2048, help="scale only: cells per side")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="scale only")
     args = ap.parse_args(argv)
-    rep = {"c1": config_c1, "c2": config_c2, "c3": config_c3, "c5": config_c5}[args.config](args)
+    rep = {"c1": config_c1, "c2": config_c2, "c3": config_c3, "c5": config_c5, "scale": config_scale}[args.config](args)
     print(json.dumps(rep), flush=True)
 
 
