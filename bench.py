@@ -269,6 +269,8 @@ def batched_arm(world, rank, local_rank):
             "value": res["case_steps_per_s"], "unit": "case-steps/s", "steps": BATCH_STEPS, "warmup": 1,
             "seconds": res["seconds"], "dtype": "f32 inner / f64 outer", "max_true_residual":
             max(r["max_res"] for r in rows), "failed_cases": [r["case"] for r in rows if r["status"] != 0],
+            "solver": "FP64 defect correction around flexible GMRES(30) + PCD (PCG cap adaptive 40-150, "
+                      "red-black SOR velocity smoother omega 1.5, sweeps adaptive 6-24)", "solver_params": ensemble.SOLVER,
             "fp64_single_case": {"value": fp64_single, "unit": "case-steps/s", "cases": n64},
             "batched_mixed_over_fp64_single": res["case_steps_per_s"] / world / fp64_single,
             "timing": "host wall clock around the batch run, CUDA-synchronised, max over ranks"}

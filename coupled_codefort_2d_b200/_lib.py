@@ -43,7 +43,8 @@ class FuguParams(C.Structure):
         ("svof_tol", C.c_double), ("limiter", C.c_int), ("free_slip_x", C.c_int),
         ("krylov_bc_fix", C.c_int), ("refine", C.c_int), ("refine_inner_tol", C.c_double),
         ("refine_max_inner", C.c_int), ("refine_max_outer", C.c_int), ("precision", C.c_int),
-        ("pcg_cap_start", C.c_int), ("pcd_sweeps_max", C.c_int),
+        ("pcg_cap_start", C.c_int), ("pcd_sweeps_max", C.c_int), ("pcd_smoother", C.c_int),
+        ("pcd_sor_omega", C.c_double),
     ]
 
 

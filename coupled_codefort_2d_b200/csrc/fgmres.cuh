@@ -155,10 +155,24 @@ __global__ void __launch_bounds__(MDOT_TPB) k_mdot(MdotArgs<T> a) {
       base = 2 * a.n + g.at(1, 1 + (int)(r / cv));
       len = nx;
     }
-    const int i1 = min(len, (c + 1) * MDOT_CHUNK);
-    for (int i = c * MDOT_CHUNK + lane; i < i1; i += 32) {
-      const long e = base + i;
-      dd_add(acc, (double(a.w[e]) * double(V[e])) * a.vol);
+    const int i0 = c * MDOT_CHUNK + lane, i1 = min(len, (c + 1) * MDOT_CHUNK);
+    if (i1 - c * MDOT_CHUNK == MDOT_CHUNK) {
+      // a full chunk: issue the lane's 2 x 4 loads before the dependent
+      // double-double chain (same accumulation order as the loop below)
+      constexpr int U = MDOT_CHUNK / 32;
+      T wv[U], vv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        wv[u] = a.w[base + i0 + 32 * u];
+        vv[u] = V[base + i0 + 32 * u];
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) dd_add(acc, (double(wv[u]) * double(vv[u])) * a.vol);
+    } else {
+      for (int i = i0; i < i1; i += 32) {
+        const long e = base + i;
+        dd_add(acc, (double(a.w[e]) * double(V[e])) * a.vol);
+      }
     }
   }
   for (int o = 16; o > 0; o >>= 1) acc = dd_merge(acc, dd_shfl_down(acc, o));
@@ -206,7 +220,17 @@ __global__ void k_maxpy(long n3, T* w, const T* V0, long stride, const double* c
   __syncthreads();
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n3; q += (long)gridDim.x * blockDim.x) {
     T x = w[q];
-    for (int i = 0; i < nvec; ++i) x = x + s[i] * V0[i * stride + q];
+    int i = 0;
+    // four vectors' loads in flight before the (ordered) dependent updates
+    for (; i + 4 <= nvec; i += 4) {
+      const T v0 = V0[i * stride + q], v1 = V0[(i + 1) * stride + q];
+      const T v2 = V0[(i + 2) * stride + q], v3 = V0[(i + 3) * stride + q];
+      x = x + s[i] * v0;
+      x = x + s[i + 1] * v1;
+      x = x + s[i + 2] * v2;
+      x = x + s[i + 3] * v3;
+    }
+    for (; i < nvec; ++i) x = x + s[i] * V0[i * stride + q];
     w[q] = x;
   }
 }

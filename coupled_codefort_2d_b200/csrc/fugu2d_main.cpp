@@ -10,7 +10,8 @@
 //
 // Extra namelist keys (this build): use_gpu (accepted, the path is the GPU),
 // precision ('fp64' | 'mixed'), refine (logical or 0 / 1 / 2), refine_inner_tol, refine_max_inner,
-// refine_max_outer, pcg_max_iter, pcg_cap_start, pcd_sweeps, pcd_sweeps_max, krylov_bc_fix,
+// refine_max_outer, pcg_max_iter, pcg_cap_start, pcd_sweeps, pcd_sweeps_max, pcd_smoother
+// ('jacobi' | 'rbsor'), pcd_sor_omega, krylov_bc_fix,
 // limiter ('vanleer' | 'superbee'),
 // free_slip_x, device.
 //
@@ -51,10 +52,10 @@ struct Settings {
   int max_iter_bicgstab2 = 500;
   double alpha_penalty = 1.0e12;
   // extensions
-  std::string precision = "fp64", limiter = "vanleer";
+  std::string precision = "fp64", limiter = "vanleer", pcd_smoother = "jacobi";
   int refine = 0, refine_max_inner = 20, refine_max_outer = 30, krylov_bc_fix = 0, free_slip_x = 0, device = 0;
   int pcg_max_iter = 150, pcg_cap_start = 0, pcd_sweeps = 3, pcd_sweeps_max = 0;
-  double refine_inner_tol = 1.0e-2;
+  double refine_inner_tol = 1.0e-2, pcd_sor_omega = 1.0;
 };
 
 std::string lower(std::string s) {
@@ -209,6 +210,8 @@ bool apply(Settings& st, const std::map<std::string, std::string>& kv, std::stri
     else if (k == "pcg_cap_start") st.pcg_cap_start = (int)fnum(v);
     else if (k == "pcd_sweeps") st.pcd_sweeps = (int)fnum(v);
     else if (k == "pcd_sweeps_max") st.pcd_sweeps_max = (int)fnum(v);
+    else if (k == "pcd_smoother") st.pcd_smoother = lower(fstr(v));
+    else if (k == "pcd_sor_omega") st.pcd_sor_omega = fnum(v);
     else if (k == "krylov_bc_fix") st.krylov_bc_fix = flog(v) ? 1 : 0;
     else if (k == "free_slip_x") st.free_slip_x = flog(v) ? 1 : 0;
     else if (k == "device") st.device = (int)fnum(v);
@@ -366,6 +369,7 @@ int main(int argc, char** argv) {
   p.refine_max_inner = st.refine_max_inner; p.refine_max_outer = st.refine_max_outer;
   p.pcg_max_iter = st.pcg_max_iter; p.pcg_cap_start = st.pcg_cap_start;
   p.pcd_sweeps = st.pcd_sweeps; p.pcd_sweeps_max = st.pcd_sweeps_max;
+  p.pcd_smoother = st.pcd_smoother == "rbsor" ? 1 : 0; p.pcd_sor_omega = st.pcd_sor_omega;
   p.precision = st.precision == "mixed" ? FUGU_MIXED : FUGU_FP64;
   fugu_ctx* ctx = nullptr;
   int rc = fugu_create(&p, st.device, &ctx);

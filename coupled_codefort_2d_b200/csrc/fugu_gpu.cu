@@ -566,6 +566,20 @@ void helmholtz(fugu_ctx* c, bool is_u, T* sol, T* tmp, const T* rhs, const CoefB
   T* cur = sol;
   T* nxt = tmp;
   const T* pen = o.pen ? (is_u ? cb.pen_u : cb.pen_v) : nullptr;
+  if (c->prm.pcd_smoother == 1) {  // red-black SOR in place (extension)
+    for (int s = 0; s < n_sweeps; ++s)
+      for (int col = 0; col < 2; ++col) {
+        halo(c, sol, is_u ? K_U : K_V, active);
+        if (is_u)
+          k_rbsor_u<T><<<b.grid, b.block, 0, c->s>>>(c->g, sol, rhs, cb.rho_u, cb.kappa, cb.zeta, cb.eta, pen,
+                                                     T(dt), T(c->prm.pcd_sor_omega), col, active);
+        else
+          k_rbsor_v<T><<<b.grid, b.block, 0, c->s>>>(c->g, sol, rhs, cb.rho_v, cb.kappa, cb.zeta, cb.eta, pen,
+                                                     T(dt), T(c->prm.pcd_sor_omega), col, active);
+        CKL("k_rbsor");
+      }
+    return;
+  }
   for (int s = 0; s < n_sweeps; ++s) {
     halo(c, cur, is_u ? K_U : K_V, active);
     if (is_u)
@@ -800,9 +814,10 @@ void mdot(fugu_ctx* c, const T* w, const T* V0, int nvec, int op, int j, double 
   a.op = op;
   a.j = j;
   a.tol = tol;
-  // about two CTAs per SM over all vectors, each with a work item per warp
+  // about four CTAs per SM over all vectors (enough loads in flight when the
+  // vectors stream from HBM), each with a work item per warp
   const long per_cta = MDOT_TPB / 32;
-  long G = (2L * c->nsm + nvec - 1) / nvec;
+  long G = (4L * c->nsm + nvec - 1) / nvec;
   const long gmax = (mdot_items(c->g) + per_cta - 1) / per_cta;
   if (G > gmax) G = gmax;
   if (G < 1) G = 1;
@@ -1213,6 +1228,8 @@ int check_params(const fugu_params* p) {
   // flexible GMRES keeps one projection per basis vector in shared memory
   if (p->refine == 2 && (p->refine_max_inner < 1 || p->refine_max_inner > 127)) return FUGU_EINVAL;
   if (p->precision != FUGU_FP64 && p->precision != FUGU_MIXED) return FUGU_EINVAL;
+  if (p->pcd_smoother < 0 || p->pcd_smoother > 1) return FUGU_EINVAL;
+  if (p->pcd_smoother == 1 && !(p->pcd_sor_omega > 0.0 && p->pcd_sor_omega < 2.0)) return FUGU_EINVAL;
   return FUGU_OK;
 }
 
@@ -1357,6 +1374,7 @@ void fugu_params_default(fugu_params* p) {
   p->svof_delta_h = 1.5; p->svof_max_iter = 150; p->svof_tol = 1.0e-7;
   p->refine_inner_tol = 1.0e-2; p->refine_max_inner = 20; p->refine_max_outer = 30;
   p->precision = FUGU_FP64;
+  p->pcd_smoother = 0; p->pcd_sor_omega = 1.0;
 }
 
 const char* fugu_version(void) { return "fugu-b200 1 (sm_100a)"; }

@@ -521,6 +521,30 @@ __global__ void k_jacobi_v(Geo g, const T* vo, T* vn, const T* rhs, const T* rho
   vn[k] = jacobi_v_at<T>(g, k, i, j, vo, rhs, rho_v, kap, zeta, eta, pen, dt, om);
 }
 
+// One colour pass of the red-black SOR smoother (extension, pcd_smoother = 1):
+// the faces with (i + j) & 1 == col take the damped-Jacobi formula above with
+// omega = pcd_sor_omega, reading u in place.  Every neighbour of such a face
+// has the other colour (ghosts were refreshed before the pass and are not
+// written), so the pass is race-free and order-independent.
+template <typename T>
+__global__ void k_rbsor_u(Geo g, T* u, const T* rhs, const T* rho_u, const T* kap, const T* zeta, const T* eta,
+                          const T* pen, T dt, T om, int col, const int* active) {
+  if (active && !*active) return;
+  FUGU_BOX_IJ
+  if (j < 1 || j > g.ny || ((i + j) & 1) != col) return;
+  if (!((i >= 1 && i <= g.imax()) || (!g.px && (i == 0 || i == g.nx)))) return;
+  u[k] = jacobi_u_at<T>(g, k, i, j, u, rhs, rho_u, kap, zeta, eta, pen, dt, om);
+}
+template <typename T>
+__global__ void k_rbsor_v(Geo g, T* v, const T* rhs, const T* rho_v, const T* kap, const T* zeta, const T* eta,
+                          const T* pen, T dt, T om, int col, const int* active) {
+  if (active && !*active) return;
+  FUGU_BOX_IJ
+  if (i < 1 || i > g.nx || ((i + j) & 1) != col) return;
+  if (!((j >= 1 && j <= g.jmax()) || (!g.py && (j == 0 || j == g.ny)))) return;
+  v[k] = jacobi_v_at<T>(g, k, i, j, v, rhs, rho_v, kap, zeta, eta, pen, dt, om);
+}
+
 // ------------------------------------------------------------ Krylov vectors
 // Whole-buffer linear combinations over a coupled triple (u, v, p buffers of
 // n elements each, contiguous in one allocation of 3n).  Coefficients are

@@ -52,6 +52,11 @@ class Params:
     # refine = 2: when the PCG cap cannot grow, a missed inner tolerance doubles
     # the PCD's Jacobi sweeps up to this many (<= pcd_sweeps: off)
     pcd_sweeps_max: int = 0
+    # the PCD's velocity smoother: 0 damped Jacobi (jacobi_omega, the
+    # reference), 1 red-black SOR with pcd_sor_omega (in place, two colour
+    # passes per sweep)
+    pcd_smoother: int = 0
+    pcd_sor_omega: float = 1.0
 
     def with_(self, **kw) -> "Params":
         return replace(self, **kw)

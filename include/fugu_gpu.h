@@ -92,6 +92,13 @@ typedef struct {
                                  refine_inner_tol doubles the PCD's Jacobi
                                  sweeps instead, up to this many; carried
                                  from step to step like the cap              */
+  int pcd_smoother;           /* velocity smoother of the PCD: 0 the
+                                 reference's damped Jacobi (jacobi_omega,
+                                 mod_subsolvers.f90:252-372); 1 red-black SOR
+                                 with pcd_sor_omega: each sweep updates the
+                                 faces with (i + j) even, then the odd ones,
+                                 in place, the halo refreshed before each     */
+  double pcd_sor_omega;       /* 1.0 (Gauss-Seidel); 0 < omega < 2          */
 } fugu_params;
 
 /* Optional arguments of advance_coupled_step (src/mod_solver_coupled.f90:137-160):

@@ -77,6 +77,7 @@ void fo_model_defaults(fo_model* m) {
   m->pcg_tol = 1.0e-5; m->pcg_max_iter = 150; m->pcd_sweeps = 3;
   m->jacobi_omega = 0.8; m->svof_delta_h = 1.5; m->svof_max_iter = 150;
   m->svof_tol = 1.0e-7; m->limiter = 0; m->free_slip_x = 0;
+  m->pcd_smoother = 0; m->pcd_sor_omega = 1.0;
 }
 
 /* ---------------------------------------------------------------------- */
@@ -573,6 +574,34 @@ void fo_solve_helmholtz_u(const fo_model* m, double* u_sol, const double* rhs_u,
   const int nx = m->nx, ny = m->ny, imax = iu_max(m);
   const double om = m->jacobi_omega;
   const double idx2 = 1.0 / (m->dx * m->dx), idy2 = 1.0 / (m->dy * m->dy);
+  if (m->pcd_smoother == 1) {
+    /* red-black SOR (extension): in place, colour (i + j) & 1 per pass */
+    const double w = m->pcd_sor_omega;
+    for (int s = 0; s < n_sweeps; ++s)
+      for (int col = 0; col < 2; ++col) {
+        fo_halo_u(m, u_sol);
+        for (int j = 1; j <= ny; ++j) {
+          for (int i = 1; i <= imax; ++i) {
+            if (((i + j) & 1) != col) continue;
+            double cE = AC(kappa, i + 1, j) * idx2;
+            double cW = AC(kappa, i, j) * idx2;
+            double cN = (AW(zeta, i, j) - AW(eta, i, j)) * idy2;
+            double cS = (AW(zeta, i, j - 1) - AW(eta, i, j - 1)) * idy2;
+            double diag = (AU(rho_u, i, j) / dt) + cE + cW + cN + cS;
+            if (pen_u) diag = diag + AU(pen_u, i, j);
+            double off = cE * AU(u_sol, i + 1, j) + cW * AU(u_sol, i - 1, j) +
+                         cN * AU(u_sol, i, j + 1) + cS * AU(u_sol, i, j - 1);
+            if (diag > 1.0e-15)
+              AU(u_sol, i, j) = (1.0 - w) * AU(u_sol, i, j) + w * ((AU(rhs_u, i, j) + off) / diag);
+          }
+          if (!m->periodic_x) {
+            if ((j & 1) == col) AU(u_sol, 0, j) = AU(rhs_u, 0, j);
+            if (((nx + j) & 1) == col) AU(u_sol, nx, j) = AU(rhs_u, nx, j);
+          }
+        }
+      }
+    return;
+  }
   double* u_old = zalloc(n_u(m));
   for (int s = 0; s < n_sweeps; ++s) {
     fo_halo_u(m, u_sol);
@@ -606,6 +635,34 @@ void fo_solve_helmholtz_v(const fo_model* m, double* v_sol, const double* rhs_v,
   const int nx = m->nx, ny = m->ny, jmax = jv_max(m);
   const double om = m->jacobi_omega;
   const double idx2 = 1.0 / (m->dx * m->dx), idy2 = 1.0 / (m->dy * m->dy);
+  if (m->pcd_smoother == 1) {
+    /* red-black SOR (extension): in place, colour (i + j) & 1 per pass */
+    const double w = m->pcd_sor_omega;
+    for (int s = 0; s < n_sweeps; ++s)
+      for (int col = 0; col < 2; ++col) {
+        fo_halo_v(m, v_sol);
+        for (int j = 1; j <= jmax; ++j)
+          for (int i = 1; i <= nx; ++i) {
+            if (((i + j) & 1) != col) continue;
+            double cE = (AW(zeta, i, j) - AW(eta, i, j)) * idx2;
+            double cW = (AW(zeta, i - 1, j) - AW(eta, i - 1, j)) * idx2;
+            double cN = AC(kappa, i, j + 1) * idy2;
+            double cS = AC(kappa, i, j) * idy2;
+            double diag = (AV(rho_v, i, j) / dt) + cE + cW + cN + cS;
+            if (pen_v) diag = diag + AV(pen_v, i, j);
+            double off = cE * AV(v_sol, i + 1, j) + cW * AV(v_sol, i - 1, j) +
+                         cN * AV(v_sol, i, j + 1) + cS * AV(v_sol, i, j - 1);
+            if (diag > 1.0e-15)
+              AV(v_sol, i, j) = (1.0 - w) * AV(v_sol, i, j) + w * ((AV(rhs_v, i, j) + off) / diag);
+          }
+        if (!m->periodic_y)
+          for (int i = 1; i <= nx; ++i) {
+            if ((i & 1) == col) AV(v_sol, i, 0) = AV(rhs_v, i, 0);
+            if (((i + ny) & 1) == col) AV(v_sol, i, ny) = AV(rhs_v, i, ny);
+          }
+      }
+    return;
+  }
   double* v_old = zalloc(n_v(m));
   for (int s = 0; s < n_sweeps; ++s) {
     fo_halo_v(m, v_sol);

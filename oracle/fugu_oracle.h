@@ -74,6 +74,12 @@ typedef struct {
   /* refine = 2: once the cap cannot grow, a missed inner tolerance doubles
    * the PCD's Jacobi sweeps up to pcd_sweeps_max (<= pcd_sweeps: off) */
   int pcd_sweeps_max;
+  /* velocity smoother of the PCD (extension): 0 damped Jacobi with
+   * jacobi_omega (mod_subsolvers.f90:252-372), 1 red-black SOR with
+   * pcd_sor_omega: each sweep updates the faces with (i + j) even, then
+   * those with (i + j) odd, in place, refreshing the halo before each colour */
+  int pcd_smoother;
+  double pcd_sor_omega;
 } fo_model;
 
 void fo_model_defaults(fo_model* m);

@@ -45,10 +45,17 @@ def batched(specs, prms, prec, **kw):
     return out, states, prof
 
 
-@pytest.mark.parametrize("prec", [FP64, MIXED])
-def test_batch_equals_lone_contexts_bitwise(gpu, prec):
+# the batched ensemble's own solver: flexible GMRES, adaptive PCD with the
+# red-black SOR velocity smoother
+ENSEMBLE_LIKE = dict(tol_bicgstab2=1e-8, max_iter_bicgstab2=200, refine=2, refine_inner_tol=1e-2, refine_max_inner=30,
+                     refine_max_outer=40, krylov_bc_fix=1, pcg_cap_start=4, pcd_sweeps=2, pcd_sweeps_max=8,
+                     pcd_smoother=1, pcd_sor_omega=1.5)
+
+
+@pytest.mark.parametrize("prec,solver", [(FP64, SOLVER), (MIXED, SOLVER), (MIXED, ENSEMBLE_LIKE)])
+def test_batch_equals_lone_contexts_bitwise(gpu, prec, solver):
     specs = cases.bubble_ensemble(4, grids=SMALL_GRIDS)
-    prms = [ensemble_params(s, **SOLVER) for s in specs]
+    prms = [ensemble_params(s, **solver) for s in specs]
     out, states, _ = batched(specs, prms, prec, nthreads=4, max_cluster=16)
     assert out["status"] == [0] * len(specs)
     for i, (s, p) in enumerate(zip(specs, prms)):

@@ -142,9 +142,11 @@ def test_matvec_coupled(gpu, oracle_mod, grid, variant):
 
 
 @pytest.mark.parametrize("use_pen", [False, True])
-def test_helmholtz_sweeps(gpu, oracle_mod, grid, use_pen):
+@pytest.mark.parametrize("smoother", [0, 1])
+def test_helmholtz_sweeps(gpu, oracle_mod, grid, use_pen, smoother):
+    """damped Jacobi (the reference) and the red-black SOR extension"""
     rng = np.random.default_rng(6)
-    prm = two_phase_params()
+    prm = two_phase_params(pcd_smoother=smoother, pcd_sor_omega=1.5)
     o = oracle_mod.Oracle(grid, prm)
     c, pr = props(o, grid, rng, prm)
     with Context(grid, prm) as ctx:
@@ -252,12 +254,12 @@ def test_poisson_pcg(gpu, oracle_mod, grid, zero_init, pcg_variant):
     exact(pg, po)
 
 
-@pytest.mark.parametrize("sweeps,penalty", [(3, False), (4, True)])
-def test_pcd_precond(gpu, oracle_mod, grid, pcg_variant, sweeps, penalty):
-    """apply_pcd_precond: 3 sweeps (odd: the Jacobi result is copied back) and
-    4 sweeps with the Darcy penalty diagonal."""
+@pytest.mark.parametrize("sweeps,penalty,smoother", [(3, False, 0), (4, True, 0), (3, True, 1)])
+def test_pcd_precond(gpu, oracle_mod, grid, pcg_variant, sweeps, penalty, smoother):
+    """apply_pcd_precond: 3 sweeps (odd: the Jacobi result is copied back),
+    4 sweeps with the Darcy penalty diagonal, and 3 red-black SOR sweeps."""
     rng = np.random.default_rng(11)
-    prm = two_phase_params(pcd_sweeps=sweeps)
+    prm = two_phase_params(pcd_sweeps=sweeps, pcd_smoother=smoother, pcd_sor_omega=1.5)
     o = oracle_mod.Oracle(grid, prm)
     c, pr = props(o, grid, rng, prm)
     z = [rfield(rng, grid, k) for k in ("u", "v", "cell")]

@@ -121,17 +121,19 @@ def test_step_parity_grid_wide_pcg(gpu, oracle_mod, name, monkeypatch):
         np.testing.assert_array_equal(st_g[k], st_o[k], err_msg=k)
 
 
-@pytest.mark.parametrize("name,refine,cap0,swmax", [("droplet", 1, 0, 0), ("droplet", 2, 0, 0),
-                                                    ("bubble_freeslip", 2, 0, 0), ("droplet", 2, 3, 0),
-                                                    ("bubble_freeslip", 2, 2, 0), ("bubble_freeslip", 2, 2, 8)])
-def test_refine_fp64_parity(gpu, oracle_mod, name, refine, cap0, swmax):
+@pytest.mark.parametrize("name,refine,cap0,swmax,smoother", [
+    ("droplet", 1, 0, 0, 0), ("droplet", 2, 0, 0, 0), ("bubble_freeslip", 2, 0, 0, 0), ("droplet", 2, 3, 0, 0),
+    ("bubble_freeslip", 2, 2, 0, 0), ("bubble_freeslip", 2, 2, 8, 0), ("droplet", 2, 0, 0, 1),
+    ("bubble_freeslip", 2, 2, 8, 1), ("poiseuille", 2, 0, 0, 1)])
+def test_refine_fp64_parity(gpu, oracle_mod, name, refine, cap0, swmax, smoother):
     """FP64 defect correction around BiCGStab (refine 1) or flexible GMRES
     (refine 2): same outer and inner iteration counts as the oracle, and the
     same bits.  cap0 > 0 runs the adaptive PCG cap from a start so low that
     it must grow, swmax > 0 then also the PCD sweeps from 1; both carry
-    across the steps on both sides."""
+    across the steps on both sides.  smoother 1: the PCD's red-black SOR
+    velocity smoother (omega 1.5; the periodic channel wraps its colours)."""
     over = dict(refine=refine, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=30, krylov_bc_fix=1,
-                tol_bicgstab2=1e-9, pcg_cap_start=cap0)
+                tol_bicgstab2=1e-9, pcg_cap_start=cap0, pcd_smoother=smoother, pcd_sor_omega=1.5)
     if swmax:  # a low PCG ceiling, so that the sweeps must grow too
         over.update(pcd_sweeps=1, pcd_sweeps_max=swmax, pcg_max_iter=8)
     g, st_o, st_g, hist = run_pair(oracle_mod, name, over)
@@ -145,15 +147,17 @@ def test_refine_fp64_parity(gpu, oracle_mod, name, refine, cap0, swmax):
         np.testing.assert_array_equal(st_g[k], st_o[k], err_msg=k)
 
 
-@pytest.mark.parametrize("refine", [1, 2])
+@pytest.mark.parametrize("refine,smoother", [(1, 0), (2, 0), (2, 1)])
 @pytest.mark.parametrize("name", ["cavity", "droplet", "bubble_amp", "bubble_freeslip"])
-def test_mixed_precision_error_vs_fp64_oracle(gpu, oracle_mod, name, refine):
+def test_mixed_precision_error_vs_fp64_oracle(gpu, oracle_mod, name, refine, smoother):
     """FP32 inner Krylov+PCD inside FP64 defect correction: every step reaches
     the FP64 true residual tolerance (1e-9 relative), and the coupled state
     (u, v, p) stays within 1e-6 relative L2 of the FP64 oracle solving the
-    same steps to the same tolerance; per-field errors are reported."""
+    same steps to the same tolerance; per-field errors are reported.
+    smoother 1: both sides smooth the PCD's velocity blocks by red-black SOR
+    (omega 1.5)."""
     over = dict(refine=refine, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=40, krylov_bc_fix=1,
-                tol_bicgstab2=1e-9)
+                tol_bicgstab2=1e-9, pcd_smoother=smoother, pcd_sor_omega=1.5)
     g, st_o, st_g, hist = run_pair(oracle_mod, name, over, precision=1)
     for so, sg in hist:
         assert sg["res"] < 1e-9, sg
