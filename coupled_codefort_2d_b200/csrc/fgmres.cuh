@@ -240,8 +240,16 @@ template <typename T>
 __global__ void k_fg_scale(long n3, T* dst, const T* src, const double* s, const int* active) {
   if (active && !*active) return;
   const T f = T(*s);
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n3; q += (long)gridDim.x * blockDim.x)
-    dst[q] = T(0) + f * src[q];
+  const long S = (long)gridDim.x * blockDim.x;
+  for (long q0 = blockIdx.x * (long)blockDim.x + threadIdx.x; q0 < n3; q0 += 4 * S) {
+    T a[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (q0 + u * S < n3) a[u] = src[q0 + u * S];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (q0 + u * S < n3) dst[q0 + u * S] = T(0) + f * a[u];
+  }
 }
 
 // back substitution R y = g over the k columns used

@@ -562,18 +562,36 @@ struct Lin {
   const double* c3;
   double s1, s2, s3;
 };
+//
+// The element-wise kernels below take four elements per thread per pass of
+// their grid-stride loop (q, q + S, q + 2S, q + 3S; S = the grid's thread
+// count): all four elements' loads come before any store (the output may be
+// one of the inputs, element by element), so they are in flight together and
+// a pass over buffers larger than L2 runs at HBM bandwidth instead of at the
+// latency of one load per thread.
 template <typename T>
 __global__ void k_lin(long n3, T* y, Lin<T> L, const int* active) {
   if (active && !*active) return;
   const T c1 = L.c1 ? T(L.s1 * *L.c1) : T(0);
   const T c2 = L.c2 ? T(L.s2 * *L.c2) : T(0);
   const T c3 = L.c3 ? T(L.s3 * *L.c3) : T(0);
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n3; q += (long)gridDim.x * blockDim.x) {
-    T a = L.x[q];
-    if (L.z1) a = a + c1 * L.z1[q];
-    if (L.z2) a = a + c2 * L.z2[q];
-    if (L.z3) a = a + c3 * L.z3[q];
-    y[q] = a;
+  const long S = (long)gridDim.x * blockDim.x;
+  for (long q0 = blockIdx.x * (long)blockDim.x + threadIdx.x; q0 < n3; q0 += 4 * S) {
+    T a[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const long q = q0 + u * S;
+      if (q < n3) {
+        T t = L.x[q];
+        if (L.z1) t = t + c1 * L.z1[q];
+        if (L.z2) t = t + c2 * L.z2[q];
+        if (L.z3) t = t + c3 * L.z3[q];
+        a[u] = t;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (q0 + u * S < n3) y[q0 + u * S] = a[u];
   }
 }
 // bicgstab_solve direction update p = r + beta (p - omega v) (mod_bicgstab2.f90:244-246)
@@ -582,8 +600,18 @@ __global__ void k_pupdate(long n3, T* p, const T* r, const T* v, const double* b
                           const double* omega, const int* active) {
   if (active && !*active) return;
   const T b = T(*beta), w = T(*omega);
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n3; q += (long)gridDim.x * blockDim.x)
-    p[q] = r[q] + b * (p[q] - w * v[q]);
+  const long S = (long)gridDim.x * blockDim.x;
+  for (long q0 = blockIdx.x * (long)blockDim.x + threadIdx.x; q0 < n3; q0 += 4 * S) {
+    T a[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const long q = q0 + u * S;
+      if (q < n3) a[u] = r[q] + b * (p[q] - w * v[q]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (q0 + u * S < n3) p[q0 + u * S] = a[u];
+  }
 }
 
 // ------------------------------------------------------------ VOF transport
@@ -738,22 +766,43 @@ __global__ void k_axpby(long n, double* a, double s1, const double* x, double s2
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
     a[q] = y ? s1 * x[q] + s2 * y[q] : s1 * x[q];
 }
+// dst = T(src * s), four elements per thread per pass (loads first)
+template <typename T>
+__device__ __forceinline__ void convert4(long n, T* dst, const double* src, double s) {
+  const long S = (long)gridDim.x * blockDim.x;
+  for (long q0 = blockIdx.x * (long)blockDim.x + threadIdx.x; q0 < n; q0 += 4 * S) {
+    double a[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (q0 + u * S < n) a[u] = src[q0 + u * S];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (q0 + u * S < n) dst[q0 + u * S] = T(a[u] * s);
+  }
+}
 template <typename T>
 __global__ void k_convert(long n, T* dst, const double* src, double scale) {
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
-    dst[q] = T(src[q] * scale);
+  convert4<T>(n, dst, src, scale);
 }
 template <typename T>
 __global__ void k_convert_scaled(long n, T* dst, const double* src, const double* scale) {
-  const double s = *scale;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
-    dst[q] = T(src[q] * s);
+  convert4<T>(n, dst, src, *scale);
 }
 template <typename T>
 __global__ void k_accumulate(long n, double* x, const T* d, const double* scale) {
   const double s = *scale;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n; q += (long)gridDim.x * blockDim.x)
-    x[q] = x[q] + s * double(d[q]);
+  const long S = (long)gridDim.x * blockDim.x;
+  for (long q0 = blockIdx.x * (long)blockDim.x + threadIdx.x; q0 < n; q0 += 4 * S) {
+    double a[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const long q = q0 + u * S;
+      if (q < n) a[u] = x[q] + s * double(d[q]);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (q0 + u * S < n) x[q0 + u * S] = a[u];
+  }
 }
 
 // monolithic right-hand side (mod_solver_coupled.f90:261-303)
