@@ -10,7 +10,8 @@ these parameters (no dataset).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-value : mixed form (FP32 inner BiCGStab(2)+PCD inside FP64 defect correction),
+value : mixed form (FP32 inner flexible GMRES(30) + PCD inside the FP64
+        defect correction, each Arnoldi step replayed from a CUDA graph),
         device-resident state, CUDA events on the library's stream around
         each timed step, L2 flushed (256 MiB write) between timed steps.
 e2e   : the same steps through the drop-in C entry fugu_advance_coupled_step
@@ -65,7 +66,7 @@ def case_params(refine=2):
                   tol_bicgstab2=TOL, max_iter_bicgstab2=500, refine=refine, refine_inner_tol=1e-2,
                   refine_max_inner=30, refine_max_outer=60, krylov_bc_fix=1,
                   pcg_cap_start=PCG_CAP_START if fg else 0, pcd_sweeps=PCD_SWEEPS if fg else 3,
-                  pcd_sweeps_max=PCD_SWEEPS_MAX if fg else 0)
+                  pcd_sweeps_max=PCD_SWEEPS_MAX if fg else 0, graphs=1)
 
 
 def initial_state(g, prm):
@@ -483,7 +484,8 @@ def main():
         "data": "synthetic (droplet case fully determined by its parameters)",
         "config": workload_config(f"FP64 defect correction around FP32 {INNER_NAME[INNER[args.inner]]}+PCD "
                                   "(inner tol 1e-2" + (f", PCD PCG cap adaptive {PCG_CAP_START}-150, sweeps "
-                                                       f"{PCD_SWEEPS}-{PCD_SWEEPS_MAX})"
+                                                       f"{PCD_SWEEPS}-{PCD_SWEEPS_MAX}; Arnoldi steps "
+                                                       "replayed from CUDA graphs)"
                                                        if INNER[args.inner] == 2 else ")")),
         "max_true_residual": max(r["res"] for r in s_m),
         "per_step": {"outer": [r["outer"] for r in s_m], "inner_iters": [r["iter"] for r in s_m],

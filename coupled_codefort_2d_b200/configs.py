@@ -57,7 +57,7 @@ from .layout import Grid, at
 from .params import Params
 
 SOLVER = dict(refine=2, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=60, krylov_bc_fix=1,
-              pcg_cap_start=40, pcd_sweeps=6, pcd_sweeps_max=24)
+              pcg_cap_start=40, pcd_sweeps=6, pcd_sweeps_max=24, graphs=1)
 STATE = ("u_vel", "v_vel", "p_field", "c_field", "u_prev", "v_prev", "rho_c", "rho_u", "rho_v", "kappa", "zeta",
          "eta", "kappa_curv", "f_sigma_u", "f_sigma_v")
 

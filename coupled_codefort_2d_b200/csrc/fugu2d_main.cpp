@@ -11,7 +11,7 @@
 // Extra namelist keys (this build): use_gpu (accepted, the path is the GPU),
 // precision ('fp64' | 'mixed'), refine (logical or 0 / 1 / 2), refine_inner_tol, refine_max_inner,
 // refine_max_outer, pcg_max_iter, pcg_cap_start, pcd_sweeps, pcd_sweeps_max, pcd_smoother
-// ('jacobi' | 'rbsor'), pcd_sor_omega, krylov_bc_fix,
+// ('jacobi' | 'rbsor'), pcd_sor_omega, graphs (logical), krylov_bc_fix,
 // limiter ('vanleer' | 'superbee'),
 // free_slip_x, device.
 //
@@ -54,7 +54,7 @@ struct Settings {
   // extensions
   std::string precision = "fp64", limiter = "vanleer", pcd_smoother = "jacobi";
   int refine = 0, refine_max_inner = 20, refine_max_outer = 30, krylov_bc_fix = 0, free_slip_x = 0, device = 0;
-  int pcg_max_iter = 150, pcg_cap_start = 0, pcd_sweeps = 3, pcd_sweeps_max = 0;
+  int pcg_max_iter = 150, pcg_cap_start = 0, pcd_sweeps = 3, pcd_sweeps_max = 0, graphs = 0;
   double refine_inner_tol = 1.0e-2, pcd_sor_omega = 1.0;
 };
 
@@ -212,6 +212,7 @@ bool apply(Settings& st, const std::map<std::string, std::string>& kv, std::stri
     else if (k == "pcd_sweeps_max") st.pcd_sweeps_max = (int)fnum(v);
     else if (k == "pcd_smoother") st.pcd_smoother = lower(fstr(v));
     else if (k == "pcd_sor_omega") st.pcd_sor_omega = fnum(v);
+    else if (k == "graphs") st.graphs = flog(v) ? 1 : 0;
     else if (k == "krylov_bc_fix") st.krylov_bc_fix = flog(v) ? 1 : 0;
     else if (k == "free_slip_x") st.free_slip_x = flog(v) ? 1 : 0;
     else if (k == "device") st.device = (int)fnum(v);
@@ -370,6 +371,7 @@ int main(int argc, char** argv) {
   p.pcg_max_iter = st.pcg_max_iter; p.pcg_cap_start = st.pcg_cap_start;
   p.pcd_sweeps = st.pcd_sweeps; p.pcd_sweeps_max = st.pcd_sweeps_max;
   p.pcd_smoother = st.pcd_smoother == "rbsor" ? 1 : 0; p.pcd_sor_omega = st.pcd_sor_omega;
+  p.graphs = st.graphs;
   p.precision = st.precision == "mixed" ? FUGU_MIXED : FUGU_FP64;
   fugu_ctx* ctx = nullptr;
   int rc = fugu_create(&p, st.device, &ctx);

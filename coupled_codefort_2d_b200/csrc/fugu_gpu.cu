@@ -195,6 +195,22 @@ struct fugu_ctx {
     int C = 0, rows_per = 0, cpt = 0;
     size_t smem = 0;
   } pcgc[2];
+  // CUDA graphs of the flexible-GMRES Arnoldi steps (graphs = 1), per
+  // precision (0 FP64, 1 FP32) and step index j
+  struct StepGraph {
+    std::vector<unsigned char> key;  // everything the captured launches depend on
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long launches = 0;  // kernel launches in one replay
+    // around its PCG launches (profiling): one pair per launch in the body
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+    size_t ev_used = 0;
+  };
+  std::vector<StepGraph> fg_graphs[2];
+  // one BiCGStab (index 0) / BiCGStab(2) (index 1) iteration per precision,
+  // its iteration index on the device (KState::kiter)
+  StepGraph kr_graphs[2][2];
+  StepGraph* capturing = nullptr;     // the step graph being captured
+  StepGraph* pcg_timed = nullptr;     // replayed with PCG events, not yet read
   // measurement: launch count, CUDA-event timing of the persistent kernels
   unsigned long long launches = 0;
   int prof = 0;
@@ -528,9 +544,18 @@ void pcg(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, double tol, int max_i
   const fugu_ctx::ClusterPlan& cp = c->pcgc[sizeof(T) == 8 ? 0 : 1];
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (c->prof) {
-    e0 = ev_get(c);
-    e1 = ev_get(c);
-    CK(cudaEventRecord(e0, c->s));
+    if (c->capturing) {  // a captured step records its own pairs, as graph nodes
+      fugu_ctx::StepGraph& sg = *c->capturing;
+      if (sg.ev_used >= sg.ev.size()) throw ApiError{FUGU_EINVAL, "captured step: too many PCG launches"};
+      e0 = sg.ev[sg.ev_used].first;
+      e1 = sg.ev[sg.ev_used].second;
+      ++sg.ev_used;
+      CK(cudaEventRecordWithFlags(e0, c->s, cudaEventRecordExternal));
+    } else {
+      e0 = ev_get(c);
+      e1 = ev_get(c);
+      CK(cudaEventRecord(e0, c->s));
+    }
   }
   if (cp.ok) {
     PcgClusterArgs<T> ca;
@@ -546,8 +571,12 @@ void pcg(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, double tol, int max_i
   }
   ++c->launches;
   if (c->prof) {
-    CK(cudaEventRecord(e1, c->s));
-    c->ev_pcg.push_back({e0, e1});
+    if (c->capturing) {
+      CK(cudaEventRecordWithFlags(e1, c->s, cudaEventRecordExternal));
+    } else {
+      CK(cudaEventRecord(e1, c->s));
+      c->ev_pcg.push_back({e0, e1});
+    }
   }
 }
 
@@ -628,7 +657,7 @@ void zero_trip(fugu_ctx* c, Trip<T> t) {
 
 // restart the Krylov flags (the matvec counter survives; it is per step)
 void reset_ks(fugu_ctx* c) {
-  static const KState k0 = {1, 0, 0, 0u, 0ull};
+  static const KState k0 = {1, 0, 0, 0u, 1, 0ull};
   CK(cudaMemcpyAsync(c->ks, &k0, offsetof(KState, matvecs), cudaMemcpyHostToDevice, c->s));
 }
 // poll the device Krylov state (one round trip)
@@ -649,6 +678,104 @@ struct KrylovResult {
   int status = FUGU_CONVERGED;
 };
 
+void graph_prof_read(fugu_ctx* c);
+
+// Run body() on the context's stream from a CUDA graph: the captured graph
+// is replayed while key (every value its launches depend on) is unchanged;
+// otherwise body() is captured again and the executable graph updated in
+// place (or instantiated anew when its topology changed).  Capture is
+// thread-local, so other host threads (a batch) keep launching meanwhile.
+template <typename F>
+void run_graphed(fugu_ctx* c, fugu_ctx::StepGraph& sg, std::vector<unsigned char>&& key, F body) {
+  if (!sg.exec || sg.key != key) {
+    // event pairs for the PCG launches of the body (at most 4: BiCGStab(2)
+    // applies PCD four times per iteration), created before the capture
+    while (c->prof && sg.ev.size() < 4) {
+      cudaEvent_t a, b;
+      CK(cudaEventCreate(&a));
+      CK(cudaEventCreate(&b));
+      sg.ev.push_back({a, b});
+    }
+    sg.ev_used = 0;
+    cudaGraph_t graph = nullptr;
+    const unsigned long long l0 = c->launches;
+    CK(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
+    c->capturing = &sg;
+    try {
+      body();
+    } catch (...) {
+      c->capturing = nullptr;
+      cudaStreamEndCapture(c->s, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      cudaGetLastError();
+      throw;
+    }
+    c->capturing = nullptr;
+    CK(cudaStreamEndCapture(c->s, &graph));
+    sg.launches = c->launches - l0;
+    c->launches = l0;
+    bool updated = false;
+    if (sg.exec) {
+      cudaGraphExecUpdateResultInfo info;
+      if (cudaGraphExecUpdate(sg.exec, graph, &info) == cudaSuccess) {
+        updated = true;
+      } else {
+        cudaGetLastError();
+        cudaGraphExecDestroy(sg.exec);
+        sg.exec = nullptr;
+      }
+    }
+    if (!updated) {
+      const cudaError_t e = cudaGraphInstantiate(&sg.exec, graph, 0);
+      if (e != cudaSuccess) {
+        sg.exec = nullptr;
+        cudaGraphDestroy(graph);
+        throw CudaError{e, "cudaGraphInstantiate"};
+      }
+    }
+    cudaGraphDestroy(graph);
+    sg.key = std::move(key);
+  }
+  // the PCG intervals of the step replayed before this one are read while
+  // this one runs (its events completed at the step's synchronisation), or
+  // before the launch when this replay is about to record the same events
+  if (c->pcg_timed == &sg) graph_prof_read(c);
+  CK(cudaGraphLaunch(sg.exec, c->s));
+  c->launches += sg.launches;
+  graph_prof_read(c);
+  if (c->prof) c->pcg_timed = &sg;
+}
+
+// fold the PCG intervals of the last replayed step graph into the profile
+// (once the stream passed it, before a replay of it records them again)
+void graph_prof_read(fugu_ctx* c) {
+  if (!c->pcg_timed) return;
+  for (size_t i = 0; i < c->pcg_timed->ev_used; ++i) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->pcg_timed->ev[i].first, c->pcg_timed->ev[i].second));
+    c->prof_pcg_ms += ms;
+    c->prof_pcg_launches += 1;
+  }
+  c->pcg_timed = nullptr;
+}
+
+template <typename V>
+void key_put(std::vector<unsigned char>& k, const V& v) {
+  const unsigned char* b = reinterpret_cast<const unsigned char*>(&v);
+  k.insert(k.end(), b, b + sizeof(V));
+}
+
+// what a captured BiCGStab(l) iteration depends on
+template <typename T>
+std::vector<unsigned char> krylov_key(fugu_ctx* c, const KrylovWork<T>& w, const CoefBufs<T>& cb, const SolveOpt& o,
+                                      Trip<T> X, double dt, double tol) {
+  std::vector<unsigned char> key;
+  key_put(key, w.t[0].base); key_put(key, cb); key_put(key, o); key_put(key, X.base); key_put(key, dt);
+  key_put(key, tol); key_put(key, c->pcg_cap_cur); key_put(key, c->pcd_sweeps_cur); key_put(key, c->adj_on);
+  key_put(key, c->prm); key_put(key, c->prof);
+  return key;
+}
+
 // bicgstab_solve, mod_bicgstab2.f90:77-264
 template <typename T>
 KrylovResult bicgstab1(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const SolveOpt& o, Trip<T> X,
@@ -668,28 +795,39 @@ KrylovResult bicgstab1(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, con
   CK(cudaMemcpyAsync(p.base, r.base, sizeof(T) * 3 * c->n, cudaMemcpyDeviceToDevice, c->s));
   dot_op<T>(c, {{r0, r}, {r, r}}, OpArgs{OP_B1_INIT, 1, tol}, false);
   KState ks = read_ks(c);
+  // graphs = 1: one captured iteration, replayed for every k (k on the device)
+  const int pi = sizeof(T) == 8 ? 0 : 1;
+  const bool graphed = c->prm.graphs == 1 && c->pcgc[pi].ok;
   int k = 1;
   for (; k <= max_iter && ks.active; ++k) {
-    vbcs(c, p.u, p.v, 0.0, act);
-    matvec<T>(c, cb, o, p, z, dt, act);
-    pcd<T>(c, w, cb, o, z, v, dt, act);
-    vbcs(c, v.u, v.v, 0.0, act);
-    dot_op<T>(c, {{r0, v}}, OpArgs{OP_B1_ALPHA, k, tol}, true);
-    lin<T>(c, s, r, -1.0, sc + S_ALPHA, v, 0, nullptr, {}, 0, nullptr, {}, act);
-    vbcs(c, s.u, s.v, 0.0, act);
-    matvec<T>(c, cb, o, s, z, dt, act);
-    pcd<T>(c, w, cb, o, z, t, dt, act);
-    vbcs(c, t.u, t.v, 0.0, act);
-    dot_op<T>(c, {{t, t}, {t, s}}, OpArgs{OP_B1_OMEGA, k, tol}, true);
-    lin<T>(c, X, X, 1.0, sc + S_ALPHA, p, 1.0, sc + S_OMEGA, s, 0, nullptr, {}, act);
-    lin<T>(c, r, s, -1.0, sc + S_OMEGA, t, 0, nullptr, {}, 0, nullptr, {}, act);
-    dot_op<T>(c, {{r, r}, {r0, r}}, OpArgs{OP_B1_END, k, tol}, true);
-    k_pupdate<T><<<grid1d(c, 3 * c->n), 256, 0, c->s>>>(3 * c->n, p.base, r.base, v.base, sc + S_BETA,
-                                                          sc + S_OMEGA, act);
-    CKL("k_pupdate");
-    vbcs(c, X.u, X.v, 0.0, act);
+    const int kk = graphed ? -1 : k;
+    auto iteration = [&] {
+      vbcs(c, p.u, p.v, 0.0, act);
+      matvec<T>(c, cb, o, p, z, dt, act);
+      pcd<T>(c, w, cb, o, z, v, dt, act);
+      vbcs(c, v.u, v.v, 0.0, act);
+      dot_op<T>(c, {{r0, v}}, OpArgs{OP_B1_ALPHA, kk, tol}, true);
+      lin<T>(c, s, r, -1.0, sc + S_ALPHA, v, 0, nullptr, {}, 0, nullptr, {}, act);
+      vbcs(c, s.u, s.v, 0.0, act);
+      matvec<T>(c, cb, o, s, z, dt, act);
+      pcd<T>(c, w, cb, o, z, t, dt, act);
+      vbcs(c, t.u, t.v, 0.0, act);
+      dot_op<T>(c, {{t, t}, {t, s}}, OpArgs{OP_B1_OMEGA, kk, tol}, true);
+      lin<T>(c, X, X, 1.0, sc + S_ALPHA, p, 1.0, sc + S_OMEGA, s, 0, nullptr, {}, act);
+      lin<T>(c, r, s, -1.0, sc + S_OMEGA, t, 0, nullptr, {}, 0, nullptr, {}, act);
+      dot_op<T>(c, {{r, r}, {r0, r}}, OpArgs{OP_B1_END, kk, tol}, true);
+      k_pupdate<T><<<grid1d(c, 3 * c->n), 256, 0, c->s>>>(3 * c->n, p.base, r.base, v.base, sc + S_BETA,
+                                                            sc + S_OMEGA, act);
+      CKL("k_pupdate");
+      vbcs(c, X.u, X.v, 0.0, act);
+    };
+    if (graphed)
+      run_graphed(c, c->kr_graphs[pi][0], krylov_key(c, w, cb, o, X, dt, tol), iteration);
+    else
+      iteration();
     ks = read_ks(c);
   }
+  graph_prof_read(c);
   if (has_lid) vbcs(c, X.u, X.v, lid);
   ks = read_ks(c);
   KrylovResult res;
@@ -719,46 +857,57 @@ KrylovResult bicgstab2(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, con
   zero_trip(c, vv);
   dot_op<T>(c, {{r, r}}, OpArgs{OP_B2_INIT, 1, tol}, false);
   KState ks = read_ks(c);
+  // graphs = 1: one captured iteration, replayed for every k (k on the device)
+  const int pi = sizeof(T) == 8 ? 0 : 1;
+  const bool graphed = c->prm.graphs == 1 && c->pcgc[pi].ok;
   int k = 1;
   for (; k <= max_iter && ks.active; ++k) {
-    // even half
-    dot_op<T>(c, {{rt, r}}, OpArgs{OP_B2_XI_EVEN, k, tol}, true);
-    lin<T>(c, uu, r, -1.0, sc + S_BETA, uu, 0, nullptr, {}, 0, nullptr, {}, act);
-    vbcs(c, uu.u, uu.v, 0.0, act);
-    matvec<T>(c, cb, o, uu, z, dt, act);
-    pcd<T>(c, w, cb, o, z, vv, dt, act);
-    vbcs(c, vv.u, vv.v, 0.0, act);
-    dot_op<T>(c, {{rt, vv}}, OpArgs{OP_B2_GAMMA, k, tol}, true);
-    lin<T>(c, r, r, -1.0, sc + S_ALPHA, vv, 0, nullptr, {}, 0, nullptr, {}, act);
-    if (c->prm.krylov_bc_fix) vbcs(c, r.u, r.v, 0.0, act);
-    matvec<T>(c, cb, o, r, z, dt, act);
-    pcd<T>(c, w, cb, o, z, ss, dt, act);
-    vbcs(c, ss.u, ss.v, 0.0, act);
-    lin<T>(c, X, X, 1.0, sc + S_ALPHA, uu, 0, nullptr, {}, 0, nullptr, {}, act);
-    // odd half
-    dot_op<T>(c, {{rt, ss}}, OpArgs{OP_B2_XI_ODD, k, tol}, true);
-    lin<T>(c, vv, ss, -1.0, sc + S_BETA, vv, 0, nullptr, {}, 0, nullptr, {}, act);
-    vbcs(c, vv.u, vv.v, 0.0, act);
-    matvec<T>(c, cb, o, vv, z, dt, act);
-    pcd<T>(c, w, cb, o, z, ww, dt, act);
-    vbcs(c, ww.u, ww.v, 0.0, act);
-    dot_op<T>(c, {{rt, ww}}, OpArgs{OP_B2_GAMMA, k, tol}, true);
-    lin<T>(c, uu, r, -1.0, sc + S_BETA, uu, 0, nullptr, {}, 0, nullptr, {}, act);
-    lin<T>(c, r, r, -1.0, sc + S_ALPHA, vv, 0, nullptr, {}, 0, nullptr, {}, act);
-    lin<T>(c, ss, ss, -1.0, sc + S_ALPHA, ww, 0, nullptr, {}, 0, nullptr, {}, act);
-    matvec<T>(c, cb, o, ss, z, dt, act);
-    pcd<T>(c, w, cb, o, z, tt, dt, act);
-    vbcs(c, tt.u, tt.v, 0.0, act);
-    // GCR(2)
-    dot_op<T>(c, {{r, ss}, {ss, ss}, {ss, tt}, {tt, tt}, {r, tt}}, OpArgs{OP_B2_GCR, k, tol}, true);
-    lin<T>(c, X, X, 1.0, sc + S_OM1, r, 1.0, sc + S_OM2, ss, 1.0, sc + S_ALPHA, uu, act);
-    lin<T>(c, r, r, -1.0, sc + S_OM1, ss, -1.0, sc + S_OM2, tt, 0, nullptr, {}, act);
-    lin<T>(c, uu, uu, -1.0, sc + S_OM1, vv, -1.0, sc + S_OM2, ww, 0, nullptr, {}, act);
-    dot_op<T>(c, {{r, r}}, OpArgs{OP_B2_REL, k, tol}, true);
-    vbcs(c, X.u, X.v, 0.0, act);
-    scalar_op(c, OpArgs{OP_TOPCHECK, k + 1, tol}, true);
+    const int kk = graphed ? -1 : k;
+    auto iteration = [&] {
+      // even half
+      dot_op<T>(c, {{rt, r}}, OpArgs{OP_B2_XI_EVEN, kk, tol}, true);
+      lin<T>(c, uu, r, -1.0, sc + S_BETA, uu, 0, nullptr, {}, 0, nullptr, {}, act);
+      vbcs(c, uu.u, uu.v, 0.0, act);
+      matvec<T>(c, cb, o, uu, z, dt, act);
+      pcd<T>(c, w, cb, o, z, vv, dt, act);
+      vbcs(c, vv.u, vv.v, 0.0, act);
+      dot_op<T>(c, {{rt, vv}}, OpArgs{OP_B2_GAMMA, kk, tol}, true);
+      lin<T>(c, r, r, -1.0, sc + S_ALPHA, vv, 0, nullptr, {}, 0, nullptr, {}, act);
+      if (c->prm.krylov_bc_fix) vbcs(c, r.u, r.v, 0.0, act);
+      matvec<T>(c, cb, o, r, z, dt, act);
+      pcd<T>(c, w, cb, o, z, ss, dt, act);
+      vbcs(c, ss.u, ss.v, 0.0, act);
+      lin<T>(c, X, X, 1.0, sc + S_ALPHA, uu, 0, nullptr, {}, 0, nullptr, {}, act);
+      // odd half
+      dot_op<T>(c, {{rt, ss}}, OpArgs{OP_B2_XI_ODD, kk, tol}, true);
+      lin<T>(c, vv, ss, -1.0, sc + S_BETA, vv, 0, nullptr, {}, 0, nullptr, {}, act);
+      vbcs(c, vv.u, vv.v, 0.0, act);
+      matvec<T>(c, cb, o, vv, z, dt, act);
+      pcd<T>(c, w, cb, o, z, ww, dt, act);
+      vbcs(c, ww.u, ww.v, 0.0, act);
+      dot_op<T>(c, {{rt, ww}}, OpArgs{OP_B2_GAMMA, kk, tol}, true);
+      lin<T>(c, uu, r, -1.0, sc + S_BETA, uu, 0, nullptr, {}, 0, nullptr, {}, act);
+      lin<T>(c, r, r, -1.0, sc + S_ALPHA, vv, 0, nullptr, {}, 0, nullptr, {}, act);
+      lin<T>(c, ss, ss, -1.0, sc + S_ALPHA, ww, 0, nullptr, {}, 0, nullptr, {}, act);
+      matvec<T>(c, cb, o, ss, z, dt, act);
+      pcd<T>(c, w, cb, o, z, tt, dt, act);
+      vbcs(c, tt.u, tt.v, 0.0, act);
+      // GCR(2)
+      dot_op<T>(c, {{r, ss}, {ss, ss}, {ss, tt}, {tt, tt}, {r, tt}}, OpArgs{OP_B2_GCR, kk, tol}, true);
+      lin<T>(c, X, X, 1.0, sc + S_OM1, r, 1.0, sc + S_OM2, ss, 1.0, sc + S_ALPHA, uu, act);
+      lin<T>(c, r, r, -1.0, sc + S_OM1, ss, -1.0, sc + S_OM2, tt, 0, nullptr, {}, act);
+      lin<T>(c, uu, uu, -1.0, sc + S_OM1, vv, -1.0, sc + S_OM2, ww, 0, nullptr, {}, act);
+      dot_op<T>(c, {{r, r}}, OpArgs{OP_B2_REL, kk, tol}, true);
+      vbcs(c, X.u, X.v, 0.0, act);
+      scalar_op(c, OpArgs{OP_TOPCHECK, graphed ? -1 : k + 1, tol}, true);
+    };
+    if (graphed)
+      run_graphed(c, c->kr_graphs[pi][1], krylov_key(c, w, cb, o, X, dt, tol), iteration);
+    else
+      iteration();
     ks = read_ks(c);
   }
+  graph_prof_read(c);
   if (has_lid) vbcs(c, X.u, X.v, lid);
   ks = read_ks(c);
   KrylovResult res;
@@ -843,23 +992,42 @@ KrylovResult fgmres(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const 
   k_fg_scale<T><<<g1, 256, 0, c->s>>>(n3, f.V, B.base, f.st + L.inv(), act);
   CKL("k_fg_scale");
   KState ks = read_ks(c);
+  // graphs = 1: each Arnoldi step is replayed from a CUDA graph (not with
+  // the grid-wide PCG, a cooperative launch); while profiling, the graph
+  // records the PCG interval on its own event pair, read after each step
+  const int pi = sizeof(T) == 8 ? 0 : 1;
+  const bool graphed = c->prm.graphs == 1 && c->pcgc[pi].ok;
+  if (graphed && (int)c->fg_graphs[pi].size() < m) c->fg_graphs[pi].resize(m);
   for (int j = 0; j < m && ks.active; ++j) {
     Trip<T> Vj = trip_at(f.V, j, c->n), Zj = trip_at(f.Z, j, c->n);
-    pcd<T>(c, w, cb, o, Vj, Zj, dt, act);
-    vbcs(c, Zj.u, Zj.v, 0.0, act);
-    matvec<T>(c, cb, o, Zj, wv, dt, act);
-    // classical Gram-Schmidt, twice
-    mdot<T>(c, wv.base, f.V, j + 1, FG_PROJ1, j, tol, L, f.st);
-    k_maxpy<T><<<g1, 256, 0, c->s>>>(n3, wv.base, f.V, n3, f.st + L.h(), j + 1, -1.0, act);
-    CKL("k_maxpy");
-    mdot<T>(c, wv.base, f.V, j + 1, FG_PROJ2, j, tol, L, f.st);
-    k_maxpy<T><<<g1, 256, 0, c->s>>>(n3, wv.base, f.V, n3, f.st + L.h(), j + 1, -1.0, act);
-    CKL("k_maxpy");
-    mdot<T>(c, wv.base, wv.base, 1, FG_ROTATE, j, tol, L, f.st);
-    k_fg_scale<T><<<g1, 256, 0, c->s>>>(n3, f.V + (long)(j + 1) * n3, wv.base, f.st + L.inv(), act);
-    CKL("k_fg_scale");
+    auto arnoldi_step = [&] {
+      pcd<T>(c, w, cb, o, Vj, Zj, dt, act);
+      vbcs(c, Zj.u, Zj.v, 0.0, act);
+      matvec<T>(c, cb, o, Zj, wv, dt, act);
+      // classical Gram-Schmidt, twice
+      mdot<T>(c, wv.base, f.V, j + 1, FG_PROJ1, j, tol, L, f.st);
+      k_maxpy<T><<<g1, 256, 0, c->s>>>(n3, wv.base, f.V, n3, f.st + L.h(), j + 1, -1.0, act);
+      CKL("k_maxpy");
+      mdot<T>(c, wv.base, f.V, j + 1, FG_PROJ2, j, tol, L, f.st);
+      k_maxpy<T><<<g1, 256, 0, c->s>>>(n3, wv.base, f.V, n3, f.st + L.h(), j + 1, -1.0, act);
+      CKL("k_maxpy");
+      mdot<T>(c, wv.base, wv.base, 1, FG_ROTATE, j, tol, L, f.st);
+      k_fg_scale<T><<<g1, 256, 0, c->s>>>(n3, f.V + (long)(j + 1) * n3, wv.base, f.st + L.inv(), act);
+      CKL("k_fg_scale");
+    };
+    if (graphed) {
+      std::vector<unsigned char> key;
+      key_put(key, j); key_put(key, m); key_put(key, f.V); key_put(key, f.Z); key_put(key, f.st);
+      key_put(key, wv.base); key_put(key, cb); key_put(key, o); key_put(key, dt); key_put(key, tol);
+      key_put(key, c->pcg_cap_cur); key_put(key, c->pcd_sweeps_cur); key_put(key, c->adj_on);
+      key_put(key, c->prm); key_put(key, c->prof);
+      run_graphed(c, c->fg_graphs[pi][j], std::move(key), arnoldi_step);
+    } else {
+      arnoldi_step();
+    }
     ks = read_ks(c);
   }
+  graph_prof_read(c);
   const int k = ks.active ? m : ks.exit_iter;
   KrylovResult res;
   if (k > 0) {
@@ -1229,6 +1397,7 @@ int check_params(const fugu_params* p) {
   if (p->refine == 2 && (p->refine_max_inner < 1 || p->refine_max_inner > 127)) return FUGU_EINVAL;
   if (p->precision != FUGU_FP64 && p->precision != FUGU_MIXED) return FUGU_EINVAL;
   if (p->pcd_smoother < 0 || p->pcd_smoother > 1) return FUGU_EINVAL;
+  if (p->graphs < 0 || p->graphs > 1) return FUGU_EINVAL;
   if (p->pcd_smoother == 1 && !(p->pcd_sor_omega > 0.0 && p->pcd_sor_omega < 2.0)) return FUGU_EINVAL;
   return FUGU_OK;
 }
@@ -1309,6 +1478,17 @@ void destroy(fugu_ctx* c) {
   if (c->s) cudaStreamSynchronize(c->s);
   for (auto& pr : c->ev_pcg) { cudaEventDestroy(pr.first); cudaEventDestroy(pr.second); }
   for (auto e : c->ev_pool) cudaEventDestroy(e);
+  auto drop = [](fugu_ctx::StepGraph& sg) {
+    if (sg.exec) cudaGraphExecDestroy(sg.exec);
+    for (auto& pr : sg.ev) {
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
+  };
+  for (auto& v : c->fg_graphs)
+    for (auto& sg : v) drop(sg);
+  for (auto& pr : c->kr_graphs)
+    for (auto& sg : pr) drop(sg);
   for (void* p : c->allocs) cudaFree(p);
   if (c->h_ks) cudaFreeHost(c->h_ks);
   if (c->h_sc) cudaFreeHost(c->h_sc);
@@ -1374,7 +1554,7 @@ void fugu_params_default(fugu_params* p) {
   p->svof_delta_h = 1.5; p->svof_max_iter = 150; p->svof_tol = 1.0e-7;
   p->refine_inner_tol = 1.0e-2; p->refine_max_inner = 20; p->refine_max_outer = 30;
   p->precision = FUGU_FP64;
-  p->pcd_smoother = 0; p->pcd_sor_omega = 1.0;
+  p->pcd_smoother = 0; p->pcd_sor_omega = 1.0; p->graphs = 0;
 }
 
 const char* fugu_version(void) { return "fugu-b200 1 (sm_100a)"; }
@@ -1425,6 +1605,7 @@ int fugu_profile(fugu_ctx* c, int enable, fugu_profile_stats* out) {
   return guard(c, [&] {
     sync(c);
     prof_drain(c);
+    graph_prof_read(c);
     if (out) {
       out->kernel_launches = c->launches;
       out->pcg_ms = c->prof_pcg_ms;

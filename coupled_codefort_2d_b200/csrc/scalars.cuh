@@ -47,6 +47,7 @@ struct KState {
   int exit_iter;   // iteration at which the reference's loop exits (0 = ran out)
   int nan;
   unsigned int ticket;
+  int kiter;       // iteration index of a BiCGStab(l) replayed from a CUDA graph
   unsigned long long matvecs;
 };
 
@@ -55,7 +56,20 @@ __device__ __forceinline__ void kexit(KState* ks, int k) {
   ks->exit_iter = k;
 }
 
+// The iteration index an op reports on exit: o.k, or, when o.k < 0, the
+// device counter ks->kiter, so that one captured BiCGStab(l) iteration serves
+// every k.  OP_TOPCHECK tests the top of the next iteration (k + 1); it and
+// OP_B1_END, the last op of an iteration, advance the counter.
+__device__ __forceinline__ int op_k(const OpArgs& o, const KState* ks) {
+  return o.k >= 0 ? o.k : ks->kiter + (o.op == OP_TOPCHECK ? 1 : 0);
+}
+
+__device__ inline void krylov_op_body(const OpArgs& o, double* sc, KState* ks);
 __device__ inline void krylov_op(const OpArgs& o, double* sc, KState* ks) {
+  krylov_op_body(o, sc, ks);
+  if (o.k < 0 && (o.op == OP_TOPCHECK || o.op == OP_B1_END)) ks->kiter += 1;
+}
+__device__ inline void krylov_op_body(const OpArgs& o, double* sc, KState* ks) {
   const double d0 = sc[S_D0], d1 = sc[S_D1], d2 = sc[S_D2], d3 = sc[S_D3], d4 = sc[S_D4];
   switch (o.op) {
     case OP_STORE:
@@ -74,7 +88,7 @@ __device__ inline void krylov_op(const OpArgs& o, double* sc, KState* ks) {
       if (sc[S_REL] < o.tol) kexit(ks, 1);
       break;
     case OP_B1_ALPHA:
-      if (fabs(d0) < 1.0e-30) { kexit(ks, o.k); break; }
+      if (fabs(d0) < 1.0e-30) { kexit(ks, op_k(o, ks)); break; }
       sc[S_ALPHA] = sc[S_RHO] / d0;
       break;
     case OP_B1_OMEGA:
@@ -85,11 +99,11 @@ __device__ inline void krylov_op(const OpArgs& o, double* sc, KState* ks) {
     case OP_B1_END: {
       const double rel = sqrt(d0) / sc[S_NORMB];
       sc[S_REL] = rel;
-      if (isnan(rel)) { ks->nan = 1; kexit(ks, o.k); break; }
-      if (rel < o.tol) { kexit(ks, o.k); break; }
-      if (fabs(sc[S_OMEGA]) < 1.0e-30) { kexit(ks, o.k); break; }
+      if (isnan(rel)) { ks->nan = 1; kexit(ks, op_k(o, ks)); break; }
+      if (rel < o.tol) { kexit(ks, op_k(o, ks)); break; }
+      if (fabs(sc[S_OMEGA]) < 1.0e-30) { kexit(ks, op_k(o, ks)); break; }
       const double rho_new = d1;
-      if (fabs(sc[S_RHO]) < 1.0e-30) { kexit(ks, o.k); break; }
+      if (fabs(sc[S_RHO]) < 1.0e-30) { kexit(ks, op_k(o, ks)); break; }
       sc[S_BETA] = (rho_new / sc[S_RHO]) * (sc[S_ALPHA] / sc[S_OMEGA]);
       sc[S_RHO] = rho_new;
       break;
@@ -109,7 +123,7 @@ __device__ inline void krylov_op(const OpArgs& o, double* sc, KState* ks) {
       else xi0 = -xi0;
       sc[S_XI0] = xi0;
       sc[S_XI1] = d0;
-      if (fabs(xi0) < 1.0e-30) { kexit(ks, o.k); break; }
+      if (fabs(xi0) < 1.0e-30) { kexit(ks, op_k(o, ks)); break; }
       sc[S_BETA] = sc[S_ALPHA] * (d0 / xi0);
       sc[S_XI0] = d0;
       break;
@@ -117,14 +131,14 @@ __device__ inline void krylov_op(const OpArgs& o, double* sc, KState* ks) {
     case OP_B2_XI_ODD: {
       const double xi0 = sc[S_XI0];
       sc[S_XI1] = d0;
-      if (fabs(xi0) < 1.0e-30) { kexit(ks, o.k); break; }
+      if (fabs(xi0) < 1.0e-30) { kexit(ks, op_k(o, ks)); break; }
       sc[S_BETA] = sc[S_ALPHA] * (d0 / xi0);
       sc[S_XI0] = d0;
       break;
     }
     case OP_B2_GAMMA:
       sc[S_GAMMA] = d0;
-      if (fabs(d0) < 1.0e-30) { kexit(ks, o.k); break; }
+      if (fabs(d0) < 1.0e-30) { kexit(ks, op_k(o, ks)); break; }
       sc[S_ALPHA] = sc[S_XI0] / d0;
       break;
     case OP_B2_GCR: {
@@ -158,11 +172,11 @@ __device__ inline void krylov_op(const OpArgs& o, double* sc, KState* ks) {
     case OP_B2_REL: {
       const double rel = sqrt(d0) / sc[S_NORMB];
       sc[S_REL] = rel;
-      if (isnan(rel)) { ks->nan = 1; kexit(ks, o.k); }
+      if (isnan(rel)) { ks->nan = 1; kexit(ks, op_k(o, ks)); }
       break;
     }
     case OP_TOPCHECK:
-      if (sc[S_REL] < o.tol) kexit(ks, o.k);
+      if (sc[S_REL] < o.tol) kexit(ks, op_k(o, ks));
       break;
     case OP_REF_NORMB: {
       double nb = sqrt(d0);

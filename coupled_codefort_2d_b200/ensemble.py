@@ -25,10 +25,11 @@ from . import cases
 # flexible GMRES(30) inside the FP64 defect correction; the PCD's PCG cap
 # adapts from 40 and its velocity smoothing from 6 sweeps of red-black SOR
 # (omega 1.5), which on the hard high-density-ratio cases needs fewer Arnoldi
-# steps than the reference's damped Jacobi at four times the sweeps
+# steps than the reference's damped Jacobi at four times the sweeps; every
+# Arnoldi step is replayed from a CUDA graph (one launch per step)
 SOLVER = dict(tol_bicgstab2=1e-8, max_iter_bicgstab2=500, refine=2, refine_inner_tol=1e-2, refine_max_inner=30,
               refine_max_outer=60, krylov_bc_fix=1, pcg_cap_start=40, pcd_sweeps=6, pcd_sweeps_max=24,
-              pcd_smoother=1, pcd_sor_omega=1.5)
+              pcd_smoother=1, pcd_sor_omega=1.5, graphs=1)
 DT = 5e-4
 
 
@@ -155,11 +156,14 @@ def main(argv=None):
     ap.add_argument("--omega", type=float, default=None, help="red-black SOR over-relaxation")
     ap.add_argument("--sweeps", type=int, default=None, help="PCD velocity sweeps")
     ap.add_argument("--sweeps-max", type=int, default=None, help="adaptive sweeps ceiling (0: fixed)")
+    ap.add_argument("--graphs", type=int, choices=[0, 1], default=None,
+                    help="replay the Arnoldi steps from CUDA graphs (default: the SOLVER setting)")
     args = ap.parse_args(argv)
     solver = dict(SOLVER)
     if args.smoother:
         solver["pcd_smoother"] = 1 if args.smoother == "rbsor" else 0
-    for key, val in (("pcd_sor_omega", args.omega), ("pcd_sweeps", args.sweeps), ("pcd_sweeps_max", args.sweeps_max)):
+    for key, val in (("pcd_sor_omega", args.omega), ("pcd_sweeps", args.sweeps), ("pcd_sweeps_max", args.sweeps_max),
+                     ("graphs", args.graphs)):
         if val is not None:
             solver[key] = val
     import datetime

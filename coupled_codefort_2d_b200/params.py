@@ -57,6 +57,9 @@ class Params:
     # passes per sweep)
     pcd_smoother: int = 0
     pcd_sor_omega: float = 1.0
+    # 1: replay each flexible-GMRES Arnoldi step from a CUDA graph (execution
+    # only; the results are the same)
+    graphs: int = 0
 
     def with_(self, **kw) -> "Params":
         return replace(self, **kw)

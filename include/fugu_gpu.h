@@ -99,6 +99,10 @@ typedef struct {
                                  faces with (i + j) even, then the odd ones,
                                  in place, the halo refreshed before each     */
   double pcd_sor_omega;       /* 1.0 (Gauss-Seidel); 0 < omega < 2          */
+  int graphs;                 /* 1: each flexible-GMRES Arnoldi step (refine
+                                 = 2) is captured once as a CUDA graph and
+                                 replayed (same kernels, same results); 0:
+                                 launched kernel by kernel                   */
 } fugu_params;
 
 /* Optional arguments of advance_coupled_step (src/mod_solver_coupled.f90:137-160):

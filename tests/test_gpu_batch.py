@@ -46,10 +46,10 @@ def batched(specs, prms, prec, **kw):
 
 
 # the batched ensemble's own solver: flexible GMRES, adaptive PCD with the
-# red-black SOR velocity smoother
+# red-black SOR velocity smoother, Arnoldi steps replayed from CUDA graphs
 ENSEMBLE_LIKE = dict(tol_bicgstab2=1e-8, max_iter_bicgstab2=200, refine=2, refine_inner_tol=1e-2, refine_max_inner=30,
                      refine_max_outer=40, krylov_bc_fix=1, pcg_cap_start=4, pcd_sweeps=2, pcd_sweeps_max=8,
-                     pcd_smoother=1, pcd_sor_omega=1.5)
+                     pcd_smoother=1, pcd_sor_omega=1.5, graphs=1)
 
 
 @pytest.mark.parametrize("prec,solver", [(FP64, SOLVER), (MIXED, SOLVER), (MIXED, ENSEMBLE_LIKE)])

@@ -94,10 +94,13 @@ def run_pair(oracle_mod, name, prm_override=None, precision=0, nsteps=None):
     return g, st_o, st_g, hist
 
 
+@pytest.mark.parametrize("graphs", [0, 1])
 @pytest.mark.parametrize("name", ["cavity", "droplet", "bubble_amp", "bubble_freeslip", "poiseuille", "cylinder",
                                   "cavity_b2"])
-def test_step_parity_plain_fp64(gpu, oracle_mod, name):
-    g, st_o, st_g, hist = run_pair(oracle_mod, name)
+def test_step_parity_plain_fp64(gpu, oracle_mod, name, graphs):
+    """graphs = 1 replays each BiCGStab / BiCGStab(2) iteration from one
+    captured CUDA graph, its iteration index kept on the device."""
+    g, st_o, st_g, hist = run_pair(oracle_mod, name, dict(graphs=graphs))
     for so, sg in hist:
         assert sg["iter"] == so.iter, (sg["iter"], so.iter)
         assert sg["pcg_calls"] == so.pcg_calls
@@ -124,16 +127,19 @@ def test_step_parity_grid_wide_pcg(gpu, oracle_mod, name, monkeypatch):
 @pytest.mark.parametrize("name,refine,cap0,swmax,smoother", [
     ("droplet", 1, 0, 0, 0), ("droplet", 2, 0, 0, 0), ("bubble_freeslip", 2, 0, 0, 0), ("droplet", 2, 3, 0, 0),
     ("bubble_freeslip", 2, 2, 0, 0), ("bubble_freeslip", 2, 2, 8, 0), ("droplet", 2, 0, 0, 1),
-    ("bubble_freeslip", 2, 2, 8, 1), ("poiseuille", 2, 0, 0, 1)])
+    ("bubble_freeslip", 2, 2, 8, 1), ("poiseuille", 2, 0, 0, 1), ("droplet", 2, 3, 0, 2),
+    ("bubble_freeslip", 2, 2, 8, 2)])
 def test_refine_fp64_parity(gpu, oracle_mod, name, refine, cap0, swmax, smoother):
     """FP64 defect correction around BiCGStab (refine 1) or flexible GMRES
     (refine 2): same outer and inner iteration counts as the oracle, and the
     same bits.  cap0 > 0 runs the adaptive PCG cap from a start so low that
     it must grow, swmax > 0 then also the PCD sweeps from 1; both carry
     across the steps on both sides.  smoother 1: the PCD's red-black SOR
-    velocity smoother (omega 1.5; the periodic channel wraps its colours)."""
+    velocity smoother (omega 1.5; the periodic channel wraps its colours).
+    smoother 2: the same with every Arnoldi step replayed from a CUDA graph."""
     over = dict(refine=refine, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=30, krylov_bc_fix=1,
-                tol_bicgstab2=1e-9, pcg_cap_start=cap0, pcd_smoother=smoother, pcd_sor_omega=1.5)
+                tol_bicgstab2=1e-9, pcg_cap_start=cap0, pcd_smoother=min(smoother, 1), pcd_sor_omega=1.5,
+                graphs=int(smoother == 2))
     if swmax:  # a low PCG ceiling, so that the sweeps must grow too
         over.update(pcd_sweeps=1, pcd_sweeps_max=swmax, pcg_max_iter=8)
     g, st_o, st_g, hist = run_pair(oracle_mod, name, over)
@@ -179,6 +185,51 @@ def test_mixed_precision_error_vs_fp64_oracle(gpu, oracle_mod, name, refine, smo
     assert coupled <= 1e-6, (coupled, per_field)
     vo, vg = cases.fluid1_volume(g, st_o["c_field"]), cases.fluid1_volume(g, st_g["c_field"])
     assert abs(vg - vo) <= 1e-6 * abs(vo), (vg, vo)
+
+
+def _device_run(name, over, precision, prof):
+    """the case's steps on the GPU alone (device-resident state); returns the
+    final state, per-step stats and the launch / PCG profile counters"""
+    g, p, c0, kw, dt, n, _ = case(name)
+    p = p.with_(**over)
+    from oracle import oracle as o  # the initial state only
+
+    st = o.new_state(g, c0, p)
+    with Context(g, p, precision=precision) as ctx:
+        ctx.upload_state(st)
+        ctx.profile(1 if prof else 0)
+        opts = ctx.step_opts(**kw)
+        stats = [ctx.step(dt, s, opts) for s in range(1, n + 1)]
+        counters = ctx.profile(-1)
+        out = ctx.download_state(STATE)
+    return out, stats, counters
+
+
+@pytest.mark.parametrize("prof", [False, True])
+@pytest.mark.parametrize("precision,refine", [(0, 2), (1, 2), (1, 1)])
+@pytest.mark.parametrize("name", ["droplet", "bubble_freeslip"])
+def test_graph_replay_is_bitwise(gpu, name, precision, refine, prof):
+    """graphs = 1 replays each flexible-GMRES Arnoldi step (refine 2) or
+    BiCGStab(2) iteration (refine 1) from a CUDA graph: the same kernels with
+    the same arguments, so the same bits, iteration counts and kernel-launch
+    count as launching them one by one.  Under flexible GMRES the PCG cap and
+    the PCD sweeps start low and adapt, so the graphs are re-captured and
+    updated in place mid-run; with profiling on, the graphs carry the PCG
+    interval events and every PCG launch is still timed."""
+    over = dict(refine=refine, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=30, krylov_bc_fix=1,
+                tol_bicgstab2=1e-9)
+    if refine == 2:
+        over.update(pcg_cap_start=2, pcd_sweeps=1, pcd_sweeps_max=8, pcg_max_iter=8)
+    runs = {gr: _device_run(name, dict(over, graphs=gr), precision, prof) for gr in (0, 1)}
+    (s0, h0, c0), (s1, h1, c1) = runs[0], runs[1]
+    for a, b in zip(h0, h1):  # the low PCG ceiling may stop a mixed solve short: equal either way
+        assert a == b
+    for k in STATE:
+        np.testing.assert_array_equal(s0[k], s1[k], err_msg=k)
+    assert c0["kernel_launches"] == c1["kernel_launches"]
+    if prof:
+        assert c0["pcg_launches"] == c1["pcg_launches"] > 0
+        assert c1["pcg_ms"] > 0.0
 
 
 def test_checkpoint_restart_bitwise(gpu, oracle_mod):
