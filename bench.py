@@ -215,8 +215,9 @@ def gpu_arm(args, rank, world, local_rank):
         # FP64 inner form of the same solver, same steps
         t64, s64, _, _ = run_form(FP64, args.steps, args.warmup)
         out["t_fp64"], out["s_fp64"] = t64, s64
-        # the reference algorithm as written (preconditioned residual, max 500 its)
-        pref = prm.with_(refine=0, krylov_bc_fix=0)
+        # the reference algorithm as written (preconditioned residual, max 500 its,
+        # the reference's 3 PCD sweeps and uncapped PCG)
+        pref = prm.with_(refine=0, krylov_bc_fix=0, pcd_sweeps=3, pcd_sweeps_max=0, pcg_cap_start=0)
         tref, sref, _, _ = run_form(FP64, 2, 1, use_b2=False, prm_=pref)
         out["t_ref"], out["s_ref"] = tref, sref
         out["e2e"] = e2e_arm(args, g, prm, st0, local_rank)
