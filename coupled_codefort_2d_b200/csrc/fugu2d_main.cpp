@@ -229,6 +229,10 @@ bool apply(Settings& st, const std::map<std::string, std::string>& kv, std::stri
     err = "limiter must be 'vanleer' or 'superbee'";
     return false;
   }
+  if (st.pcd_smoother != "jacobi" && st.pcd_smoother != "rbsor") {
+    err = "pcd_smoother must be 'jacobi' or 'rbsor'";
+    return false;
+  }
   return true;
 }
 
@@ -240,14 +244,17 @@ void print_json(const Settings& s) {
          "\"periodic_x\": %s, \"periodic_y\": %s, \"adaptive_dt\": %s, \"consistent_amp\": %s, "
          "\"use_bicgstab2\": %s, \"restart\": %s, \"vtk_freq\": %d, \"chk_freq\": %d, \"u_lid\": %.17g, "
          "\"cyl_xc\": %.17g, \"cyl_yc\": %.17g, \"cyl_rad\": %.17g, \"drop_rad\": %.17g, \"chk_prefix\": \"%s\", "
-         "\"precision\": \"%s\", \"limiter\": \"%s\", \"refine\": %d, \"krylov_bc_fix\": %d}\n",
+         "\"precision\": \"%s\", \"limiter\": \"%s\", \"refine\": %d, \"krylov_bc_fix\": %d, "
+         "\"pcd_sweeps\": %d, \"pcd_sweeps_max\": %d, \"pcd_smoother\": \"%s\", \"pcd_sor_omega\": %.17g, "
+         "\"graphs\": %d}\n",
          s.case_type.c_str(), s.Lx, s.Ly, s.Nx_global, s.Ny_global, s.rho1, s.rho2, s.mu1, s.mu2, s.sigma, s.gx,
          s.gy, s.dt, s.t_final, s.cfl_target, s.max_time_steps, s.time_order, s.tol_bicgstab2,
          s.max_iter_bicgstab2, s.alpha_penalty, s.periodic_x ? "true" : "false", s.periodic_y ? "true" : "false",
          s.adaptive_dt ? "true" : "false", s.consistent_amp ? "true" : "false",
          s.use_bicgstab2 ? "true" : "false", s.restart ? "true" : "false", s.vtk_freq, s.chk_freq, s.u_lid,
          s.cyl_xc, s.cyl_yc, s.cyl_rad, s.drop_rad, s.chk_prefix.c_str(), s.precision.c_str(), s.limiter.c_str(),
-         s.refine, s.krylov_bc_fix);
+         s.refine, s.krylov_bc_fix, s.pcd_sweeps, s.pcd_sweeps_max, s.pcd_smoother.c_str(), s.pcd_sor_omega,
+         s.graphs);
 }
 
 // ---------------------------------------------------------------- fields

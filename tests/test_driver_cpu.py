@@ -102,6 +102,21 @@ def test_comments_commas_and_extensions(driver, tmp_path):
     assert s["case_type"] == "cavity" and s["Nx_global"] == 128 and s["Ny_global"] == 128
     assert s["periodic_x"] is True and s["dt"] == 1e-2
     assert s["precision"] == "mixed" and s["limiter"] == "superbee" and s["krylov_bc_fix"] == 1
+    assert (s["pcd_smoother"], s["graphs"]) == ("jacobi", 0)
+
+
+def test_smoother_and_graph_keys(driver, tmp_path):
+    text = """&sim_params
+  pcd_smoother = 'RBSOR', pcd_sor_omega = 1.5d0, pcd_sweeps = 6, pcd_sweeps_max = 24, graphs = .true.
+/
+"""
+    r = run(driver, text, tmp_path)
+    assert r.returncode == 0, r.stderr
+    s = json.loads(r.stdout)
+    assert (s["pcd_smoother"], s["pcd_sor_omega"], s["pcd_sweeps"], s["pcd_sweeps_max"], s["graphs"]) == \
+        ("rbsor", 1.5, 6, 24, 1)
+    r = run(driver, "&sim_params\n  pcd_smoother = 'gauss'\n/\n", tmp_path)
+    assert r.returncode == 2 and "pcd_smoother" in r.stderr
 
 
 def test_unknown_key_rejected(driver, tmp_path):
