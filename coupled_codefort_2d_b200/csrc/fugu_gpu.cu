@@ -997,7 +997,14 @@ KrylovResult fgmres(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const 
   // records the PCG interval on its own event pair, read after each step
   const int pi = sizeof(T) == 8 ? 0 : 1;
   const bool graphed = c->prm.graphs == 1 && c->pcgc[pi].ok;
-  if (graphed && (int)c->fg_graphs[pi].size() < m) c->fg_graphs[pi].resize(m);
+  if (graphed && (int)c->fg_graphs[pi].size() < m) {
+    // a solve that ended in an error may have left a sample pending in the
+    // vector that is about to move
+    if (c->pcg_timed && c->pcg_timed >= c->fg_graphs[pi].data() &&
+        c->pcg_timed < c->fg_graphs[pi].data() + c->fg_graphs[pi].size())
+      c->pcg_timed = nullptr;
+    c->fg_graphs[pi].resize(m);
+  }
   for (int j = 0; j < m && ks.active; ++j) {
     Trip<T> Vj = trip_at(f.V, j, c->n), Zj = trip_at(f.Z, j, c->n);
     auto arnoldi_step = [&] {
