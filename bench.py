@@ -248,7 +248,7 @@ def batched_arm(world, rank, local_rank):
         barrier, max_reduce, gather = (lambda: None), (lambda x: x), (lambda o: [o])
     res = ensemble.run_ensemble(
         specs, BATCH_STEPS, rank, world,
-        lambda idx: ensemble.run_shard_gpu(specs, idx, BATCH_STEPS, local_rank, nthreads=8, warmup=1),
+        lambda idx: ensemble.run_shard_gpu(specs, idx, BATCH_STEPS, local_rank, nthreads=0, warmup=1),
         barrier, max_reduce, gather)
     if rank != 0:
         return None

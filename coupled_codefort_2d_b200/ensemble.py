@@ -148,7 +148,7 @@ def main(argv=None):
     ap.add_argument("--cases", type=int, default=256)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--seed", type=int, default=cases.ENSEMBLE_SEED)
-    ap.add_argument("--threads", type=int, default=8, help="host threads per rank")
+    ap.add_argument("--threads", type=int, default=0, help="host threads per rank (0: one per host core)")
     ap.add_argument("--out", default=None, help="write the per-case table (JSON) here")
     ap.add_argument("--warmup", type=int, default=0, help="untimed steps first")
     ap.add_argument("--smoother", choices=["jacobi", "rbsor"], default=None,
