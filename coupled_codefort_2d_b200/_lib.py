@@ -71,7 +71,7 @@ class FuguProfile(C.Structure):
     _fields_ = [
         ("kernel_launches", C.c_ulonglong), ("pcg_ms", C.c_double), ("pcg_launches", C.c_ulonglong),
         ("pcg_iters", C.c_ulonglong), ("pcg_cells", C.c_ulonglong), ("pcg_grid", C.c_int), ("svof_grid", C.c_int),
-        ("pcg_cluster_fp64", C.c_int), ("pcg_cluster_fp32", C.c_int),
+        ("pcg_cluster_fp64", C.c_int), ("pcg_cluster_fp32", C.c_int), ("pcg_iters_timed", C.c_ulonglong),
     ]
 
     def as_dict(self):

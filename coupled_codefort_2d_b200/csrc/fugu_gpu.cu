@@ -204,6 +204,7 @@ struct fugu_ctx {
     // around its PCG launches (profiling): one pair per launch in the body
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
     size_t ev_used = 0;
+    bool timed = false;  // its PCG launches are timed (profiling)
   };
   std::vector<StepGraph> fg_graphs[2];
   // one BiCGStab (index 0) / BiCGStab(2) (index 1) iteration per precision,
@@ -217,7 +218,7 @@ struct fugu_ctx {
   std::vector<cudaEvent_t> ev_pool;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pcg;
   double prof_pcg_ms = 0.0;
-  unsigned long long prof_pcg_launches = 0, prof_pcg_iters = 0, prof_pcg_cells = 0;
+  unsigned long long prof_pcg_launches = 0, prof_pcg_iters = 0, prof_pcg_cells = 0, prof_pcg_iters_timed = 0;
   std::string err;
 };
 
@@ -542,8 +543,11 @@ void pcg(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, double tol, int max_i
   a.part = c->part; a.gs = c->gs; a.out = c->pcg_out; a.active = active;
   a.tol = tol; a.max_iter = max_iter; a.phi_zero = phi_zero ? 1 : 0;
   const fugu_ctx::ClusterPlan& cp = c->pcgc[sizeof(T) == 8 ? 0 : 1];
+  // timed: profiling, and not inside a captured step that is not sampled
+  const bool rec = c->prof && (!c->capturing || c->capturing->timed);
+  a.timed = rec ? 1 : 0;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (c->prof) {
+  if (rec) {
     if (c->capturing) {  // a captured step records its own pairs, as graph nodes
       fugu_ctx::StepGraph& sg = *c->capturing;
       if (sg.ev_used >= sg.ev.size()) throw ApiError{FUGU_EINVAL, "captured step: too many PCG launches"};
@@ -562,7 +566,7 @@ void pcg(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, double tol, int max_i
     ca.g = c->g;
     ca.rhs = rhs; ca.cx = w.cx; ca.cy = w.cy; ca.dinv = w.dinv; ca.phi = phi;
     ca.out = c->pcg_out; ca.active = active; ca.tol = tol; ca.max_iter = max_iter;
-    ca.phi_zero = phi_zero ? 1 : 0; ca.rows_per = cp.rows_per;
+    ca.phi_zero = phi_zero ? 1 : 0; ca.rows_per = cp.rows_per; ca.timed = a.timed;
     CK(launch_pcg_cluster<T>(ca, cp.C, cp.cpt, cp.smem, c->s));
   } else {
     CK(cudaMemsetAsync(c->gs, 0, sizeof(GridSync), c->s));
@@ -570,7 +574,7 @@ void pcg(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, double tol, int max_i
     launch_coop(c, (const void*)k_pcg<T>, c->pcg_grid, args);
   }
   ++c->launches;
-  if (c->prof) {
+  if (rec) {
     if (c->capturing) {
       CK(cudaEventRecordWithFlags(e1, c->s, cudaEventRecordExternal));
     } else {
@@ -686,11 +690,12 @@ void graph_prof_read(fugu_ctx* c);
 // place (or instantiated anew when its topology changed).  Capture is
 // thread-local, so other host threads (a batch) keep launching meanwhile.
 template <typename F>
-void run_graphed(fugu_ctx* c, fugu_ctx::StepGraph& sg, std::vector<unsigned char>&& key, F body) {
+void run_graphed(fugu_ctx* c, fugu_ctx::StepGraph& sg, std::vector<unsigned char>&& key, bool timed, F body) {
   if (!sg.exec || sg.key != key) {
-    // event pairs for the PCG launches of the body (at most 4: BiCGStab(2)
+    // event pairs for the PCG launches of a timed body (at most 4: BiCGStab(2)
     // applies PCD four times per iteration), created before the capture
-    while (c->prof && sg.ev.size() < 4) {
+    sg.timed = timed;
+    while (timed && sg.ev.size() < 4) {
       cudaEvent_t a, b;
       CK(cudaEventCreate(&a));
       CK(cudaEventCreate(&b));
@@ -743,7 +748,7 @@ void run_graphed(fugu_ctx* c, fugu_ctx::StepGraph& sg, std::vector<unsigned char
   CK(cudaGraphLaunch(sg.exec, c->s));
   c->launches += sg.launches;
   graph_prof_read(c);
-  if (c->prof) c->pcg_timed = &sg;
+  if (sg.timed) c->pcg_timed = &sg;
 }
 
 // fold the PCG intervals of the last replayed step graph into the profile
@@ -822,7 +827,7 @@ KrylovResult bicgstab1(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, con
       vbcs(c, X.u, X.v, 0.0, act);
     };
     if (graphed)
-      run_graphed(c, c->kr_graphs[pi][0], krylov_key(c, w, cb, o, X, dt, tol), iteration);
+      run_graphed(c, c->kr_graphs[pi][0], krylov_key(c, w, cb, o, X, dt, tol), c->prof != 0, iteration);
     else
       iteration();
     ks = read_ks(c);
@@ -902,7 +907,7 @@ KrylovResult bicgstab2(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, con
       scalar_op(c, OpArgs{OP_TOPCHECK, graphed ? -1 : k + 1, tol}, true);
     };
     if (graphed)
-      run_graphed(c, c->kr_graphs[pi][1], krylov_key(c, w, cb, o, X, dt, tol), iteration);
+      run_graphed(c, c->kr_graphs[pi][1], krylov_key(c, w, cb, o, X, dt, tol), c->prof != 0, iteration);
     else
       iteration();
     ks = read_ks(c);
@@ -1027,8 +1032,12 @@ KrylovResult fgmres(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const 
       key_put(key, j); key_put(key, m); key_put(key, f.V); key_put(key, f.Z); key_put(key, f.st);
       key_put(key, wv.base); key_put(key, cb); key_put(key, o); key_put(key, dt); key_put(key, tol);
       key_put(key, c->pcg_cap_cur); key_put(key, c->pcd_sweeps_cur); key_put(key, c->adj_on);
-      key_put(key, c->prm); key_put(key, c->prof);
-      run_graphed(c, c->fg_graphs[pi][j], std::move(key), arnoldi_step);
+      // profiling samples the PCG of the first Arnoldi step of each cycle:
+      // event-record nodes split a graph's launch sequence, so timing every
+      // step would slow the replay it measures
+      const bool timed = c->prof && j == 0;
+      key_put(key, c->prm); key_put(key, timed);
+      run_graphed(c, c->fg_graphs[pi][j], std::move(key), timed, arnoldi_step);
     } else {
       arnoldi_step();
     }
@@ -1264,6 +1273,7 @@ void collect(fugu_ctx* c, fugu_stats* st) {
   if (c->prof) {
     prof_drain(c);
     c->prof_pcg_iters += c->h_pcg->total_iters;
+    c->prof_pcg_iters_timed += c->h_pcg->timed_iters;
     c->prof_pcg_cells = (unsigned long long)c->prm.nx * c->prm.ny;
   }
 }
@@ -1623,12 +1633,13 @@ int fugu_profile(fugu_ctx* c, int enable, fugu_profile_stats* out) {
       out->svof_grid = c->svof_grid;
       out->pcg_cluster_fp64 = c->pcgc[0].ok ? c->pcgc[0].C : 0;
       out->pcg_cluster_fp32 = c->pcgc[1].ok ? c->pcgc[1].C : 0;
+      out->pcg_iters_timed = c->prof_pcg_iters_timed;
     }
     if (enable >= 0) {
       c->prof = enable;
       c->launches = 0;
       c->prof_pcg_ms = 0.0;
-      c->prof_pcg_launches = c->prof_pcg_iters = 0;
+      c->prof_pcg_launches = c->prof_pcg_iters = c->prof_pcg_iters_timed = 0;
     }
   });
 }

@@ -53,6 +53,7 @@ struct PcgClusterArgs {
   int max_iter;
   int phi_zero;
   int rows_per;  // rows of every CTA but possibly the last
+  int timed;     // the launch is timed: add its iterations to out->timed_iters
 };
 
 // shared-memory footprint in elements of T for rows_per rows of nx cells
@@ -367,6 +368,7 @@ __global__ void __launch_bounds__(PCGC_TPB, 1) k_pcg_cluster(PcgClusterArgs<T> a
     a.out->iters = it;
     a.out->res = res_norm / rhs_norm;
     a.out->total_iters += (unsigned long long)it;
+    if (a.timed) a.out->timed_iters += (unsigned long long)it;
     a.out->calls += 1;
   }
   cl.sync();  // no CTA leaves while another may still read its shared memory

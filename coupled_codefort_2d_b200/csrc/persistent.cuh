@@ -15,6 +15,7 @@ struct PcgOut {
   double res;           // res_out of the last solve
   unsigned long long total_iters;  // accumulated over solves (statistics)
   unsigned long long calls;
+  unsigned long long timed_iters;  // accumulated over the launches with timed = 1
 };
 
 template <typename T>
@@ -37,6 +38,7 @@ struct PcgArgs {
   double tol;
   int max_iter;
   int phi_zero;        // phi is identically zero on entry (preconditioner use)
+  int timed;           // the launch is timed: add its iterations to out->timed_iters
 };
 
 // Grid-wide order-independent sum of one (or two) DD values per thread: CTA
@@ -220,6 +222,7 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
     a.out->iters = it;
     a.out->res = res_norm / rhs_norm;
     a.out->total_iters += (unsigned long long)it;
+    if (a.timed) a.out->timed_iters += (unsigned long long)it;
     a.out->calls += 1;
   }
 #undef CELL_LOOP

@@ -146,13 +146,18 @@ typedef struct fugu_ctx fugu_ctx;
 /* Measurement counters (no counterpart in the reference, which has none). */
 typedef struct {
   unsigned long long kernel_launches; /* kernels launched since the last reset */
-  double pcg_ms;                      /* CUDA-event time of the PCG launches   */
-  unsigned long long pcg_launches;
-  unsigned long long pcg_iters;       /* PCG iterations in those launches      */
+  double pcg_ms;                      /* CUDA-event time of the timed PCG
+                                         launches: every launch, except that a
+                                         flexible-GMRES cycle replayed from CUDA
+                                         graphs times the PCG of its first
+                                         Arnoldi step only                     */
+  unsigned long long pcg_launches;    /* timed PCG launches                    */
+  unsigned long long pcg_iters;       /* PCG iterations of all launches        */
   unsigned long long pcg_cells;       /* cells per PCG iteration (nx*ny)       */
   int pcg_grid, svof_grid;            /* CTAs of the persistent kernels        */
   int pcg_cluster_fp64;               /* CTAs of the cluster-resident PCG (0 =  */
   int pcg_cluster_fp32;               /*   grid-wide kernel used instead)       */
+  unsigned long long pcg_iters_timed; /* PCG iterations of the timed launches  */
 } fugu_profile_stats;
 
 /* ---------------------------------------------------------------- context */

@@ -215,7 +215,7 @@ def test_graph_replay_is_bitwise(gpu, name, precision, refine, prof):
     count as launching them one by one.  Under flexible GMRES the PCG cap and
     the PCD sweeps start low and adapt, so the graphs are re-captured and
     updated in place mid-run; with profiling on, the graphs carry the PCG
-    interval events and every PCG launch is still timed."""
+    interval events of the launches they time."""
     over = dict(refine=refine, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=30, krylov_bc_fix=1,
                 tol_bicgstab2=1e-9)
     if refine == 2:
@@ -228,8 +228,16 @@ def test_graph_replay_is_bitwise(gpu, name, precision, refine, prof):
         np.testing.assert_array_equal(s0[k], s1[k], err_msg=k)
     assert c0["kernel_launches"] == c1["kernel_launches"]
     if prof:
-        assert c0["pcg_launches"] == c1["pcg_launches"] > 0
-        assert c1["pcg_ms"] > 0.0
+        # launched one by one every PCG launch is timed; replayed, a BiCGStab
+        # iteration times all of its launches and a flexible-GMRES cycle the
+        # PCG of its first Arnoldi step
+        assert c0["pcg_iters_timed"] == c0["pcg_iters"] == c1["pcg_iters"]
+        assert c1["pcg_ms"] > 0.0 and c1["pcg_launches"] > 0
+        if refine == 1:
+            assert (c1["pcg_launches"], c1["pcg_iters_timed"]) == (c0["pcg_launches"], c0["pcg_iters_timed"])
+        else:
+            assert c1["pcg_launches"] < c0["pcg_launches"]
+            assert 0 < c1["pcg_iters_timed"] < c1["pcg_iters"]
 
 
 def test_checkpoint_restart_bitwise(gpu, oracle_mod):
