@@ -2907,7 +2907,7 @@ extern "C" int fugu_solve_poisson_pressure_noalloc(const fugu_params* p, void* s
   a.rhs = f[1]; a.cx = f[4]; a.cy = f[5]; a.dinv = f[6];
   a.phi = f[0]; a.r = f[7]; a.z = f[8]; a.pb0 = f[9]; a.pb1 = f[10]; a.ap = f[11];
   a.part = part; a.gs = gs; a.out = out; a.active = nullptr;
-  a.tol = tol; a.max_iter = max_iter; a.phi_zero = 0;
+  a.tol = tol; a.max_iter = max_iter; a.phi_zero = 0; a.timed = 0;
   long want = ((long)p->nx * p->ny + PCG_TPB - 1) / PCG_TPB;
   const int grid = (int)(want < d.max_ctas ? (want < 1 ? 1 : want) : d.max_ctas);
   void* args[] = {&a};
