@@ -143,6 +143,18 @@ def _dist_ops():
     return barrier, max_reduce, gather
 
 
+def solver_from_args(args) -> dict:
+    """SOLVER with the command line's overrides (None keeps a setting)."""
+    solver = dict(SOLVER)
+    if args.smoother:
+        solver["pcd_smoother"] = 1 if args.smoother == "rbsor" else 0
+    for key, val in (("pcd_sor_omega", args.omega), ("pcd_sweeps", args.sweeps), ("pcd_sweeps_max", args.sweeps_max),
+                     ("graphs", args.graphs)):
+        if val is not None:
+            solver[key] = val
+    return solver
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--cases", type=int, default=256)
@@ -159,13 +171,7 @@ def main(argv=None):
     ap.add_argument("--graphs", type=int, choices=[0, 1], default=None,
                     help="replay the Arnoldi steps from CUDA graphs (default: the SOLVER setting)")
     args = ap.parse_args(argv)
-    solver = dict(SOLVER)
-    if args.smoother:
-        solver["pcd_smoother"] = 1 if args.smoother == "rbsor" else 0
-    for key, val in (("pcd_sor_omega", args.omega), ("pcd_sweeps", args.sweeps), ("pcd_sweeps_max", args.sweeps_max),
-                     ("graphs", args.graphs)):
-        if val is not None:
-            solver[key] = val
+    solver = solver_from_args(args)
     import datetime
 
     import torch

@@ -80,3 +80,17 @@ def test_gloo_two_ranks_reassemble_the_ensemble(tmp_path):
     # the timed region is the slower rank's (max over ranks)
     assert res["seconds"] >= 0.1
     assert res["case_steps_per_s"] == pytest.approx(12 * 5 / res["seconds"])
+
+
+def test_solver_overrides_from_the_command_line():
+    import argparse
+
+    from coupled_codefort_2d_b200.ensemble import SOLVER, solver_from_args
+
+    none = argparse.Namespace(smoother=None, omega=None, sweeps=None, sweeps_max=None, graphs=None)
+    assert solver_from_args(none) == SOLVER
+    assert SOLVER["pcd_smoother"] == 1 and SOLVER["graphs"] == 1
+    a = argparse.Namespace(smoother="jacobi", omega=None, sweeps=3, sweeps_max=0, graphs=0)
+    s = solver_from_args(a)
+    assert (s["pcd_smoother"], s["pcd_sweeps"], s["pcd_sweeps_max"], s["graphs"]) == (0, 3, 0, 0)
+    assert s["pcd_sor_omega"] == SOLVER["pcd_sor_omega"] and SOLVER["pcd_sweeps"] == 6  # the default is untouched
