@@ -710,6 +710,7 @@ void run_graphed(fugu_ctx* c, fugu_ctx::StepGraph& sg, std::vector<unsigned char
       body();
     } catch (...) {
       c->capturing = nullptr;
+      c->launches = l0;
       cudaStreamEndCapture(c->s, &graph);
       if (graph) cudaGraphDestroy(graph);
       cudaGetLastError();
