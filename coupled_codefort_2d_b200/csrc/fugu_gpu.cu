@@ -9,6 +9,7 @@
 // Compiled for sm_100a with --fmad=false (see build.py): the FP64 plain form
 // then rounds every operation as the CPU oracle does.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <array>
@@ -55,6 +56,15 @@ struct CudaError {
     if (e_ != cudaSuccess) throw CudaError{e_, what};      \
     ++c->launches;                                         \
   } while (0)
+
+// NVTX range over a host scope: the phases of a step and each Krylov
+// iteration show as named ranges in a timeline profiler (no-ops otherwise)
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 struct ApiError {
   int code;
@@ -806,6 +816,7 @@ KrylovResult bicgstab1(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, con
   const bool graphed = c->prm.graphs == 1 && c->pcgc[pi].ok;
   int k = 1;
   for (; k <= max_iter && ks.active; ++k) {
+    NvtxRange r_it("bicgstab_iteration");
     const int kk = graphed ? -1 : k;
     auto iteration = [&] {
       vbcs(c, p.u, p.v, 0.0, act);
@@ -868,6 +879,7 @@ KrylovResult bicgstab2(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, con
   const bool graphed = c->prm.graphs == 1 && c->pcgc[pi].ok;
   int k = 1;
   for (; k <= max_iter && ks.active; ++k) {
+    NvtxRange r_it("bicgstab2_iteration");
     const int kk = graphed ? -1 : k;
     auto iteration = [&] {
       // even half
@@ -1012,6 +1024,7 @@ KrylovResult fgmres(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const 
     c->fg_graphs[pi].resize(m);
   }
   for (int j = 0; j < m && ks.active; ++j) {
+    NvtxRange r_it("arnoldi_step");
     Trip<T> Vj = trip_at(f.V, j, c->n), Zj = trip_at(f.Z, j, c->n);
     auto arnoldi_step = [&] {
       pcd<T>(c, w, cb, o, Vj, Zj, dt, act);
@@ -1144,6 +1157,7 @@ KrylovResult refine_solve(fugu_ctx* c, int solver, const CoefBufs<double>& cb64,
   if (adapt_sw)
     c->pcd_sweeps_cur = std::min(std::max(c->prm.pcd_sweeps, c->pcd_sweeps_state), c->prm.pcd_sweeps_max);
   for (;; ++outer) {
+    NvtxRange r_pass("defect_correction_pass");
     matvec<double>(c, cb64, o, X, ax, dt, nullptr);
     lin<double>(c, r, B, -1.0, c->sc + S_ONE, ax);
     dot_op<double>(c, {{r, r}}, OpArgs{OP_REF_REL, 0, tol}, false);
@@ -1317,6 +1331,7 @@ void step(fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o, fugu_st
   const double lid = o->has_lid ? o->u_top_lid : 0.0;
   const bool bdf2 = (p.time_order == 2 && step_idx >= 2);
   const double dt_eff = bdf2 ? dt / 1.5 : dt;
+  NvtxRange r_step("fugu_step");
   reset_counters(c);
   // 1. AB extrapolation u_adv = 2u^n - u^(n-1); u_prev <- u^n (u_prev then holds u^n)
   k_extrapolate<<<grid1d(c, n), 256, 0, c->s>>>(n, f[FUGU_F_U_VEL], f[FUGU_F_U_PREV], c->u_nm1, c->u_adv,
@@ -1327,6 +1342,8 @@ void step(fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o, fugu_st
   const double* u_n = f[FUGU_F_U_PREV];
   const double* v_n = f[FUGU_F_V_PREV];
   // 2. VOF transport with u^n (+ AMP mass fluxes)
+  {
+  NvtxRange r_vof("vof_transport");
   vof(c, f[FUGU_F_C_FIELD], c->c_new, u_n, v_n, dt, amp ? c->fcx : nullptr, amp ? c->fcy : nullptr);
   if (amp) {
     k_axpby<<<grid1d(c, n), 256, 0, c->s>>>(n, c->mdu, p.rho1 - p.rho2, c->fcx, p.rho2, c->u_adv);
@@ -1334,11 +1351,13 @@ void step(fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o, fugu_st
     CKL("k_axpby");
   }
   CK(cudaMemcpyAsync(f[FUGU_F_C_FIELD], c->c_new, sizeof(double) * n, cudaMemcpyDeviceToDevice, c->s));
+  }
   // 3. properties at t^(n+1)
   properties(c, f[FUGU_F_C_FIELD], f[FUGU_F_RHO_C], f[FUGU_F_RHO_U], f[FUGU_F_RHO_V], f[FUGU_F_KAPPA],
              f[FUGU_F_ZETA], f[FUGU_F_ETA]);
   // 4. SVOF + curvature + CSF
   if (p.sigma > 1.0e-14) {
+    NvtxRange r_st("svof_curvature_csf");
     const double delta = p.svof_delta_h * (c->g.dx < c->g.dy ? c->g.dx : c->g.dy);
     svof(c, f[FUGU_F_C_FIELD], c->c_s, c->svof_w, delta, p.svof_max_iter, p.svof_tol);
     curvature(c, c->c_s, f[FUGU_F_KAPPA_CURV]);
@@ -1379,7 +1398,10 @@ void step(fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o, fugu_st
   Trip<double> Xc = c->Xstate;
   KrylovResult kr;
   int outer = 0;
-  kr = solve(c, o->use_bicgstab2 ? 2 : 1, cb, so, Xc, c->B, dt_eff, tol, max_it, true, lid, &outer);
+  {
+    NvtxRange r_solve("coupled_solve");
+    kr = solve(c, o->use_bicgstab2 ? 2 : 1, cb, so, Xc, c->B, dt_eff, tol, max_it, true, lid, &outer);
+  }
   // 8. final halos and BCs
   halo(c, Xc.u, K_U);
   halo(c, Xc.v, K_V);
