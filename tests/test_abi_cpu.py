@@ -63,7 +63,8 @@ def test_ctypes_structs_match_header_layout():
 
     src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
     for cname, py in (("fugu_params", _lib.FuguParams), ("fugu_step_opts", _lib.FuguStepOpts),
-                      ("fugu_stats", _lib.FuguStats), ("fugu_batch_opts", _lib.FuguBatchOpts)):
+                      ("fugu_stats", _lib.FuguStats), ("fugu_batch_opts", _lib.FuguBatchOpts),
+                      ("fugu_profile_stats", _lib.FuguProfile)):
         body = re.search(r"typedef struct \{([^}]*)\}\s*" + cname + ";", src).group(1)
         names = []
         for decl in body.split(";"):
@@ -123,3 +124,21 @@ def test_layout_shapes_match_fortran_bounds():
     a[0, 0] = 1.0  # the lower-bound element u(0-nh, 1-nh) is the first in memory
     assert at(a, "u", -2, -1) == 1.0 and a.ravel(order="F")[0] == 1.0
     np.testing.assert_array_equal(at(a, "u", slice(0, 7), 3).shape, (8,))
+
+
+def test_fortran_binding_matches_header_layout():
+    """The bind(C) fugu_params of the Fortran interface module shown in
+    INTEGRATION.md declares the C struct's fields in the same order."""
+    src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    body = re.search(r"typedef struct \{([^}]*)\}\s*fugu_params;", src).group(1)
+    c_names = []
+    for decl in body.split(";"):
+        toks = decl.replace(",", " , ").split()
+        c_names += [t for t in toks[1:] if t not in (",", "long", "double", "int")]
+    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    ftype = re.search(r"type, bind\(C\) :: fugu_params(.*?)end type", doc, flags=re.S).group(1)
+    f_names = []
+    for line in ftype.replace("&\n", " ").splitlines():
+        if "::" in line:
+            f_names += [n.strip() for n in line.split("::", 1)[1].split(",") if n.strip()]
+    assert f_names == c_names
