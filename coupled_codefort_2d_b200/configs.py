@@ -4,6 +4,7 @@ per configuration).
     python -m coupled_codefort_2d_b200.configs c1            # lid-driven cavity, 128^2, 200 steps
     python -m coupled_codefort_2d_b200.configs c2            # static droplet, 256^2, 500 steps
     python -m coupled_codefort_2d_b200.configs c3 --steps N  # rising bubble, 320x640 (6000 steps to t = 3)
+    python -m coupled_codefort_2d_b200.configs c4            # 256-case ensemble, 200 steps (the ensemble runner)
     python -m coupled_codefort_2d_b200.configs c5            # adjoint gradients, 160x320, 400 steps
     python -m coupled_codefort_2d_b200.configs scale --n 2048 --steps 1   # droplet at n x n (HBM-bound)
 
@@ -24,6 +25,11 @@ free-slip sides, BDF2, dt = 5e-4; the high-contrast variant has bubble rho 1,
 mu 0.1, sigma 1.96.  Mixed precision against FP64: centroid height, rise
 velocity (``tests/test_rising_bubble.f90:134-155``) and circularity, and their
 differences.
+
+c4: the batched rising-bubble ensemble (256 seeded cases on the grids 64 x 128
+to 256 x 512, 200 BDF2 steps each, mixed precision); runs
+``python -m coupled_codefort_2d_b200.ensemble --cases 256 --steps N`` and
+prints its report (aggregate case-steps/s, per-case failures, max residual).
 
 c5: the discrete adjoint.  Rising bubble (outer rho 1000, mu 10; bubble rho
 100, mu 1; sigma 24.5; g = 0.98; area-fraction disc) on 160 x 320, 400 BDF2
@@ -256,13 +262,18 @@ def config_scale(args):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description="run a benchmark configuration and print its report")
-    ap.add_argument("config", choices=["c1", "c2", "c3", "c5", "scale"])
+    ap.add_argument("config", choices=["c1", "c2", "c3", "c4", "c5", "scale"])
     ap.add_argument("--steps", type=int, default=0, help="override the configuration's step count")
     ap.add_argument("--variant", default="standard", choices=["standard", "high_contrast"], help="c3 only")
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--n", type=int, default=2048, help="scale only: cells per side")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="scale only")
     args = ap.parse_args(argv)
+    if args.config == "c4":  # the ensemble runner prints its own report
+        from . import ensemble
+
+        ensemble.main(["--cases", "256", "--steps", str(args.steps or 200)])
+        return
     rep = {"c1": config_c1, "c2": config_c2, "c3": config_c3, "c5": config_c5, "scale": config_scale}[args.config](args)
     print(json.dumps(rep), flush=True)
 
