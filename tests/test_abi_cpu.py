@@ -126,17 +126,18 @@ def test_layout_shapes_match_fortran_bounds():
     np.testing.assert_array_equal(at(a, "u", slice(0, 7), 3).shape, (8,))
 
 
-def test_fortran_binding_matches_header_layout():
-    """The bind(C) fugu_params of the Fortran interface module shown in
-    INTEGRATION.md declares the C struct's fields in the same order."""
+@pytest.mark.parametrize("cname", ["fugu_params", "fugu_step_opts", "fugu_stats"])
+def test_fortran_binding_matches_header_layout(cname):
+    """The bind(C) types of the Fortran interface module shown in
+    INTEGRATION.md declare the C structs' fields in the same order."""
     src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
-    body = re.search(r"typedef struct \{([^}]*)\}\s*fugu_params;", src).group(1)
+    body = re.search(r"typedef struct \{([^}]*)\}\s*" + cname + ";", src).group(1)
     c_names = []
     for decl in body.split(";"):
         toks = decl.replace(",", " , ").split()
         c_names += [t for t in toks[1:] if t not in (",", "long", "double", "int")]
     doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    ftype = re.search(r"type, bind\(C\) :: fugu_params(.*?)end type", doc, flags=re.S).group(1)
+    ftype = re.search(r"type, bind\(C\) :: " + cname + r"\n(.*?)end type", doc, flags=re.S).group(1)
     f_names = []
     for line in ftype.replace("&\n", " ").splitlines():
         if "::" in line:
