@@ -154,7 +154,7 @@ def test_refine_fp64_parity(gpu, oracle_mod, name, refine, cap0, swmax, smoother
 
 
 @pytest.mark.parametrize("refine,smoother", [(1, 0), (2, 0), (2, 1)])
-@pytest.mark.parametrize("name", ["cavity", "droplet", "bubble_amp", "bubble_freeslip"])
+@pytest.mark.parametrize("name", ["cavity", "droplet", "bubble_amp", "bubble_freeslip", "cylinder"])
 def test_mixed_precision_error_vs_fp64_oracle(gpu, oracle_mod, name, refine, smoother):
     """FP32 inner Krylov+PCD inside FP64 defect correction: every step reaches
     the FP64 true residual tolerance (1e-9 relative), and the coupled state
