@@ -650,7 +650,8 @@ void pcd(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const SolveOpt& o
   pcg<T>(c, w.pcg, pw.phi, z.p, c->prm.pcg_tol, c->pcg_cap_cur > 0 ? c->pcg_cap_cur : c->prm.pcg_max_iter, true,
          active);
   halo(c, pw.phi, K_CELL, active);
-  k_pcd_schur<T><<<b.grid, b.block, 0, c->s>>>(c->g, pw.phi, cb.u_adv, cb.v_adv, r.p, T(1.0 / dt), active);
+  k_pcd_schur<T><<<b.grid, b.block, 0, c->s>>>(c->g, pw.phi, cb.u_adv, cb.v_adv, r.p, T(1.0 / dt), cb.kappa, z.p,
+                                                T(c->prm.pcd_visc_scale), active);
   CKL("k_pcd_schur");
   halo(c, r.p, K_CELL, active);
   k_pcd_zwork<T><<<b.grid, b.block, 0, c->s>>>(c->g, z.u, z.v, r.p, pw.zuw, pw.zvw, active);
@@ -1438,6 +1439,7 @@ int check_params(const fugu_params* p) {
   if (p->precision != FUGU_FP64 && p->precision != FUGU_MIXED) return FUGU_EINVAL;
   if (p->pcd_smoother < 0 || p->pcd_smoother > 1) return FUGU_EINVAL;
   if (p->graphs < 0 || p->graphs > 1) return FUGU_EINVAL;
+  if (!(p->pcd_visc_scale >= 0.0 && p->pcd_visc_scale < 1.0e6)) return FUGU_EINVAL;
   if (p->pcd_smoother == 1 && !(p->pcd_sor_omega > 0.0 && p->pcd_sor_omega < 2.0)) return FUGU_EINVAL;
   return FUGU_OK;
 }
@@ -1594,7 +1596,7 @@ void fugu_params_default(fugu_params* p) {
   p->svof_delta_h = 1.5; p->svof_max_iter = 150; p->svof_tol = 1.0e-7;
   p->refine_inner_tol = 1.0e-2; p->refine_max_inner = 20; p->refine_max_outer = 30;
   p->precision = FUGU_FP64;
-  p->pcd_smoother = 0; p->pcd_sor_omega = 1.0; p->graphs = 0;
+  p->pcd_smoother = 0; p->pcd_sor_omega = 1.0; p->graphs = 0; p->pcd_visc_scale = 0.0;
 }
 
 const char* fugu_version(void) { return "fugu-b200 1 (sm_100a)"; }

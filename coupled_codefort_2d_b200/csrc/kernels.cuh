@@ -392,7 +392,7 @@ __global__ void k_poisson_coefs(Geo g, const double* rho_u, const double* rho_v,
 // Each PCD step is an element function plus a thin whole-box kernel around it.
 template <typename T>
 __device__ __forceinline__ T pcd_schur_at(const Geo& g, int k, int i, int j, const T* phi, const T* ua,
-                                          const T* va, T inv_dt) {
+                                          const T* va, T inv_dt, const T* kap, const T* zp, T visc) {
   T r = T(0);
   if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny) {
     const T h = T(0.5);
@@ -401,14 +401,17 @@ __device__ __forceinline__ T pcd_schur_at(const Geo& g, int k, int i, int j, con
     const T conv = uavg * (phi[g.at(i + 1, j)] - phi[g.at(i - 1, j)]) * (h * T(g.idx)) +
                    vavg * (phi[g.at(i, j + 1)] - phi[g.at(i, j - 1)]) * (h * T(g.idy));
     r = -(inv_dt * phi[k] + conv);
+    // extension (visc > 0): the viscous Cahouet-Chabard part, visc * mu_c * z_p
+    if (visc != T(0)) r = r - ((visc * T(0.5)) * kap[k]) * zp[k];
   }
   return r;
 }
 template <typename T>
-__global__ void k_pcd_schur(Geo g, const T* phi, const T* ua, const T* va, T* rp, T inv_dt, const int* active) {
+__global__ void k_pcd_schur(Geo g, const T* phi, const T* ua, const T* va, T* rp, T inv_dt, const T* kap,
+                            const T* zp, T visc, const int* active) {
   if (active && !*active) return;
   FUGU_BOX_IJ
-  rp[k] = pcd_schur_at<T>(g, k, i, j, phi, ua, va, inv_dt);
+  rp[k] = pcd_schur_at<T>(g, k, i, j, phi, ua, va, inv_dt, kap, zp, visc);
 }
 
 // velocity residual update z - B_p^T r_p (mod_pcd_precond.f90:66-84)

@@ -60,6 +60,9 @@ class Params:
     # 1: replay each flexible-GMRES Arnoldi step from a CUDA graph (execution
     # only; the results are the same)
     graphs: int = 0
+    # > 0: the PCD's Schur step adds the viscous (Cahouet-Chabard) term
+    # r_p -= pcd_visc_scale * mu_cell * z_p (0 = the reference's PCD)
+    pcd_visc_scale: float = 0.0
 
     def with_(self, **kw) -> "Params":
         return replace(self, **kw)

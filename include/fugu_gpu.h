@@ -103,6 +103,11 @@ typedef struct {
                                  = 2) is captured once as a CUDA graph and
                                  replayed (same kernels, same results); 0:
                                  launched kernel by kernel                   */
+  double pcd_visc_scale;      /* > 0: the PCD's Schur step adds the viscous
+                                 (Cahouet-Chabard) part of the Schur
+                                 complement, r_p -= pcd_visc_scale * mu_c *
+                                 z_p with mu_c = kappa / 2 at the cell; 0 =
+                                 the reference (mod_pcd_precond.f90:49-64)   */
 } fugu_params;
 
 /* Optional arguments of advance_coupled_step (src/mod_solver_coupled.f90:137-160):

@@ -77,7 +77,7 @@ void fo_model_defaults(fo_model* m) {
   m->pcg_tol = 1.0e-5; m->pcg_max_iter = 150; m->pcd_sweeps = 3;
   m->jacobi_omega = 0.8; m->svof_delta_h = 1.5; m->svof_max_iter = 150;
   m->svof_tol = 1.0e-7; m->limiter = 0; m->free_slip_x = 0;
-  m->pcd_smoother = 0; m->pcd_sor_omega = 1.0;
+  m->pcd_smoother = 0; m->pcd_sor_omega = 1.0; m->pcd_visc_scale = 0.0;
 }
 
 /* ---------------------------------------------------------------------- */
@@ -720,6 +720,8 @@ void fo_apply_pcd_precond(const fo_model* m, const double* z_u, const double* z_
       double conv = ua * (AC(phi, i + 1, j) - AC(phi, i - 1, j)) * (0.5 * idx) +
                     va * (AC(phi, i, j + 1) - AC(phi, i, j - 1)) * (0.5 * idy);
       AC(r_p, i, j) = -((1.0 / dt) * AC(phi, i, j) + conv);
+      /* extension: the viscous part of the Schur complement */
+      if (m->pcd_visc_scale != 0.0) AC(r_p, i, j) -= m->pcd_visc_scale * 0.5 * AC(kappa, i, j) * AC(z_p, i, j);
     }
   fo_halo_scalar(m, r_p);
 

@@ -80,6 +80,10 @@ typedef struct {
    * those with (i + j) odd, in place, refreshing the halo before each colour */
   int pcd_smoother;
   double pcd_sor_omega;
+  /* Schur-complement step of the PCD (extension): > 0 adds the viscous
+   * (Cahouet-Chabard) term, r_p -= pcd_visc_scale * mu_c * z_p with
+   * mu_c = kappa / 2 the cell viscosity; 0 = the reference */
+  double pcd_visc_scale;
 } fo_model;
 
 void fo_model_defaults(fo_model* m);

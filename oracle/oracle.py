@@ -33,6 +33,7 @@ class FoModel(C.Structure):
         ("krylov_bc_fix", C.c_int), ("refine", C.c_int), ("refine_inner_tol", C.c_double),
         ("refine_max_inner", C.c_int), ("refine_max_outer", C.c_int), ("pcg_cap_start", C.c_int),
         ("pcd_sweeps_max", C.c_int), ("pcd_smoother", C.c_int), ("pcd_sor_omega", C.c_double),
+        ("pcd_visc_scale", C.c_double),
     ]
 
 

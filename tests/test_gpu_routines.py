@@ -254,12 +254,14 @@ def test_poisson_pcg(gpu, oracle_mod, grid, zero_init, pcg_variant):
     exact(pg, po)
 
 
-@pytest.mark.parametrize("sweeps,penalty,smoother", [(3, False, 0), (4, True, 0), (3, True, 1)])
-def test_pcd_precond(gpu, oracle_mod, grid, pcg_variant, sweeps, penalty, smoother):
+@pytest.mark.parametrize("sweeps,penalty,smoother,visc", [(3, False, 0, 0.0), (4, True, 0, 0.0), (3, True, 1, 0.0),
+                                                         (3, False, 0, 1.0)])
+def test_pcd_precond(gpu, oracle_mod, grid, pcg_variant, sweeps, penalty, smoother, visc):
     """apply_pcd_precond: 3 sweeps (odd: the Jacobi result is copied back),
-    4 sweeps with the Darcy penalty diagonal, and 3 red-black SOR sweeps."""
+    4 sweeps with the Darcy penalty diagonal, 3 red-black SOR sweeps, and the
+    viscous (Cahouet-Chabard) term in the Schur step."""
     rng = np.random.default_rng(11)
-    prm = two_phase_params(pcd_sweeps=sweeps, pcd_smoother=smoother, pcd_sor_omega=1.5)
+    prm = two_phase_params(pcd_sweeps=sweeps, pcd_smoother=smoother, pcd_sor_omega=1.5, pcd_visc_scale=visc)
     o = oracle_mod.Oracle(grid, prm)
     c, pr = props(o, grid, rng, prm)
     z = [rfield(rng, grid, k) for k in ("u", "v", "cell")]

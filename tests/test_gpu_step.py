@@ -187,6 +187,21 @@ def test_mixed_precision_error_vs_fp64_oracle(gpu, oracle_mod, name, refine, smo
     assert abs(vg - vo) <= 1e-6 * abs(vo), (vg, vo)
 
 
+@pytest.mark.parametrize("name", ["droplet", "bubble_freeslip"])
+def test_pcd_viscous_term_fp64_parity(gpu, oracle_mod, name):
+    """The PCD with the viscous (Cahouet-Chabard) Schur term inside the FP64
+    defect correction around flexible GMRES, with the red-black SOR smoother
+    and CUDA graphs: the oracle's iteration counts and bits."""
+    over = dict(refine=2, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=30, krylov_bc_fix=1,
+                tol_bicgstab2=1e-9, pcg_cap_start=4, pcd_smoother=1, pcd_sor_omega=1.5, pcd_visc_scale=1.0, graphs=1)
+    g, st_o, st_g, hist = run_pair(oracle_mod, name, over)
+    for so, sg in hist:
+        assert sg["res"] < 1e-9 and so.res < 1e-9
+        assert sg["outer"] == so.outer and sg["iter"] == so.iter
+    for k in STATE:
+        np.testing.assert_array_equal(st_g[k], st_o[k], err_msg=k)
+
+
 def _device_run(name, over, precision, prof):
     """the case's steps on the GPU alone (device-resident state); returns the
     final state, per-step stats and the launch / PCG profile counters"""
