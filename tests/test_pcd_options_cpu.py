@@ -33,3 +33,30 @@ def test_viscous_schur_term_cuts_arnoldi_steps_on_a_hard_bubble(oracle_mod):
     ref = _arnoldi_steps(oracle_mod, spec, 0.0)
     cc = _arnoldi_steps(oracle_mod, spec, 1.0)
     assert cc[1] * 1.5 < ref[1], (ref, cc)  # 36 -> 17 Arnoldi steps in the second step
+
+
+def test_viscous_schur_term_is_the_stated_formula(oracle_mod):
+    """r_p with the term equals r_p without it minus (s * 0.5 * kappa) * z_p,
+    cell by cell on the interior, bit for bit (the rest of r_p is unchanged)."""
+    import numpy as np
+
+    from conftest import colour, rfield, two_phase_params
+    from coupled_codefort_2d_b200.layout import Grid
+
+    g = Grid(13, 9, 1.0, 0.7)
+    out = {}
+    for s in (0.0, 1.0):
+        rng = np.random.default_rng(31)
+        prm = two_phase_params(pcd_visc_scale=s)
+        o = oracle_mod.Oracle(g, prm)
+        pr = o.properties(colour(rng, g))
+        z = [rfield(rng, g, k) for k in ("u", "v", "cell")]
+        ua, va = rfield(rng, g, "u"), rfield(rng, g, "v")
+        r = [g.zeros(k) for k in ("u", "v", "cell")]
+        o.pcd(*z, *r, ua, va, pr, 2e-3)
+        out[s] = (r[2], z[2], pr["kappa"])
+    rp0, zp, kap = out[0.0]
+    rp1 = out[1.0][0]
+    inner = (slice(2, g.nx + 2), slice(2, g.ny + 2))  # cells 1..nx, 1..ny of the (1-nh) layout
+    expect = rp0[inner] - ((1.0 * 0.5) * kap[inner]) * zp[inner]
+    np.testing.assert_array_equal(rp1[inner], expect)
