@@ -47,3 +47,6 @@ def test_measured_forms_solver_settings():
         (2, 1, 40, 6, 24)
     assert mixed.tol_bicgstab2 == bench.TOL == 1e-8
     assert mixed.pcd_smoother == 0  # the bench keeps the reference's damped Jacobi
+    assert mixed.pcd_visc_scale == 0.0  # the headline keeps the reference's PCD
+    v = bench.viscous_params(mixed)  # the secondary arm
+    assert (v.pcd_visc_scale, v.pcg_cap_start, v.refine, v.graphs, v.tol_bicgstab2) == (1.0, 80, 2, 1, 1e-8)
