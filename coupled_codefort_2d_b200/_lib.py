@@ -128,6 +128,7 @@ SIGNATURES = {
     "fugu_matvec_coupled_t": (_i, [_vp] * 15 + [_d] + [_vp] * 4),
     "fugu_adjoint_solve": (_i, [_vp] * 15 + [_d, _d] + [_vp] * 5),
     "fugu_step_vjp": (_i, [_vp, _d, _i, _vp] + [_vp] * 12),
+    "fugu_test_arm_barrier_timeout": (_i, [_vp, C.c_uint]),
 }
 
 

@@ -102,6 +102,13 @@ class Context:
         self._ck(self.L.fugu_profile(self.h, int(enable), C.byref(out)))
         return out.as_dict()
 
+    def arm_barrier_timeout(self, spin_limit: int = 1000):
+        """Failure-detection test hook: the next grid-wide PCG launch of this
+        context waits for one CTA too many at its grid barriers and gives up
+        after ``spin_limit`` polls, so the call that made it raises
+        FUGU_ETIMEOUT (``fugu_test_arm_barrier_timeout``)."""
+        self._ck(self.L.fugu_test_arm_barrier_timeout(self.h, int(spin_limit)))
+
     def _f(self, a, kind):
         return ptr(as_fortran(a, self.g, kind))
 

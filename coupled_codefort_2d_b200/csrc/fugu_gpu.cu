@@ -196,6 +196,9 @@ struct fugu_ctx {
   int svof_grid = 0;
   int dot_grid = 0;
   // limits for concurrent use (a batch lowers them so many cases fit at once)
+  // failure-detection test hook: > 0 arms the next grid-wide PCG launch to
+  // wait for one CTA too many and give up after this many polls
+  unsigned int test_spin_limit = 0;
   int max_cluster = 16;  // CTAs of the cluster-resident PCG
   int max_coop = 1 << 30;  // CTAs of a grid-wide cooperative kernel
   bool coop_as_cluster = false;  // launch those as one cluster (max_coop <= 8)
@@ -546,7 +549,7 @@ void prof_drain(fugu_ctx* c) {
 template <typename T>
 void pcg(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, double tol, int max_iter, bool phi_zero,
          const int* active) {
-  PcgArgs<T> a;
+  PcgArgs<T> a{};
   a.g = c->g;
   a.rhs = rhs; a.cx = w.cx; a.cy = w.cy; a.dinv = w.dinv;
   a.phi = phi; a.r = w.r; a.z = w.z; a.pb0 = w.pb0; a.pb1 = w.pb1; a.ap = w.ap;
@@ -571,7 +574,15 @@ void pcg(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, double tol, int max_i
       CK(cudaEventRecord(e0, c->s));
     }
   }
-  if (cp.ok) {
+  // an armed failure-detection test takes the grid-wide kernel (the one with
+  // software waits) for this launch only; never inside a capture
+  const bool armed = c->test_spin_limit > 0 && !c->capturing;
+  if (armed) {
+    a.spin_limit = c->test_spin_limit;
+    a.extra_arrivals = 1;
+    c->test_spin_limit = 0;
+  }
+  if (cp.ok && !armed) {
     PcgClusterArgs<T> ca;
     ca.g = c->g;
     ca.rhs = rhs; ca.cx = w.cx; ca.cy = w.cy; ca.dinv = w.dinv; ca.phi = phi;
@@ -2839,14 +2850,37 @@ static_assert(sizeof(GridSync) <= 16 * sizeof(double) && sizeof(PcgOut) <= 16 * 
 
 static __device__ __align__(256) double na_scratch[NA_TOTAL];
 
-// per-device set-up, done by the first call with that device current
+// Per-device set-up, done by the first call with that device current and
+// redone whenever the device's current CUDA context has changed since (after
+// cudaDeviceReset the library's module, and with it na_scratch, is loaded
+// again, possibly at another address).
 struct NaDevice {
   bool ready = false;
-  double* base = nullptr;  // device address of na_scratch in this device's context
+  void* cu_ctx = nullptr;  // the CUDA context the address below belongs to
+  double* base = nullptr;  // device address of na_scratch in that context
   int max_ctas = 0;        // co-resident CTAs of k_pcg<double>, one per SM at most
 };
 std::mutex na_mu;
 NaDevice na_dev[NA_MAX_DEVICES];
+// failure-detection test hook for this entry (fugu_test_arm_barrier_timeout
+// with a NULL context): > 0 arms the next call's PCG launch
+std::atomic<unsigned int> na_test_spin_limit{0};
+
+// the calling thread's current CUDA context (driver cuCtxGetCurrent, found
+// through the runtime so the library does not link the driver library)
+cudaError_t na_current_context(void** out) {
+  using GetCurrent = int (*)(void**);
+  static GetCurrent fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return e;
+    if (q != cudaDriverEntryPointSuccess || !f) return cudaErrorSymbolNotFound;
+    fn = (GetCurrent)f;
+  }
+  return fn(out) == 0 ? cudaSuccess : cudaErrorDeviceUninitialized;
+}
 
 // message into the caller's buffer (no heap use on any path of the entry)
 int na_fail(char* err, int err_len, int code, const char* what, const char* detail = "") {
@@ -2877,11 +2911,22 @@ extern "C" int fugu_solve_poisson_pressure_noalloc(const fugu_params* p, void* s
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return na_fail(err, err_len, FUGU_ECUDA, "cudaGetDevice: ", cudaGetErrorString(e));
   if (dev < 0 || dev >= NA_MAX_DEVICES) return na_fail(err, err_len, FUGU_EINVAL, "device ordinal out of range");
+  void* cu_ctx = nullptr;
+  e = na_current_context(&cu_ctx);
+  if (e == cudaSuccess && !cu_ctx) {
+    // no context is current yet: cudaSetDevice makes the device's primary
+    // context current (it allocates no device memory)
+    e = cudaSetDevice(dev);
+    if (e == cudaSuccess) e = na_current_context(&cu_ctx);
+  }
+  if (e == cudaSuccess && !cu_ctx) e = cudaErrorDeviceUninitialized;
+  if (e != cudaSuccess) return na_fail(err, err_len, FUGU_ECUDA, "current CUDA context: ", cudaGetErrorString(e));
   NaDevice d;
   {
     std::lock_guard<std::mutex> lk(na_mu);
     NaDevice& nd = na_dev[dev];
-    if (!nd.ready) {
+    if (!nd.ready || nd.cu_ctx != cu_ctx) {
+      nd.ready = false;
       double* ptr = nullptr;
       e = cudaGetSymbolAddress((void**)&ptr, na_scratch);
       if (e != cudaSuccess)
@@ -2892,6 +2937,7 @@ extern "C" int fugu_solve_poisson_pressure_noalloc(const fugu_params* p, void* s
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, (const void*)k_pcg<double>, PCG_TPB, 0);
       if (e != cudaSuccess || nsm < 1 || occ < 1)
         return na_fail(err, err_len, FUGU_ECUDA, "no co-resident grid for the PCG kernel on this device");
+      nd.cu_ctx = cu_ctx;
       nd.base = ptr;
       nd.max_ctas = nsm < NA_MAX_CTAS ? nsm : NA_MAX_CTAS;
       nd.ready = true;
@@ -2927,24 +2973,43 @@ extern "C" int fugu_solve_poisson_pressure_noalloc(const fugu_params* p, void* s
   k_poisson_coefs<double><<<b.grid, b.block, 0, s>>>(g, f[2], f[3], f[4], f[5], f[6]);
   e = cudaGetLastError();
   if (e != cudaSuccess) return na_fail(err, err_len, FUGU_ECUDA, "k_poisson_coefs: ", cudaGetErrorString(e));
-  PcgArgs<double> a;
+  PcgArgs<double> a{};
   a.g = g;
   a.rhs = f[1]; a.cx = f[4]; a.cy = f[5]; a.dinv = f[6];
   a.phi = f[0]; a.r = f[7]; a.z = f[8]; a.pb0 = f[9]; a.pb1 = f[10]; a.ap = f[11];
   a.part = part; a.gs = gs; a.out = out; a.active = nullptr;
   a.tol = tol; a.max_iter = max_iter; a.phi_zero = 0; a.timed = 0;
+  const unsigned int test_lim = na_test_spin_limit.exchange(0u);
+  if (test_lim > 0) {
+    a.spin_limit = test_lim;
+    a.extra_arrivals = 1;
+  }
   long want = ((long)p->nx * p->ny + PCG_TPB - 1) / PCG_TPB;
   const int grid = (int)(want < d.max_ctas ? (want < 1 ? 1 : want) : d.max_ctas);
   void* args[] = {&a};
   e = cudaLaunchCooperativeKernel((void*)k_pcg<double>, dim3(grid), dim3(PCG_TPB), args, 0, s);
   if (e != cudaSuccess) return na_fail(err, err_len, FUGU_ECUDA, "k_pcg: ", cudaGetErrorString(e));
   e = copy(nullptr, nullptr, phi, f[0], K_CELL);
-  PcgOut h{};
-  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, out, sizeof(PcgOut), cudaMemcpyDeviceToHost, s);
+  // the barrier record and the result record (one 256-byte header) together
+  double hdr[NA_PART];
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hdr, d.base, sizeof hdr, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return na_fail(err, err_len, FUGU_ECUDA, "copy out: ", cudaGetErrorString(e));
-  if (h.status != 0) return na_fail(err, err_len, FUGU_ETIMEOUT, "k_pcg: a grid barrier wait gave up");
+  GridSync hg;
+  PcgOut h;
+  std::memcpy(&hg, hdr, sizeof hg);
+  std::memcpy(&h, hdr + 16, sizeof h);
+  if (hg.error != 0 || h.status != 0)
+    return na_fail(err, err_len, FUGU_ETIMEOUT,
+                   "k_pcg: a grid barrier wait gave up; phi holds a partial result");
   if (iter_out) *iter_out = h.iters;
   if (res_out) *res_out = h.res;
+  return FUGU_OK;
+}
+
+extern "C" int fugu_test_arm_barrier_timeout(fugu_ctx* ctx, unsigned int spin_limit) {
+  if (spin_limit == 0) return FUGU_EINVAL;
+  if (ctx) ctx->test_spin_limit = spin_limit;
+  else na_test_spin_limit.store(spin_limit);
   return FUGU_OK;
 }

@@ -83,8 +83,12 @@ __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
   return v;
 }
 
-// Returns true when every CTA arrived; false on timeout / error.
-__device__ __forceinline__ bool grid_sync(GridSync* gs, unsigned int nblocks, unsigned int& gen) {
+// Returns true when every CTA arrived; false on timeout / error.  nblocks is
+// the arrival count the barrier waits for (gridDim.x, or one more in the
+// failure-detection test, which makes every wait run out); spin_limit bounds
+// each wait in polls.
+__device__ __forceinline__ bool grid_sync(GridSync* gs, unsigned int nblocks, unsigned int& gen,
+                                          unsigned int spin_limit = FUGU_SPIN_LIMIT) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -99,7 +103,7 @@ __device__ __forceinline__ bool grid_sync(GridSync* gs, unsigned int nblocks, un
     } else {
       unsigned int spins = 0;
       while (ld_acquire_u32(&gs->gen) == my) {
-        if (++spins > FUGU_SPIN_LIMIT || ld_relaxed_i32(&gs->error) != 0) {
+        if (++spins > spin_limit || ld_relaxed_i32(&gs->error) != 0) {
           atomicExch(&gs->error, 1);
           ok = 0;
           break;

@@ -39,26 +39,38 @@ struct PcgArgs {
   int max_iter;
   int phi_zero;        // phi is identically zero on entry (preconditioner use)
   int timed;           // the launch is timed: add its iterations to out->timed_iters
+  // failure-detection test: each grid barrier waits for gridDim.x +
+  // extra_arrivals CTAs (1 makes every wait run out) and gives up after
+  // spin_limit polls (0: FUGU_SPIN_LIMIT).  Both 0 in normal use.
+  unsigned int spin_limit;
+  int extra_arrivals;
+};
+
+// the arrival count and poll limit of one grid-wide launch's barriers
+struct Barrier {
+  GridSync* gs;
+  unsigned int nb;
+  unsigned int lim;
+  unsigned int gen;
 };
 
 // Grid-wide order-independent sum of one (or two) DD values per thread: CTA
 // partials, one bounded grid barrier, then every CTA sums the partials in
 // the same order.  Returns false when the barrier gave up.
-__device__ __forceinline__ bool grid_allreduce(GridSync* gs, unsigned int& gen, double* part, DD v, DD* sh,
-                                               double& out) {
+__device__ __forceinline__ bool grid_allreduce(Barrier& bar, double* part, DD v, DD* sh, double& out) {
   v = block_sum_dd(v, sh);
   if (threadIdx.x == 0) put_partial(part, blockIdx.x, v);
-  if (!grid_sync(gs, gridDim.x, gen)) return false;
+  if (!grid_sync(bar.gs, bar.nb, bar.gen, bar.lim)) return false;
   out = sum_partials_dd(part, gridDim.x);
   return true;
 }
-__device__ __forceinline__ bool grid_allreduce2(GridSync* gs, unsigned int& gen, double* pa, double* pb, DD a,
-                                                DD b, DD* sh, double& oa, double& ob) {
+__device__ __forceinline__ bool grid_allreduce2(Barrier& bar, double* pa, double* pb, DD a, DD b, DD* sh,
+                                                double& oa, double& ob) {
   a = block_sum_dd(a, sh);
   if (threadIdx.x == 0) put_partial(pa, blockIdx.x, a);
   b = block_sum_dd(b, sh);
   if (threadIdx.x == 0) put_partial(pb, blockIdx.x, b);
-  if (!grid_sync(gs, gridDim.x, gen)) return false;
+  if (!grid_sync(bar.gs, bar.nb, bar.gen, bar.lim)) return false;
   oa = sum_partials_dd(pa, gridDim.x);
   ob = sum_partials_dd(pb, gridDim.x);
   return true;
@@ -88,7 +100,12 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
   const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long nthr = (long)G * blockDim.x;
   const bool closed = !g.px && !g.py;
-  unsigned int gen = 0;
+  Barrier bar{a.gs, (unsigned int)(G + a.extra_arrivals), a.spin_limit ? a.spin_limit : FUGU_SPIN_LIMIT, 0u};
+  // a barrier that gave up: record it in the result (the host reads it as
+  // FUGU_ETIMEOUT) and unwind; every CTA writes the same value
+  auto gave_up = [&]() {
+    if (threadIdx.x == 0) a.out->status = 1;
+  };
   double* P0 = a.part;           // setup sum / final mean
   double* P1 = a.part + 2 * G;   // rhs norm
   double* P2 = a.part + 4 * G;   // initial r.z
@@ -104,7 +121,7 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
     DD s{0.0, 0.0};
     CELL_LOOP { CELL_IJ dd_add(s, double(a.rhs[c])); }
     double tot;
-    if (!grid_allreduce(a.gs, gen, P0, s, sh, tot)) return;
+    if (!grid_allreduce(bar, P0, s, sh, tot)) { gave_up(); return; }
     mean = tot / (double)(g.nx * g.ny);
   }
   DD ss{0.0, 0.0};
@@ -115,7 +132,7 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
     dd_add(ss, double(rw) * double(rw));
   }
   double ssum;
-  if (!grid_allreduce(a.gs, gen, P1, ss, sh, ssum)) return;
+  if (!grid_allreduce(bar, P1, ss, sh, ssum)) { gave_up(); return; }
   const double rhs_norm = sqrt(ssum);
   if (rhs_norm < 1.0e-14) {
     for (long q = tid; q < g.n(); q += nthr) a.phi[q] = T(0);
@@ -153,7 +170,7 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
     dd_add(rz, double(rr) * double(zz));
   }
   double rz_old;
-  if (!grid_allreduce(a.gs, gen, P2, rz, sh, rz_old)) return;
+  if (!grid_allreduce(bar, P2, rz, sh, rz_old)) { gave_up(); return; }
 
   // (d) PCG iterations; the direction update p = z + beta p of iteration k-1
   // is evaluated where iteration k needs it (own cell and stencil
@@ -186,7 +203,7 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
       dd_add(papd, double(pown) * double(apv));
     }
     double pap;
-    if (!grid_allreduce(a.gs, gen, PA, papd, sh, pap)) return;
+    if (!grid_allreduce(bar, PA, papd, sh, pap)) { gave_up(); return; }
     if (fabs(pap) < 1.0e-30) break;
     const double alpha = rz_old / pap;
     const T ta = T(alpha);
@@ -203,7 +220,7 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
       dd_add(rzd, double(rv) * double(zv));
     }
     double rr, rz_new;
-    if (!grid_allreduce2(a.gs, gen, PB, PC, rrd, rzd, sh, rr, rz_new)) return;
+    if (!grid_allreduce2(bar, PB, PC, rrd, rzd, sh, rr, rz_new)) { gave_up(); return; }
     res_norm = sqrt(rr);
     if (res_norm / rhs_norm < a.tol) break;
     beta = rz_new / rz_old;
@@ -213,7 +230,7 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
     DD s{0.0, 0.0};
     CELL_LOOP { CELL_IJ dd_add(s, double(a.phi[c])); }
     double tot;
-    if (!grid_allreduce(a.gs, gen, P0, s, sh, tot)) return;
+    if (!grid_allreduce(bar, P0, s, sh, tot)) { gave_up(); return; }
     const double m = tot / (double)(g.nx * g.ny);
     CELL_LOOP { CELL_IJ a.phi[c] = T(double(a.phi[c]) - m); }
   }

@@ -25,11 +25,13 @@ from . import cases
 # flexible GMRES(30) inside the FP64 defect correction; the PCD's PCG cap
 # adapts from 40 and its velocity smoothing from 6 sweeps of red-black SOR
 # (omega 1.5), which on the hard high-density-ratio cases needs fewer Arnoldi
-# steps than the reference's damped Jacobi at four times the sweeps; every
-# Arnoldi step is replayed from a CUDA graph (one launch per step)
+# steps than the reference's damped Jacobi at four times the sweeps; the
+# PCD's Schur step carries the viscous (Cahouet-Chabard) term, which the
+# viscous-dominated bubbles need most; every Arnoldi step is replayed from a
+# CUDA graph (one launch per step)
 SOLVER = dict(tol_bicgstab2=1e-8, max_iter_bicgstab2=500, refine=2, refine_inner_tol=1e-2, refine_max_inner=30,
               refine_max_outer=60, krylov_bc_fix=1, pcg_cap_start=40, pcd_sweeps=6, pcd_sweeps_max=24,
-              pcd_smoother=1, pcd_sor_omega=1.5, graphs=1)
+              pcd_smoother=1, pcd_sor_omega=1.5, graphs=1, pcd_visc_scale=1.0)
 DT = 5e-4
 
 

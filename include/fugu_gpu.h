@@ -417,7 +417,13 @@ int fugu_batch_run(fugu_batch* b, int nsteps, const double* dt, const int* step0
  * grids are rejected with FUGU_EINVAL.
  * Set-up: the first call on a device, with that device current, takes the
  * static array's device address (cudaGetSymbolAddress) and queries the
- * device.  Make that first call before any stream capture.
+ * device; a later call redoes this when the device's current CUDA context
+ * is no longer the one the address was taken in (after cudaDeviceReset).
+ * Blocking: every call waits on `stream` (cudaStreamSynchronize) to read the
+ * solve's result, so no call can be made while `stream` is being captured
+ * into a CUDA graph.
+ * A grid-barrier wait that gives up (see fugu_test_arm_barrier_timeout)
+ * returns FUGU_ETIMEOUT with a message; phi then holds a partial result.
  * Zero state: the grid-barrier counters, the result record and the fields
  * must start at zero.  Every call clears them on `stream` before its
  * kernels run.
@@ -430,6 +436,19 @@ int fugu_solve_poisson_pressure_noalloc(const fugu_params* p, void* stream, doub
                                         const double* rhs, const double* rho_u, const double* rho_v,
                                         double tol, int max_iter, int* iter_out, double* res_out,
                                         char* err, int err_len);
+
+/* ------------------------------------------------ failure-detection test hook
+ * No counterpart in the reference, which has no device-side waits.  Arms the
+ * next launch of the grid-wide persistent PCG kernel -- in ctx, or, with ctx
+ * NULL, in the next fugu_solve_poisson_pressure_noalloc call of the process
+ * -- so that each of its grid barriers waits for one CTA more than the launch
+ * has and gives up after spin_limit polls (>= 1; about 40 ns each).  The
+ * kernel then ends early, and the entry that made the launch returns
+ * FUGU_ETIMEOUT with a message; the context stays usable.  In ctx, the armed
+ * launch takes the grid-wide kernel even where the cluster-resident one
+ * would run, and a launch inside a CUDA-graph capture is never armed.
+ * One-shot: later launches run normally. */
+int fugu_test_arm_barrier_timeout(fugu_ctx* ctx, unsigned int spin_limit);
 
 #ifdef __cplusplus
 }

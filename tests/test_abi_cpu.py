@@ -126,20 +126,67 @@ def test_layout_shapes_match_fortran_bounds():
     np.testing.assert_array_equal(at(a, "u", slice(0, 7), 3).shape, (8,))
 
 
-@pytest.mark.parametrize("cname", ["fugu_params", "fugu_step_opts", "fugu_stats"])
-def test_fortran_binding_matches_header_layout(cname):
-    """The bind(C) types of the Fortran interface module shown in
-    INTEGRATION.md declare the C structs' fields in the same order."""
+FORTRAN = os.path.join(ROOT, "fortran", "mod_fugu_gpu.f90")
+PATCH = os.path.join(ROOT, "fortran", "use_gpu.patch")
+
+
+def header_struct_fields(cname):
     src = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
     body = re.search(r"typedef struct \{([^}]*)\}\s*" + cname + ";", src).group(1)
     c_names = []
     for decl in body.split(";"):
         toks = decl.replace(",", " , ").split()
         c_names += [t for t in toks[1:] if t not in (",", "long", "double", "int")]
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    ftype = re.search(r"type, bind\(C\) :: " + cname + r"\n(.*?)end type", doc, flags=re.S).group(1)
+    return c_names
+
+
+def fortran_source():
+    """mod_fugu_gpu.f90 without comments, continuation lines joined"""
+    lines = [ln.split("!", 1)[0].rstrip() for ln in open(FORTRAN).read().splitlines()]
+    return re.sub(r"&\s*\n\s*", " ", "\n".join(lines))
+
+
+@pytest.mark.parametrize("cname", ["fugu_params", "fugu_step_opts", "fugu_stats"])
+def test_fortran_binding_matches_header_layout(cname):
+    """The bind(C) types of the Fortran bridge module fortran/mod_fugu_gpu.f90
+    declare the C structs' fields in the same order."""
+    ftype = re.search(r"type, bind\(C\) :: " + cname + r"\n(.*?)end type", fortran_source(), flags=re.S).group(1)
     f_names = []
-    for line in ftype.replace("&\n", " ").splitlines():
+    for line in ftype.splitlines():
         if "::" in line:
             f_names += [n.strip() for n in line.split("::", 1)[1].split(",") if n.strip()]
-    assert f_names == c_names
+    assert f_names == header_struct_fields(cname)
+
+
+def test_fortran_interfaces_bind_header_entries():
+    """Every bind(C) procedure of the bridge names an entry of the header and
+    takes as many arguments as the C declaration."""
+    src = fortran_source()
+    hdr = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    binds = re.findall(r"(?:function|subroutine)\s+(\w+)\s*\(([^)]*)\)\s*bind\(C,\s*name=\"(\w+)\"\)", src)
+    assert {b[2] for b in binds} >= {"fugu_create", "fugu_advance_coupled_step", "fugu_destroy", "fugu_last_error"}
+    for fname, args, cname in binds:
+        assert fname == cname
+        decl = re.search(r"\b" + cname + r"\s*\(([^)]*)\)\s*;", hdr, flags=re.S)
+        assert decl, cname
+        c_args = [a for a in decl.group(1).split(",") if a.strip() and a.strip() != "void"]
+        f_args = [a for a in args.split(",") if a.strip()]
+        assert len(f_args) == len(c_args), (cname, f_args, c_args)
+
+
+def test_use_gpu_patch_only_adds_lines():
+    """The patch that wires the bridge into the reference adds lines at stated
+    positions and changes none of the reference's own."""
+    hunks = 0
+    files = set()
+    for ln in open(PATCH).read().splitlines():
+        if ln.startswith("+++ b/"):
+            files.add(ln[6:])
+        elif ln.startswith("@@"):
+            m = re.match(r"@@ -(\d+),0 \+(\d+)(?:,(\d+))? @@$", ln)
+            assert m, ln
+            hunks += 1
+        elif files and ln and ln[0] == "-" and not ln.startswith("--- a/"):
+            raise AssertionError("removes a reference line: " + ln)
+    assert files == {"src/main.f90", "src/mod_solver_coupled.f90", "Makefile"}
+    assert hunks == 7

@@ -15,7 +15,7 @@ def test_roofline_uses_the_timed_launches():
     # all launches together ran 2240 iterations
     prof = {"pcg_launches": 4, "pcg_ms": 0.8, "pcg_iters": 2240, "pcg_iters_timed": 160, "pcg_cells": 65536}
     r = bench.roofline(prof, {"hbm_gbs": 7000.0})
-    bytes_per_launch = 11 * 4 * 65536 * 40
+    bytes_per_launch = 9 * 4 * 65536 * 40  # the fused PCG iteration's 9 values per cell
     assert r["bytes_per_launch"] == bytes_per_launch
     assert abs(r["ms_per_launch"] - 0.2) < 1e-12
     assert abs(r["achieved"] - bytes_per_launch / 0.2e-3 / 1e9) < 1e-9
@@ -44,9 +44,11 @@ def test_clock_summary_flags_throttle_reasons():
 def test_measured_forms_solver_settings():
     mixed = bench.case_params(2)
     assert (mixed.refine, mixed.graphs, mixed.pcg_cap_start, mixed.pcd_sweeps, mixed.pcd_sweeps_max) == \
-        (2, 1, 40, 6, 24)
+        (2, 1, 80, 6, 24)
     assert mixed.tol_bicgstab2 == bench.TOL == 1e-8
     assert mixed.pcd_smoother == 0  # the bench keeps the reference's damped Jacobi
-    assert mixed.pcd_visc_scale == 0.0  # the headline keeps the reference's PCD
-    v = bench.viscous_params(mixed)  # the secondary arm
-    assert (v.pcd_visc_scale, v.pcg_cap_start, v.refine, v.graphs, v.tol_bicgstab2) == (1.0, 80, 2, 1, 1e-8)
+    assert mixed.pcd_visc_scale == 1.0  # the headline carries the viscous Schur term
+    r = bench.reference_pcd_params(mixed)  # the arm with the reference's PCD
+    assert (r.pcd_visc_scale, r.pcg_cap_start, r.refine, r.graphs, r.tol_bicgstab2) == (0.0, 40, 2, 1, 1e-8)
+    b2 = bench.case_params(1)  # BiCGStab(2) inner solve: the reference's fixed PCD
+    assert (b2.pcd_visc_scale, b2.pcg_cap_start, b2.pcd_sweeps) == (0.0, 0, 3)

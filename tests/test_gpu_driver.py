@@ -3,6 +3,8 @@ shape (rising bubble, adaptive dt, AMP, BiCGStab, VTK and checkpoint output)
 runs the time loop of main.f90:193-248, and the state it checkpoints is the
 oracle's, bit for bit, after the same loop on the CPU (adaptive dt from
 compute_adaptive_dt, mod_solver_coupled.f90:41-91, then advance_coupled_step).
+The VTK file of the same step holds the oracle's fields, value for value, in
+the layout of write_vtk_fields (mod_io.f90:29-164).
 """
 import subprocess
 
@@ -46,7 +48,6 @@ def test_driver_run_matches_oracle_loop(gpu, oracle_mod, driver, tmp_path):
     for name in ("fugu2d_0000.vtk", "fugu2d_0002.vtk", "fugu2d_0004.vtk", "chk_fugu2d_r0000.bin"):
         assert (tmp_path / "output" / name).exists(), name
     vtk = (tmp_path / "output" / "fugu2d_0004.vtk").read_text()
-    assert vtk.startswith("# vtk DataFile Version") and "DIMENSIONS" in vtk
 
     g = Grid(16, 32, 1.0, 2.0)
     p = Params(rho1=1000.0, rho2=100.0, mu1=10.0, mu2=1.0, sigma=24.5, gx=0.0, gy=-0.98, cfl_target=0.25,
@@ -65,6 +66,41 @@ def test_driver_run_matches_oracle_loop(gpu, oracle_mod, driver, tmp_path):
     assert t_chk == t
     for k in ("u_vel", "v_vel", "u_prev", "v_prev", "p_field", "c_field"):
         np.testing.assert_array_equal(chk[k], st[k], err_msg=k)
+    check_vtk(vtk, g, st)
+
+
+def fmt(x):
+    """the ES15.7 edit descriptor of mod_io.f90:117-152 (C's %15.7E)"""
+    return "%15.7E" % x
+
+
+def check_vtk(text, g, st):
+    """The VTK file of mod_io.f90:106-156 written from the oracle's state:
+    header, the four cell scalars in i-fastest order, and the cell-centred
+    velocity half*(u(i-1,j)+u(i,j)), half*(v(i,j-1)+v(i,j)) (mod_io.f90:47-52),
+    every value as the same 15-character field."""
+    lines = text.splitlines()
+    nx, ny = g.nx, g.ny
+    assert lines[:4] == ["# vtk DataFile Version 3.0", "FUGU-2D Coupled Two-Phase Solver Output", "ASCII",
+                         "DATASET STRUCTURED_POINTS"]
+    assert lines[4] == "DIMENSIONS " + "%8d%8d%8d" % (nx, ny, 1)
+    assert lines[5] == "ORIGIN " + fmt(0.5 * g.dx) + fmt(0.5 * g.dy) + fmt(0.0)
+    assert lines[6] == "SPACING " + fmt(g.dx) + fmt(g.dy) + fmt(g.dx)
+    assert lines[7] == "POINT_DATA %10d" % (nx * ny)
+    at = 8
+    cell = lambda a, i, j: a[i + 1, j + 1]  # cell (i, j) of a (1-nh:nx+nh, 1-nh:ny+nh) array
+    for name, key in (("VOF_C", "c_field"), ("Pressure", "p_field"), ("Density", "rho_c"),
+                      ("Curvature", "kappa_curv")):
+        assert lines[at:at + 2] == ["SCALARS %s double 1" % name, "LOOKUP_TABLE default"], name
+        want = [fmt(cell(st[key], i, j)) for j in range(1, ny + 1) for i in range(1, nx + 1)]
+        assert lines[at + 2:at + 2 + nx * ny] == want, name
+        at += 2 + nx * ny
+    assert lines[at] == "VECTORS Velocity double"
+    u, v = st["u_vel"], st["v_vel"]  # u (0-nh:nx+nh, 1-nh:ny+nh), v (1-nh:nx+nh, 0-nh:ny+nh)
+    want = [fmt(0.5 * (u[i + 1, j + 1] + u[i + 2, j + 1])) + fmt(0.5 * (v[i + 1, j + 1] + v[i + 1, j + 2])) + fmt(0.0)
+            for j in range(1, ny + 1) for i in range(1, nx + 1)]
+    assert lines[at + 1:at + 1 + nx * ny] == want
+    assert len(lines) == at + 1 + nx * ny
 
 
 def test_driver_restart_continues_the_run(gpu, driver, tmp_path):
