@@ -122,9 +122,9 @@ __host__ __device__ inline long mdot_items(const Geo& g) {
   return (long)g.ny * cu + (long)g.jmax() * cv + (long)g.ny * cv;
 }
 
+// CTA (bx, by) of a (Gx, Gy = nvec) grid
 template <typename T>
-__global__ void __launch_bounds__(MDOT_TPB) k_mdot(MdotArgs<T> a) {
-  if (!a.ks->active) return;
+__device__ __forceinline__ void mdot_body(const MdotArgs<T>& a, int bx, int by, int Gx, int Gy) {
   constexpr int NW = MDOT_TPB / 32;
   __shared__ DD wsum[NW];
   __shared__ double dsum[MDOT_MAXV];
@@ -135,9 +135,9 @@ __global__ void __launch_bounds__(MDOT_TPB) k_mdot(MdotArgs<T> a) {
   const int cu = (imax + MDOT_CHUNK - 1) / MDOT_CHUNK, cv = (nx + MDOT_CHUNK - 1) / MDOT_CHUNK;
   const long iu = (long)ny * cu, iv = (long)jmax * cv, ip = (long)ny * cv;
   const long items = iu + iv + ip;
-  const T* V = a.V0 + blockIdx.y * a.stride;  // this grid row's vector
+  const T* V = a.V0 + by * a.stride;  // this grid row's vector
   DD acc{0.0, 0.0};
-  for (long it = (long)blockIdx.x * NW + warp; it < items; it += (long)gridDim.x * NW) {
+  for (long it = (long)bx * NW + warp; it < items; it += (long)Gx * NW) {
     long base;
     int len, c;
     if (it < iu) {
@@ -181,18 +181,18 @@ __global__ void __launch_bounds__(MDOT_TPB) k_mdot(MdotArgs<T> a) {
   if (threadIdx.x == 0) {
     DD s = wsum[0];
     for (int k = 1; k < NW; ++k) s = dd_merge(s, wsum[k]);
-    put_partial(a.part + 2L * blockIdx.y * gridDim.x, blockIdx.x, s);
+    put_partial(a.part + 2L * by * Gx, bx, s);
     __threadfence();
     const unsigned int t = atomicAdd(&a.ks->ticket, 1u);
-    last = (t == gridDim.x * gridDim.y - 1);
+    last = (t == (unsigned int)(Gx * Gy) - 1);
   }
   __syncthreads();
   if (!last) return;
   __threadfence();
   for (int v = warp; v < a.nvec; v += NW) {
-    const double* pv = a.part + 2L * v * gridDim.x;
+    const double* pv = a.part + 2L * v * Gx;
     DD s{0.0, 0.0};
-    for (int k = lane; k < (int)gridDim.x; k += 32) {
+    for (int k = lane; k < Gx; k += 32) {
       DD q;
       q.hi = __ldcg(pv + 2 * k);
       q.lo = __ldcg(pv + 2 * k + 1);
@@ -207,32 +207,42 @@ __global__ void __launch_bounds__(MDOT_TPB) k_mdot(MdotArgs<T> a) {
     fg_op(a.op, dsum, a.j, a.tol, a.L, a.st, a.ks);
   }
 }
+template <typename T>
+__global__ void __launch_bounds__(MDOT_TPB) k_mdot(MdotArgs<T> a) {
+  if (!a.ks->active) return;
+  mdot_body<T>(a, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y);
+}
 
 // w = (...((w + s_0 V_0) + s_1 V_1) ...) + s_{nvec-1} V_{nvec-1}, s_i = sign * coef[i],
 // over every element of the triple (whole-array, as the reference's array
 // expressions)
 template <typename T>
-__global__ void k_maxpy(long n3, T* w, const T* V0, long stride, const double* coef, int nvec, double sign,
-                        const int* active) {
-  if (active && !*active) return;
+__device__ __forceinline__ void maxpy_body(long n3, T* w, const T* V0, long stride, const double* coef, int nvec,
+                                           double sign, int b, int G) {
   __shared__ T s[MDOT_MAXV];  // the coefficients, converted once per CTA
   for (int i = threadIdx.x; i < nvec; i += blockDim.x) s[i] = T(sign * coef[i]);
   __syncthreads();
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < n3; q += (long)gridDim.x * blockDim.x) {
+  for (long q = b * (long)blockDim.x + threadIdx.x; q < n3; q += (long)G * blockDim.x) {
     T x = w[q];
     int i = 0;
     // four vectors' loads in flight before the (ordered) dependent updates
     for (; i + 4 <= nvec; i += 4) {
       const T v0 = V0[i * stride + q], v1 = V0[(i + 1) * stride + q];
       const T v2 = V0[(i + 2) * stride + q], v3 = V0[(i + 3) * stride + q];
-      x = x + s[i] * v0;
-      x = x + s[i + 1] * v1;
-      x = x + s[i + 2] * v2;
-      x = x + s[i + 3] * v3;
+      x = madd(s[i], v0, x);
+      x = madd(s[i + 1], v1, x);
+      x = madd(s[i + 2], v2, x);
+      x = madd(s[i + 3], v3, x);
     }
-    for (; i < nvec; ++i) x = x + s[i] * V0[i * stride + q];
+    for (; i < nvec; ++i) x = madd(s[i], V0[i * stride + q], x);
     w[q] = x;
   }
+}
+template <typename T>
+__global__ void k_maxpy(long n3, T* w, const T* V0, long stride, const double* coef, int nvec, double sign,
+                        const int* active) {
+  if (active && !*active) return;
+  maxpy_body<T>(n3, w, V0, stride, coef, nvec, sign, blockIdx.x, gridDim.x);
 }
 
 // dst = 0 + s * src (the reference-style array expression of a fresh vector)
@@ -253,8 +263,7 @@ __global__ void k_fg_scale(long n3, T* dst, const T* src, const double* s, const
 }
 
 // back substitution R y = g over the k columns used
-__global__ void k_fg_solve(double* st, FgLayout L, int k) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void fg_solve_body(double* st, FgLayout L, int k) {
   const double* g = st + L.g();
   double* y = st + L.y();
   for (int i = k - 1; i >= 0; --i) {
@@ -263,6 +272,10 @@ __global__ void k_fg_solve(double* st, FgLayout L, int k) {
     const double hii = st[L.H(i, i)];
     y[i] = hii != 0.0 ? s / hii : 0.0;
   }
+}
+__global__ void k_fg_solve(double* st, FgLayout L, int k) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  fg_solve_body(st, L, k);
 }
 
 }  // namespace fugu

@@ -620,7 +620,21 @@ void helmholtz(fugu_ctx* c, bool is_u, T* sol, T* tmp, const T* rhs, const CoefB
   T* cur = sol;
   T* nxt = tmp;
   const T* pen = o.pen ? (is_u ? cb.pen_u : cb.pen_v) : nullptr;
-  if (c->prm.pcd_smoother == 1) {  // red-black SOR in place (extension)
+  if (c->prm.pcd_smoother == 1 && !c->g.px && !c->g.py) {
+    // red-black SOR, both colours of a sweep in one launch (extension)
+    const dim3 grid((c->g.P + RB_TX - 1) / RB_TX, (c->g.R + RB_TY - 1) / RB_TY);
+    for (int s = 0; s < n_sweeps; ++s) {
+      if (is_u)
+        k_rbsor_sweep<T><<<grid, RB_TPB, 0, c->s>>>(c->g, 0, sol, rhs, cb.rho_u, cb.kappa, cb.zeta, cb.eta, pen,
+                                                    T(dt), T(c->prm.pcd_sor_omega), active);
+      else
+        k_rbsor_sweep<T><<<grid, RB_TPB, 0, c->s>>>(c->g, 1, sol, rhs, cb.rho_v, cb.kappa, cb.zeta, cb.eta, pen,
+                                                    T(dt), T(c->prm.pcd_sor_omega), active);
+      CKL("k_rbsor_sweep");
+    }
+    return;
+  }
+  if (c->prm.pcd_smoother == 1) {  // red-black SOR in place, one launch per colour (periodic cases)
     for (int s = 0; s < n_sweeps; ++s)
       for (int col = 0; col < 2; ++col) {
         halo(c, sol, is_u ? K_U : K_V, active);
@@ -1331,19 +1345,34 @@ KrylovResult solve(fugu_ctx* c, int solver, const CoefBufs<double>& cb, const So
   return krylov_inner<double>(c, solver, c->w64, cb, o, X, B, dt, tol, max_iter, has_lid, lid);
 }
 
-// advance_coupled_step, mod_solver_coupled.f90:137-380, on the device state
-void step(fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o, fugu_stats* st) {
+// the settings of one step that its stages share
+struct StepSetup {
+  bool amp, pen, bdf2;
+  double tol, lid, dt_eff;
+  int max_it;
+};
+StepSetup step_setup(const fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o) {
+  const fugu_params& p = c->prm;
+  StepSetup s;
+  s.amp = o->consistent_amp != 0;
+  s.pen = o->has_penalty != 0;
+  s.tol = o->has_tol ? o->tol : p.tol_bicgstab2;
+  s.max_it = o->has_max_iter ? o->max_iter : p.max_iter_bicgstab2;
+  s.lid = o->has_lid ? o->u_top_lid : 0.0;
+  s.bdf2 = (p.time_order == 2 && step_idx >= 2);
+  s.dt_eff = s.bdf2 ? dt / 1.5 : dt;
+  return s;
+}
+
+// advance_coupled_step, mod_solver_coupled.f90:137-380, before the solve:
+// the explicit stages 1-6 up to the right-hand side
+void step_pre(fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o) {
   const fugu_params& p = c->prm;
   double** f = c->f;
   const long n = c->n;
-  const bool amp = o->consistent_amp != 0;
-  const bool pen = o->has_penalty != 0;
-  const double tol = o->has_tol ? o->tol : p.tol_bicgstab2;
-  const int max_it = o->has_max_iter ? o->max_iter : p.max_iter_bicgstab2;
-  const double lid = o->has_lid ? o->u_top_lid : 0.0;
-  const bool bdf2 = (p.time_order == 2 && step_idx >= 2);
-  const double dt_eff = bdf2 ? dt / 1.5 : dt;
-  NvtxRange r_step("fugu_step");
+  const StepSetup su = step_setup(c, dt, step_idx, o);
+  const bool amp = su.amp, pen = su.pen, bdf2 = su.bdf2;
+  const double lid = su.lid;
   reset_counters(c);
   // 1. AB extrapolation u_adv = 2u^n - u^(n-1); u_prev <- u^n (u_prev then holds u^n)
   k_extrapolate<<<grid1d(c, n), 256, 0, c->s>>>(n, f[FUGU_F_U_VEL], f[FUGU_F_U_PREV], c->u_nm1, c->u_adv,
@@ -1401,24 +1430,15 @@ void step(fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o, fugu_st
   Box b = box_launch(c->g);
   k_rhs<<<b.grid, b.block, 0, c->s>>>(c->g, ra, c->B.u, c->B.v, c->B.p);
   CKL("k_rhs");
-  // 7. monolithic solve (u_top_lid is always present in this call); the
-  // state u_vel, v_vel, p_field is one contiguous coupled triple
-  SolveOpt so;
-  so.pen = pen;
-  so.amp = amp;
-  CoefBufs<double> cb = coef64(c, c->u_adv, c->v_adv);
+}
+
+// after the solve: 8. final halos and BCs, then the step's statistics
+void step_post(fugu_ctx* c, const StepSetup& su, const KrylovResult& kr, int outer, fugu_stats* st) {
   Trip<double> Xc = c->Xstate;
-  KrylovResult kr;
-  int outer = 0;
-  {
-    NvtxRange r_solve("coupled_solve");
-    kr = solve(c, o->use_bicgstab2 ? 2 : 1, cb, so, Xc, c->B, dt_eff, tol, max_it, true, lid, &outer);
-  }
-  // 8. final halos and BCs
   halo(c, Xc.u, K_U);
   halo(c, Xc.v, K_V);
   halo(c, Xc.p, K_CELL);
-  vbcs(c, Xc.u, Xc.v, lid);
+  vbcs(c, Xc.u, Xc.v, su.lid);
   collect(c, st);
   if (st) {
     st->iter = kr.iter;
@@ -1428,6 +1448,27 @@ void step(fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o, fugu_st
     KState ks = read_ks(c);
     st->matvecs = (int)ks.matvecs;
   }
+}
+
+// advance_coupled_step, mod_solver_coupled.f90:137-380, on the device state
+void step(fugu_ctx* c, double dt, int step_idx, const fugu_step_opts* o, fugu_stats* st) {
+  NvtxRange r_step("fugu_step");
+  const StepSetup su = step_setup(c, dt, step_idx, o);
+  step_pre(c, dt, step_idx, o);
+  // 7. monolithic solve (u_top_lid is always present in this call); the
+  // state u_vel, v_vel, p_field is one contiguous coupled triple
+  SolveOpt so;
+  so.pen = su.pen;
+  so.amp = su.amp;
+  CoefBufs<double> cb = coef64(c, c->u_adv, c->v_adv);
+  KrylovResult kr;
+  int outer = 0;
+  {
+    NvtxRange r_solve("coupled_solve");
+    kr = solve(c, o->use_bicgstab2 ? 2 : 1, cb, so, c->Xstate, c->B, su.dt_eff, su.tol, su.max_it, true, su.lid,
+               &outer);
+  }
+  step_post(c, su, kr, outer, st);
 }
 
 }  // namespace

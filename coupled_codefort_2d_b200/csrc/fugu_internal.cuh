@@ -53,6 +53,22 @@ inline Box box_launch(const Geo& g) {
   return b;
 }
 
+// a * b + c.  FP32 (the mixed form's inner solve, which needs no bit parity
+// with the oracle): one fused multiply-add, one rounding and one issue slot.
+// Every other type: the product and the sum rounded separately -- the library
+// is compiled without contraction, so the FP64 plain form stays bit-exact
+// with the CPU oracle.  Callers write a * b + c as madd(a, b, c) only where
+// the sum's operands are the same two values either way (IEEE addition is
+// commutative and x + (-y) equals x - y), so the FP64 bits do not change.
+template <typename T>
+__device__ __forceinline__ T madd(T a, T b, T c) {
+  return a * b + c;
+}
+template <>
+__device__ __forceinline__ float madd<float>(float a, float b, float c) {
+  return __fmaf_rn(a, b, c);
+}
+
 // --------------------------------------------------------------------------
 // Bounded grid barrier for persistent kernels launched cooperatively (all
 // CTAs co-resident).  One thread per CTA arrives on a counter; the last one

@@ -36,8 +36,7 @@ __device__ __forceinline__ bool in_kind(const Geo& g, int kind, int i, int j) {
 // full j range first, then y pass over the full i range); a wall direction is
 // untouched.  One CTA; phases separated by __syncthreads.
 template <typename T>
-__global__ void k_halo(Geo g, T* a, int kind, const int* active) {
-  if (active && !*active) return;
+__device__ __forceinline__ void halo_body(const Geo& g, T* a, int kind) {
   int i0, i1, j0, j1;
   g.extent(kind, i0, i1, j0, j1);
   const int nx = g.nx, ny = g.ny;
@@ -67,14 +66,18 @@ __global__ void k_halo(Geo g, T* a, int kind, const int* active) {
     }
   }
 }
+template <typename T>
+__global__ void k_halo(Geo g, T* a, int kind, const int* active) {
+  if (active && !*active) return;
+  halo_body<T>(g, a, kind);
+}
 
 // ------------------------------------------------------------ velocity BCs
 // apply_velocity_bcs, mod_operators.f90:254-333: west, east, south, north in
 // that order (each phase reads what the previous one wrote at the corners).
 // Extension fsx: symmetric (free-slip) tangential ghosts at the side walls.
 template <typename T>
-__global__ void k_velocity_bcs(Geo g, T* u, T* v, T u_lid, const int* active) {
-  if (active && !*active) return;
+__device__ __forceinline__ void vbcs_body(const Geo& g, T* u, T* v, T u_lid) {
   const int nx = g.nx, ny = g.ny;
   const T vs = g.fsx ? T(1) : T(-1);
   if (!g.px) {
@@ -125,6 +128,11 @@ __global__ void k_velocity_bcs(Geo g, T* u, T* v, T u_lid, const int* active) {
       u[g.at(i, ny + 2)] = two_lid - u[g.at(i, ny - 1)];
     }
   }
+}
+template <typename T>
+__global__ void k_velocity_bcs(Geo g, T* u, T* v, T u_lid, const int* active) {
+  if (active && !*active) return;
+  vbcs_body<T>(g, u, v, u_lid);
 }
 
 // ------------------------------------------------------------ properties
@@ -284,13 +292,10 @@ struct Coefs {
 // gradient, the advection and the divergence from X on the fly.  X must
 // already hold its periodic halo (k_halo).
 template <typename T>
-__global__ void k_matvec(Geo g, Coefs<T> c, const T* __restrict__ Xu, const T* __restrict__ Xv,
-                         const T* __restrict__ Xp, T* __restrict__ Yu, T* __restrict__ Yv,
-                         T* __restrict__ Yp, T dt, int with_adv, const int* active,
-                         unsigned long long* count) {
-  if (active && !*active) return;
-  if (count && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) atomicAdd(count, 1ull);
-  FUGU_BOX_IJ
+__device__ __forceinline__ void matvec_at(const Geo& g, const Coefs<T>& c, const T* __restrict__ Xu,
+                                          const T* __restrict__ Xv, const T* __restrict__ Xp, T* __restrict__ Yu,
+                                          T* __restrict__ Yv, T* __restrict__ Yp, T dt, int with_adv, int k, int i,
+                                          int j) {
   const int nx = g.nx, ny = g.ny;
   const T idx = T(g.idx), idy = T(g.idy);
   // u row
@@ -327,6 +332,16 @@ __global__ void k_matvec(Geo g, Coefs<T> c, const T* __restrict__ Xu, const T* _
     yp = (Xu[k] - Xu[g.at(i - 1, j)]) * idx + (Xv[k] - Xv[g.at(i, j - 1)]) * idy;
   Yp[k] = yp;
 }
+template <typename T>
+__global__ void k_matvec(Geo g, Coefs<T> c, const T* __restrict__ Xu, const T* __restrict__ Xv,
+                         const T* __restrict__ Xp, T* __restrict__ Yu, T* __restrict__ Yv,
+                         T* __restrict__ Yp, T dt, int with_adv, const int* active,
+                         unsigned long long* count) {
+  if (active && !*active) return;
+  if (count && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) atomicAdd(count, 1ull);
+  FUGU_BOX_IJ
+  matvec_at<T>(g, c, Xu, Xv, Xp, Yu, Yv, Yp, dt, with_adv, k, i, j);
+}
 
 // The individual operators of mod_operators.f90 (routine-level entries).
 __global__ void k_op_divergence(Geo g, const double* u, const double* v, double* div) {
@@ -360,8 +375,8 @@ __global__ void k_op_adv(Geo g, Coefs<double> c, const double* u, const double* 
 // (mod_subsolvers.f90:61-87): cx on u faces (i = 0..nx), cy on v faces
 // (j = 0..ny), and the Jacobi inverse diagonal at cells.
 template <typename T>
-__global__ void k_poisson_coefs(Geo g, const double* rho_u, const double* rho_v, T* cx, T* cy, T* dinv) {
-  FUGU_BOX_IJ
+__device__ __forceinline__ void poisson_coefs_at(const Geo& g, const double* rho_u, const double* rho_v, T* cx,
+                                                 T* cy, T* dinv, int k, int i, int j) {
   const int nx = g.nx, ny = g.ny;
   T vx = T(0), vy = T(0), di = T(1);
   if (j >= 1 && j <= ny && i >= 0 && i <= nx) {
@@ -385,6 +400,11 @@ __global__ void k_poisson_coefs(Geo g, const double* rho_u, const double* rho_v,
   cx[k] = vx;
   cy[k] = vy;
   dinv[k] = di;
+}
+template <typename T>
+__global__ void k_poisson_coefs(Geo g, const double* rho_u, const double* rho_v, T* cx, T* cy, T* dinv) {
+  FUGU_BOX_IJ
+  poisson_coefs_at<T>(g, rho_u, rho_v, cx, cy, dinv, k, i, j);
 }
 
 // PCD Schur step r_p = -((1/dt) phi + u.grad phi) (mod_pcd_precond.f90:54-62);
@@ -474,9 +494,9 @@ __device__ __forceinline__ T jacobi_u_at(const Geo& g, int k, int i, int j, cons
       const T cS = (zeta[g.at(i, j - 1)] - eta[g.at(i, j - 1)]) * iy2;
       T diag = (rho_u[k] / dt) + cE + cW + cN + cS;
       if (pen) diag = diag + pen[k];
-      const T off = cE * uo[g.at(i + 1, j)] + cW * uo[g.at(i - 1, j)] + cN * uo[g.at(i, j + 1)] +
-                    cS * uo[g.at(i, j - 1)];
-      if (diag > T(1.0e-15)) val = (T(1) - om) * uo[k] + om * ((rhs[k] + off) / diag);
+      const T off = madd(cS, uo[g.at(i, j - 1)],
+                         madd(cN, uo[g.at(i, j + 1)], madd(cW, uo[g.at(i - 1, j)], cE * uo[g.at(i + 1, j)])));
+      if (diag > T(1.0e-15)) val = madd(T(1) - om, uo[k], om * ((rhs[k] + off) / diag));
     } else if (!g.px && (i == 0 || i == nx)) {
       val = rhs[k];
     }
@@ -507,9 +527,9 @@ __device__ __forceinline__ T jacobi_v_at(const Geo& g, int k, int i, int j, cons
       const T cS = kap[k] * iy2;
       T diag = (rho_v[k] / dt) + cE + cW + cN + cS;
       if (pen) diag = diag + pen[k];
-      const T off = cE * vo[g.at(i + 1, j)] + cW * vo[g.at(i - 1, j)] + cN * vo[g.at(i, j + 1)] +
-                    cS * vo[g.at(i, j - 1)];
-      if (diag > T(1.0e-15)) val = (T(1) - om) * vo[k] + om * ((rhs[k] + off) / diag);
+      const T off = madd(cS, vo[g.at(i, j - 1)],
+                         madd(cN, vo[g.at(i, j + 1)], madd(cW, vo[g.at(i - 1, j)], cE * vo[g.at(i + 1, j)])));
+      if (diag > T(1.0e-15)) val = madd(T(1) - om, vo[k], om * ((rhs[k] + off) / diag));
     } else if (!g.py && (j == 0 || j == ny)) {
       val = rhs[k];
     }
@@ -529,13 +549,21 @@ __global__ void k_jacobi_v(Geo g, const T* vo, T* vn, const T* rhs, const T* rho
 // omega = pcd_sor_omega, reading u in place.  Every neighbour of such a face
 // has the other colour (ghosts were refreshed before the pass and are not
 // written), so the pass is race-free and order-independent.
+// the faces one colour pass of the u / v smoother updates
+__device__ __forceinline__ bool rbsor_u_face(const Geo& g, int i, int j, int col) {
+  if (j < 1 || j > g.ny || ((i + j) & 1) != col) return false;
+  return (i >= 1 && i <= g.imax()) || (!g.px && (i == 0 || i == g.nx));
+}
+__device__ __forceinline__ bool rbsor_v_face(const Geo& g, int i, int j, int col) {
+  if (i < 1 || i > g.nx || ((i + j) & 1) != col) return false;
+  return (j >= 1 && j <= g.jmax()) || (!g.py && (j == 0 || j == g.ny));
+}
 template <typename T>
 __global__ void k_rbsor_u(Geo g, T* u, const T* rhs, const T* rho_u, const T* kap, const T* zeta, const T* eta,
                           const T* pen, T dt, T om, int col, const int* active) {
   if (active && !*active) return;
   FUGU_BOX_IJ
-  if (j < 1 || j > g.ny || ((i + j) & 1) != col) return;
-  if (!((i >= 1 && i <= g.imax()) || (!g.px && (i == 0 || i == g.nx)))) return;
+  if (!rbsor_u_face(g, i, j, col)) return;
   u[k] = jacobi_u_at<T>(g, k, i, j, u, rhs, rho_u, kap, zeta, eta, pen, dt, om);
 }
 template <typename T>
@@ -543,9 +571,120 @@ __global__ void k_rbsor_v(Geo g, T* v, const T* rhs, const T* rho_v, const T* ka
                           const T* pen, T dt, T om, int col, const int* active) {
   if (active && !*active) return;
   FUGU_BOX_IJ
-  if (i < 1 || i > g.nx || ((i + j) & 1) != col) return;
-  if (!((j >= 1 && j <= g.jmax()) || (!g.py && (j == 0 || j == g.ny)))) return;
+  if (!rbsor_v_face(g, i, j, col)) return;
   v[k] = jacobi_v_at<T>(g, k, i, j, v, rhs, rho_v, kap, zeta, eta, pen, dt, om);
+}
+
+// ------------------------------------------------- fused red-black SOR sweep
+// One whole red-black SOR sweep (both colour passes) of one velocity
+// component of a wall-bounded case, per tile of RB_TX x RB_TY faces.  The
+// tile and a ring of two faces of u are staged in shared memory; the
+// coefficients of the tile and a ring of one (cE, cW, cN, cS, the diagonal
+// and the right-hand side of jacobi_u_at / jacobi_v_at) are formed once per
+// face.  The red faces (i + j even) of the tile and of its ring are updated
+// there, then the black faces of the tile from those red values, and the
+// tile's faces are written back.  Each update is jacobi_u_at / jacobi_v_at's
+// formula with its operand order, so a sweep gives the bits of the two
+// colour-pass launches (k_rbsor_u / k_rbsor_v) it replaces while it reads and
+// writes each array once instead of twice.  A periodic case refreshes its
+// ghosts between the two colours, so it keeps the two launches.
+constexpr int RB_TX = 32, RB_TY = 16;
+constexpr int RB_SX = RB_TX + 4, RB_SY = RB_TY + 4;  // with the ring of two
+constexpr int RB_CX = RB_TX + 2, RB_CY = RB_TY + 2;  // with the ring of one
+constexpr int RB_TPB = 256;
+
+template <typename T>
+struct RbSmem {
+  T u[RB_SY][RB_SX];
+  T cE[RB_CY][RB_CX], cW[RB_CY][RB_CX], cN[RB_CY][RB_CX], cS[RB_CY][RB_CX], dg[RB_CY][RB_CX], rh[RB_CY][RB_CX];
+  unsigned char kind[RB_CY][RB_CX];  // 0 not updated, 1 owned face (Jacobi formula), 2 wall face (= rhs)
+};
+
+// tile (tx, ty) of component comp (0 u, 1 v); needs !g.px && !g.py
+template <typename T>
+__device__ __forceinline__ void rbsor_sweep_tile(const Geo& g, int comp, int tx, int ty, T* u, const T* rhs,
+                                                 const T* rho, const T* kap, const T* zeta, const T* eta,
+                                                 const T* pen, T dt, T om, RbSmem<T>& sm) {
+  const int ii0 = tx * RB_TX - 2, jj0 = ty * RB_TY - 2;  // padded-box coordinates of sm.u[0][0]
+  const int nx = g.nx, ny = g.ny;
+  const T ix2 = T(g.idx2), iy2 = T(g.idy2);
+  for (int q = threadIdx.x; q < RB_SX * RB_SY; q += blockDim.x) {
+    const int a = q % RB_SX, b = q / RB_SX;
+    const int ii = ii0 + a, jj = jj0 + b;
+    sm.u[b][a] = (ii >= 0 && ii < g.P && jj >= 0 && jj < g.R) ? u[ii + jj * g.P] : T(0);
+  }
+  for (int q = threadIdx.x; q < RB_CX * RB_CY; q += blockDim.x) {
+    const int a = q % RB_CX, b = q / RB_CX;
+    const int ii = ii0 + 1 + a, jj = jj0 + 1 + b;
+    const int i = ii - 2, j = jj - 2;
+    unsigned char kd = 0;
+    if (ii >= 0 && ii < g.P && jj >= 0 && jj < g.R) {
+      const int k = ii + jj * g.P;
+      if (comp == 0 && j >= 1 && j <= ny) {
+        if (i >= 1 && i <= nx - 1) {
+          kd = 1;
+          const T e = kap[g.at(i + 1, j)] * ix2, w = kap[k] * ix2;
+          const T nn = (zeta[k] - eta[k]) * iy2, ss = (zeta[g.at(i, j - 1)] - eta[g.at(i, j - 1)]) * iy2;
+          T d = (rho[k] / dt) + e + w + nn + ss;
+          if (pen) d = d + pen[k];
+          sm.cE[b][a] = e; sm.cW[b][a] = w; sm.cN[b][a] = nn; sm.cS[b][a] = ss; sm.dg[b][a] = d;
+        } else if (i == 0 || i == nx) {
+          kd = 2;
+        }
+      } else if (comp == 1 && i >= 1 && i <= nx) {
+        if (j >= 1 && j <= ny - 1) {
+          kd = 1;
+          const T e = (zeta[k] - eta[k]) * ix2, w = (zeta[g.at(i - 1, j)] - eta[g.at(i - 1, j)]) * ix2;
+          const T nn = kap[g.at(i, j + 1)] * iy2, ss = kap[k] * iy2;
+          T d = (rho[k] / dt) + e + w + nn + ss;
+          if (pen) d = d + pen[k];
+          sm.cE[b][a] = e; sm.cW[b][a] = w; sm.cN[b][a] = nn; sm.cS[b][a] = ss; sm.dg[b][a] = d;
+        } else if (j == 0 || j == ny) {
+          kd = 2;
+        }
+      }
+      if (kd) sm.rh[b][a] = rhs[k];
+    }
+    sm.kind[b][a] = kd;
+  }
+  __syncthreads();
+  // red on the tile and its ring, then black on the tile
+  for (int col = 0; col < 2; ++col) {
+    const int lo = col == 0 ? 0 : 1, cx = col == 0 ? RB_CX : RB_TX, cy = col == 0 ? RB_CY : RB_TY;
+    for (int q = threadIdx.x; q < cx * cy; q += blockDim.x) {
+      const int a = lo + q % cx, b = lo + q / cx;  // coefficient-array indices
+      const unsigned char kd = sm.kind[b][a];
+      const int i = ii0 + a - 1, j = jj0 + b - 1;
+      if (!kd || ((i + j) & 1) != col) continue;
+      const int ua = a + 1, ub = b + 1;  // the same face in sm.u
+      if (kd == 2) {
+        sm.u[ub][ua] = sm.rh[b][a];
+        continue;
+      }
+      const T d = sm.dg[b][a];
+      if (d > T(1.0e-15)) {
+        const T off = madd(sm.cS[b][a], sm.u[ub - 1][ua],
+                           madd(sm.cN[b][a], sm.u[ub + 1][ua], madd(sm.cW[b][a], sm.u[ub][ua - 1],
+                                                                  sm.cE[b][a] * sm.u[ub][ua + 1])));
+        sm.u[ub][ua] = madd(T(1) - om, sm.u[ub][ua], om * ((sm.rh[b][a] + off) / d));
+      }
+    }
+    __syncthreads();
+  }
+  for (int q = threadIdx.x; q < RB_TX * RB_TY; q += blockDim.x) {
+    const int a = 1 + q % RB_TX, b = 1 + q / RB_TX;
+    if (!sm.kind[b][a]) continue;
+    const int ii = ii0 + 1 + a, jj = jj0 + 1 + b;
+    u[ii + jj * g.P] = sm.u[b + 1][a + 1];
+  }
+}
+template <typename T>
+__global__ void __launch_bounds__(RB_TPB) k_rbsor_sweep(Geo g, int comp, T* u, const T* rhs, const T* rho,
+                                                        const T* kap, const T* zeta, const T* eta, const T* pen,
+                                                        T dt, T om, const int* active) {
+  if (active && !*active) return;
+  __shared__ RbSmem<T> sm;
+  rbsor_sweep_tile<T>(g, comp, blockIdx.x, blockIdx.y, u, rhs, rho, kap, zeta, eta, pen, dt, om, sm);
 }
 
 // ------------------------------------------------------------ Krylov vectors

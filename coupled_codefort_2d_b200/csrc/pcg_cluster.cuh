@@ -73,8 +73,7 @@ struct RAcc {
 };
 
 template <typename T, int CPT>
-__global__ void __launch_bounds__(PCGC_TPB, 1) k_pcg_cluster(PcgClusterArgs<T> a) {
-  if (a.active && !*a.active) return;
+__device__ __forceinline__ void pcg_cluster_body(const PcgClusterArgs<T>& a) {
   cgc::cluster_group cl = cgc::this_cluster();
   const int C = (int)cl.num_blocks();
   const int rank = (int)cl.block_rank();
@@ -305,7 +304,7 @@ __global__ void __launch_bounds__(PCGC_TPB, 1) k_pcg_cluster(PcgClusterArgs<T> a
     // phase A: p_k of the own cells, then A p_k
     PCGC_CELLS {
       PCGC_CELL
-      const T pk = (iter == 1) ? z_r[c] : z_r[c] + tb * p_r[c];
+      const T pk = (iter == 1) ? z_r[c] : madd(tb, p_r[c], z_r[c]);
       p_r[c] = pk;
       pcs[lr * nx + (i - 1)] = pk;
     }
@@ -321,12 +320,14 @@ __global__ void __launch_bounds__(PCGC_TPB, 1) k_pcg_cluster(PcgClusterArgs<T> a
       if (j == ny && !g.py) pN = pk;
       else if (c + 1 < nr) pN = p_r[c + 1];
       else if (lr + 1 < R) pN = pcs[(lr + 1) * nx + (i - 1)];
-      else pN = (iter == 1) ? zt[i - 1] : zt[i - 1] + tb * pt[i - 1];
+      else pN = (iter == 1) ? zt[i - 1] : madd(tb, pt[i - 1], zt[i - 1]);
       if (j == 1 && !g.py) pS = pk;
       else if (c > 0) pS = p_r[c - 1];
       else if (lr > 0) pS = pcs[(lr - 1) * nx + (i - 1)];
-      else pS = (iter == 1) ? zb[i - 1] : zb[i - 1] + tb * pb[i - 1];
-      const T apv = (cE + cW + cN + cS) * pk - (cE * pE + cW * pW + cN * pN + cS * pS);
+      else pS = (iter == 1) ? zb[i - 1] : madd(tb, pb[i - 1], zb[i - 1]);
+      // (cE + cW + cN + cS) pk - (((cE pE + cW pW) + cN pN) + cS pS)
+      const T off = madd(cS, pS, madd(cN, pN, madd(cW, pW, cE * pE)));
+      const T apv = madd(cE + cW + cN + cS, pk, -off);
       ap_r[c] = apv;
       papd.add(double(pk) * double(apv));
     }
@@ -338,9 +339,9 @@ __global__ void __launch_bounds__(PCGC_TPB, 1) k_pcg_cluster(PcgClusterArgs<T> a
     RAcc<T> rrd, rzd;
     PCGC_CELLS {
       PCGC_CELL
-      const T rv = r_r[c] - ta * ap_r[c];
+      const T rv = madd(-ta, ap_r[c], r_r[c]);
       const T zv = dis[lr * nx + (i - 1)] * rv;
-      phi_r[c] = phi_r[c] + ta * p_r[c];
+      phi_r[c] = madd(ta, p_r[c], phi_r[c]);
       r_r[c] = rv;
       z_r[c] = zv;
       push(c, zv, p_r[c]);
@@ -374,6 +375,11 @@ __global__ void __launch_bounds__(PCGC_TPB, 1) k_pcg_cluster(PcgClusterArgs<T> a
   cl.sync();  // no CTA leaves while another may still read its shared memory
 #undef PCGC_CELLS
 #undef PCGC_CELL
+}
+template <typename T, int CPT>
+__global__ void __launch_bounds__(PCGC_TPB, 1) k_pcg_cluster(PcgClusterArgs<T> a) {
+  if (a.active && !*a.active) return;
+  pcg_cluster_body<T, CPT>(a);
 }
 
 }  // namespace fugu

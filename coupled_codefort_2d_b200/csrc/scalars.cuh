@@ -212,9 +212,10 @@ struct DotArgs {
   int check_active;  // skip when the solve has exited
 };
 
+// one CTA's share (block b of G) of the coupled dots; the last CTA to finish
+// runs the scalar op
 template <typename T>
-__global__ void __launch_bounds__(256) k_dot_op(DotArgs<T> d) {
-  if (d.check_active && !d.ks->active) return;
+__device__ __forceinline__ void dot_op_body(const DotArgs<T>& d, int b, int G) {
   __shared__ DD sh[32];
   __shared__ bool last;
   const Geo g = d.g;
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(256) k_dot_op(DotArgs<T> d) {
   for (int p = 0; p < 5; ++p) acc[p] = DD{0.0, 0.0};
   const int nx = g.nx, ny = g.ny, imax = g.imax(), jmax = g.jmax();
   const long nu = (long)imax * ny, nv = (long)nx * jmax, np = (long)nx * ny;
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < nu + nv + np; q += (long)gridDim.x * blockDim.x) {
+  for (long q = b * (long)blockDim.x + threadIdx.x; q < nu + nv + np; q += (long)G * blockDim.x) {
     long e;
     if (q < nu) {
       e = g.at(1 + (int)(q % imax), 1 + (int)(q / imax));
@@ -240,24 +241,29 @@ __global__ void __launch_bounds__(256) k_dot_op(DotArgs<T> d) {
   }
   for (int p = 0; p < d.npairs; ++p) {
     const DD s = block_sum_dd(acc[p], sh);
-    if (threadIdx.x == 0) put_partial(d.part + 2 * p * gridDim.x, blockIdx.x, s);
+    if (threadIdx.x == 0) put_partial(d.part + 2 * p * G, b, s);
   }
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned int t = atomicAdd(&d.ks->ticket, 1u);
-    last = (t == gridDim.x - 1);
+    last = (t == (unsigned int)G - 1);
   }
   __syncthreads();
   if (!last) return;
   __threadfence();
   for (int p = 0; p < d.npairs; ++p) {
-    const double s = sum_partials_dd(d.part + 2 * p * gridDim.x, gridDim.x);
+    const double s = sum_partials_dd(d.part + 2 * p * G, G);
     if (threadIdx.x == 0) d.sc[S_D0 + p] = s;
   }
   if (threadIdx.x == 0) {
     d.ks->ticket = 0;
     krylov_op(d.op, d.sc, d.ks);
   }
+}
+template <typename T>
+__global__ void __launch_bounds__(256) k_dot_op(DotArgs<T> d) {
+  if (d.check_active && !d.ks->active) return;
+  dot_op_body<T>(d, blockIdx.x, gridDim.x);
 }
 
 __global__ void k_scalar_op(OpArgs op, double* sc, KState* ks, int check_active) {
