@@ -2,9 +2,11 @@
 
 :class:`Batch` wraps ``fugu_batch_*`` of the C ABI.  Every case is a full
 context on the device (its own state, work space and stream); the library
-steps them from a pool of host threads, largest grid first, and autotunes the
-thread-block-cluster size of each case's PCG at creation.  The reference runs
-one case per ``mpirun`` and has no counterpart.
+autotunes the thread-block-cluster size of each case's PCG at creation.  By
+default a pool of host threads steps the cases, largest grid first; with
+``lockstep=True`` the coupled solves of all cases advance together, one launch
+per kernel family serving every case still running, with the same results per
+case.  The reference runs one case per ``mpirun`` and has no counterpart.
 """
 from __future__ import annotations
 
@@ -25,12 +27,13 @@ STATE_FIELDS = ("u_vel", "v_vel", "p_field", "c_field", "u_prev", "v_prev", "rho
 class Batch:
     """``cases``: a list of ``(Grid, Params, precision)``."""
 
-    def __init__(self, specs, device: int = 0, nthreads: int = 0, max_cluster: int = 0, max_coop: int = 0):
+    def __init__(self, specs, device: int = 0, nthreads: int = 0, max_cluster: int = 0, max_coop: int = 0,
+                 lockstep: bool = False):
         self.L = _lib.lib()
         self.specs = list(specs)
         n = len(self.specs)
         arr = (FuguParams * n)(*[make_params(g, prm, prec) for g, prm, prec in self.specs])
-        opts = FuguBatchOpts(nthreads, max_cluster, max_coop)
+        opts = FuguBatchOpts(nthreads, max_cluster, max_coop, int(lockstep))
         h = C.c_void_p()
         rc = self.L.fugu_batch_create(arr, n, int(device), C.byref(opts), C.byref(h))
         if rc != 0:
@@ -69,6 +72,19 @@ class Batch:
             g, prm, prec = self.specs[i]
             self._views[i] = Context.view(h, g, prm, prec)
         return self._views[i]
+
+    def stream_handle(self) -> int:
+        """cudaStream_t of the batch: events recorded on it around
+        :meth:`run` bracket all of the run's device work."""
+        h = C.c_void_p()
+        rc = self.L.fugu_batch_get_stream(self.h, C.byref(h))
+        if rc != 0:
+            raise FuguError(rc, "fugu_batch_get_stream")
+        return h.value or 0
+
+    def launches(self) -> int:
+        """Kernel launches issued by the batch so far (graph replays included)."""
+        return int(self.L.fugu_batch_launches(self.h))
 
     def run(self, nsteps: int, dt, step0, opts) -> dict:
         """Advance every case ``nsteps`` steps (``dt``, ``step0`` scalars or

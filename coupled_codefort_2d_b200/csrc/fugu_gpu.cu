@@ -2644,12 +2644,28 @@ int fugu_read_checkpoint(fugu_ctx* c, const char* path, int* step_no, double* t)
 // timed on the case's own coefficients and the one with the least SM time
 // per iteration (CTAs x microseconds) wins, because a full GPU is limited by
 // SM time, not by one case's latency.
+//
+// With fugu_batch_opts.lockstep the coupled solves of all cases run in
+// lockstep instead: one launch per kernel family serves every running case
+// (lockstep.cuh, lockstep_host.cuh), and the host threads only issue each
+// case's explicit stages and final BCs.
+#include "lockstep_host.cuh"
+
 struct fugu_batch {
   int device = 0;
   int nthreads = 1;
   std::vector<fugu_ctx*> cases;
   std::vector<int> order;
   std::string err;
+  LockstepBase* ls = nullptr;  // the lockstep solver (lockstep = 1)
+  // the batch stream: a run starts after the work queued on it before the
+  // run and ends before the work queued on it after (the lockstep solver's
+  // own stream, or a stream of the batch)
+  cudaStream_t s = nullptr;
+  bool own_s = false;
+  cudaEvent_t ev_start = nullptr;
+  std::vector<cudaEvent_t> ev_case;  // per case: its stage of the run is done
+  cudaEvent_t ev_solve = nullptr;    // the lockstep solves are done
 };
 
 namespace {
@@ -2754,6 +2770,188 @@ void batch_worker(fugu_batch* b, BatchRun* r) {
   }
 }
 
+// Lockstep set-up: every case runs the flexible-GMRES defect correction
+// (refine = 2) in one precision with one smoother and cycle length, and its
+// PCG fits a thread-block cluster.
+int lockstep_create(fugu_batch* b) {
+  const int nc = (int)b->cases.size();
+  if (nc > LS_MAX) {
+    b->err = "lockstep batch: at most " + std::to_string(LS_MAX) + " cases";
+    return FUGU_EINVAL;
+  }
+  const fugu_params& p0 = b->cases[0]->prm;
+  for (int i = 0; i < nc; ++i) {
+    const fugu_ctx* c = b->cases[i];
+    const fugu_params& p = c->prm;
+    const int pi = p.precision == FUGU_MIXED ? 1 : 0;
+    std::string why;
+    if (p.refine != 2) why = "refine must be 2 (flexible GMRES inside the defect correction)";
+    else if (p.precision != p0.precision) why = "every case needs the same precision";
+    else if (p.refine_max_inner != p0.refine_max_inner) why = "every case needs the same refine_max_inner";
+    else if (p.pcd_smoother != p0.pcd_smoother) why = "every case needs the same pcd_smoother";
+    else if (!c->pcgc[pi].ok) why = "the PCG of the case does not fit a thread-block cluster";
+    if (!why.empty()) {
+      b->err = "lockstep batch, case " + std::to_string(i) + ": " + why;
+      return FUGU_EINVAL;
+    }
+  }
+  try {
+    CK(cudaSetDevice(b->device));
+    if (p0.precision == FUGU_MIXED) {
+      Lockstep<float>* ls = new Lockstep<float>();
+      b->ls = ls;
+      ls->create(b->cases);
+    } else {
+      Lockstep<double>* ls = new Lockstep<double>();
+      b->ls = ls;
+      ls->create(b->cases);
+    }
+    CK(cudaEventCreateWithFlags(&b->ev_solve, cudaEventDisableTiming));
+  } catch (const CudaError& e) {
+    b->err = std::string("lockstep batch: ") + e.what + ": " + cudaGetErrorString(e.e);
+    return FUGU_ECUDA;
+  } catch (const ApiError& e) {
+    b->err = "lockstep batch: " + e.msg;
+    return e.code;
+  }
+  return FUGU_OK;
+}
+
+// the batch stream and its events (created with the batch)
+void batch_streams(fugu_batch* b) {
+  CK(cudaSetDevice(b->device));
+  if (b->ls) {
+    b->s = b->ls->stream();
+  } else {
+    CK(cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking));
+    b->own_s = true;
+  }
+  CK(cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming));
+  b->ev_case.resize(b->cases.size(), nullptr);
+  for (auto& e : b->ev_case) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+}
+// every case stream waits for the work queued on the batch stream so far
+void batch_begin(fugu_batch* b) {
+  CK(cudaSetDevice(b->device));
+  CK(cudaEventRecord(b->ev_start, b->s));
+  for (fugu_ctx* c : b->cases) CK(cudaStreamWaitEvent(c->s, b->ev_start, 0));
+}
+// the batch stream waits for every case stream's work of the run
+void batch_end(fugu_batch* b) {
+  CK(cudaSetDevice(b->device));
+  for (size_t i = 0; i < b->cases.size(); ++i) {
+    CK(cudaEventRecord(b->ev_case[i], b->cases[i]->s));
+    CK(cudaStreamWaitEvent(b->s, b->ev_case[i], 0));
+  }
+}
+
+// run fn(i) for every case from the batch's host threads (largest first);
+// returns each case's status
+template <typename F>
+std::vector<int> for_cases(fugu_batch* b, F fn) {
+  const int nc = (int)b->cases.size();
+  std::vector<int> st(nc, FUGU_OK);
+  std::atomic<int> next{0};
+  auto work = [&] {
+    for (;;) {
+      const int k = next.fetch_add(1);
+      if (k >= nc) return;
+      const int i = b->order[k];
+      st[i] = guard(b->cases[i], [&] { fn(i); });
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int t = 1; t < b->nthreads; ++t) pool.emplace_back(work);
+  work();
+  for (auto& th : pool) th.join();
+  return st;
+}
+
+int lockstep_run(fugu_batch* b, int nsteps, const double* dt, const int* step0, const fugu_step_opts* opts,
+                 fugu_stats* last, double* max_res, int* status) {
+  const int nc = (int)b->cases.size();
+  std::vector<double> mres(nc, 0.0);
+  std::vector<int> cst(nc, FUGU_OK);
+  std::vector<fugu_stats> lst(nc);
+  int rc = FUGU_OK;
+  cudaStream_t ls_s = b->ls->stream();
+  try {
+    batch_begin(b);
+  } catch (const CudaError& e) {
+    b->err = std::string("batch stream: ") + e.what + ": " + cudaGetErrorString(e.e);
+    return FUGU_ECUDA;
+  }
+  for (int stp = 0; stp < nsteps && rc == FUGU_OK; ++stp) {
+    std::vector<StepSetup> su(nc);
+    for (int i = 0; i < nc; ++i) su[i] = step_setup(b->cases[i], dt[i], step0[i] + stp, &opts[i]);
+    // 1. explicit stages of every case on its own stream
+    std::vector<int> st = for_cases(b, [&](int i) {
+      fugu_ctx* c = b->cases[i];
+      step_pre(c, dt[i], step0[i] + stp, &opts[i]);
+      CK(cudaEventRecord(b->ev_case[i], c->s));
+    });
+    for (int i = 0; i < nc; ++i)
+      if (st[i] != FUGU_OK) {
+        cst[i] = st[i];
+        if (rc == FUGU_OK) {
+          rc = st[i];
+          b->err = "case " + std::to_string(i) + ": " + b->cases[i]->err;
+        }
+      }
+    if (rc != FUGU_OK) break;
+    // 2. the coupled solves in lockstep
+    std::vector<KrylovResult> kr;
+    std::vector<int> outer;
+    try {
+      CK(cudaSetDevice(b->device));
+      for (int i = 0; i < nc; ++i) CK(cudaStreamWaitEvent(ls_s, b->ev_case[i], 0));
+      NvtxRange r_solve("lockstep_coupled_solves");
+      b->ls->solve(su, kr, outer);
+      CK(cudaEventRecord(b->ev_solve, ls_s));
+    } catch (const CudaError& e) {
+      b->err = std::string("lockstep solve: ") + e.what + ": " + cudaGetErrorString(e.e);
+      rc = FUGU_ECUDA;
+    } catch (const ApiError& e) {
+      b->err = "lockstep solve: " + e.msg;
+      rc = e.code;
+    }
+    if (rc != FUGU_OK) {
+      for (int i = 0; i < nc; ++i) cst[i] = rc;
+      break;
+    }
+    // 3. final BCs and statistics of every case
+    st = for_cases(b, [&](int i) {
+      fugu_ctx* c = b->cases[i];
+      CK(cudaStreamWaitEvent(c->s, b->ev_solve, 0));
+      std::memset(&lst[i], 0, sizeof(fugu_stats));
+      step_post(c, su[i], kr[i], outer[i], &lst[i]);
+      if (lst[i].res > mres[i] || std::isnan(lst[i].res)) mres[i] = lst[i].res;
+    });
+    for (int i = 0; i < nc; ++i)
+      if (st[i] != FUGU_OK) {
+        cst[i] = st[i];
+        if (rc == FUGU_OK) {
+          rc = st[i];
+          b->err = "case " + std::to_string(i) + ": " + b->cases[i]->err;
+        }
+      }
+  }
+  if (rc == FUGU_OK) {
+    try {
+      batch_end(b);
+    } catch (const CudaError& e) {
+      b->err = std::string("batch stream: ") + e.what + ": " + cudaGetErrorString(e.e);
+      rc = FUGU_ECUDA;
+    }
+  }
+  for (int i = 0; i < nc; ++i) {
+    if (last) last[i] = lst[i];
+    if (max_res) max_res[i] = mres[i];
+    if (status) status[i] = cst[i];
+  }
+  return rc;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2767,7 +2965,9 @@ int fugu_batch_create(const fugu_params* params, int ncases, int device, const f
     if (check_params(&params[i]) != FUGU_OK) return FUGU_EINVAL;
   fugu_batch_opts o{};
   if (opts) o = *opts;
-  if (o.nthreads < 0 || o.max_cluster < 0 || o.max_cluster > 16 || o.max_coop < 0) return FUGU_EINVAL;
+  if (o.nthreads < 0 || o.max_cluster < 0 || o.max_cluster > 16 || o.max_coop < 0 || o.lockstep < 0 ||
+      o.lockstep > 1)
+    return FUGU_EINVAL;
   fugu_batch* b = new fugu_batch();
   b->device = device;
   const int hw = (int)std::thread::hardware_concurrency();
@@ -2806,6 +3006,22 @@ int fugu_batch_create(const fugu_params* params, int ncases, int device, const f
       return rc;
     }
   }
+  if (o.lockstep) {
+    const int rc = lockstep_create(b);
+    if (rc) {
+      fprintf(stderr, "fugu_batch_create: %s\n", b->err.c_str());
+      fugu_batch_destroy(b);
+      return rc;
+    }
+  }
+  try {
+    batch_streams(b);
+  } catch (const CudaError& e) {
+    b->err = std::string("batch stream: ") + e.what + ": " + cudaGetErrorString(e.e);
+    fprintf(stderr, "fugu_batch_create: %s\n", b->err.c_str());
+    fugu_batch_destroy(b);
+    return FUGU_ECUDA;
+  }
   b->order.resize(ncases);
   for (int i = 0; i < ncases; ++i) b->order[i] = i;
   std::stable_sort(b->order.begin(), b->order.end(), [&](int a, int z) {
@@ -2817,6 +3033,15 @@ int fugu_batch_create(const fugu_params* params, int ncases, int device, const f
 
 void fugu_batch_destroy(fugu_batch* b) {
   if (!b) return;
+  cudaSetDevice(b->device);
+  for (cudaEvent_t e : b->ev_case) cudaEventDestroy(e);
+  if (b->ev_solve) cudaEventDestroy(b->ev_solve);
+  if (b->ev_start) cudaEventDestroy(b->ev_start);
+  if (b->own_s && b->s) {
+    cudaStreamSynchronize(b->s);
+    cudaStreamDestroy(b->s);
+  }
+  delete b->ls;
   for (fugu_ctx* c : b->cases) destroy(c);
   delete b;
 }
@@ -2838,6 +3063,13 @@ int fugu_batch_run(fugu_batch* b, int nsteps, const double* dt, const int* step0
     b->err = "fugu_batch_run: NULL dt/step0/opts or nsteps < 0";
     return FUGU_EINVAL;
   }
+  if (b->ls) return lockstep_run(b, nsteps, dt, step0, opts, last, max_res, status);
+  try {
+    batch_begin(b);
+  } catch (const CudaError& e) {
+    b->err = std::string("batch stream: ") + e.what + ": " + cudaGetErrorString(e.e);
+    return FUGU_ECUDA;
+  }
   BatchRun r;
   r.nsteps = nsteps;
   r.dt = dt;
@@ -2857,7 +3089,26 @@ int fugu_batch_run(fugu_batch* b, int nsteps, const double* dt, const int* step0
       b->err = "case " + std::to_string(i) + ": " + b->cases[i]->err;
       return st[i];
     }
+  try {
+    batch_end(b);
+  } catch (const CudaError& e) {
+    b->err = std::string("batch stream: ") + e.what + ": " + cudaGetErrorString(e.e);
+    return FUGU_ECUDA;
+  }
   return FUGU_OK;
+}
+
+int fugu_batch_get_stream(fugu_batch* b, void** stream) {
+  if (!b || !stream) return FUGU_EINVAL;
+  *stream = (void*)b->s;
+  return FUGU_OK;
+}
+
+unsigned long long fugu_batch_launches(const fugu_batch* b) {
+  if (!b) return 0;
+  unsigned long long n = b->ls ? b->ls->launch_count() : 0;
+  for (const fugu_ctx* c : b->cases) n += c->launches;
+  return n;
 }
 
 }  // extern "C"

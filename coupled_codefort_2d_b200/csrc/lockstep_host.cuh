@@ -1,0 +1,676 @@
+// lockstep_host.cuh -- host side of the fused batched form (lockstep.cuh).
+// Included by fugu_gpu.cu after the context, the step and the solvers.
+//
+// One batch step:
+//   1. each case's explicit stages (AB extrapolation, VOF, properties, SVOF,
+//      curvature, CSF, right-hand side) on the case's own stream, issued by
+//      the batch's host threads (step_pre);
+//   2. the coupled solves of all cases in lockstep on the lockstep stream:
+//      the FP64 defect correction around flexible GMRES + PCD (refine_solve
+//      and fgmres in fugu_gpu.cu), every phase one launch per kernel family
+//      for all cases still running; each flexible-GMRES cycle is one CUDA
+//      graph whose Arnoldi steps sit in conditional nodes armed on the device;
+//   3. each case's final halos, wall BCs and statistics (step_post).
+// The host synchronises twice per defect-correction pass for the whole batch
+// (the single-case form does so per Arnoldi step and per case).
+#pragma once
+
+#include "lockstep.cuh"
+
+namespace {
+
+// check a launch of the lockstep solver and count it
+#define LSCKL(what)                                        \
+  do {                                                     \
+    cudaError_t e_ = cudaGetLastError();                   \
+    if (e_ != cudaSuccess) throw CudaError{e_, what};      \
+    ++launches;                                            \
+  } while (0)
+
+struct LsClass {
+  int C = 0, cpt = 0, rows_per = 0;
+  size_t smem = 0;
+  std::vector<int> cases;
+  int* d_list = nullptr;
+};
+
+// per-case bookkeeping of one solve
+struct LsCaseRun {
+  bool adapt = false, adapt_sw = false;
+  int cap = 0, sweeps = 0;     // current adaptive values (0: fixed)
+  int outer = 0, inner_total = 0;
+  double rel = 0.0, tol = 0.0;
+  int status = FUGU_CONVERGED;
+  bool done = false;
+};
+
+struct LockstepBase {
+  virtual ~LockstepBase() {}
+  virtual void solve(const std::vector<StepSetup>& su, std::vector<KrylovResult>& kr, std::vector<int>& outer) = 0;
+  virtual cudaStream_t stream() const = 0;
+  virtual unsigned long long launch_count() const = 0;
+};
+
+template <typename T>
+struct Lockstep : LockstepBase {
+  std::vector<fugu_ctx*> cases;
+  int ncase = 0, m = 0, smoother = 0, device = 0, nsm = 148;
+  bool any_periodic = false;
+  cudaStream_t s = nullptr;   // the lockstep stream
+  cudaStream_t q = nullptr;   // the stream launches are issued on (s, or s2 while a body is captured)
+  cudaStream_t s2 = nullptr;  // captures the bodies of the cycle graph's conditional nodes
+  std::vector<cudaStream_t> side;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
+  LsCase<T>* d_cases = nullptr;
+  LsDyn* d_dyn = nullptr;
+  LsDyn* h_dyn = nullptr;
+  LsPlan* d_plan = nullptr;
+  LsRead* d_read = nullptr;
+  LsRead* h_read = nullptr;
+  int* h_nact = nullptr;
+  std::vector<LsClass> classes;
+  std::map<const void*, int> grids;  // persistent grid per family kernel
+  unsigned long long launches = 0;   // kernel launches issued, replays included
+  // per Arnoldi step, one graph (the host checks between steps)
+  struct Graph {
+    int max_sweeps = -1;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long launches = 0;  // kernel launches of one replay
+  };
+  std::vector<Graph> graphs;
+  // one whole flexible-GMRES cycle as one graph (a conditional IF node per
+  // Arnoldi step), rebuilt when the sweep count changes
+  struct Cycle {
+    int max_sweeps = -1;
+    cudaGraphExec_t exec = nullptr;
+    unsigned long long head = 0, body = 0;  // launches outside the steps, per executed step
+  } cyc;
+  bool use_cycle_graph = true;
+  std::vector<void*> allocs;
+
+  cudaStream_t stream() const override { return s; }
+  unsigned long long launch_count() const override { return launches; }
+
+  ~Lockstep() override {
+    if (s) cudaStreamSynchronize(s);
+    for (auto& g : graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (cyc.exec) cudaGraphExecDestroy(cyc.exec);
+    for (auto& c : classes)
+      if (c.d_list) cudaFree(c.d_list);
+    for (void* p : allocs) cudaFree(p);
+    if (h_dyn) cudaFreeHost(h_dyn);
+    if (h_read) cudaFreeHost(h_read);
+    if (h_nact) cudaFreeHost(h_nact);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    for (auto e : ev_join) cudaEventDestroy(e);
+    for (auto x : side) cudaStreamDestroy(x);
+    if (s2) cudaStreamDestroy(s2);
+    if (s) cudaStreamDestroy(s);
+  }
+
+  template <typename U>
+  U* dal(long n) {
+    U* p = nullptr;
+    CK(cudaMalloc(&p, sizeof(U) * (size_t)n));
+    allocs.push_back(p);
+    return p;
+  }
+
+  // --------------------------------------------------------- set-up
+  void create(const std::vector<fugu_ctx*>& cs) {
+    cases = cs;
+    ncase = (int)cs.size();
+    fugu_ctx* c0 = cs[0];
+    device = c0->device;
+    nsm = c0->nsm;
+    m = c0->prm.refine_max_inner;
+    smoother = c0->prm.pcd_smoother;
+    const int pi = sizeof(T) == 8 ? 0 : 1;
+    CK(cudaSetDevice(device));
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking));
+    q = s;
+    std::vector<LsCase<T>> rec(ncase);
+    std::map<std::array<long, 4>, int> cls_of;
+    for (int i = 0; i < ncase; ++i) {
+      fugu_ctx* c = cs[i];
+      if (c->g.px || c->g.py) any_periodic = true;
+      LsCase<T>& r = rec[i];
+      std::memset(&r, 0, sizeof r);
+      r.g = c->g;
+      r.n = c->n;
+      r.dot_grid = c->dot_grid;
+      r.nsm = c->nsm;
+      r.mdot_gmax = (mdot_items(c->g) + MDOT_TPB / 32 - 1) / (MDOT_TPB / 32);
+      r.X = c->Xstate.base;
+      r.B = c->B.base;
+      r.r64 = c->w64.t[10].base;
+      r.ax = c->w64.t[12].base;
+      const CoefBufs<double> cb = coef64(c, c->u_adv, c->v_adv);
+      r.c64.u_adv = cb.u_adv; r.c64.v_adv = cb.v_adv; r.c64.rho_c = cb.rho_c; r.c64.rho_u = cb.rho_u;
+      r.c64.rho_v = cb.rho_v; r.c64.kappa = cb.kappa; r.c64.zeta = cb.zeta; r.c64.eta = cb.eta;
+      r.c64.pen_u = cb.pen_u; r.c64.pen_v = cb.pen_v; r.c64.mdot_u = cb.mdu; r.c64.mdot_v = cb.mdv;
+      r.sc = c->sc;
+      r.part = c->part;
+      r.ks = c->ks;
+      r.pcg_out = c->pcg_out;
+      FgWork<T>& f = ensure_fg<T>(c, m);
+      r.V = f.V;
+      r.Z = f.Z;
+      r.st = f.st;
+      if constexpr (sizeof(T) == 8) {
+        KrylovWork<double>& w = c->w64;
+        r.ri = w.t[10].base;
+        r.di = w.t[11].base;
+        r.w = w.t[0].base;
+        r.cf = r.c64;
+        r.cx = w.pcg.cx; r.cy = w.pcg.cy; r.dinv = w.pcg.dinv;
+        r.phi = w.pcd.phi; r.zuw = w.pcd.zuw; r.zvw = w.pcd.zvw; r.tmp = w.pcd.tmp;
+      } else {
+        ensure_w32(c);
+        KrylovWork<float>& w = c->w32;
+        r.ri = w.t[10].base;
+        r.di = w.t[11].base;
+        r.w = w.t[0].base;
+        const CoefBufs<float>& qf = w.cf;
+        r.cf.u_adv = qf.u_adv; r.cf.v_adv = qf.v_adv; r.cf.rho_c = qf.rho_c; r.cf.rho_u = qf.rho_u;
+        r.cf.rho_v = qf.rho_v; r.cf.kappa = qf.kappa; r.cf.zeta = qf.zeta; r.cf.eta = qf.eta;
+        r.cf.pen_u = qf.pen_u; r.cf.pen_v = qf.pen_v; r.cf.mdot_u = qf.mdu; r.cf.mdot_v = qf.mdv;
+        r.cx = w.pcg.cx; r.cy = w.pcg.cy; r.dinv = w.pcg.dinv;
+        r.phi = w.pcd.phi; r.zuw = w.pcd.zuw; r.zvw = w.pcd.zvw; r.tmp = w.pcd.tmp;
+      }
+      r.pcg_tol = c->prm.pcg_tol;
+      r.inner_tol = c->prm.refine_inner_tol;
+      r.jac_omega = c->prm.jacobi_omega;
+      r.sor_omega = c->prm.pcd_sor_omega;
+      r.visc = c->prm.pcd_visc_scale;
+      // PCG grid class: the cluster plan of the case's inner precision
+      const fugu_ctx::ClusterPlan& pl = c->pcgc[pi];
+      const std::array<long, 4> key = {pl.C, pl.cpt, pl.rows_per, (long)pl.smem};
+      auto it = cls_of.find(key);
+      if (it == cls_of.end()) {
+        LsClass k;
+        k.C = pl.C;
+        k.cpt = pl.cpt;
+        k.rows_per = pl.rows_per;
+        k.smem = pl.smem;
+        classes.push_back(k);
+        it = cls_of.emplace(key, (int)classes.size() - 1).first;
+      }
+      classes[it->second].cases.push_back(i);
+    }
+    d_cases = dal<LsCase<T>>(ncase);
+    CK(cudaMemcpy(d_cases, rec.data(), sizeof(LsCase<T>) * ncase, cudaMemcpyHostToDevice));
+    d_dyn = dal<LsDyn>(ncase);
+    d_plan = dal<LsPlan>(1);
+    d_read = dal<LsRead>(ncase);
+    CK(cudaMallocHost(&h_dyn, sizeof(LsDyn) * ncase));
+    CK(cudaMallocHost(&h_read, sizeof(LsRead) * ncase));
+    CK(cudaMallocHost(&h_nact, sizeof(int)));
+    std::memset(h_dyn, 0, sizeof(LsDyn) * ncase);
+    for (auto& k : classes) {
+      CK(cudaMalloc(&k.d_list, sizeof(int) * k.cases.size()));
+      CK(cudaMemcpy(k.d_list, k.cases.data(), sizeof(int) * k.cases.size(), cudaMemcpyHostToDevice));
+      const void* fn = pcg_fn(k.cpt);
+      int optin = 0;
+      CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+      cudaFuncAttributes fa;
+      CK(cudaFuncGetAttributes(&fa, fn));
+      CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes));
+      CK(cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    }
+    for (size_t k = 1; k < classes.size(); ++k) {
+      cudaStream_t x;
+      CK(cudaStreamCreateWithFlags(&x, cudaStreamNonBlocking));
+      side.push_back(x);
+    }
+    CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    for (size_t k = 0; k < classes.size(); ++k) {
+      cudaEvent_t e;
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      ev_join.push_back(e);
+    }
+    graphs.resize(m);
+    warm_grids();
+  }
+
+  const void* pcg_fn(int cpt) {
+    switch (cpt) {
+      case 1: return (const void*)k_ls_pcg<T, 1>;
+      case 2: return (const void*)k_ls_pcg<T, 2>;
+      case 4: return (const void*)k_ls_pcg<T, 4>;
+      case 8: return (const void*)k_ls_pcg<T, 8>;
+      case 16: return (const void*)k_ls_pcg<T, 16>;
+    }
+    throw ApiError{FUGU_EINVAL, "lockstep batch: no PCG kernel for this cluster plan"};
+  }
+
+  // co-resident CTAs of a family kernel (its persistent grid)
+  int grid_of(const void* fn, int tpb) {
+    auto it = grids.find(fn);
+    if (it != grids.end()) return it->second;
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, tpb, 0));
+    const int g = nsm * (occ > 0 ? occ : 1);
+    grids.emplace(fn, g);
+    return g;
+  }
+  // the persistent grid of every family kernel, taken before any capture
+  template <class F>
+  void warm_box() { grid_of((const void*)k_ls_box<T, F>, LS_TPB); }
+  template <class F>
+  void warm_e1() { grid_of((const void*)k_ls_e1<T, F>, LS_TPB); }
+  void warm_grids() {
+    warm_box<LsMatvecOuter<T>>(); warm_box<LsMatvecInner<T>>(); warm_box<LsPoissonCoefs<T>>();
+    warm_box<LsSchur<T>>(); warm_box<LsZwork<T>>(); warm_box<LsCross<T>>(); warm_box<LsRbsor<T>>();
+    warm_box<LsJacobi<T>>();
+    warm_e1<LsCvtCoefs<T>>(); warm_e1<LsDefect<T>>(); warm_e1<LsUpdate64<T>>(); warm_e1<LsScaleDefect<T>>();
+    warm_e1<LsZeroCorrection<T>>(); warm_e1<LsAccumulate<T>>(); warm_e1<LsFgScale<T>>(); warm_e1<LsZeroPcd<T>>();
+    warm_e1<LsJacobiCopy<T>>();
+    grid_of((const void*)k_ls_dot<T>, DOT_TPB);
+    grid_of((const void*)k_ls_mdot<T>, MDOT_TPB);
+    grid_of((const void*)k_ls_maxpy<T>, LS_TPB);
+    grid_of((const void*)k_ls_rbsor<T>, RB_TPB);
+  }
+
+  // ------------------------------------------------------- launches
+  template <class F>
+  void box(F f) {
+    const void* fn = (const void*)k_ls_box<T, F>;
+    k_ls_box<T, F><<<grid_of(fn, LS_TPB), LS_TPB, 0, q>>>(d_cases, d_dyn, d_plan, f);
+    LSCKL("k_ls_box");
+  }
+  template <class F>
+  void e1(F f) {
+    const void* fn = (const void*)k_ls_e1<T, F>;
+    k_ls_e1<T, F><<<grid_of(fn, LS_TPB), LS_TPB, 0, q>>>(d_cases, d_dyn, d_plan, f);
+    LSCKL("k_ls_e1");
+  }
+  template <class F>
+  void one(F f) {
+    k_ls_one<T, F><<<ncase, 1024, 0, q>>>(d_cases, d_dyn, d_plan, f);
+    LSCKL("k_ls_one");
+  }
+  template <class F>
+  void all(F f) {
+    k_ls_all<T, F><<<ncase, 128, 0, q>>>(d_cases, d_dyn, ncase, f);
+    LSCKL("k_ls_all");
+  }
+  void plan(int src, int nvec) {
+    k_ls_plan<T><<<1, LS_MAX, 0, q>>>(d_cases, d_dyn, ncase, src, nvec, d_plan);
+    LSCKL("k_ls_plan");
+  }
+  void dot(int which, int op) {
+    const void* fn = (const void*)k_ls_dot<T>;
+    k_ls_dot<T><<<grid_of(fn, DOT_TPB), DOT_TPB, 0, q>>>(d_cases, d_plan, which, OpArgs{op, 0, 0.0});
+    LSCKL("k_ls_dot");
+  }
+  void mdot(int which, int nvec, int op, int j) {
+    const void* fn = (const void*)k_ls_mdot<T>;
+    k_ls_mdot<T><<<grid_of(fn, MDOT_TPB), MDOT_TPB, 0, q>>>(d_cases, d_plan, which, nvec, op, j, m);
+    LSCKL("k_ls_mdot");
+  }
+  void maxpy(int which, int nvec) {
+    const void* fn = (const void*)k_ls_maxpy<T>;
+    k_ls_maxpy<T><<<grid_of(fn, LS_TPB), LS_TPB, 0, q>>>(d_cases, d_plan, which, nvec, m);
+    LSCKL("k_ls_maxpy");
+  }
+  // the PCD's PCG of every grid class, the classes side by side
+  void pcg(int j) {
+    if (classes.size() > 1) CK(cudaEventRecord(ev_fork, q));
+    for (size_t k = 0; k < classes.size(); ++k) {
+      const LsClass& cl = classes[k];
+      cudaStream_t st = k == 0 ? q : side[k - 1];
+      if (k > 0) CK(cudaStreamWaitEvent(st, ev_fork, 0));
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)(cl.C * cl.cases.size()), 1, 1);
+      cfg.blockDim = dim3(PCGC_TPB, 1, 1);
+      cfg.dynamicSmemBytes = cl.smem;
+      cfg.stream = st;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = cl.C;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      const LsCase<T>* a0 = d_cases;
+      const LsDyn* a1 = d_dyn;
+      const int* a2 = cl.d_list;
+      int a3 = cl.rows_per, a4 = j;
+      void* args[] = {&a0, &a1, &a2, &a3, &a4};
+      CK(cudaLaunchKernelExC(&cfg, pcg_fn(cl.cpt), args));
+      ++launches;
+      if (k > 0) {
+        CK(cudaEventRecord(ev_join[k], st));
+        CK(cudaStreamWaitEvent(q, ev_join[k], 0));
+      }
+    }
+  }
+  void upload_dyn() { CK(cudaMemcpyAsync(d_dyn, h_dyn, sizeof(LsDyn) * ncase, cudaMemcpyHostToDevice, s)); }
+  void readback() {
+    all(LsReadback<T>{d_read, m});
+    CK(cudaMemcpyAsync(h_read, d_read, sizeof(LsRead) * ncase, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+  }
+
+  // ----------------------------------------------- one Arnoldi step j
+  // (pcd, wall BCs, matvec, CGS2, new basis vector: fgmres() in fugu_gpu.cu),
+  // then the plan of step j + 1
+  void helmholtz(int j, int comp, int max_sw) {
+    if (smoother == 1 && !any_periodic) {  // both colours of a sweep in one launch
+      const void* fn = (const void*)k_ls_rbsor<T>;
+      for (int sw = 0; sw < max_sw; ++sw) {
+        k_ls_rbsor<T><<<grid_of(fn, RB_TPB), RB_TPB, 0, q>>>(d_cases, d_dyn, d_plan, j, comp, sw);
+        LSCKL("k_ls_rbsor");
+      }
+      return;
+    }
+    if (smoother == 1) {
+      for (int sw = 0; sw < max_sw; ++sw)
+        for (int col = 0; col < 2; ++col) {
+          if (any_periodic) one(LsHalo<T>{LB_ZJ, comp, j, sw});
+          box(LsRbsor<T>{j, comp, sw, col});
+        }
+      return;
+    }
+    for (int sw = 0; sw < max_sw; ++sw) {
+      if (any_periodic) one(LsHalo<T>{LB_JTMP, comp, j, sw});
+      box(LsJacobi<T>{j, comp, sw});
+    }
+    e1(LsJacobiCopy<T>{j, comp});
+  }
+  void arnoldi_step(int j, int max_sw, bool count_to_host) {
+    const FgLayout L{m};
+    e1(LsZeroPcd<T>{j});
+    pcg(j);
+    if (any_periodic) one(LsHalo<T>{LB_PHI, 2, j, -1});
+    box(LsSchur<T>{j});
+    if (any_periodic) one(LsHalo<T>{LB_ZJ, 2, j, -1});
+    box(LsZwork<T>{j});
+    helmholtz(j, 1, max_sw);
+    if (any_periodic) one(LsHalo<T>{LB_ZJ, 1, j, -1});
+    box(LsCross<T>{j});
+    helmholtz(j, 0, max_sw);
+    if (any_periodic) one(LsHalo<T>{LB_ZJ, 0, j, -1});
+    one(LsVbcs<T>{LB_ZJ, j, 0});
+    if (any_periodic)
+      for (int comp = 0; comp < 3; ++comp) one(LsHalo<T>{LB_ZJ, comp, j, -1});
+    box(LsMatvecInner<T>{j});
+    mdot(1, j + 1, FG_PROJ1, j);
+    maxpy(0, j + 1);
+    mdot(1, j + 1, FG_PROJ2, j);
+    maxpy(0, j + 1);
+    mdot(2, 1, FG_ROTATE, j);
+    e1(LsFgScale<T>{j + 1, L.inv()});
+    plan(1, j + 2);
+    if (count_to_host) CK(cudaMemcpyAsync(h_nact, &d_plan->n, sizeof(int), cudaMemcpyDeviceToHost, q));
+  }
+  void run_step_graph(int j, int max_sw) {
+    Graph& g = graphs[j];
+    if (!g.exec || g.max_sweeps != max_sw) {
+      cudaGraph_t graph;
+      const unsigned long long before = launches;
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      try {
+        arnoldi_step(j, max_sw, true);
+        g.launches = launches - before;
+        launches = before;
+      } catch (...) {
+        launches = before;
+        cudaGraph_t junk;
+        cudaStreamEndCapture(s, &junk);
+        if (junk) cudaGraphDestroy(junk);
+        throw;
+      }
+      CK(cudaStreamEndCapture(s, &graph));
+      if (g.exec) CK(cudaGraphExecDestroy(g.exec));
+      g.exec = nullptr;
+      const cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      CK(e);
+      g.max_sweeps = max_sw;
+    }
+    CK(cudaGraphLaunch(g.exec, s));
+    launches += g.launches;
+  }
+
+  // The whole cycle as one graph: the cycle's set-up, then per Arnoldi step j
+  // a one-thread kernel that arms a conditional IF node with "some case is
+  // still active" and the IF node whose body is step j (ending with the plan
+  // of step j + 1), then the back substitution and the update.  A step whose
+  // node is not armed is skipped on the device, and so is every later one.
+  void build_cycle(int max_sw) {
+    const FgLayout L{m};
+    if (cyc.exec) CK(cudaGraphExecDestroy(cyc.exec));
+    cyc.exec = nullptr;
+    const unsigned long long before = launches;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    bool body_open = false;
+    try {
+      q = s;
+      all(LsResetKs{});
+      plan(0, 1);
+      one(LsZeroSt<T>{L.size()});
+      mdot(0, 1, FG_BETA, 0);
+      e1(LsFgScale<T>{0, L.inv()});
+      plan(1, 1);
+      const unsigned long long head0 = launches - before;
+      unsigned long long body = 0;
+      for (int j = 0; j < m; ++j) {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cg = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd));
+        cudaGraphConditionalHandle h;
+        CK(cudaGraphConditionalHandleCreate(&h, cg, 0, 0));
+        k_ls_cond<<<1, 32, 0, s>>>(d_plan, h);
+        LSCKL("k_ls_cond");
+        CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &nd));
+        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        CK(cudaGraphAddNode(&node, cg, deps, nd, &cp));
+        CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+        cudaGraph_t bg = cp.conditional.phGraph_out[0];
+        CK(cudaStreamBeginCaptureToGraph(s2, bg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        body_open = true;
+        q = s2;
+        const unsigned long long b0 = launches;
+        arnoldi_step(j, max_sw, false);
+        body = launches - b0;
+        q = s;
+        cudaGraph_t bout = nullptr;
+        body_open = false;
+        CK(cudaStreamEndCapture(s2, &bout));
+      }
+      const unsigned long long t0 = launches;
+      plan(0, 1);
+      one(LsFgSolve<T>{m});
+      maxpy(1, 0);
+      cyc.head = head0 + (unsigned long long)m + (launches - t0);
+      cyc.body = body;
+    } catch (...) {
+      q = s;
+      launches = before;
+      if (body_open) {
+        cudaGraph_t junk = nullptr;
+        cudaStreamEndCapture(s2, &junk);
+      }
+      cudaGraph_t junk = nullptr;
+      cudaStreamEndCapture(s, &junk);
+      if (junk) cudaGraphDestroy(junk);
+      throw;
+    }
+    launches = before;
+    CK(cudaStreamEndCapture(s, &graph));
+    const cudaError_t e = cudaGraphInstantiate(&cyc.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CK(e);
+    cyc.max_sweeps = max_sw;
+  }
+
+  // one flexible-GMRES(m) cycle of every running case from a zero correction
+  void fgmres_cycle(int max_sw) {
+    if (use_cycle_graph && (!cyc.exec || cyc.max_sweeps != max_sw)) {
+      try {
+        build_cycle(max_sw);
+      } catch (const CudaError&) {
+        // a runtime that cannot build the conditional graph: launch the
+        // steps one graph at a time, with a host check between them
+        cudaGetLastError();
+        use_cycle_graph = false;
+      }
+    }
+    if (use_cycle_graph) {
+      CK(cudaGraphLaunch(cyc.exec, s));
+      launches += cyc.head;  // the executed steps' launches are added by the caller
+      return;
+    }
+    const FgLayout L{m};
+    all(LsResetKs{});
+    plan(0, 1);
+    one(LsZeroSt<T>{L.size()});
+    mdot(0, 1, FG_BETA, 0);
+    e1(LsFgScale<T>{0, L.inv()});
+    plan(1, 1);
+    CK(cudaMemcpyAsync(h_nact, &d_plan->n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (int j = 0; j < m && *h_nact > 0; ++j) {
+      NvtxRange r_it("lockstep_arnoldi_step");
+      run_step_graph(j, max_sw);
+      CK(cudaStreamSynchronize(s));
+    }
+    plan(0, 1);
+    one(LsFgSolve<T>{m});
+    maxpy(1, 0);
+  }
+
+  // ------------------------------------------------ the lockstep solve
+  // refine_solve (fugu_gpu.cu) for every case at once
+  void solve(const std::vector<StepSetup>& su, std::vector<KrylovResult>& kr, std::vector<int>& outer) override {
+    CK(cudaSetDevice(device));
+    q = s;
+    std::vector<LsCaseRun> cr(ncase);
+    for (int i = 0; i < ncase; ++i) {
+      fugu_ctx* c = cases[i];
+      const fugu_params& p = c->prm;
+      LsCaseRun& r = cr[i];
+      r.adapt = p.pcg_cap_start > 0;
+      r.adapt_sw = p.pcd_sweeps_max > p.pcd_sweeps;
+      if (r.adapt) r.cap = std::min(std::max(p.pcg_cap_start, c->pcg_cap_state), p.pcg_max_iter);
+      if (r.adapt_sw) r.sweeps = std::min(std::max(p.pcd_sweeps, c->pcd_sweeps_state), p.pcd_sweeps_max);
+      r.tol = su[i].tol;
+      LsDyn& d = h_dyn[i];
+      d.run = 1;
+      d.pcg_cap = r.cap > 0 ? r.cap : p.pcg_max_iter;
+      d.sweeps = r.sweeps > 0 ? r.sweeps : p.pcd_sweeps;
+      d.pen = su[i].pen ? 1 : 0;
+      d.amp = su[i].amp ? 1 : 0;
+      d.has_lid = 1;  // the step always passes its lid (zero when absent)
+      d.dt = su[i].dt_eff;
+      d.lid = su[i].lid;
+    }
+    upload_dyn();
+    plan(0, 1);
+    if constexpr (sizeof(T) == 4) e1(LsCvtCoefs<T>{});
+    box(LsPoissonCoefs<T>{});
+    all(LsResetKs{});
+    one(LsVbcs<T>{LB_X, 0, 0});
+    dot(0, OP_REF_NORMB);
+    for (;;) {
+      NvtxRange r_pass("lockstep_defect_correction_pass");
+      plan(0, 1);
+      if (any_periodic)
+        for (int comp = 0; comp < 3; ++comp) one(LsHalo<T>{LB_X, comp, 0, -1});
+      box(LsMatvecOuter<T>{});
+      e1(LsDefect<T>{});
+      dot(1, OP_REF_REL);
+      readback();
+      int nrun = 0, max_sw = 0;
+      for (int i = 0; i < ncase; ++i) {
+        LsCaseRun& r = cr[i];
+        LsDyn& d = h_dyn[i];
+        if (r.done) continue;
+        const double rel = h_read[i].true_rel;
+        r.rel = rel;
+        if (h_read[i].nan || std::isnan(rel)) {
+          r.status = FUGU_NAN;
+          r.done = true;
+        } else if (rel < r.tol) {
+          r.status = FUGU_CONVERGED;
+          r.done = true;
+        } else if (r.outer >= cases[i]->prm.refine_max_outer) {
+          r.status = FUGU_MAXITER;
+          r.done = true;
+        }
+        d.run = r.done ? 0 : 1;
+        if (!r.done) {
+          ++nrun;
+          max_sw = std::max(max_sw, d.sweeps);
+        }
+      }
+      if (!nrun) break;
+      upload_dyn();
+      plan(0, 1);
+      if constexpr (sizeof(T) == 4) e1(LsScaleDefect<T>{});
+      else e1(LsZeroCorrection<T>{});
+      fgmres_cycle(max_sw);
+      plan(0, 1);
+      if constexpr (sizeof(T) == 4) e1(LsAccumulate<T>{});
+      else e1(LsUpdate64<T>{});
+      readback();
+      int steps_run = 0;
+      for (int i = 0; i < ncase; ++i)
+        if (!cr[i].done) steps_run = std::max(steps_run, h_read[i].active ? m : h_read[i].exit_iter);
+      if (use_cycle_graph) launches += cyc.body * (unsigned long long)steps_run;
+      for (int i = 0; i < ncase; ++i) {
+        LsCaseRun& r = cr[i];
+        if (r.done) continue;
+        const fugu_params& p = cases[i]->prm;
+        const LsRead& rd = h_read[i];
+        r.inner_total += rd.active ? m : rd.exit_iter;
+        const double ir = rd.inner_rel;
+        LsDyn& d = h_dyn[i];
+        if (!(ir < p.refine_inner_tol)) {
+          if (r.adapt && r.cap < p.pcg_max_iter) {
+            r.cap = std::min(2 * r.cap, p.pcg_max_iter);
+            d.pcg_cap = r.cap;
+          } else if (r.adapt_sw && r.sweeps < p.pcd_sweeps_max) {
+            r.sweeps = std::min(2 * r.sweeps, p.pcd_sweeps_max);
+            d.sweeps = r.sweeps;
+          }
+        }
+        ++r.outer;
+      }
+      upload_dyn();
+      all(LsResetKs{});
+      one(LsVbcs<T>{LB_X, 0, 0});
+    }
+    // the lid of every case (refine_solve's final vbcs with has_lid)
+    for (int i = 0; i < ncase; ++i) h_dyn[i].run = 1;
+    upload_dyn();
+    plan(0, 1);
+    one(LsVbcs<T>{LB_X, 0, 1});
+    kr.assign(ncase, KrylovResult{});
+    outer.assign(ncase, 0);
+    for (int i = 0; i < ncase; ++i) {
+      fugu_ctx* c = cases[i];
+      LsCaseRun& r = cr[i];
+      if (r.adapt) c->pcg_cap_state = r.cap;
+      if (r.adapt_sw) c->pcd_sweeps_state = r.sweeps;
+      kr[i].iter = r.inner_total;
+      kr[i].res = r.rel;
+      kr[i].status = r.status;
+      outer[i] = r.outer;
+    }
+  }
+};
+
+}  // namespace

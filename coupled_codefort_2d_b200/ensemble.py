@@ -1,7 +1,8 @@
 """The batched ensemble across GPUs: independent cases sharded over ranks.
 
 One process per GPU (``torchrun``); every rank advances its own shard of the
-cases with a :class:`~coupled_codefort_2d_b200.batch.Batch` on its GPU.
+cases with a :class:`~coupled_codefort_2d_b200.batch.Batch` on its GPU (the
+lockstep form by default: one launch per kernel family for all its cases).
 Cases never exchange data, so the data path has no collective: the ranks
 meet only at the barriers around the timed region, in one max-reduction of
 the elapsed time, and in a final gather of per-case scalars (status,
@@ -58,12 +59,54 @@ def case_cost(spec: dict) -> float:
     return float(spec["grid"].ncells)
 
 
-def run_shard_gpu(specs, idx, nsteps, device, nthreads=0, precision=None, warmup=0, solver=None):
+def solve_bytes(spec: dict, steps: list, solver: dict | None = None, inner_bytes: int = 4) -> float:
+    """Algorithmic bytes of one case's coupled solves over its steps: each
+    distinct array read once and written once per kernel invocation, over the
+    case's nx * ny cells (N) and its 3N coupled unknowns.  Counted per step
+    from its statistics (``steps``: dicts with iter = Arnoldi steps, outer =
+    defect-correction passes, pcg_iters):
+
+    - PCG: 9 values per cell and iteration (reads of p, cx, cy, dinv, phi, r;
+      writes of p, phi, r);
+    - per Arnoldi step j (taken as the mean j of a cycle of ``iter / outer``
+      steps): PCD Schur step 6 values, residual update 5, cross term 4,
+      zeroing 4; the velocity smoother at least ``pcd_sweeps`` sweeps of both
+      components at 7 values per face (u, rhs, rho, kappa, zeta, eta read, u
+      written; the adaptive count can only be higher); the coupled matvec 14
+      values; classical Gram-Schmidt twice: (j + 2) vectors read by each dot,
+      (j + 3) moved by each update, the norm and the scaling of the new basis
+      vector (3 vectors);
+    - per outer pass: the FP64 matvec (14 values at 8 B), the defect and its
+      norm (4 FP64 vectors), its conversion and the accumulation.
+
+    A lower bound where counts are not reported (the smoother's adaptive
+    sweeps), exact otherwise."""
+    sv = SOLVER if solver is None else solver
+    n = float(spec["grid"].ncells)
+    n3 = 3.0 * n
+    b = float(inner_bytes)
+    sweeps = sv.get("pcd_sweeps", 6)
+    total = 0.0
+    for st in steps:
+        a = float(st["iter"])
+        outer = max(int(st["outer"]), 1)
+        jbar = 0.5 * (a / outer - 1.0) if a > 0 else 0.0
+        pcd = (6 + 5 + 4 + 4) * n * b + 2 * sweeps * 7 * n * b
+        matvec = 14 * n * b
+        cgs2 = (2 * (jbar + 2) + 2 * (jbar + 3) + 1 + 3) * n3 * b
+        total += a * (pcd + matvec + cgs2) + 9 * n * b * float(st["pcg_iters"])
+        total += outer * (14 * n * 8 + 4 * n3 * 8 + n3 * (8 + 4) + n3 * (8 + 8 + 4))
+    return total
+
+
+def run_shard_gpu(specs, idx, nsteps, device, nthreads=0, precision=None, warmup=0, solver=None, lockstep=True):
     """Advance the cases ``idx`` on ``device`` and return their per-case
-    scalars and the elapsed seconds of the stepping (barrier-free; the caller
-    brackets it).  ``warmup`` untimed steps come first (work space
-    allocation, the adaptive PCG cap settling).  ``solver`` overrides the
-    solver settings (default ``SOLVER``)."""
+    scalars and the elapsed seconds of the stepping, timed with CUDA events
+    on the batch stream (barrier-free; the caller brackets it).  ``warmup``
+    untimed steps come first (work space allocation, the adaptive PCG cap
+    settling).  ``solver`` overrides the solver settings (default
+    ``SOLVER``); ``lockstep`` selects the lockstep batch (one launch per
+    kernel family for all cases) over the thread-pool batch."""
     import torch
 
     from ._lib import MIXED
@@ -77,24 +120,39 @@ def run_shard_gpu(specs, idx, nsteps, device, nthreads=0, precision=None, warmup
         return
     sv = SOLVER if solver is None else solver
     with Batch([(s["grid"], ensemble_params(s, **sv), prec) for s in sub], device=device,
-               nthreads=nthreads) as b:
+               nthreads=nthreads, lockstep=lockstep) as b:
         for k, s in enumerate(sub):
             initial_bubble_state(b.case(k), s)
         opts = b.case(0).step_opts(use_bicgstab2=True)
         if warmup:
             b.run(warmup, DT, 1, opts)
         torch.cuda.synchronize(device)
+        stream = torch.cuda.ExternalStream(b.stream_handle(), device=f"cuda:{device}")
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
         yield "ready", None
+        n0 = b.launches()
         t0 = time.perf_counter()
-        out = b.run(nsteps, DT, warmup + 1, opts)
+        e0.record(stream)
+        outs = [b.run(1, DT, warmup + 1 + k, opts) for k in range(nsteps)]
+        e1.record(stream)
+        e1.synchronize()
+        elapsed = e0.elapsed_time(e1) / 1000.0
+        wall = time.perf_counter() - t0
+        launches = b.launches() - n0
         torch.cuda.synchronize(device)
-        elapsed = time.perf_counter() - t0
         rows = []
         for k, s in enumerate(sub):
             st = b.case(k).download_state(["c_field", "v_vel"])
             ycm, vr = cases.bubble_centroid_velocity(s["grid"], st["c_field"], st["v_vel"])
-            rows.append({"case": s["case"], "status": out["status"][k], "max_res": out["max_res"][k],
-                         "last_iter": out["last"][k]["iter"], "y_centroid": ycm, "rise_velocity": vr})
+            steps = [o["last"][k] for o in outs]
+            rows.append({"case": s["case"], "status": max((o["status"][k] for o in outs), key=abs),
+                         "max_res": max(o["max_res"][k] for o in outs),
+                         "arnoldi_steps": sum(x["iter"] for x in steps), "outer": sum(x["outer"] for x in steps),
+                         "pcg_iters": sum(x["pcg_iters"] for x in steps),
+                         "bytes": solve_bytes(s, steps, sv, 4 if prec == MIXED else 8),
+                         "y_centroid": ycm, "rise_velocity": vr, "host_wall_s": wall,
+                         "shard_launches": launches})
         yield "done", (rows, elapsed)
 
 
@@ -120,8 +178,10 @@ def run_ensemble(specs, nsteps, rank, world, runner, barrier, max_reduce, gather
     if rank != 0:
         return None
     merged = sorted((r for part in all_rows for r in part), key=lambda r: r["case"])
+    total_bytes = sum(r.get("bytes", 0.0) for r in merged)
     return {"cases": len(specs), "steps": nsteps, "world": world, "seconds": slowest,
             "case_steps_per_s": len(specs) * nsteps / slowest if slowest > 0 else float("inf"),
+            "algorithmic_gb_per_s": total_bytes / slowest / 1e9 if slowest > 0 else 0.0,
             "shard_cells": [sum(specs[i]["grid"].ncells for i in s) for s in shards], "rows": merged}
 
 
@@ -172,6 +232,8 @@ def main(argv=None):
     ap.add_argument("--sweeps-max", type=int, default=None, help="adaptive sweeps ceiling (0: fixed)")
     ap.add_argument("--graphs", type=int, choices=[0, 1], default=None,
                     help="replay the Arnoldi steps from CUDA graphs (default: the SOLVER setting)")
+    ap.add_argument("--thread-pool", action="store_true",
+                    help="step the cases from host threads instead of in lockstep")
     args = ap.parse_args(argv)
     solver = solver_from_args(args)
     import datetime
@@ -191,7 +253,7 @@ def main(argv=None):
     specs = cases.bubble_ensemble(args.cases, seed=args.seed)
     res = run_ensemble(specs, args.steps, rank, world,
                        lambda idx: run_shard_gpu(specs, idx, args.steps, local, args.threads, warmup=args.warmup,
-                                                 solver=solver),
+                                                 solver=solver, lockstep=not args.thread_pool),
                        barrier, max_reduce, gather)
     if world > 1:
         dist.destroy_process_group()
@@ -199,6 +261,8 @@ def main(argv=None):
         rows = res.pop("rows")
         res["failed"] = [r["case"] for r in rows if r["status"] != 0]
         res["max_res"] = max(r["max_res"] for r in rows)
+        res["form"] = "thread pool" if args.thread_pool else "lockstep"
+        res["launches_rank0"] = rows[0].get("shard_launches") if rows else None
         res["solver"] = solver
         print(json.dumps(res), flush=True)
         if args.out:

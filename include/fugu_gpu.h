@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define FUGU_ABI_VERSION 2
+#define FUGU_ABI_VERSION 3
 
 /* return codes */
 #define FUGU_OK 0
@@ -377,6 +377,16 @@ typedef struct {
   int max_cluster;  /* CTAs of each cluster-resident PCG, 1..16 (0: autotune)     */
   int max_coop;     /* CTAs of each grid-wide persistent kernel, launched as one  */
                     /* thread-block cluster so that it is scheduled whole (<= 8; 0: 8) */
+  int lockstep;     /* 1: the coupled solves of all cases advance in lockstep,
+                       one launch per kernel family serving every case still
+                       running (work lists of (case, tile) items on the device,
+                       per-case Krylov scalars and activity flags, each
+                       flexible-GMRES cycle one CUDA graph whose Arnoldi steps
+                       are conditional nodes armed on the device); needs every
+                       case at refine = 2 with one precision, pcd_smoother and
+                       refine_max_inner, and a PCG that fits a cluster; at most
+                       1024 cases.  Each case's results equal those of the
+                       thread-pool form (0) bit for bit.                      */
 } fugu_batch_opts;
 int fugu_batch_create(const fugu_params* params, int ncases, int device, const fugu_batch_opts* opts,
                       fugu_batch** out);
@@ -391,6 +401,14 @@ int fugu_batch_case(fugu_batch* b, int i, fugu_ctx** ctx);
  * that stopped it.  Returns FUGU_OK, or the first failing case's code. */
 int fugu_batch_run(fugu_batch* b, int nsteps, const double* dt, const int* step0, const fugu_step_opts* opts,
                    fugu_stats* last, double* max_res, int* status);
+/* The batch stream (cudaStream_t): all device work of a fugu_batch_run
+ * starts after the work queued on it before the call and ends before the
+ * work queued on it after the call, so CUDA events recorded on it around a
+ * run time the run on the device.  No counterpart in the reference. */
+int fugu_batch_get_stream(fugu_batch* b, void** stream);
+/* Kernel launches the batch has issued so far, replays of CUDA graphs
+ * included (a measurement counter; no counterpart in the reference). */
+unsigned long long fugu_batch_launches(const fugu_batch* b);
 
 /* ------------------------------------------------ allocation-free entry
  * solve_poisson_pressure (mod_subsolvers.f90:32-246) with no context and no

@@ -25,7 +25,8 @@ def libpath():
 def header_functions():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:int|void|const char\s*\*)\s+(fugu_\w+)\s*\(", src, flags=re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|void|const char\s*\*|unsigned long long)\s+(fugu_\w+)\s*\(", src,
+                                 flags=re.M)))
 
 
 def test_header_declares_the_hot_path_entries():

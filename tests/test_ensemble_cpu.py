@@ -94,3 +94,20 @@ def test_solver_overrides_from_the_command_line():
     s = solver_from_args(a)
     assert (s["pcd_smoother"], s["pcd_sweeps"], s["pcd_sweeps_max"], s["graphs"]) == (0, 3, 0, 0)
     assert s["pcd_sor_omega"] == SOLVER["pcd_sor_omega"] and SOLVER["pcd_sweeps"] == 6  # the default is untouched
+
+
+def test_solve_bytes_counts_each_kernel_family():
+    """The batched roofline's algorithmic bytes, by hand for one step of a
+    64 x 128 case: 40 Arnoldi steps in 2 passes (mean j = 9.5), 1000 PCG
+    iterations, FP32 inner solve, 6 smoother sweeps."""
+    from coupled_codefort_2d_b200.ensemble import solve_bytes
+    from coupled_codefort_2d_b200.layout import Grid
+
+    spec = {"grid": Grid(64, 128)}
+    n = 64 * 128.0
+    n3 = 3 * n
+    per_arnoldi = (19 * n + 2 * 6 * 7 * n + 14 * n + (2 * 11.5 + 2 * 12.5 + 4) * n3) * 4
+    per_outer = 14 * n * 8 + 4 * n3 * 8 + 12 * n3 + 20 * n3
+    want = 40 * per_arnoldi + 9 * n * 4 * 1000 + 2 * per_outer
+    got = solve_bytes(spec, [{"iter": 40, "outer": 2, "pcg_iters": 1000}], {"pcd_sweeps": 6}, 4)
+    assert abs(got - want) <= 1e-9 * want
