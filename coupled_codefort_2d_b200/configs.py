@@ -179,9 +179,54 @@ def _fd_check(ad, fd):
             "rel_difference": float(abs(ad - fd) / max(abs(fd), 1e-300))}
 
 
+def smooth_interface_direction(pb):
+    """A smooth perturbation of the initial colour on the interface cells
+    (0.02 < C0 < 0.98), zero on pure cells and ghosts, unit maximum: C0 +- h
+    times it stays inside (0, 1) for h < 0.02, so no cell crosses the clip."""
+    g = pb.g
+    ci = at(pb.c0, "cell", slice(1, g.nx), slice(1, g.ny))
+    X, Y = cases.cell_centres_interior(g)
+    w = ci * (1.0 - ci) * (1.0 + 0.5 * np.cos(2.0 * np.pi * X) * np.sin(np.pi * Y))
+    w[(ci <= 0.02) | (ci >= 0.98)] = 0.0
+    out = g.zeros("cell")
+    at(out, "cell", slice(1, g.nx), slice(1, g.ny))[...] = w / np.max(w)
+    return out
+
+
+def _h_sweep(pb, grads, dc0, hs):
+    """Central differences of J at each h against the adjoint: sigma and mu1
+    (h relative to the value) and the smooth interface direction of C0 (h
+    absolute, the direction's maximum being 1)."""
+    out = {}
+    for name in ("sigma", "mu1"):
+        v0 = pb.phys[name]
+        rows = []
+        for hr in hs:
+            h = hr * v0
+            fd = (pb.value(**{name: v0 + h}) - pb.value(**{name: v0 - h})) / (2 * h)
+            rows.append({"h_relative": hr, "central_difference": fd,
+                         "relative_difference": abs(grads[name] - fd) / abs(fd)})
+        out[f"d{name}"] = {"adjoint": float(grads[name]), "sweep": rows}
+    d = smooth_interface_direction(pb)
+    ad = float(np.sum(dc0 * d))
+    rows = []
+    for h in hs:
+        fd = (pb.value(c0=pb.c0 + h * d) - pb.value(c0=pb.c0 - h * d)) / (2 * h)
+        rows.append({"h": h, "central_difference": fd, "relative_difference": abs(ad - fd) / abs(fd)})
+    out["dC0_along_smooth_interface_direction"] = {"adjoint": ad, "sweep": rows}
+    return out
+
+
 def config_c5(args):
     from .adjoint import RisingBubble, SteadyPoiseuille, analytic_grad
 
+    if args.sweep:
+        # the h sweep at a smaller size (each central difference is two forward runs)
+        steps = args.steps or 100
+        pb = RisingBubble(80, 160, nsteps=steps, T=steps * 2.5e-3, checkpoint=20, tol=1e-12, device=args.device)
+        J, grads, dc0 = pb.value_and_grad()
+        return {"config": "c5", "workload": f"rising_bubble_adjoint_80x160_{steps}_steps_h_sweep", "J": J,
+                "checks": _h_sweep(pb, grads, dc0, (1e-8, 1e-7, 1e-6, 1e-5, 1e-4, 1e-3))}
     steps = args.steps or 400
     pb = RisingBubble(160, 320, nsteps=steps, T=steps * 2.5e-3, checkpoint=20, tol=1e-12, device=args.device)
     g = pb.g
@@ -268,6 +313,8 @@ def main(argv=None):
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--n", type=int, default=2048, help="scale only: cells per side")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="scale only")
+    ap.add_argument("--sweep", action="store_true",
+                    help="c5 only: central differences over h = 1e-8 .. 1e-3 at 80 x 160 (the plateau)")
     args = ap.parse_args(argv)
     if args.config == "c4":  # the ensemble runner prints its own report
         from . import ensemble

@@ -1,0 +1,172 @@
+"""Parity at the benchmark configurations' own horizons and tolerances, with
+the error against the FP64 oracle stated per result.
+
+- c2, static droplet 256^2, BDF2, dt = 1e-4: 50 steps of the mixed form
+  (FP32 inner, FP64 defect correction to 1e-8) against the FP64 oracle on the
+  same steps and tolerance; u, v, p within the mixed bound 1e-6 relative L2,
+  fluid-1 volume equal to 1e-12 relative (VOF transport is FP64 in both).
+- c4, the batched ensemble: the first case of each grid class (64x128 ..
+  256x512) with the ensemble's own solver (flexible GMRES + PCD with the
+  viscous Schur term and red-black SOR, adaptive cap and sweeps), 2 steps of
+  the lockstep batch in mixed precision against the FP64 oracle; the same
+  bounds as c2.
+- c3, rising bubble 320 x 640, free-slip sides, BDF2, dt = 5e-4: to t = 0.1
+  (200 steps), mixed against FP64 on the GPU; centroid height and rise
+  velocity (test_rising_bubble.f90:134-155) and circularity within 1e-6
+  relative of the FP64 run.
+- c1, lid-driven cavity 128^2, Re = 1000, BDF1, dt = 1e-2: all 200 steps at
+  the configuration's tolerance 1e-10, FP64 GPU against the FP64 oracle; u, v
+  and p (mean removed) within 1e-8 relative L2.
+
+Each comparison's errors are printed (pytest -s shows them).  The oracle runs
+in background threads (its ctypes calls release the GIL) while the GPU runs,
+so the module costs about the oracle's longest run (c1, ~4 minutes on one
+host core), which is why c1 comes last.
+"""
+import concurrent.futures as cf
+
+import numpy as np
+import pytest
+
+from coupled_codefort_2d_b200 import cases, ensemble
+from coupled_codefort_2d_b200._lib import FP64, MIXED
+from coupled_codefort_2d_b200.batch import STATE_FIELDS, Batch, ensemble_params, initial_bubble_state
+from coupled_codefort_2d_b200.configs import SOLVER
+from coupled_codefort_2d_b200.context import Context
+from coupled_codefort_2d_b200.layout import Grid, at
+from coupled_codefort_2d_b200.params import Params
+
+pytestmark = [pytest.mark.gpu, pytest.mark.slow]
+
+STATE = list(STATE_FIELDS)
+MIXED_BOUND = 1e-6
+C4_STEPS = 2
+
+
+def c1_case():
+    g = Grid(128, 128)
+    p = Params(rho1=1.0, rho2=1.0, mu1=1e-3, mu2=1e-3, sigma=0.0, gx=0.0, gy=0.0, time_order=1,
+               tol_bicgstab2=1e-10, max_iter_bicgstab2=500, **SOLVER)
+    return g, p, g.full("cell", 1.0), 1e-2, 200, dict(u_top_lid=1.0)
+
+
+def c2_case():
+    g = Grid(256, 256)
+    p = Params(rho1=1.0, rho2=0.1, mu1=0.1, mu2=0.01, sigma=1.0, gx=0.0, gy=0.0, time_order=2,
+               tol_bicgstab2=1e-8, max_iter_bicgstab2=500, **SOLVER)
+    return g, p, cases.circle_fraction(g, 0.5, 0.5, 0.25, inside=1.0, ns=16), 1e-4, 50, {}
+
+
+def c4_cases():
+    """the first ensemble case of each grid class"""
+    first = {}
+    for s in cases.bubble_ensemble(256):
+        first.setdefault((s["grid"].nx, s["grid"].ny), s)
+    return [first[k] for k in sorted(first)]
+
+
+def oracle_run(oracle_mod, g, p, c0, dt, nsteps, kw):
+    st = oracle_mod.new_state(g, c0, p)
+    o = oracle_mod.Oracle(g, p)
+    stats = [o.step(st, dt, s, **kw) for s in range(1, nsteps + 1)]
+    return st, [(s.res, s.iter) for s in stats]
+
+
+@pytest.fixture(scope="module")
+def oracle_runs(oracle_mod):
+    """Every oracle run of the module, started at once in host threads."""
+    pool = cf.ThreadPoolExecutor(max_workers=8)
+    jobs = {"c1": pool.submit(oracle_run, oracle_mod, *c1_case()),
+            "c2": pool.submit(oracle_run, oracle_mod, *c2_case())}
+    for s in c4_cases():
+        g = s["grid"]
+        p = ensemble_params(s, **ensemble.SOLVER)
+        c0 = cases.binary_circle(g, s["xc"], s["yc"], s["radius"], inside=0.0)
+        jobs[("c4", s["case"])] = pool.submit(oracle_run, oracle_mod, g, p, c0, ensemble.DT, C4_STEPS, {})
+    yield jobs
+    pool.shutdown(wait=True)
+
+
+def gpu_run(oracle_mod, g, p, c0, dt, nsteps, kw, precision):
+    st = {k: a.copy(order="F") for k, a in oracle_mod.new_state(g, c0, p).items()}
+    with Context(g, p, precision=precision) as ctx:
+        ctx.upload_state(st)
+        o = ctx.step_opts(use_bicgstab2=True, **kw)
+        stats = [ctx.step(dt, s, o) for s in range(1, nsteps + 1)]
+        return ctx.download_state(STATE), stats
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def errors(g, st_g, st_o):
+    def p0(p):
+        pi = at(p, "cell", slice(1, g.nx), slice(1, g.ny))
+        return pi - pi.mean()
+
+    vo, vg = cases.fluid1_volume(g, st_o["c_field"]), cases.fluid1_volume(g, st_g["c_field"])
+    return {"u": rel(st_g["u_vel"], st_o["u_vel"]), "v": rel(st_g["v_vel"], st_o["v_vel"]),
+            "p": rel(p0(st_g["p_field"]), p0(st_o["p_field"])), "volume": abs(vg - vo) / abs(vo)}
+
+
+def test_c2_droplet_50_steps_mixed(gpu, oracle_mod, oracle_runs):
+    g, p, c0, dt, n, kw = c2_case()
+    st_g, sg = gpu_run(oracle_mod, g, p, c0, dt, n, kw, MIXED)
+    st_o, so = oracle_runs["c2"].result()
+    assert all(s["status"] == 0 and s["res"] < 1e-8 for s in sg)
+    e = errors(g, st_g, st_o)
+    print("c2 droplet 256^2, 50 BDF2 steps at 1e-8, mixed GPU vs FP64 oracle:", e)
+    assert max(e["u"], e["v"], e["p"]) <= MIXED_BOUND, e
+    assert e["volume"] <= 1e-12, e
+
+
+def test_c4_one_case_per_grid_class_lockstep_mixed(gpu, oracle_mod, oracle_runs):
+    specs = c4_cases()
+    prms = [ensemble_params(s, **ensemble.SOLVER) for s in specs]
+    with Batch([(s["grid"], p, MIXED) for s, p in zip(specs, prms)], lockstep=True) as b:
+        for i, s in enumerate(specs):
+            initial_bubble_state(b.case(i), s)
+        out = b.run(C4_STEPS, ensemble.DT, 1, b.case(0).step_opts(use_bicgstab2=True))
+        states = [b.case(i).download_state(STATE) for i in range(len(specs))]
+    assert out["status"] == [0] * len(specs)
+    for i, s in enumerate(specs):
+        st_o, so = oracle_runs[("c4", s["case"])].result()
+        assert out["max_res"][i] < 1e-8 and all(r < 1e-8 for r, _ in so)
+        e = errors(s["grid"], states[i], st_o)
+        print(f"c4 case {s['case']} {s['grid'].nx}x{s['grid'].ny}, {C4_STEPS} steps, lockstep mixed vs FP64 "
+              f"oracle:", e)
+        assert max(e["u"], e["v"], e["p"]) <= MIXED_BOUND, (s["case"], e)
+        assert e["volume"] <= 1e-12, (s["case"], e)
+
+
+def test_c3_bubble_mixed_vs_fp64_diagnostics(gpu, oracle_mod):
+    g = Grid(320, 640, 1.0, 2.0)
+    p = Params(rho1=1000.0, rho2=100.0, mu1=10.0, mu2=1.0, sigma=24.5, gx=0.0, gy=-0.98, time_order=2,
+               tol_bicgstab2=1e-8, max_iter_bicgstab2=500, free_slip_x=1, **SOLVER)
+    c0 = cases.binary_circle(g, 0.5, 0.5, 0.25, inside=0.0)
+    n = 200  # t = 0.1
+    res = {}
+    for prec in (FP64, MIXED):
+        st, stats = gpu_run(oracle_mod, g, p, c0, 5e-4, n, {}, prec)
+        assert all(s["status"] == 0 and s["res"] < 1e-8 for s in stats)
+        ycm, vr = cases.bubble_centroid_velocity(g, st["c_field"], st["v_vel"])
+        res[prec] = (ycm, vr, cases.circularity(g, st["c_field"]))
+    (y64, v64, c64), (y32, v32, c32) = res[FP64], res[MIXED]
+    e = {"centroid": abs(y32 - y64) / abs(y64), "rise_velocity": abs(v32 - v64) / abs(v64),
+         "circularity": abs(c32 - c64) / abs(c64)}
+    print("c3 rising bubble 320x640 to t = 0.1, mixed vs FP64:", e, "FP64 values:", res[FP64])
+    assert y64 > 0.5 and v64 > 0.0
+    assert max(e.values()) <= MIXED_BOUND, e
+
+
+# last: its oracle run (the longest) overlaps with the GPU work of the tests above
+def test_c1_cavity_200_steps_fp64(gpu, oracle_mod, oracle_runs):
+    g, p, c0, dt, n, kw = c1_case()
+    st_g, sg = gpu_run(oracle_mod, g, p, c0, dt, n, kw, FP64)
+    st_o, so = oracle_runs["c1"].result()
+    assert all(s["status"] == 0 and s["res"] < 1e-10 for s in sg)
+    assert all(r < 1e-10 for r, _ in so)
+    e = errors(g, st_g, st_o)
+    print("c1 cavity 128^2, 200 BDF1 steps at 1e-10, FP64 GPU vs FP64 oracle:", e)
+    assert max(e["u"], e["v"], e["p"]) <= 1e-8, e

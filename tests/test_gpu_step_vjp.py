@@ -182,3 +182,32 @@ def test_step_vjp_rejects_unsupported_cases(gpu):
     with Context(g, Params(sigma=1.0)) as ctx:
         with pytest.raises(FuguError):
             ctx.step_vjp(1e-3, 1, ctx.step_opts(consistent_amp=True), {})
+
+
+@pytest.mark.slow
+def test_bubble_gradient_c5_like_size(gpu):
+    """The rising-bubble gradient at a size like the adjoint configuration's
+    (80 x 160, 100 BDF2 steps of dt = 2.5e-3, checkpoints every 20, FP64
+    solves to 1e-12): dJ/dsigma, dJ/dmu1 and the derivative along a smooth
+    interface direction of C0, each within 1e-6 relative of the central
+    difference at h = 1e-4 (relative for the parameters, absolute along the
+    unit-maximum direction), the plateau of the h sweep: smaller h lets the
+    solver noise of J (~1e-14) through, larger h the curvature of J."""
+    from coupled_codefort_2d_b200.configs import smooth_interface_direction
+
+    pb = RisingBubble(nx=80, ny=160, nsteps=100, T=100 * DT, checkpoint=20, tol=1e-12)
+    J, grads, dc0 = pb.value_and_grad()
+    assert J > 0.5
+    for name in ("sigma", "mu1"):
+        v0 = pb.phys[name]
+        h = 1e-4 * v0
+        fd = (pb.value(**{name: v0 + h}) - pb.value(**{name: v0 - h})) / (2 * h)
+        print(f"dJ/d{name}: adjoint {grads[name]:.12e}, central difference {fd:.12e}, "
+              f"relative {abs(grads[name] - fd) / abs(fd):.2e}")
+        assert abs(grads[name] - fd) <= 1e-6 * abs(fd), (name, grads[name], fd)
+    d = smooth_interface_direction(pb)
+    h = 1e-4
+    fd = (pb.value(c0=pb.c0 + h * d) - pb.value(c0=pb.c0 - h * d)) / (2 * h)
+    ad = float(np.sum(dc0 * d))
+    print(f"dJ/dC0 . dir: adjoint {ad:.12e}, central difference {fd:.12e}, relative {abs(ad - fd) / abs(fd):.2e}")
+    assert abs(ad - fd) <= 1e-6 * abs(fd), (ad, fd)
