@@ -230,7 +230,11 @@ def gpu_arm(args, rank, world, local_rank):
     out = {"t_mixed": t_mixed, "s_mixed": s_mixed, "prof": prof, "total_ms": total_ms, "clocks": sampler.summary()}
 
     if not args.quick:  # every rank: the ensemble is sharded over the ranks
-        out["batched"] = batched_arm(world, rank, local_rank)
+        peaks = {}
+        pk = os.path.join(ROOT, "MEASURED_PEAKS.json")
+        if os.path.exists(pk):
+            peaks = json.load(open(pk))
+        out["batched"] = batched_arm(world, rank, local_rank, peaks)
 
     if rank == 0 and not args.quick:
         # FP64 inner form of the same solver, same steps
@@ -256,21 +260,55 @@ def gpu_arm(args, rank, world, local_rank):
     return out
 
 
-BATCH_CASES_PER_GPU = 32
-BATCH_STEPS = 2
+# the batched line: the whole rising-bubble ensemble of the configuration
+# (256 cases per GPU), lockstep mixed form, device-timed steps after warm-up
+BATCH_CASES_PER_GPU = 256
+BATCH_STEPS, BATCH_WARMUP = 20, 2
+# the like-for-like comparison with the plain FP64 single-case form: the same
+# cases and the same steps in both forms
+SAME_CASES, SAME_STEPS, SAME_WARMUP = 32, 3, 1
 
 
-def batched_arm(world, rank, local_rank):
-    """The batched form on the rising-bubble ensemble (first 32 x N cases of
-    the seeded ensemble, grids 64x128 .. 256x512, density ratios 10-1000),
-    sharded over the N ranks, mixed precision; beside it, on rank 0, the
-    plain FP64 single-case form on the first cases, one context at a time."""
+def _fp64_single(specs, steps, warmup, local_rank):
+    """The plain FP64 form of the same solver, one context at a time: CUDA
+    events on each context's stream around its timed steps, summed."""
     import torch
 
-    from coupled_codefort_2d_b200 import cases, ensemble
+    from coupled_codefort_2d_b200 import ensemble
     from coupled_codefort_2d_b200._lib import FP64
     from coupled_codefort_2d_b200.batch import ensemble_params, initial_bubble_state
     from coupled_codefort_2d_b200.context import Context
+
+    ms, n, res = 0.0, 0, 0.0
+    for s in specs:
+        with Context(s["grid"], ensemble_params(s, **ensemble.SOLVER), device=local_rank, precision=FP64) as ctx:
+            initial_bubble_state(ctx, s)
+            o = ctx.step_opts(use_bicgstab2=True)
+            for k in range(1, warmup + 1):
+                ctx.step(ensemble.DT, k, o)
+            stream = torch.cuda.ExternalStream(ctx.stream_handle(), device=f"cuda:{local_rank}")
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for k in range(warmup + 1, warmup + steps + 1):
+                r = ctx.step(ensemble.DT, k, o)
+                res = max(res, r["res"])
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            n += steps
+    return {"value": 1000.0 * n / ms, "unit": "case-steps/s", "case_steps": n, "max_true_residual": res}
+
+
+def batched_arm(world, rank, local_rank, peaks):
+    """The batched form on the rising-bubble ensemble of the configuration
+    (256 x N cases of the seeded ensemble, grids 64x128 .. 256x512, density
+    ratios 10-1000), sharded over the N ranks, lockstep mixed precision,
+    device-timed.  Beside it, on rank 0, the same comparison on equal work:
+    the first 32 cases, the same steps, lockstep mixed against the plain
+    FP64 single-case form one context at a time."""
+    from coupled_codefort_2d_b200 import cases, ensemble
 
     specs = cases.bubble_ensemble(BATCH_CASES_PER_GPU * world)
     if world > 1:
@@ -279,38 +317,43 @@ def batched_arm(world, rank, local_rank):
         barrier, max_reduce, gather = (lambda: None), (lambda x: x), (lambda o: [o])
     res = ensemble.run_ensemble(
         specs, BATCH_STEPS, rank, world,
-        lambda idx: ensemble.run_shard_gpu(specs, idx, BATCH_STEPS, local_rank, nthreads=0, warmup=1),
+        lambda idx: ensemble.run_shard_gpu(specs, idx, BATCH_STEPS, local_rank, nthreads=0, warmup=BATCH_WARMUP),
         barrier, max_reduce, gather)
     if rank != 0:
         return None
     rows = res.pop("rows")
-    # plain FP64 form, one case at a time, on the same cases with the same
-    # solver, warm-up and timed steps as the batch
-    n64, t64 = 0, 0.0
-    for s in specs:
-        with Context(s["grid"], ensemble_params(s, **ensemble.SOLVER), device=local_rank, precision=FP64) as ctx:
-            initial_bubble_state(ctx, s)
-            o = ctx.step_opts(use_bicgstab2=True)
-            ctx.step(ensemble.DT, 1, o)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            for k in range(BATCH_STEPS):
-                ctx.step(ensemble.DT, 2 + k, o)
-            torch.cuda.synchronize()
-            t64 += time.perf_counter() - t0
-            n64 += BATCH_STEPS
-    fp64_single = n64 / t64
-    return {"workload": f"rising_bubble_ensemble_{len(specs)} (seed {cases.ENSEMBLE_SEED}, first cases)",
-            "value": res["case_steps_per_s"], "unit": "case-steps/s", "steps": BATCH_STEPS, "warmup": 1,
-            "seconds": res["seconds"], "dtype": "f32 inner / f64 outer", "max_true_residual":
-            max(r["max_res"] for r in rows), "failed_cases": [r["case"] for r in rows if r["status"] != 0],
-            "solver": "FP64 defect correction around flexible GMRES(30) + PCD with the viscous Schur term (PCG cap "
-                      "adaptive 40-150, red-black SOR velocity smoother omega 1.5, sweeps adaptive 6-24)",
-            "solver_params": ensemble.SOLVER,
-            "fp64_single_case": {"value": fp64_single, "unit": "case-steps/s", "case_steps": n64,
-                                 "cases": "the same cases, steps and solver, one context at a time, FP64"},
-            "batched_mixed_over_fp64_single": res["case_steps_per_s"] / world / fp64_single,
-            "timing": "host wall clock around the batch run, CUDA-synchronised, max over ranks"}
+    peak = (peaks or {}).get("hbm_gbs")
+    src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    out = {"workload": f"rising_bubble_ensemble_{len(specs)} (seed {cases.ENSEMBLE_SEED})",
+           "value": res["case_steps_per_s"], "unit": "case-steps/s", "steps": BATCH_STEPS, "warmup": BATCH_WARMUP,
+           "seconds": res["seconds"], "dtype": "f32 inner / f64 outer",
+           "max_true_residual": max(r["max_res"] for r in rows),
+           "failed_cases": [r["case"] for r in rows if r["status"] != 0],
+           "solver": "lockstep batch: FP64 defect correction around flexible GMRES(30) + PCD with the viscous Schur "
+                     "term (PCG cap adaptive 40-150, red-black SOR velocity smoother omega 1.5, sweeps adaptive "
+                     "6-24), one launch per kernel family for all running cases",
+           "solver_params": ensemble.SOLVER,
+           "gpu_launches_rank0": rows[0].get("shard_launches"),
+           "roofline": {"bound": "hbm", "achieved": res["algorithmic_gb_per_s"] / world, "peak": peak,
+                        "peak_source": src, "unit": "GB/s", "frac": res["algorithmic_gb_per_s"] / world / peak,
+                        "traffic": None,
+                        "bytes": "algorithmic bytes of every case's solves (ensemble.solve_bytes: PCG iterations, "
+                                 "Arnoldi steps with PCD, matvec and Gram-Schmidt, outer passes; smoother sweeps at "
+                                 "their minimum) / device time, per GPU"},
+           "timing": "CUDA events on the batch stream around the timed steps, max over ranks"}
+    if world == 1:
+        same = specs[:SAME_CASES]
+        r2 = ensemble.run_ensemble(
+            same, SAME_STEPS, 0, 1,
+            lambda idx: ensemble.run_shard_gpu(same, idx, SAME_STEPS, local_rank, nthreads=0, warmup=SAME_WARMUP),
+            barrier, max_reduce, gather)
+        f64 = _fp64_single(same, SAME_STEPS, SAME_WARMUP, local_rank)
+        out["equal_work"] = {"cases": len(same), "steps": SAME_STEPS, "warmup": SAME_WARMUP,
+                             "lockstep_mixed": r2["case_steps_per_s"], "fp64_single_case": f64,
+                             "lockstep_mixed_over_fp64_single": r2["case_steps_per_s"] / f64["value"],
+                             "note": "the same cases and steps in both forms, device-timed"}
+    return out
 
 
 class _Null:

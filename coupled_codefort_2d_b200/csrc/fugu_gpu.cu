@@ -621,17 +621,17 @@ void helmholtz(fugu_ctx* c, bool is_u, T* sol, T* tmp, const T* rhs, const CoefB
   T* nxt = tmp;
   const T* pen = o.pen ? (is_u ? cb.pen_u : cb.pen_v) : nullptr;
   if (c->prm.pcd_smoother == 1 && !c->g.px && !c->g.py) {
-    // red-black SOR, both colours of a sweep in one launch (extension)
+    // red-black SOR, both colours of a sweep in one launch, alternating
+    // between sol and tmp (extension)
     const dim3 grid((c->g.P + RB_TX - 1) / RB_TX, (c->g.R + RB_TY - 1) / RB_TY);
     for (int s = 0; s < n_sweeps; ++s) {
-      if (is_u)
-        k_rbsor_sweep<T><<<grid, RB_TPB, 0, c->s>>>(c->g, 0, sol, rhs, cb.rho_u, cb.kappa, cb.zeta, cb.eta, pen,
-                                                    T(dt), T(c->prm.pcd_sor_omega), active);
-      else
-        k_rbsor_sweep<T><<<grid, RB_TPB, 0, c->s>>>(c->g, 1, sol, rhs, cb.rho_v, cb.kappa, cb.zeta, cb.eta, pen,
-                                                    T(dt), T(c->prm.pcd_sor_omega), active);
+      k_rbsor_sweep<T><<<grid, RB_TPB, 0, c->s>>>(c->g, is_u ? 0 : 1, cur, nxt, rhs, is_u ? cb.rho_u : cb.rho_v,
+                                                  cb.kappa, cb.zeta, cb.eta, pen, T(dt), T(c->prm.pcd_sor_omega),
+                                                  active);
       CKL("k_rbsor_sweep");
+      std::swap(cur, nxt);
     }
+    if (cur != sol) CK(cudaMemcpyAsync(sol, cur, sizeof(T) * c->n, cudaMemcpyDeviceToDevice, c->s));
     return;
   }
   if (c->prm.pcd_smoother == 1) {  // red-black SOR in place, one launch per colour (periodic cases)

@@ -577,16 +577,20 @@ __global__ void k_rbsor_v(Geo g, T* v, const T* rhs, const T* rho_v, const T* ka
 
 // ------------------------------------------------- fused red-black SOR sweep
 // One whole red-black SOR sweep (both colour passes) of one velocity
-// component of a wall-bounded case, per tile of RB_TX x RB_TY faces.  The
-// tile and a ring of two faces of u are staged in shared memory; the
-// coefficients of the tile and a ring of one (cE, cW, cN, cS, the diagonal
-// and the right-hand side of jacobi_u_at / jacobi_v_at) are formed once per
-// face.  The red faces (i + j even) of the tile and of its ring are updated
-// there, then the black faces of the tile from those red values, and the
-// tile's faces are written back.  Each update is jacobi_u_at / jacobi_v_at's
-// formula with its operand order, so a sweep gives the bits of the two
-// colour-pass launches (k_rbsor_u / k_rbsor_v) it replaces while it reads and
-// writes each array once instead of twice.  A periodic case refreshes its
+// component of a wall-bounded case, per tile of RB_TX x RB_TY faces, from
+// the buffer uin into the buffer uout.  The tile and a ring of two faces of
+// uin are staged in shared memory; the coefficients of the tile and a ring of
+// one (cE, cW, cN, cS, the diagonal and the right-hand side of jacobi_u_at /
+// jacobi_v_at) are formed once per face.  The red faces (i + j even) of the
+// tile and of its ring are updated there, then the black faces of the tile
+// from those red values, and every element of the tile goes to uout.  Each
+// update is jacobi_u_at / jacobi_v_at's formula with its operand order, so a
+// sweep gives the bits of the two in-place colour-pass launches (k_rbsor_u /
+// k_rbsor_v) it replaces while it reads and writes each array once instead
+// of twice.  Two buffers, because a tile reads its ring while the
+// neighbouring tiles of the same launch write theirs: in place, it could read
+// a value its neighbour has already updated.  Callers alternate the buffers
+// and copy back after an odd number of sweeps.  A periodic case refreshes its
 // ghosts between the two colours, so it keeps the two launches.
 constexpr int RB_TX = 32, RB_TY = 16;
 constexpr int RB_SX = RB_TX + 4, RB_SY = RB_TY + 4;  // with the ring of two
@@ -602,16 +606,16 @@ struct RbSmem {
 
 // tile (tx, ty) of component comp (0 u, 1 v); needs !g.px && !g.py
 template <typename T>
-__device__ __forceinline__ void rbsor_sweep_tile(const Geo& g, int comp, int tx, int ty, T* u, const T* rhs,
-                                                 const T* rho, const T* kap, const T* zeta, const T* eta,
-                                                 const T* pen, T dt, T om, RbSmem<T>& sm) {
+__device__ __forceinline__ void rbsor_sweep_tile(const Geo& g, int comp, int tx, int ty, const T* uin, T* uout,
+                                                 const T* rhs, const T* rho, const T* kap, const T* zeta,
+                                                 const T* eta, const T* pen, T dt, T om, RbSmem<T>& sm) {
   const int ii0 = tx * RB_TX - 2, jj0 = ty * RB_TY - 2;  // padded-box coordinates of sm.u[0][0]
   const int nx = g.nx, ny = g.ny;
   const T ix2 = T(g.idx2), iy2 = T(g.idy2);
   for (int q = threadIdx.x; q < RB_SX * RB_SY; q += blockDim.x) {
     const int a = q % RB_SX, b = q / RB_SX;
     const int ii = ii0 + a, jj = jj0 + b;
-    sm.u[b][a] = (ii >= 0 && ii < g.P && jj >= 0 && jj < g.R) ? u[ii + jj * g.P] : T(0);
+    sm.u[b][a] = (ii >= 0 && ii < g.P && jj >= 0 && jj < g.R) ? uin[ii + jj * g.P] : T(0);
   }
   for (int q = threadIdx.x; q < RB_CX * RB_CY; q += blockDim.x) {
     const int a = q % RB_CX, b = q / RB_CX;
@@ -673,18 +677,17 @@ __device__ __forceinline__ void rbsor_sweep_tile(const Geo& g, int comp, int tx,
   }
   for (int q = threadIdx.x; q < RB_TX * RB_TY; q += blockDim.x) {
     const int a = 1 + q % RB_TX, b = 1 + q / RB_TX;
-    if (!sm.kind[b][a]) continue;
     const int ii = ii0 + 1 + a, jj = jj0 + 1 + b;
-    u[ii + jj * g.P] = sm.u[b + 1][a + 1];
+    if (ii < g.P && jj < g.R) uout[ii + jj * g.P] = sm.u[b + 1][a + 1];
   }
 }
 template <typename T>
-__global__ void __launch_bounds__(RB_TPB) k_rbsor_sweep(Geo g, int comp, T* u, const T* rhs, const T* rho,
-                                                        const T* kap, const T* zeta, const T* eta, const T* pen,
-                                                        T dt, T om, const int* active) {
+__global__ void __launch_bounds__(RB_TPB) k_rbsor_sweep(Geo g, int comp, const T* uin, T* uout, const T* rhs,
+                                                        const T* rho, const T* kap, const T* zeta, const T* eta,
+                                                        const T* pen, T dt, T om, const int* active) {
   if (active && !*active) return;
   __shared__ RbSmem<T> sm;
-  rbsor_sweep_tile<T>(g, comp, blockIdx.x, blockIdx.y, u, rhs, rho, kap, zeta, eta, pen, dt, om, sm);
+  rbsor_sweep_tile<T>(g, comp, blockIdx.x, blockIdx.y, uin, uout, rhs, rho, kap, zeta, eta, pen, dt, om, sm);
 }
 
 // ------------------------------------------------------------ Krylov vectors

@@ -659,9 +659,12 @@ __global__ void __launch_bounds__(RB_TPB) k_ls_rbsor(const LsCase<T>* cs, const 
     __syncthreads();  // the previous tile is done with shared memory
     if (!c.ks->active || sweep >= d.sweeps) continue;
     const int lb = vb - P->tile[kk], ntx = (c.g.P + RB_TX - 1) / RB_TX;
+    // even sweeps from Z_j into tmp, odd ones back (LsJacobiCopy after an odd count)
     T* z = c.Z + (long)jj * 3 * c.n + comp * c.n;
+    const T* src = (sweep & 1) ? c.tmp : z;
+    T* dst = (sweep & 1) ? z : c.tmp;
     const T* pen = d.pen ? (comp == 0 ? c.cf.pen_u : c.cf.pen_v) : nullptr;
-    rbsor_sweep_tile<T>(c.g, comp, lb % ntx, lb / ntx, z, comp == 0 ? c.zuw : c.zvw,
+    rbsor_sweep_tile<T>(c.g, comp, lb % ntx, lb / ntx, src, dst, comp == 0 ? c.zuw : c.zvw,
                         comp == 0 ? c.cf.rho_u : c.cf.rho_v, c.cf.kappa, c.cf.zeta, c.cf.eta, pen, T(d.dt),
                         T(c.sor_omega), sm);
   }

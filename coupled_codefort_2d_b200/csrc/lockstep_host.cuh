@@ -366,6 +366,7 @@ struct Lockstep : LockstepBase {
         k_ls_rbsor<T><<<grid_of(fn, RB_TPB), RB_TPB, 0, q>>>(d_cases, d_dyn, d_plan, j, comp, sw);
         LSCKL("k_ls_rbsor");
       }
+      e1(LsJacobiCopy<T>{j, comp});
       return;
     }
     if (smoother == 1) {
