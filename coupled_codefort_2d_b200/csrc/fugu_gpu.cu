@@ -1296,6 +1296,9 @@ void reset_counters(fugu_ctx* c) {
   CK(cudaMemsetAsync(c->pcg_out, 0, sizeof(PcgOut), c->s));
   CK(cudaMemsetAsync(c->svof_iters, 0, sizeof(int), c->s));
   CK(cudaMemsetAsync(c->svof_status, 0, sizeof(int), c->s));
+  // a barrier that gave up in an earlier call left its flag set; a call that
+  // takes the cluster PCG never clears it otherwise
+  CK(cudaMemsetAsync(c->gs, 0, sizeof(GridSync), c->s));
 }
 // read statistics and the device-wait status; a barrier timeout is an error
 void collect(fugu_ctx* c, fugu_stats* st) {
