@@ -14,7 +14,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libfugu_gpu.so")
 SOURCES = ["fugu_gpu.cu"]
-HEADERS = ["fugu_internal.cuh", "kernels.cuh", "persistent.cuh", "pcg_cluster.cuh", "scalars.cuh", "fgmres.cuh", "adjoint.cuh", "dual.cuh", "step_vjp.cuh"]
+HEADERS = ["fugu_internal.cuh", "kernels.cuh", "persistent.cuh", "pcg_cluster.cuh", "scalars.cuh", "fgmres.cuh", "adjoint.cuh",
+           "dual.cuh", "step_vjp.cuh", "lockstep.cuh", "lockstep_host.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
