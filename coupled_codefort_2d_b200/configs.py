@@ -11,8 +11,12 @@ per configuration).
 c1: cavity on the unit square, rho = 1, mu = 1e-3 (Re = 1000), lid u = 1, BDF1,
 dt = 1e-2, tolerance 1e-10, zero initial fields.  The reference's own solver
 cannot reach 1e-10 (its BiCGStab(2) diverges on this case), so the plain FP64
-form here is the FP64 defect correction around flexible GMRES with the
-reference's PCD.  Reports the centreline extremes and the divergence.
+form here is the FP64 defect correction around flexible GMRES + PCD.  Reports
+the centreline extremes and the divergence.
+
+c1-c3 run the PCD with the viscous Schur term (PCG cap from 80), c3 also with
+the red-black SOR velocity smoother; ``--pcd reference`` runs the reference's
+PCD instead.
 
 c2: static droplet (R = 0.25, rho 1 / 0.1, mu 0.1 / 0.01, sigma = 1, no
 gravity), area fractions by 16 x 16 sub-sampling, BDF2, dt = 1e-4, 500 steps,
@@ -64,6 +68,16 @@ from .params import Params
 
 SOLVER = dict(refine=2, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=60, krylov_bc_fix=1,
               pcg_cap_start=40, pcd_sweeps=6, pcd_sweeps_max=24, graphs=1)
+# SOLVER keeps the reference's PCD.  The runs below add (unless --pcd
+# reference) the PCD extensions that cut the Arnoldi steps: the viscous Schur
+# term with the PCG cap from 80, and on the bubble the red-black SOR smoother.
+FAST = dict(pcd_visc_scale=1.0, pcg_cap_start=80)
+BUBBLE = dict(FAST, pcd_smoother=1, pcd_sor_omega=1.5)
+
+
+def solver(args, extra):
+    """the solver settings of a run: SOLVER plus the extensions unless --pcd reference"""
+    return dict(SOLVER, **({} if getattr(args, "pcd", "fast") == "reference" else extra))
 STATE = ("u_vel", "v_vel", "p_field", "c_field", "u_prev", "v_prev", "rho_c", "rho_u", "rho_v", "kappa", "zeta",
          "eta", "kappa_curv", "f_sigma_u", "f_sigma_v")
 
@@ -105,7 +119,7 @@ def config_c1(args):
     n = 128
     g = Grid(n, n)
     prm = Params(rho1=1.0, rho2=1.0, mu1=1e-3, mu2=1e-3, sigma=0.0, gx=0.0, gy=0.0, time_order=1,
-                 tol_bicgstab2=1e-10, max_iter_bicgstab2=500, **SOLVER)
+                 tol_bicgstab2=1e-10, max_iter_bicgstab2=500, **solver(args, FAST))
     steps = args.steps or 200
     st, stats, secs, _ = _run(g, prm, g.full("cell", 1.0), FP64, steps, 1e-2, lid=1.0, device=args.device)
     u = st["u_vel"]
@@ -114,6 +128,7 @@ def config_c1(args):
     uc = at(u, "u", n // 2, slice(1, n))  # u faces at x = 0.5
     vc = at(v, "v", slice(1, n), n // 2)  # v faces at y = 0.5
     return {"config": "c1", "workload": f"lid_driven_cavity_{n}x{n}_Re1000", "steps": steps, "dtype": "f64",
+            "solver": solver(args, FAST),
             **_summary(stats, secs), "u_min_vertical_centreline": float(uc.min()),
             "v_min_horizontal_centreline": float(vc.min()), "v_max_horizontal_centreline": float(vc.max()),
             "max_divergence": cases.max_divergence(g, u, v)}
@@ -123,11 +138,12 @@ def config_c2(args):
     n = 256
     g = Grid(n, n)
     prm = Params(rho1=1.0, rho2=0.1, mu1=0.1, mu2=0.01, sigma=1.0, gx=0.0, gy=0.0, time_order=2,
-                 tol_bicgstab2=1e-8, max_iter_bicgstab2=500, **SOLVER)
+                 tol_bicgstab2=1e-8, max_iter_bicgstab2=500, **solver(args, FAST))
     steps = args.steps or 500
     c0 = cases.circle_fraction(g, 0.5, 0.5, 0.25, inside=1.0, ns=16)
     vol0 = cases.fluid1_volume(g, c0)
-    rep = {"config": "c2", "workload": f"static_droplet_{n}x{n}", "steps": steps, "sigma_over_R": 1.0 / 0.25}
+    rep = {"config": "c2", "workload": f"static_droplet_{n}x{n}", "steps": steps, "sigma_over_R": 1.0 / 0.25,
+           "solver": solver(args, FAST)}
     finals = {}
     for name, prec in (("mixed", MIXED), ("fp64", FP64)):
         st, stats, secs, _ = _run(g, prm, c0, prec, steps, 1e-4, device=args.device)
@@ -150,12 +166,13 @@ def config_c3(args):
     else:
         phys = dict(rho1=1000.0, rho2=100.0, mu1=10.0, mu2=1.0, sigma=24.5)
     prm = Params(gx=0.0, gy=-0.98, time_order=2, tol_bicgstab2=1e-8, max_iter_bicgstab2=500, free_slip_x=1,
-                 **phys, **SOLVER)
+                 **phys, **solver(args, BUBBLE))
     steps = args.steps or 6000
     dt = 5e-4
     c0 = cases.binary_circle(g, 0.5, 0.5, 0.25, inside=0.0)
     every = max(1, steps // 4)
-    rep = {"config": "c3", "workload": f"rising_bubble_320x640_{args.variant}", "steps": steps, "t": steps * dt}
+    rep = {"config": "c3", "workload": f"rising_bubble_320x640_{args.variant}", "steps": steps, "t": steps * dt,
+           "solver": solver(args, BUBBLE)}
     hists = {}
     for name, prec in (("mixed", MIXED), ("fp64", FP64)):
         st, stats, secs, hist = _run(g, prm, c0, prec, steps, dt, every=every, device=args.device)
@@ -311,6 +328,8 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=0, help="override the configuration's step count")
     ap.add_argument("--variant", default="standard", choices=["standard", "high_contrast"], help="c3 only")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--pcd", default="fast", choices=["fast", "reference"],
+                    help="c1-c3: the PCD extensions (default) or the reference's PCD")
     ap.add_argument("--n", type=int, default=2048, help="scale only: cells per side")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="scale only")
     ap.add_argument("--sweep", action="store_true",

@@ -195,13 +195,18 @@ struct fugu_ctx {
   int pcg_grid = 0;
   int svof_grid = 0;
   int dot_grid = 0;
-  // limits for concurrent use (a batch lowers them so many cases fit at once)
   // failure-detection test hook: > 0 arms the next grid-wide PCG launch to
   // wait for one CTA too many and give up after this many polls
   unsigned int test_spin_limit = 0;
+  // limits for concurrent use (a batch lowers them so many cases fit at once)
   int max_cluster = 16;  // CTAs of the cluster-resident PCG
   int max_coop = 1 << 30;  // CTAs of a grid-wide cooperative kernel
   bool coop_as_cluster = false;  // launch those as one cluster (max_coop <= 8)
+  // Krylov iterations whose PCG is the grid-wide kernel are captured into
+  // graphs as cooperative kernel nodes; cleared (for good) if a capture or an
+  // instantiation with such a node fails, and those iterations run eagerly
+  bool coop_graphs = true;
+  bool capture_coop = false;  // the capture in progress holds a grid-wide launch
   // cluster-resident PCG plan per precision (index 0 FP64, 1 FP32)
   struct ClusterPlan {
     bool ok = false;
@@ -362,10 +367,12 @@ void matvec(fugu_ctx* c, const CoefBufs<T>& cb, const SolveOpt& o, Trip<T> X, Tr
   halo(c, X.u, K_U, active);
   halo(c, X.v, K_V, active);
   halo(c, X.p, K_CELL, active);
-  Box b = box_launch(c->g);
-  k_matvec<T><<<b.grid, b.block, 0, c->s>>>(c->g, coefs_of(cb, o), X.u, X.v, X.p, Y.u, Y.v, Y.p, T(dt), 1, active,
-                                            &c->ks->matvecs);
-  CKL("k_matvec");
+  // staged tiles of MT_TX x TY outputs (rows per tile: 16 in FP32, 8 in FP64)
+  constexpr int TY = sizeof(T) == 4 ? 16 : 8;
+  const dim3 grid((c->g.P + MT_TX - 1) / MT_TX, (c->g.R + TY - 1) / TY);
+  k_matvec_tile<T, TY><<<grid, MT_TPB, mt_matvec_smem<T, TY>(), c->s>>>(c->g, coefs_of(cb, o), X.u, X.v, X.p, Y.u, Y.v,
+                                                                        Y.p, T(dt), 1, active, &c->ks->matvecs);
+  CKL("k_matvec_tile");
 }
 
 template <typename T>
@@ -501,24 +508,27 @@ void plan_pcg_cluster(fugu_ctx* c, fugu_ctx::ClusterPlan& pl) {
 // partly resident cooperative grids could each wait for CTAs the other's
 // occupy (until the bounded barrier gives up), so there the grid is launched
 // as one thread-block cluster (at most 8 CTAs), whose CTAs the hardware
-// schedules together or not at all.
+// schedules together or not at all.  Both forms are launch attributes, so a
+// stream capture records them as attributes of the kernel node.
 void launch_coop(fugu_ctx* c, const void* fn, int grid, void** args) {
-  if (!c->coop_as_cluster) {
-    CK(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(PCG_TPB), args, 0, c->s));
-    return;
-  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(PCG_TPB);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = c->s;
   cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeClusterDimension;
-  at[0].val.clusterDim.x = grid;
-  at[0].val.clusterDim.y = 1;
-  at[0].val.clusterDim.z = 1;
+  if (c->coop_as_cluster) {
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = grid;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+  } else {
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+  }
   cfg.attrs = at;
   cfg.numAttrs = 1;
+  if (c->capturing) c->capture_coop = true;
   CK(cudaLaunchKernelExC(&cfg, fn, args));
 }
 
@@ -720,6 +730,9 @@ struct KrylovResult {
 
 void graph_prof_read(fugu_ctx* c);
 
+// Krylov iterations of precision pi (0 FP64, 1 FP32) replay from graphs
+bool graphs_on(const fugu_ctx* c, int pi) { return c->prm.graphs == 1 && (c->pcgc[pi].ok || c->coop_graphs); }
+
 // Run body() on the context's stream from a CUDA graph: the captured graph
 // is replayed while key (every value its launches depend on) is unchanged;
 // otherwise body() is captured again and the executable graph updated in
@@ -740,6 +753,19 @@ void run_graphed(fugu_ctx* c, fugu_ctx::StepGraph& sg, std::vector<unsigned char
     sg.ev_used = 0;
     cudaGraph_t graph = nullptr;
     const unsigned long long l0 = c->launches;
+    // a capture or an instantiation that fails with a grid-wide kernel in it:
+    // no more such graphs in this context, and this body runs eagerly (the
+    // failed capture launched nothing)
+    auto coop_fallback = [&]() {
+      if (!c->capture_coop || !c->coop_graphs) return false;
+      c->coop_graphs = false;
+      c->capture_coop = false;
+      cudaGetLastError();
+      sg.timed = false;
+      body();
+      return true;
+    };
+    c->capture_coop = false;
     CK(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
     c->capturing = &sg;
     try {
@@ -750,12 +776,18 @@ void run_graphed(fugu_ctx* c, fugu_ctx::StepGraph& sg, std::vector<unsigned char
       cudaStreamEndCapture(c->s, &graph);
       if (graph) cudaGraphDestroy(graph);
       cudaGetLastError();
+      if (coop_fallback()) return;
       throw;
     }
     c->capturing = nullptr;
-    CK(cudaStreamEndCapture(c->s, &graph));
+    const cudaError_t ec = cudaStreamEndCapture(c->s, &graph);
     sg.launches = c->launches - l0;
     c->launches = l0;
+    if (ec != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      if (coop_fallback()) return;
+      throw CudaError{ec, "cudaStreamEndCapture"};
+    }
     bool updated = false;
     if (sg.exec) {
       cudaGraphExecUpdateResultInfo info;
@@ -772,6 +804,7 @@ void run_graphed(fugu_ctx* c, fugu_ctx::StepGraph& sg, std::vector<unsigned char
       if (e != cudaSuccess) {
         sg.exec = nullptr;
         cudaGraphDestroy(graph);
+        if (coop_fallback()) return;
         throw CudaError{e, "cudaGraphInstantiate"};
       }
     }
@@ -839,7 +872,7 @@ KrylovResult bicgstab1(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, con
   KState ks = read_ks(c);
   // graphs = 1: one captured iteration, replayed for every k (k on the device)
   const int pi = sizeof(T) == 8 ? 0 : 1;
-  const bool graphed = c->prm.graphs == 1 && c->pcgc[pi].ok;
+  const bool graphed = graphs_on(c, pi);
   int k = 1;
   for (; k <= max_iter && ks.active; ++k) {
     NvtxRange r_it("bicgstab_iteration");
@@ -902,7 +935,7 @@ KrylovResult bicgstab2(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, con
   KState ks = read_ks(c);
   // graphs = 1: one captured iteration, replayed for every k (k on the device)
   const int pi = sizeof(T) == 8 ? 0 : 1;
-  const bool graphed = c->prm.graphs == 1 && c->pcgc[pi].ok;
+  const bool graphed = graphs_on(c, pi);
   int k = 1;
   for (; k <= max_iter && ks.active; ++k) {
     NvtxRange r_it("bicgstab2_iteration");
@@ -1036,11 +1069,11 @@ KrylovResult fgmres(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const 
   k_fg_scale<T><<<g1, 256, 0, c->s>>>(n3, f.V, B.base, f.st + L.inv(), act);
   CKL("k_fg_scale");
   KState ks = read_ks(c);
-  // graphs = 1: each Arnoldi step is replayed from a CUDA graph (not with
-  // the grid-wide PCG, a cooperative launch); while profiling, the graph
-  // records the PCG interval on its own event pair, read after each step
+  // graphs = 1: each Arnoldi step is replayed from a CUDA graph; while
+  // profiling, the graph records the PCG interval on its own event pair,
+  // read after each step
   const int pi = sizeof(T) == 8 ? 0 : 1;
-  const bool graphed = c->prm.graphs == 1 && c->pcgc[pi].ok;
+  const bool graphed = graphs_on(c, pi);
   if (graphed && (int)c->fg_graphs[pi].size() < m) {
     // a solve that ended in an error may have left a sample pending in the
     // vector that is about to move

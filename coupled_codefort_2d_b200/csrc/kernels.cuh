@@ -192,89 +192,108 @@ __global__ void k_properties(Geo g, MixT<S> m, const S* __restrict__ c, S* rho_c
 }
 
 // ------------------------------------------------------------ operators
+// Field views.  The operator formulas read a field at Fortran (i, j) through
+// a view, so one expression (and one operand order) serves a field in global
+// memory and a tile of it staged in shared memory; the two give the same bits.
+template <typename T>
+struct GView {  // a whole padded box in global memory
+  const T* p;
+  int P;
+  __device__ __forceinline__ T operator()(int i, int j) const { return p[(i + 2) + (j + 2) * P]; }
+};
+template <typename T>
+__device__ __forceinline__ GView<T> gview(const Geo& g, const T* p) { return GView<T>{p, g.P}; }
+template <typename T, int W>
+struct SView {  // a staged tile of W elements per row; (i0, j0) is the Fortran index of s[0]
+  const T* s;
+  int i0, j0;
+  __device__ __forceinline__ T operator()(int i, int j) const { return s[(j - j0) * W + (i - i0)]; }
+};
+
 // T_xx, T_yy at cells and T_xy, T_yx at vertices (mod_operators.f90:119-140)
-template <typename T>
-__device__ __forceinline__ T txx(const Geo& g, const T* u, const T* kap, int i, int j, T idx) {
-  return kap[g.at(i, j)] * (u[g.at(i, j)] - u[g.at(i - 1, j)]) * idx;
+template <typename T, typename V>
+__device__ __forceinline__ T txx(const V& u, const V& kap, int i, int j, T idx) {
+  return kap(i, j) * (u(i, j) - u(i - 1, j)) * idx;
 }
-template <typename T>
-__device__ __forceinline__ T tyy(const Geo& g, const T* v, const T* kap, int i, int j, T idy) {
-  return kap[g.at(i, j)] * (v[g.at(i, j)] - v[g.at(i, j - 1)]) * idy;
+template <typename T, typename V>
+__device__ __forceinline__ T tyy(const V& v, const V& kap, int i, int j, T idy) {
+  return kap(i, j) * (v(i, j) - v(i, j - 1)) * idy;
 }
-template <typename T>
-__device__ __forceinline__ void txy_tyx(const Geo& g, const T* u, const T* v, const T* zeta,
-                                        const T* eta, int i, int j, T idx, T idy, T& txy, T& tyx) {
-  const T du_dy = (u[g.at(i, j + 1)] - u[g.at(i, j)]) * idy;
-  const T dv_dx = (v[g.at(i + 1, j)] - v[g.at(i, j)]) * idx;
-  const T z = zeta[g.at(i, j)], e = eta[g.at(i, j)];
+template <typename T, typename V>
+__device__ __forceinline__ void txy_tyx(const V& u, const V& v, const V& zeta, const V& eta, int i, int j, T idx,
+                                        T idy, T& txy, T& tyx) {
+  const T du_dy = (u(i, j + 1) - u(i, j)) * idy;
+  const T dv_dx = (v(i + 1, j) - v(i, j)) * idx;
+  const T z = zeta(i, j), e = eta(i, j);
   txy = (z - e) * du_dy + e * dv_dx;
   tyx = e * du_dy + (z - e) * dv_dx;
 }
 // -div(T) on a u face (mod_operators.f90:145-150)
-template <typename T>
-__device__ __forceinline__ T visc_u_at(const Geo& g, const T* u, const T* v, const T* kap,
-                                       const T* zeta, const T* eta, int i, int j, T idx, T idy) {
+template <typename T, typename V>
+__device__ __forceinline__ T visc_u_at(const V& u, const V& v, const V& kap, const V& zeta, const V& eta, int i,
+                                       int j, T idx, T idy) {
   T a0, b0, a1, b1;
-  txy_tyx(g, u, v, zeta, eta, i, j, idx, idy, a0, b0);
-  txy_tyx(g, u, v, zeta, eta, i, j - 1, idx, idy, a1, b1);
-  return -((txx(g, u, kap, i + 1, j, idx) - txx(g, u, kap, i, j, idx)) * idx + (a0 - a1) * idy);
+  txy_tyx<T>(u, v, zeta, eta, i, j, idx, idy, a0, b0);
+  txy_tyx<T>(u, v, zeta, eta, i, j - 1, idx, idy, a1, b1);
+  return -((txx<T>(u, kap, i + 1, j, idx) - txx<T>(u, kap, i, j, idx)) * idx + (a0 - a1) * idy);
 }
 // -div(T) on a v face (mod_operators.f90:155-160)
-template <typename T>
-__device__ __forceinline__ T visc_v_at(const Geo& g, const T* u, const T* v, const T* kap,
-                                       const T* zeta, const T* eta, int i, int j, T idx, T idy) {
+template <typename T, typename V>
+__device__ __forceinline__ T visc_v_at(const V& u, const V& v, const V& kap, const V& zeta, const V& eta, int i,
+                                       int j, T idx, T idy) {
   T a0, b0, a1, b1;
-  txy_tyx(g, u, v, zeta, eta, i, j, idx, idy, a0, b0);
-  txy_tyx(g, u, v, zeta, eta, i - 1, j, idx, idy, a1, b1);
-  return -((b0 - b1) * idx + (tyy(g, v, kap, i, j + 1, idy) - tyy(g, v, kap, i, j, idy)) * idy);
+  txy_tyx<T>(u, v, zeta, eta, i, j, idx, idy, a0, b0);
+  txy_tyx<T>(u, v, zeta, eta, i - 1, j, idx, idy, a1, b1);
+  return -((b0 - b1) * idx + (tyy<T>(v, kap, i, j + 1, idy) - tyy<T>(v, kap, i, j, idy)) * idy);
 }
 
-// op_advection, mod_operators.f90:201-222 (u component)
-template <typename T>
-__device__ __forceinline__ T adv_u_at(const Geo& g, const T* ua, const T* va, const T* rc,
-                                      const T* rv, const T* u, const T* mdu, const T* mdv, int i,
-                                      int j, T idx, T idy) {
+// op_advection, mod_operators.f90:201-222 (u component); amp: the mass fluxes
+// mdu / mdv replace rho * velocity (consistent AMP)
+template <typename T, typename V>
+__device__ __forceinline__ T adv_u_at(const V& ua, const V& va, const V& rc, const V& rv, const V& u,
+                                      const GView<T>& mdu, const GView<T>& mdv, bool amp, int i, int j, T idx,
+                                      T idy) {
   const T h = T(0.5);
   T mE, mW, mN, mS;
-  if (mdu) {
-    mE = h * (mdu[g.at(i, j)] + mdu[g.at(i + 1, j)]);
-    mW = h * (mdu[g.at(i - 1, j)] + mdu[g.at(i, j)]);
-    mN = h * (mdv[g.at(i, j)] + mdv[g.at(i + 1, j)]);
-    mS = h * (mdv[g.at(i, j - 1)] + mdv[g.at(i + 1, j - 1)]);
+  if (amp) {
+    mE = h * (mdu(i, j) + mdu(i + 1, j));
+    mW = h * (mdu(i - 1, j) + mdu(i, j));
+    mN = h * (mdv(i, j) + mdv(i + 1, j));
+    mS = h * (mdv(i, j - 1) + mdv(i + 1, j - 1));
   } else {
-    mE = rc[g.at(i + 1, j)] * h * (ua[g.at(i, j)] + ua[g.at(i + 1, j)]);
-    mW = rc[g.at(i, j)] * h * (ua[g.at(i - 1, j)] + ua[g.at(i, j)]);
-    mN = h * (rv[g.at(i, j)] + rv[g.at(i + 1, j)]) * h * (va[g.at(i, j)] + va[g.at(i + 1, j)]);
-    mS = h * (rv[g.at(i, j - 1)] + rv[g.at(i + 1, j - 1)]) * h * (va[g.at(i, j - 1)] + va[g.at(i + 1, j - 1)]);
+    mE = rc(i + 1, j) * h * (ua(i, j) + ua(i + 1, j));
+    mW = rc(i, j) * h * (ua(i - 1, j) + ua(i, j));
+    mN = h * (rv(i, j) + rv(i + 1, j)) * h * (va(i, j) + va(i + 1, j));
+    mS = h * (rv(i, j - 1) + rv(i + 1, j - 1)) * h * (va(i, j - 1) + va(i + 1, j - 1));
   }
-  const T uE = h * (u[g.at(i, j)] + u[g.at(i + 1, j)]);
-  const T uW = h * (u[g.at(i - 1, j)] + u[g.at(i, j)]);
-  const T uN = h * (u[g.at(i, j)] + u[g.at(i, j + 1)]);
-  const T uS = h * (u[g.at(i, j - 1)] + u[g.at(i, j)]);
+  const T uE = h * (u(i, j) + u(i + 1, j));
+  const T uW = h * (u(i - 1, j) + u(i, j));
+  const T uN = h * (u(i, j) + u(i, j + 1));
+  const T uS = h * (u(i, j - 1) + u(i, j));
   return (mE * uE - mW * uW) * idx + (mN * uN - mS * uS) * idy;
 }
 // op_advection, mod_operators.f90:225-247 (v component)
-template <typename T>
-__device__ __forceinline__ T adv_v_at(const Geo& g, const T* ua, const T* va, const T* rc,
-                                      const T* ru, const T* v, const T* mdu, const T* mdv, int i,
-                                      int j, T idx, T idy) {
+template <typename T, typename V>
+__device__ __forceinline__ T adv_v_at(const V& ua, const V& va, const V& rc, const V& ru, const V& v,
+                                      const GView<T>& mdu, const GView<T>& mdv, bool amp, int i, int j, T idx,
+                                      T idy) {
   const T h = T(0.5);
   T mE, mW, mN, mS;
-  if (mdu) {
-    mE = h * (mdu[g.at(i, j)] + mdu[g.at(i, j + 1)]);
-    mW = h * (mdu[g.at(i - 1, j)] + mdu[g.at(i - 1, j + 1)]);
-    mN = h * (mdv[g.at(i, j)] + mdv[g.at(i, j + 1)]);
-    mS = h * (mdv[g.at(i, j - 1)] + mdv[g.at(i, j)]);
+  if (amp) {
+    mE = h * (mdu(i, j) + mdu(i, j + 1));
+    mW = h * (mdu(i - 1, j) + mdu(i - 1, j + 1));
+    mN = h * (mdv(i, j) + mdv(i, j + 1));
+    mS = h * (mdv(i, j - 1) + mdv(i, j));
   } else {
-    mE = h * (ru[g.at(i, j)] + ru[g.at(i, j + 1)]) * h * (ua[g.at(i, j)] + ua[g.at(i, j + 1)]);
-    mW = h * (ru[g.at(i - 1, j)] + ru[g.at(i - 1, j + 1)]) * h * (ua[g.at(i - 1, j)] + ua[g.at(i - 1, j + 1)]);
-    mN = rc[g.at(i, j + 1)] * h * (va[g.at(i, j)] + va[g.at(i, j + 1)]);
-    mS = rc[g.at(i, j)] * h * (va[g.at(i, j - 1)] + va[g.at(i, j)]);
+    mE = h * (ru(i, j) + ru(i, j + 1)) * h * (ua(i, j) + ua(i, j + 1));
+    mW = h * (ru(i - 1, j) + ru(i - 1, j + 1)) * h * (ua(i - 1, j) + ua(i - 1, j + 1));
+    mN = rc(i, j + 1) * h * (va(i, j) + va(i, j + 1));
+    mS = rc(i, j) * h * (va(i, j - 1) + va(i, j));
   }
-  const T vE = h * (v[g.at(i, j)] + v[g.at(i + 1, j)]);
-  const T vW = h * (v[g.at(i - 1, j)] + v[g.at(i, j)]);
-  const T vN = h * (v[g.at(i, j)] + v[g.at(i, j + 1)]);
-  const T vS = h * (v[g.at(i, j - 1)] + v[g.at(i, j)]);
+  const T vE = h * (v(i, j) + v(i + 1, j));
+  const T vW = h * (v(i - 1, j) + v(i, j));
+  const T vN = h * (v(i, j) + v(i, j + 1));
+  const T vS = h * (v(i, j - 1) + v(i, j));
   return (mE * vE - mW * vW) * idx + (mN * vN - mS * vS) * idy;
 }
 
@@ -286,50 +305,77 @@ struct Coefs {
   const T *mdot_u, *mdot_v; // nullable (AMP)
 };
 
-// matvec_coupled, mod_operators.f90:341-443, as ONE pass: the thread at
-// (i, j) writes Y_u(i,j), Y_v(i,j) and Y_p(i,j) of the whole padded box (zero
-// where the reference zeroes), computing the viscous stresses, the pressure
-// gradient, the advection and the divergence from X on the fly.  X must
-// already hold its periodic halo (k_halo).
+// The eleven fields the coupled operator reads with a stencil, as views.
+enum { MV_XU, MV_XV, MV_XP, MV_UA, MV_VA, MV_RC, MV_RU, MV_RV, MV_KA, MV_ZE, MV_ET, MV_N };
+
+// matvec_coupled, mod_operators.f90:341-443, at one (i, j): Y_u(i,j),
+// Y_v(i,j) and Y_p(i,j) of the whole padded box (zero where the reference
+// zeroes), computing the viscous stresses, the pressure gradient, the
+// advection and the divergence from X on the fly.  X must already hold its
+// periodic halo (k_halo).  f: the stencil fields as views; the penalty (one
+// value per face) and the AMP mass fluxes are read from global memory.
+template <typename T, typename V>
+__device__ __forceinline__ void matvec_vals(const Geo& g, const V* f, const Coefs<T>& c, T dt, int with_adv, int k,
+                                            int i, int j, T& yu, T& yv, T& yp) {
+  const int nx = g.nx, ny = g.ny;
+  const T idx = T(g.idx), idy = T(g.idy);
+  const V& Xu = f[MV_XU];
+  const V& Xv = f[MV_XV];
+  const V& Xp = f[MV_XP];
+  const bool amp = c.mdot_u != nullptr;
+  const GView<T> mdu = gview(g, c.mdot_u), mdv = gview(g, c.mdot_v);
+  // u row
+  yu = T(0);
+  if (j >= 1 && j <= ny) {
+    if (i >= 1 && i <= g.imax()) {
+      const T adv = with_adv ? adv_u_at<T>(f[MV_UA], f[MV_VA], f[MV_RC], f[MV_RV], Xu, mdu, mdv, amp, i, j, idx, idy)
+                             : T(0);
+      const T vis = visc_u_at<T>(Xu, Xv, f[MV_KA], f[MV_ZE], f[MV_ET], i, j, idx, idy);
+      const T gp = (Xp(i + 1, j) - Xp(i, j)) * idx;
+      yu = (f[MV_RU](i, j) / dt) * Xu(i, j) + adv + vis + gp;
+      if (c.pen_u) yu = yu + c.pen_u[k] * Xu(i, j);
+    } else if (!g.px && (i == 0 || i == nx)) {
+      yu = Xu(i, j);
+    }
+  }
+  // v row
+  yv = T(0);
+  if (i >= 1 && i <= nx) {
+    if (j >= 1 && j <= g.jmax()) {
+      const T adv = with_adv ? adv_v_at<T>(f[MV_UA], f[MV_VA], f[MV_RC], f[MV_RU], Xv, mdu, mdv, amp, i, j, idx, idy)
+                             : T(0);
+      const T vis = visc_v_at<T>(Xu, Xv, f[MV_KA], f[MV_ZE], f[MV_ET], i, j, idx, idy);
+      const T gp = (Xp(i, j + 1) - Xp(i, j)) * idy;
+      yv = (f[MV_RV](i, j) / dt) * Xv(i, j) + adv + vis + gp;
+      if (c.pen_v) yv = yv + c.pen_v[k] * Xv(i, j);
+    } else if (!g.py && (j == 0 || j == ny)) {
+      yv = Xv(i, j);
+    }
+  }
+  // p row: op_divergence (mod_operators.f90:34-53)
+  yp = T(0);
+  if (i >= 1 && i <= nx && j >= 1 && j <= ny) yp = (Xu(i, j) - Xu(i - 1, j)) * idx + (Xv(i, j) - Xv(i, j - 1)) * idy;
+}
+template <typename T>
+__device__ __forceinline__ void mv_gviews(const Geo& g, const Coefs<T>& c, const T* Xu, const T* Xv, const T* Xp,
+                                          GView<T>* f) {
+  f[MV_XU] = gview(g, Xu); f[MV_XV] = gview(g, Xv); f[MV_XP] = gview(g, Xp);
+  f[MV_UA] = gview(g, c.u_adv); f[MV_VA] = gview(g, c.v_adv); f[MV_RC] = gview(g, c.rho_c);
+  f[MV_RU] = gview(g, c.rho_u); f[MV_RV] = gview(g, c.rho_v); f[MV_KA] = gview(g, c.kappa);
+  f[MV_ZE] = gview(g, c.zeta); f[MV_ET] = gview(g, c.eta);
+}
+// the operator at (i, j) with every field read from global memory
 template <typename T>
 __device__ __forceinline__ void matvec_at(const Geo& g, const Coefs<T>& c, const T* __restrict__ Xu,
                                           const T* __restrict__ Xv, const T* __restrict__ Xp, T* __restrict__ Yu,
                                           T* __restrict__ Yv, T* __restrict__ Yp, T dt, int with_adv, int k, int i,
                                           int j) {
-  const int nx = g.nx, ny = g.ny;
-  const T idx = T(g.idx), idy = T(g.idy);
-  // u row
-  T yu = T(0);
-  if (j >= 1 && j <= ny) {
-    if (i >= 1 && i <= g.imax()) {
-      const T adv = with_adv ? adv_u_at(g, c.u_adv, c.v_adv, c.rho_c, c.rho_v, Xu, c.mdot_u, c.mdot_v, i, j, idx, idy) : T(0);
-      const T vis = visc_u_at(g, Xu, Xv, c.kappa, c.zeta, c.eta, i, j, idx, idy);
-      const T gp = (Xp[g.at(i + 1, j)] - Xp[g.at(i, j)]) * idx;
-      yu = (c.rho_u[k] / dt) * Xu[k] + adv + vis + gp;
-      if (c.pen_u) yu = yu + c.pen_u[k] * Xu[k];
-    } else if (!g.px && (i == 0 || i == nx)) {
-      yu = Xu[k];
-    }
-  }
+  GView<T> f[MV_N];
+  mv_gviews(g, c, Xu, Xv, Xp, f);
+  T yu, yv, yp;
+  matvec_vals<T>(g, f, c, dt, with_adv, k, i, j, yu, yv, yp);
   Yu[k] = yu;
-  // v row
-  T yv = T(0);
-  if (i >= 1 && i <= nx) {
-    if (j >= 1 && j <= g.jmax()) {
-      const T adv = with_adv ? adv_v_at(g, c.u_adv, c.v_adv, c.rho_c, c.rho_u, Xv, c.mdot_u, c.mdot_v, i, j, idx, idy) : T(0);
-      const T vis = visc_v_at(g, Xu, Xv, c.kappa, c.zeta, c.eta, i, j, idx, idy);
-      const T gp = (Xp[g.at(i, j + 1)] - Xp[g.at(i, j)]) * idy;
-      yv = (c.rho_v[k] / dt) * Xv[k] + adv + vis + gp;
-      if (c.pen_v) yv = yv + c.pen_v[k] * Xv[k];
-    } else if (!g.py && (j == 0 || j == ny)) {
-      yv = Xv[k];
-    }
-  }
   Yv[k] = yv;
-  // p row: op_divergence (mod_operators.f90:34-53)
-  T yp = T(0);
-  if (i >= 1 && i <= nx && j >= 1 && j <= ny)
-    yp = (Xu[k] - Xu[g.at(i - 1, j)]) * idx + (Xv[k] - Xv[g.at(i, j - 1)]) * idy;
   Yp[k] = yp;
 }
 template <typename T>
@@ -341,6 +387,88 @@ __global__ void k_matvec(Geo g, Coefs<T> c, const T* __restrict__ Xu, const T* _
   if (count && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) atomicAdd(count, 1ull);
   FUGU_BOX_IJ
   matvec_at<T>(g, c, Xu, Xv, Xp, Yu, Yv, Yp, dt, with_adv, k, i, j);
+}
+
+// ----------------------------------------------- staged stencil tiles
+// A CTA of 256 threads stages a tile of MT_TX x TY outputs of the padded box
+// plus a ring of one (widened to four columns either side, so that every
+// row segment starts on a 16-byte boundary) for each field it reads with a
+// stencil, by 16-byte asynchronous copies (cp.async) straight into shared
+// memory, then computes the tile from there: each field element is read
+// from HBM once and the stencil's neighbour reads hit shared memory.  Parts
+// of a staged segment outside the padded box are zero-filled (no global
+// read); the formulas never use them.  Each thread computes TY / 8
+// consecutive rows of one column, so a row's neighbours above and below come
+// from the same thread's reads.  Needs 16-byte aligned field bases and
+// P * sizeof(T) a multiple of 16 (every buffer of the uniform layout).
+constexpr int MT_TX = 32;
+constexpr int MT_TPB = 256;
+template <int TY>
+struct MtShape {
+  static constexpr int W = MT_TX + 8;  // staged columns: ii0 - 4 .. ii0 + MT_TX + 3
+  static constexpr int H = TY + 2;     // staged rows: jj0 - 1 .. jj0 + TY
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool ok) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(ok ? 16 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// stage rows jj0 - 1 .. jj0 + TY and columns ii0 - 4 .. ii0 + MT_TX + 3 of
+// field src into dst (H x W elements)
+template <typename T, int TY>
+__device__ __forceinline__ void mt_stage(const Geo& g, const T* src, T* dst, int ii0, int jj0) {
+  constexpr int W = MtShape<TY>::W, H = MtShape<TY>::H, VPC = 16 / sizeof(T), CPR = W / VPC;
+  for (int q = threadIdx.x; q < H * CPR; q += MT_TPB) {
+    const int r = q / CPR, cc = q % CPR;
+    const int ii = ii0 - 4 + cc * VPC, jj = jj0 - 1 + r;
+    const bool ok = ii >= 0 && ii < g.P && jj >= 0 && jj < g.R;
+    cp_async16(dst + r * W + cc * VPC, ok ? src + ii + (long)jj * g.P : src, ok);
+  }
+}
+template <typename T, int TY>
+constexpr int mt_matvec_smem() { return MV_N * MtShape<TY>::H * MtShape<TY>::W * (int)sizeof(T); }
+
+// the coupled operator on the tile (bx, by) of the box (see k_matvec)
+template <typename T, int TY>
+__device__ __forceinline__ void matvec_tile(const Geo& g, const Coefs<T>& c, const T* Xu, const T* Xv, const T* Xp,
+                                            T* __restrict__ Yu, T* __restrict__ Yv, T* __restrict__ Yp, T dt,
+                                            int with_adv, int bx, int by, T* sm) {
+  constexpr int W = MtShape<TY>::W, H = MtShape<TY>::H, RPT = TY / 8;
+  static_assert(TY % 8 == 0 && 16 % sizeof(T) == 0, "tile shape");
+  const int ii0 = bx * MT_TX, jj0 = by * TY;
+  const T* src[MV_N] = {Xu, Xv, Xp, c.u_adv, c.v_adv, c.rho_c, c.rho_u, c.rho_v, c.kappa, c.zeta, c.eta};
+#pragma unroll
+  for (int q = 0; q < MV_N; ++q) mt_stage<T, TY>(g, src[q], sm + q * H * W, ii0, jj0);
+  cp_async_wait_all();
+  __syncthreads();
+  SView<T, W> f[MV_N];
+#pragma unroll
+  for (int q = 0; q < MV_N; ++q) f[q] = SView<T, W>{sm + q * H * W, ii0 - 6, jj0 - 3};
+  const int ii = ii0 + threadIdx.x % MT_TX;
+#pragma unroll
+  for (int r = 0; r < RPT; ++r) {
+    const int jj = jj0 + (threadIdx.x / MT_TX) * RPT + r;
+    if (ii < g.P && jj < g.R) {
+      const int k = ii + jj * g.P;
+      T yu, yv, yp;
+      matvec_vals<T>(g, f, c, dt, with_adv, k, ii - 2, jj - 2, yu, yv, yp);
+      Yu[k] = yu;
+      Yv[k] = yv;
+      Yp[k] = yp;
+    }
+  }
+}
+template <typename T, int TY>
+__global__ void __launch_bounds__(MT_TPB) k_matvec_tile(Geo g, Coefs<T> c, const T* Xu, const T* Xv, const T* Xp,
+                                                        T* __restrict__ Yu, T* __restrict__ Yv, T* __restrict__ Yp,
+                                                        T dt, int with_adv, const int* active,
+                                                        unsigned long long* count) {
+  if (active && !*active) return;
+  if (count && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) atomicAdd(count, 1ull);
+  extern __shared__ __align__(16) unsigned char mt_smem[];
+  matvec_tile<T, TY>(g, c, Xu, Xv, Xp, Yu, Yv, Yp, dt, with_adv, blockIdx.x, blockIdx.y, (T*)mt_smem);
 }
 
 // The individual operators of mod_operators.f90 (routine-level entries).
@@ -359,15 +487,19 @@ __global__ void k_op_grad(Geo g, const double* p, double* gu, double* gv) {
 __global__ void k_op_visc(Geo g, const double* u, const double* v, const double* kap,
                           const double* zeta, const double* eta, double* vu, double* vv) {
   FUGU_BOX_IJ
-  vu[k] = (j >= 1 && j <= g.ny && i >= 0 && i <= g.nx) ? visc_u_at(g, u, v, kap, zeta, eta, i, j, g.idx, g.idy) : 0.0;
-  vv[k] = (i >= 1 && i <= g.nx && j >= 0 && j <= g.ny) ? visc_v_at(g, u, v, kap, zeta, eta, i, j, g.idx, g.idy) : 0.0;
+  const GView<double> U = gview(g, u), Vv = gview(g, v), K = gview(g, kap), Z = gview(g, zeta), E = gview(g, eta);
+  vu[k] = (j >= 1 && j <= g.ny && i >= 0 && i <= g.nx) ? visc_u_at<double>(U, Vv, K, Z, E, i, j, g.idx, g.idy) : 0.0;
+  vv[k] = (i >= 1 && i <= g.nx && j >= 0 && j <= g.ny) ? visc_v_at<double>(U, Vv, K, Z, E, i, j, g.idx, g.idy) : 0.0;
 }
 __global__ void k_op_adv(Geo g, Coefs<double> c, const double* u, const double* v, double* au, double* av) {
   FUGU_BOX_IJ
+  const GView<double> ua = gview(g, c.u_adv), va = gview(g, c.v_adv), rc = gview(g, c.rho_c);
+  const GView<double> ru = gview(g, c.rho_u), rv = gview(g, c.rho_v), md_u = gview(g, c.mdot_u), md_v = gview(g, c.mdot_v);
+  const bool amp = c.mdot_u != nullptr;
   au[k] = (j >= 1 && j <= g.ny && i >= 1 && i <= g.imax())
-              ? adv_u_at(g, c.u_adv, c.v_adv, c.rho_c, c.rho_v, u, c.mdot_u, c.mdot_v, i, j, g.idx, g.idy) : 0.0;
+              ? adv_u_at<double>(ua, va, rc, rv, gview(g, u), md_u, md_v, amp, i, j, g.idx, g.idy) : 0.0;
   av[k] = (i >= 1 && i <= g.nx && j >= 1 && j <= g.jmax())
-              ? adv_v_at(g, c.u_adv, c.v_adv, c.rho_c, c.rho_u, v, c.mdot_u, c.mdot_v, i, j, g.idx, g.idy) : 0.0;
+              ? adv_v_at<double>(ua, va, rc, ru, gview(g, v), md_u, md_v, amp, i, j, g.idx, g.idy) : 0.0;
 }
 
 // ------------------------------------------------------------ PCD pieces
@@ -478,30 +610,37 @@ __global__ void k_pcd_cross(Geo g, const T* eta, const T* rv, T* zuw, const int*
 
 // One damped-Jacobi sweep of solve_helmholtz_u (mod_subsolvers.f90:284-306):
 // un = Jacobi(uo) on owned faces, rhs on wall faces, uo elsewhere (the
-// reference's u_old = u_sol copy).
-template <typename T>
-__device__ __forceinline__ T jacobi_u_at(const Geo& g, int k, int i, int j, const T* uo, const T* rhs,
-                                         const T* rho_u, const T* kap, const T* zeta, const T* eta, const T* pen,
-                                         T dt, T om) {
+// reference's u_old = u_sol copy).  uo, kap, zeta and eta (read with a
+// stencil) through views; rhs, rho_u and pen (one value per face) at k.
+template <typename T, typename V>
+__device__ __forceinline__ T jacobi_u_vals(const Geo& g, int k, int i, int j, const V& uo, const V& kap,
+                                           const V& zeta, const V& eta, const T* rhs, const T* rho_u, const T* pen,
+                                           T dt, T om) {
   const int nx = g.nx, ny = g.ny;
-  T val = uo[k];
+  T val = uo(i, j);
   if (j >= 1 && j <= ny) {
     if (i >= 1 && i <= g.imax()) {
       const T ix2 = T(g.idx2), iy2 = T(g.idy2);
-      const T cE = kap[g.at(i + 1, j)] * ix2;
-      const T cW = kap[k] * ix2;
-      const T cN = (zeta[k] - eta[k]) * iy2;
-      const T cS = (zeta[g.at(i, j - 1)] - eta[g.at(i, j - 1)]) * iy2;
+      const T cE = kap(i + 1, j) * ix2;
+      const T cW = kap(i, j) * ix2;
+      const T cN = (zeta(i, j) - eta(i, j)) * iy2;
+      const T cS = (zeta(i, j - 1) - eta(i, j - 1)) * iy2;
       T diag = (rho_u[k] / dt) + cE + cW + cN + cS;
       if (pen) diag = diag + pen[k];
-      const T off = madd(cS, uo[g.at(i, j - 1)],
-                         madd(cN, uo[g.at(i, j + 1)], madd(cW, uo[g.at(i - 1, j)], cE * uo[g.at(i + 1, j)])));
-      if (diag > T(1.0e-15)) val = madd(T(1) - om, uo[k], om * ((rhs[k] + off) / diag));
+      const T off = madd(cS, uo(i, j - 1), madd(cN, uo(i, j + 1), madd(cW, uo(i - 1, j), cE * uo(i + 1, j))));
+      if (diag > T(1.0e-15)) val = madd(T(1) - om, uo(i, j), om * ((rhs[k] + off) / diag));
     } else if (!g.px && (i == 0 || i == nx)) {
       val = rhs[k];
     }
   }
   return val;
+}
+template <typename T>
+__device__ __forceinline__ T jacobi_u_at(const Geo& g, int k, int i, int j, const T* uo, const T* rhs,
+                                         const T* rho_u, const T* kap, const T* zeta, const T* eta, const T* pen,
+                                         T dt, T om) {
+  return jacobi_u_vals<T>(g, k, i, j, gview(g, uo), gview(g, kap), gview(g, zeta), gview(g, eta), rhs, rho_u, pen, dt,
+                          om);
 }
 template <typename T>
 __global__ void k_jacobi_u(Geo g, const T* uo, T* un, const T* rhs, const T* rho_u, const T* kap,
@@ -512,29 +651,35 @@ __global__ void k_jacobi_u(Geo g, const T* uo, T* un, const T* rhs, const T* rho
 }
 
 // One damped-Jacobi sweep of solve_helmholtz_v (mod_subsolvers.f90:346-369)
-template <typename T>
-__device__ __forceinline__ T jacobi_v_at(const Geo& g, int k, int i, int j, const T* vo, const T* rhs,
-                                         const T* rho_v, const T* kap, const T* zeta, const T* eta, const T* pen,
-                                         T dt, T om) {
+template <typename T, typename V>
+__device__ __forceinline__ T jacobi_v_vals(const Geo& g, int k, int i, int j, const V& vo, const V& kap,
+                                           const V& zeta, const V& eta, const T* rhs, const T* rho_v, const T* pen,
+                                           T dt, T om) {
   const int nx = g.nx, ny = g.ny;
-  T val = vo[k];
+  T val = vo(i, j);
   if (i >= 1 && i <= nx) {
     if (j >= 1 && j <= g.jmax()) {
       const T ix2 = T(g.idx2), iy2 = T(g.idy2);
-      const T cE = (zeta[k] - eta[k]) * ix2;
-      const T cW = (zeta[g.at(i - 1, j)] - eta[g.at(i - 1, j)]) * ix2;
-      const T cN = kap[g.at(i, j + 1)] * iy2;
-      const T cS = kap[k] * iy2;
+      const T cE = (zeta(i, j) - eta(i, j)) * ix2;
+      const T cW = (zeta(i - 1, j) - eta(i - 1, j)) * ix2;
+      const T cN = kap(i, j + 1) * iy2;
+      const T cS = kap(i, j) * iy2;
       T diag = (rho_v[k] / dt) + cE + cW + cN + cS;
       if (pen) diag = diag + pen[k];
-      const T off = madd(cS, vo[g.at(i, j - 1)],
-                         madd(cN, vo[g.at(i, j + 1)], madd(cW, vo[g.at(i - 1, j)], cE * vo[g.at(i + 1, j)])));
-      if (diag > T(1.0e-15)) val = madd(T(1) - om, vo[k], om * ((rhs[k] + off) / diag));
+      const T off = madd(cS, vo(i, j - 1), madd(cN, vo(i, j + 1), madd(cW, vo(i - 1, j), cE * vo(i + 1, j))));
+      if (diag > T(1.0e-15)) val = madd(T(1) - om, vo(i, j), om * ((rhs[k] + off) / diag));
     } else if (!g.py && (j == 0 || j == ny)) {
       val = rhs[k];
     }
   }
   return val;
+}
+template <typename T>
+__device__ __forceinline__ T jacobi_v_at(const Geo& g, int k, int i, int j, const T* vo, const T* rhs,
+                                         const T* rho_v, const T* kap, const T* zeta, const T* eta, const T* pen,
+                                         T dt, T om) {
+  return jacobi_v_vals<T>(g, k, i, j, gview(g, vo), gview(g, kap), gview(g, zeta), gview(g, eta), rhs, rho_v, pen, dt,
+                          om);
 }
 template <typename T>
 __global__ void k_jacobi_v(Geo g, const T* vo, T* vn, const T* rhs, const T* rho_v, const T* kap,

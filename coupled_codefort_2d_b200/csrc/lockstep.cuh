@@ -16,7 +16,7 @@
 //
 // Families (virtual blocks of LS_TPB threads):
 //   box   32 x 8 tiles of the case's padded box (the stencil kernels)
-//   tile  RB_TX x RB_TY tiles (the fused red-black SOR sweeps)
+//   tile  RB_TX x RB_TY tiles (the fused red-black SOR sweeps, the staged matvec)
 //   e1    element-wise over a coupled triple, four elements per thread
 //   dot   the coupled dot + Krylov scalar op (dot_grid blocks per case)
 //   mdot  the FGMRES multi-vector dots (G(nvec) x nvec blocks per case)
@@ -81,7 +81,7 @@ struct LsPlan {
   int dot[LS_MAX + 1];
   int mdot[LS_MAX + 1];   // nvec vectors
   int mdot1[LS_MAX + 1];  // one vector (the norms)
-  int tile[LS_MAX + 1];   // RB_TX x RB_TY tiles (the fused red-black sweeps)
+  int tile[LS_MAX + 1];   // RB_TX x RB_TY tiles (the fused red-black sweeps, the matvec)
 };
 
 // per-case values the host reads after a phase
@@ -295,18 +295,6 @@ struct LsMatvecOuter {
     const double* X = c.X;
     double* Y = c.ax;
     matvec_at<double>(c.g, ls_coefs(c.c64, d), X, X + c.n, X + 2 * c.n, Y, Y + c.n, Y + 2 * c.n, d.dt, 1, k, i, j);
-  }
-};
-// w = A Z_j of Arnoldi step j
-template <typename T>
-struct LsMatvecInner {
-  int jj;
-  __device__ void operator()(const LsCase<T>& c, const LsDyn& d, int, int k, int i, int j) const {
-    if (!c.ks->active) return;
-    if (k == 0) atomicAdd(&c.ks->matvecs, 1ull);
-    const T* X = c.Z + (long)jj * 3 * c.n;
-    T* Y = c.w;
-    matvec_at<T>(c.g, ls_coefs(c.cf, d), X, X + c.n, X + 2 * c.n, Y, Y + c.n, Y + 2 * c.n, T(d.dt), 1, k, i, j);
   }
 };
 
@@ -667,6 +655,29 @@ __global__ void __launch_bounds__(RB_TPB) k_ls_rbsor(const LsCase<T>* cs, const 
     rbsor_sweep_tile<T>(c.g, comp, lb % ntx, lb / ntx, src, dst, comp == 0 ? c.zuw : c.zvw,
                         comp == 0 ? c.cf.rho_u : c.cf.rho_v, c.cf.kappa, c.cf.zeta, c.cf.eta, pen, T(d.dt),
                         T(c.sor_omega), sm);
+  }
+}
+
+// w = A Z_j of Arnoldi step j, on the staged tiles of k_matvec_tile (the tile
+// family: its RB_TX x RB_TY tiles are MT_TX x RB_TY matvec tiles)
+static_assert(MT_TX == RB_TX && RB_TY % 8 == 0, "the matvec tiles are the tile family's tiles");
+template <typename T>
+__global__ void __launch_bounds__(MT_TPB) k_ls_matvec(const LsCase<T>* cs, const LsDyn* dyn, const LsPlan* P,
+                                                      int jj) {
+  extern __shared__ __align__(16) unsigned char mt_smem[];
+  const int na = P->n, total = P->tile[na];
+  for (int vb = blockIdx.x; vb < total; vb += gridDim.x) {
+    const int kk = ls_find(P->tile, na, vb);
+    const int s = P->slot[kk];
+    const LsCase<T>& c = cs[s];
+    const LsDyn& d = dyn[s];
+    __syncthreads();  // the previous tile is done with shared memory
+    if (!c.ks->active) continue;
+    const int lb = vb - P->tile[kk], ntx = (c.g.P + MT_TX - 1) / MT_TX;
+    if (lb == 0 && threadIdx.x == 0) atomicAdd(&c.ks->matvecs, 1ull);
+    const T* X = c.Z + (long)jj * 3 * c.n;
+    matvec_tile<T, RB_TY>(c.g, ls_coefs(c.cf, d), X, X + c.n, X + 2 * c.n, c.w, c.w + c.n, c.w + 2 * c.n, T(d.dt), 1,
+                          lb % ntx, lb / ntx, (T*)mt_smem);
   }
 }
 

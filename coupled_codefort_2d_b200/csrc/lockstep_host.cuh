@@ -248,11 +248,11 @@ struct Lockstep : LockstepBase {
   }
 
   // co-resident CTAs of a family kernel (its persistent grid)
-  int grid_of(const void* fn, int tpb) {
+  int grid_of(const void* fn, int tpb, size_t smem = 0) {
     auto it = grids.find(fn);
     if (it != grids.end()) return it->second;
     int occ = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, tpb, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, tpb, smem));
     const int g = nsm * (occ > 0 ? occ : 1);
     grids.emplace(fn, g);
     return g;
@@ -263,7 +263,7 @@ struct Lockstep : LockstepBase {
   template <class F>
   void warm_e1() { grid_of((const void*)k_ls_e1<T, F>, LS_TPB); }
   void warm_grids() {
-    warm_box<LsMatvecOuter<T>>(); warm_box<LsMatvecInner<T>>(); warm_box<LsPoissonCoefs<T>>();
+    warm_box<LsMatvecOuter<T>>(); warm_box<LsPoissonCoefs<T>>();
     warm_box<LsSchur<T>>(); warm_box<LsZwork<T>>(); warm_box<LsCross<T>>(); warm_box<LsRbsor<T>>();
     warm_box<LsJacobi<T>>();
     warm_e1<LsCvtCoefs<T>>(); warm_e1<LsDefect<T>>(); warm_e1<LsUpdate64<T>>(); warm_e1<LsScaleDefect<T>>();
@@ -273,6 +273,9 @@ struct Lockstep : LockstepBase {
     grid_of((const void*)k_ls_mdot<T>, MDOT_TPB);
     grid_of((const void*)k_ls_maxpy<T>, LS_TPB);
     grid_of((const void*)k_ls_rbsor<T>, RB_TPB);
+    CK(cudaFuncSetAttribute((const void*)k_ls_matvec<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            mt_matvec_smem<T, RB_TY>()));
+    grid_of((const void*)k_ls_matvec<T>, MT_TPB, mt_matvec_smem<T, RB_TY>());
   }
 
   // ------------------------------------------------------- launches
@@ -399,7 +402,11 @@ struct Lockstep : LockstepBase {
     one(LsVbcs<T>{LB_ZJ, j, 0});
     if (any_periodic)
       for (int comp = 0; comp < 3; ++comp) one(LsHalo<T>{LB_ZJ, comp, j, -1});
-    box(LsMatvecInner<T>{j});
+    {
+      const void* fn = (const void*)k_ls_matvec<T>;
+      k_ls_matvec<T><<<grid_of(fn, MT_TPB), MT_TPB, mt_matvec_smem<T, RB_TY>(), q>>>(d_cases, d_dyn, d_plan, j);
+      LSCKL("k_ls_matvec");
+    }
     mdot(1, j + 1, FG_PROJ1, j);
     maxpy(0, j + 1);
     mdot(1, j + 1, FG_PROJ2, j);

@@ -8,10 +8,14 @@ the error against the FP64 oracle stated per result.
 - c4, the batched ensemble: the first case of each grid class (64x128 ..
   256x512) with the ensemble's own solver (flexible GMRES + PCD with the
   viscous Schur term and red-black SOR, adaptive cap and sweeps), 2 steps of
-  the lockstep batch in mixed precision against the FP64 oracle; the same
-  bounds as c2.
-- c3, rising bubble 320 x 640, free-slip sides, BDF2, dt = 5e-4: to t = 0.1
-  (200 steps), mixed against FP64 on the GPU; centroid height and rise
+  the lockstep batch in mixed precision against the FP64 oracle, at the
+  ensemble's tolerance 1e-8 (state difference within 1e-3: both runs meet
+  the residual, and the high density ratios amplify it) and at 1e-11 (the
+  mixed bound 1e-6); fluid-1 volume equal to 1e-12 either way.
+- c3, rising bubble 320 x 640, free-slip sides, BDF2, dt = 5e-4, with the
+  configuration runner's solver (the PCD with the viscous Schur term and
+  red-black SOR): to t = 0.1 (200 steps), mixed against FP64 on the GPU;
+  centroid height and rise
   velocity (test_rising_bubble.f90:134-155) and circularity within 1e-6
   relative of the FP64 run.
 - c1, lid-driven cavity 128^2, Re = 1000, BDF1, dt = 1e-2: all 200 steps at
@@ -31,7 +35,7 @@ import pytest
 from coupled_codefort_2d_b200 import cases, ensemble
 from coupled_codefort_2d_b200._lib import FP64, MIXED
 from coupled_codefort_2d_b200.batch import STATE_FIELDS, Batch, ensemble_params, initial_bubble_state
-from coupled_codefort_2d_b200.configs import SOLVER
+from coupled_codefort_2d_b200.configs import BUBBLE, SOLVER
 from coupled_codefort_2d_b200.context import Context
 from coupled_codefort_2d_b200.layout import Grid, at
 from coupled_codefort_2d_b200.params import Params
@@ -41,6 +45,15 @@ pytestmark = [pytest.mark.gpu, pytest.mark.slow]
 STATE = list(STATE_FIELDS)
 MIXED_BOUND = 1e-6
 C4_STEPS = 2
+# c4 at the ensemble's tolerance and at a tight one (below)
+C4_TOLS = (1e-8, 1e-11)
+# Two solutions that both meet a true relative residual of 1e-8 differ by up to
+# the system's condition number times 1e-8.  The ensemble's bubbles (density
+# ratios up to 1000 at dt = 5e-4) leave about 1e-4 there, so at the ensemble's
+# own tolerance the state difference is reported against this bound and the
+# precision bound MIXED_BOUND is checked at 1e-11, where the tolerance's share
+# is a thousand times smaller.
+C4_TOL_BOUND = 1e-3
 
 
 def c1_case():
@@ -75,14 +88,15 @@ def oracle_run(oracle_mod, g, p, c0, dt, nsteps, kw):
 @pytest.fixture(scope="module")
 def oracle_runs(oracle_mod):
     """Every oracle run of the module, started at once in host threads."""
-    pool = cf.ThreadPoolExecutor(max_workers=8)
+    pool = cf.ThreadPoolExecutor(max_workers=12)
     jobs = {"c1": pool.submit(oracle_run, oracle_mod, *c1_case()),
             "c2": pool.submit(oracle_run, oracle_mod, *c2_case())}
     for s in c4_cases():
         g = s["grid"]
-        p = ensemble_params(s, **ensemble.SOLVER)
         c0 = cases.binary_circle(g, s["xc"], s["yc"], s["radius"], inside=0.0)
-        jobs[("c4", s["case"])] = pool.submit(oracle_run, oracle_mod, g, p, c0, ensemble.DT, C4_STEPS, {})
+        for tol in C4_TOLS:
+            p = ensemble_params(s, **dict(ensemble.SOLVER, tol_bicgstab2=tol))
+            jobs[("c4", s["case"], tol)] = pool.submit(oracle_run, oracle_mod, g, p, c0, ensemble.DT, C4_STEPS, {})
     yield jobs
     pool.shutdown(wait=True)
 
@@ -121,29 +135,32 @@ def test_c2_droplet_50_steps_mixed(gpu, oracle_mod, oracle_runs):
     assert e["volume"] <= 1e-12, e
 
 
-def test_c4_one_case_per_grid_class_lockstep_mixed(gpu, oracle_mod, oracle_runs):
+@pytest.mark.parametrize("tol", C4_TOLS)
+def test_c4_one_case_per_grid_class_lockstep_mixed(gpu, oracle_mod, oracle_runs, tol):
     specs = c4_cases()
-    prms = [ensemble_params(s, **ensemble.SOLVER) for s in specs]
+    prms = [ensemble_params(s, **dict(ensemble.SOLVER, tol_bicgstab2=tol)) for s in specs]
     with Batch([(s["grid"], p, MIXED) for s, p in zip(specs, prms)], lockstep=True) as b:
         for i, s in enumerate(specs):
             initial_bubble_state(b.case(i), s)
         out = b.run(C4_STEPS, ensemble.DT, 1, b.case(0).step_opts(use_bicgstab2=True))
         states = [b.case(i).download_state(STATE) for i in range(len(specs))]
     assert out["status"] == [0] * len(specs)
+    errs = {}
     for i, s in enumerate(specs):
-        st_o, so = oracle_runs[("c4", s["case"])].result()
-        assert out["max_res"][i] < 1e-8 and all(r < 1e-8 for r, _ in so)
-        e = errors(s["grid"], states[i], st_o)
-        print(f"c4 case {s['case']} {s['grid'].nx}x{s['grid'].ny}, {C4_STEPS} steps, lockstep mixed vs FP64 "
-              f"oracle:", e)
-        assert max(e["u"], e["v"], e["p"]) <= MIXED_BOUND, (s["case"], e)
-        assert e["volume"] <= 1e-12, (s["case"], e)
+        st_o, so = oracle_runs[("c4", s["case"], tol)].result()
+        assert out["max_res"][i] < tol and all(r < tol for r, _ in so)
+        errs[s["case"]] = e = errors(s["grid"], states[i], st_o)
+        print(f"c4 case {s['case']} {s['grid'].nx}x{s['grid'].ny}, {C4_STEPS} steps at {tol:g}, lockstep mixed vs "
+              f"FP64 oracle:", e)
+    for case, e in errs.items():
+        assert max(e["u"], e["v"], e["p"]) <= (MIXED_BOUND if tol < 1e-8 else C4_TOL_BOUND), (case, e)
+        assert e["volume"] <= 1e-12, (case, e)
 
 
 def test_c3_bubble_mixed_vs_fp64_diagnostics(gpu, oracle_mod):
     g = Grid(320, 640, 1.0, 2.0)
     p = Params(rho1=1000.0, rho2=100.0, mu1=10.0, mu2=1.0, sigma=24.5, gx=0.0, gy=-0.98, time_order=2,
-               tol_bicgstab2=1e-8, max_iter_bicgstab2=500, free_slip_x=1, **SOLVER)
+               tol_bicgstab2=1e-8, max_iter_bicgstab2=500, free_slip_x=1, **dict(SOLVER, **BUBBLE))
     c0 = cases.binary_circle(g, 0.5, 0.5, 0.25, inside=0.0)
     n = 200  # t = 0.1
     res = {}

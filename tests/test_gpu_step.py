@@ -255,6 +255,31 @@ def test_graph_replay_is_bitwise(gpu, name, precision, refine, prof):
             assert 0 < c1["pcg_iters_timed"] < c1["pcg_iters"]
 
 
+@pytest.mark.parametrize("precision,refine", [(0, 2), (1, 2), (1, 1)])
+def test_graph_replay_with_grid_wide_pcg(gpu, precision, refine, monkeypatch):
+    """The grid-wide PCG (the kernel of cases that do not fit one cluster) is
+    captured into the iteration graphs as a cooperative kernel node: the same
+    bits, iteration counts and launch count as launching one by one.  With
+    profiling on, a replayed flexible-GMRES cycle times only the PCG of its
+    first Arnoldi step, so fewer timed launches show that the graphs ran."""
+    monkeypatch.setenv("FUGU_PCG", "grid")
+    over = dict(refine=refine, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=30, krylov_bc_fix=1,
+                tol_bicgstab2=1e-9)
+    if refine == 2:
+        over.update(pcg_cap_start=2, pcd_sweeps=1, pcd_sweeps_max=8, pcg_max_iter=8)
+    runs = {gr: _device_run("droplet", dict(over, graphs=gr), precision, True) for gr in (0, 1)}
+    (s0, h0, c0), (s1, h1, c1) = runs[0], runs[1]
+    assert c0["pcg_cluster_fp64"] == c0["pcg_cluster_fp32"] == 0
+    for a, b in zip(h0, h1):
+        assert a == b
+    for k in STATE:
+        np.testing.assert_array_equal(s0[k], s1[k], err_msg=k)
+    assert c0["kernel_launches"] == c1["kernel_launches"]
+    assert c0["pcg_iters"] == c1["pcg_iters"]
+    if refine == 2:
+        assert c1["pcg_launches"] < c0["pcg_launches"]
+
+
 def test_checkpoint_restart_bitwise(gpu, oracle_mod):
     """mod_io.f90:169-225 format: the GPU writes the reference's byte layout,
     the oracle reads it back, and a restart reproduces the run bit for bit
