@@ -2881,28 +2881,39 @@ void batch_end(fugu_batch* b) {
   }
 }
 
-// run fn(i) for every case from the batch's host threads (largest first);
-// returns each case's status
+// run fn(i) for the cases ids (in that order) from the batch's host threads;
+// returns a status per case of the batch
 template <typename F>
-std::vector<int> for_cases(fugu_batch* b, F fn) {
-  const int nc = (int)b->cases.size();
-  std::vector<int> st(nc, FUGU_OK);
+std::vector<int> for_ids(fugu_batch* b, const std::vector<int>& ids, F fn) {
+  std::vector<int> st(b->cases.size(), FUGU_OK);
+  const int n = (int)ids.size();
   std::atomic<int> next{0};
   auto work = [&] {
     for (;;) {
       const int k = next.fetch_add(1);
-      if (k >= nc) return;
-      const int i = b->order[k];
+      if (k >= n) return;
+      const int i = ids[k];
       st[i] = guard(b->cases[i], [&] { fn(i); });
     }
   };
+  const int nt = std::min(b->nthreads, n);
   std::vector<std::thread> pool;
-  for (int t = 1; t < b->nthreads; ++t) pool.emplace_back(work);
+  for (int t = 1; t < nt; ++t) pool.emplace_back(work);
   work();
   for (auto& th : pool) th.join();
   return st;
 }
+// the same for every case (largest first)
+template <typename F>
+std::vector<int> for_cases(fugu_batch* b, F fn) {
+  return for_ids(b, b->order, fn);
+}
 
+// The lockstep batch run (continuous batching, lockstep_host.cuh): every
+// case goes through nsteps steps; a case whose solve ends at a pass goes
+// through its final BCs and statistics and its next step's explicit stages
+// on its own stream while the other cases' next cycle runs, and joins the
+// lockstep solve again at the following pass.
 int lockstep_run(fugu_batch* b, int nsteps, const double* dt, const int* step0, const fugu_step_opts* opts,
                  fugu_stats* last, double* max_res, int* status) {
   const int nc = (int)b->cases.size();
@@ -2910,23 +2921,22 @@ int lockstep_run(fugu_batch* b, int nsteps, const double* dt, const int* step0, 
   std::vector<int> cst(nc, FUGU_OK);
   std::vector<fugu_stats> lst(nc);
   int rc = FUGU_OK;
-  cudaStream_t ls_s = b->ls->stream();
+  LockstepBase* ls = b->ls;
+  cudaStream_t ls_s = ls->stream();
   try {
+    ls->reset();
     batch_begin(b);
   } catch (const CudaError& e) {
     b->err = std::string("batch stream: ") + e.what + ": " + cudaGetErrorString(e.e);
     return FUGU_ECUDA;
   }
-  for (int stp = 0; stp < nsteps && rc == FUGU_OK; ++stp) {
-    std::vector<StepSetup> su(nc);
-    for (int i = 0; i < nc; ++i) su[i] = step_setup(b->cases[i], dt[i], step0[i] + stp, &opts[i]);
-    // 1. explicit stages of every case on its own stream
-    std::vector<int> st = for_cases(b, [&](int i) {
-      fugu_ctx* c = b->cases[i];
-      step_pre(c, dt[i], step0[i] + stp, &opts[i]);
-      CK(cudaEventRecord(b->ev_case[i], c->s));
-    });
-    for (int i = 0; i < nc; ++i)
+  std::vector<int> done(nc, 0);  // steps completed per case
+  std::vector<StepSetup> su(nc);
+  std::vector<KrylovResult> kr(nc);
+  std::vector<int> outer(nc, 0);
+  // a failed case stops the run (its status and the batch's message)
+  auto take = [&](const std::vector<int>& st, const std::vector<int>& ids) {
+    for (int i : ids)
       if (st[i] != FUGU_OK) {
         cst[i] = st[i];
         if (rc == FUGU_OK) {
@@ -2934,43 +2944,62 @@ int lockstep_run(fugu_batch* b, int nsteps, const double* dt, const int* step0, 
           b->err = "case " + std::to_string(i) + ": " + b->cases[i]->err;
         }
       }
-    if (rc != FUGU_OK) break;
-    // 2. the coupled solves in lockstep
-    std::vector<KrylovResult> kr;
-    std::vector<int> outer;
-    try {
-      CK(cudaSetDevice(b->device));
-      for (int i = 0; i < nc; ++i) CK(cudaStreamWaitEvent(ls_s, b->ev_case[i], 0));
-      NvtxRange r_solve("lockstep_coupled_solves");
-      b->ls->solve(su, kr, outer);
-      CK(cudaEventRecord(b->ev_solve, ls_s));
-    } catch (const CudaError& e) {
-      b->err = std::string("lockstep solve: ") + e.what + ": " + cudaGetErrorString(e.e);
-      rc = FUGU_ECUDA;
-    } catch (const ApiError& e) {
-      b->err = "lockstep solve: " + e.msg;
-      rc = e.code;
-    }
-    if (rc != FUGU_OK) {
-      for (int i = 0; i < nc; ++i) cst[i] = rc;
-      break;
-    }
-    // 3. final BCs and statistics of every case
-    st = for_cases(b, [&](int i) {
-      fugu_ctx* c = b->cases[i];
-      CK(cudaStreamWaitEvent(c->s, b->ev_solve, 0));
-      std::memset(&lst[i], 0, sizeof(fugu_stats));
-      step_post(c, su[i], kr[i], outer[i], &lst[i]);
-      if (lst[i].res > mres[i] || std::isnan(lst[i].res)) mres[i] = lst[i].res;
-    });
-    for (int i = 0; i < nc; ++i)
-      if (st[i] != FUGU_OK) {
-        cst[i] = st[i];
-        if (rc == FUGU_OK) {
-          rc = st[i];
-          b->err = "case " + std::to_string(i) + ": " + b->cases[i]->err;
-        }
+  };
+  // explicit stages of the next step of ids, each on its own stream
+  auto pre = [&](int i) {
+    fugu_ctx* c = b->cases[i];
+    su[i] = step_setup(c, dt[i], step0[i] + done[i], &opts[i]);
+    step_pre(c, dt[i], step0[i] + done[i], &opts[i]);
+    CK(cudaEventRecord(b->ev_case[i], c->s));
+  };
+  std::vector<int> joining;
+  if (nsteps > 0) {
+    joining = b->order;
+    take(for_ids(b, joining, pre), joining);
+  }
+  try {
+    CK(cudaSetDevice(b->device));
+    while (rc == FUGU_OK) {
+      // the cases whose explicit stages were issued join the solve
+      if (!joining.empty()) {
+        for (int i : joining) CK(cudaStreamWaitEvent(ls_s, b->ev_case[i], 0));
+        ls->join(joining, su);
+        joining.clear();
       }
+      std::vector<int> ended = ls->defect();
+      if (!ended.empty()) {
+        ls->finish(ended, kr, outer);
+        CK(cudaEventRecord(b->ev_solve, ls_s));
+      }
+      const bool cycling = ls->cycle_launch();
+      if (!ended.empty()) {
+        // meanwhile on the host threads: the ended steps' final BCs and
+        // statistics, and the next steps' explicit stages
+        std::vector<int> st = for_ids(b, ended, [&](int i) {
+          fugu_ctx* c = b->cases[i];
+          CK(cudaStreamWaitEvent(c->s, b->ev_solve, 0));
+          std::memset(&lst[i], 0, sizeof(fugu_stats));
+          step_post(c, su[i], kr[i], outer[i], &lst[i]);
+          if (lst[i].res > mres[i] || std::isnan(lst[i].res)) mres[i] = lst[i].res;
+          if (++done[i] < nsteps) pre(i);
+        });
+        take(st, ended);
+        for (int i : ended)
+          if (done[i] < nsteps) joining.push_back(i);
+      }
+      if (cycling) ls->cycle_finish();
+      if (!cycling && joining.empty()) break;
+    }
+  } catch (const CudaError& e) {
+    b->err = std::string("lockstep solve: ") + e.what + ": " + cudaGetErrorString(e.e);
+    rc = FUGU_ECUDA;
+  } catch (const ApiError& e) {
+    b->err = "lockstep solve: " + e.msg;
+    rc = e.code;
+  }
+  if (rc != FUGU_OK) {
+    for (int i = 0; i < nc; ++i)
+      if (cst[i] == FUGU_OK) cst[i] = rc;
   }
   if (rc == FUGU_OK) {
     try {

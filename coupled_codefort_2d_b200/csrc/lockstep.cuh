@@ -217,12 +217,15 @@ __global__ void k_ls_all(const LsCase<T>* cs, const LsDyn* dyn, int ncase, F f) 
   }
 
 // ------------------------------------------------------------ functors
-// Krylov state of a pass (reset_ks in fugu_gpu.cu, with active = run)
+// Krylov state of a pass (reset_ks in fugu_gpu.cu) for the cases in it
 struct LsResetKs {
   template <typename C>
   __device__ void operator()(const C& c, const LsDyn& d, int) const {
-    if (threadIdx.x == 0) {
-      c.ks->active = d.run;
+    // a case outside the pass keeps its flags: it may be between steps, its
+    // own stream working on its context (nothing reads its flags without
+    // checking d.run first)
+    if (threadIdx.x == 0 && d.run) {
+      c.ks->active = 1;
       c.ks->exit_iter = 0;
       c.ks->nan = 0;
       c.ks->ticket = 0;

@@ -1,18 +1,24 @@
 // lockstep_host.cuh -- host side of the fused batched form (lockstep.cuh).
 // Included by fugu_gpu.cu after the context, the step and the solvers.
 //
-// One batch step:
-//   1. each case's explicit stages (AB extrapolation, VOF, properties, SVOF,
+// A batch run advances every case through its steps; a case's step is
+//   1. its explicit stages (AB extrapolation, VOF, properties, SVOF,
 //      curvature, CSF, right-hand side) on the case's own stream, issued by
 //      the batch's host threads (step_pre);
-//   2. the coupled solves of all cases in lockstep on the lockstep stream:
-//      the FP64 defect correction around flexible GMRES + PCD (refine_solve
-//      and fgmres in fugu_gpu.cu), every phase one launch per kernel family
-//      for all cases still running; each flexible-GMRES cycle is one CUDA
-//      graph whose Arnoldi steps sit in conditional nodes armed on the device;
-//   3. each case's final halos, wall BCs and statistics (step_post).
-// The host synchronises twice per defect-correction pass for the whole batch
-// (the single-case form does so per Arnoldi step and per case).
+//   2. its coupled solve, in lockstep with the other running cases on the
+//      lockstep stream: the FP64 defect correction around flexible GMRES +
+//      PCD (refine_solve and fgmres in fugu_gpu.cu), every phase one launch
+//      per kernel family for all running cases; each flexible-GMRES cycle is
+//      one CUDA graph whose Arnoldi steps sit in conditional nodes armed on
+//      the device;
+//   3. its final halos, wall BCs and statistics (step_post).
+// The cases do not wait for one another between steps: a case whose solve
+// ends at a defect-correction pass goes through 3 and 1 of its next step
+// while the others' next cycle runs, and joins the lockstep solve again at
+// the following pass (continuous batching).  So the batch's time follows the
+// sum of the work rather than the slowest case of every step.  The host
+// synchronises twice per defect-correction pass for the whole batch (the
+// single-case form does so per Arnoldi step and per case).
 #pragma once
 
 #include "lockstep.cuh"
@@ -46,7 +52,21 @@ struct LsCaseRun {
 
 struct LockstepBase {
   virtual ~LockstepBase() {}
-  virtual void solve(const std::vector<StepSetup>& su, std::vector<KrylovResult>& kr, std::vector<int>& outer) = 0;
+  // a run starts: no case is in the solve (after a run that ended in an
+  // error too)
+  virtual void reset() = 0;
+  // the solves of cases ids start (their explicit stages are done before the
+  // lockstep stream's current position)
+  virtual void join(const std::vector<int>& ids, const std::vector<StepSetup>& su) = 0;
+  // a defect pass of the running cases; returns the cases whose solve ended
+  virtual std::vector<int> defect() = 0;
+  // end the solves of ids: the final wall BCs with the lid, their results
+  // and the adaptive PCG cap and sweeps back to their contexts
+  virtual void finish(const std::vector<int>& ids, std::vector<KrylovResult>& kr, std::vector<int>& outer) = 0;
+  // queue one flexible-GMRES cycle of the running cases (false: none runs)
+  virtual bool cycle_launch() = 0;
+  // wait for it, adapt the cases' PCG caps and sweeps, set up the next pass
+  virtual void cycle_finish() = 0;
   virtual cudaStream_t stream() const = 0;
   virtual unsigned long long launch_count() const = 0;
 };
@@ -64,7 +84,13 @@ struct Lockstep : LockstepBase {
   std::vector<cudaEvent_t> ev_join;
   LsCase<T>* d_cases = nullptr;
   LsDyn* d_dyn = nullptr;
-  LsDyn* h_dyn = nullptr;
+  LsDyn* h_dyn = nullptr;   // the host's copy, uploaded through h_ring
+  // pinned snapshots of h_dyn, one per upload since the lockstep stream last
+  // synchronised (a pinned copy is read when the stream reaches it, so a
+  // buffer the host changes again cannot be its source)
+  static constexpr int RING = 8;
+  LsDyn* h_ring = nullptr;
+  int ring_next = 0;
   LsPlan* d_plan = nullptr;
   LsRead* d_read = nullptr;
   LsRead* h_read = nullptr;
@@ -80,14 +106,17 @@ struct Lockstep : LockstepBase {
   };
   std::vector<Graph> graphs;
   // one whole flexible-GMRES cycle as one graph (a conditional IF node per
-  // Arnoldi step), rebuilt when the sweep count changes
+  // Arnoldi step), one per largest sweep count of the running cases
   struct Cycle {
-    int max_sweeps = -1;
     cudaGraphExec_t exec = nullptr;
     unsigned long long head = 0, body = 0;  // launches outside the steps, per executed step
-  } cyc;
+  };
+  std::map<int, Cycle> cycles;
   bool use_cycle_graph = true;
   std::vector<void*> allocs;
+  // the continuous run: per case its solve's bookkeeping and whether it runs
+  std::vector<LsCaseRun> cr;
+  std::vector<char> running;
 
   cudaStream_t stream() const override { return s; }
   unsigned long long launch_count() const override { return launches; }
@@ -96,11 +125,13 @@ struct Lockstep : LockstepBase {
     if (s) cudaStreamSynchronize(s);
     for (auto& g : graphs)
       if (g.exec) cudaGraphExecDestroy(g.exec);
-    if (cyc.exec) cudaGraphExecDestroy(cyc.exec);
+    for (auto& kv : cycles)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     for (auto& c : classes)
       if (c.d_list) cudaFree(c.d_list);
     for (void* p : allocs) cudaFree(p);
     if (h_dyn) cudaFreeHost(h_dyn);
+    if (h_ring) cudaFreeHost(h_ring);
     if (h_read) cudaFreeHost(h_read);
     if (h_nact) cudaFreeHost(h_nact);
     if (ev_fork) cudaEventDestroy(ev_fork);
@@ -207,6 +238,9 @@ struct Lockstep : LockstepBase {
     d_plan = dal<LsPlan>(1);
     d_read = dal<LsRead>(ncase);
     CK(cudaMallocHost(&h_dyn, sizeof(LsDyn) * ncase));
+    CK(cudaMallocHost(&h_ring, sizeof(LsDyn) * ncase * RING));
+    cr.assign(ncase, LsCaseRun{});
+    running.assign(ncase, 0);
     CK(cudaMallocHost(&h_read, sizeof(LsRead) * ncase));
     CK(cudaMallocHost(&h_nact, sizeof(int)));
     std::memset(h_dyn, 0, sizeof(LsDyn) * ncase);
@@ -352,11 +386,26 @@ struct Lockstep : LockstepBase {
       }
     }
   }
-  void upload_dyn() { CK(cudaMemcpyAsync(d_dyn, h_dyn, sizeof(LsDyn) * ncase, cudaMemcpyHostToDevice, s)); }
+  void sync() {
+    CK(cudaStreamSynchronize(s));
+    ring_next = 0;  // every queued upload has been read
+  }
+  void upload_dyn() {
+    if (ring_next == RING) sync();
+    LsDyn* src = h_ring + (size_t)ring_next++ * ncase;
+    std::memcpy(src, h_dyn, sizeof(LsDyn) * ncase);
+    CK(cudaMemcpyAsync(d_dyn, src, sizeof(LsDyn) * ncase, cudaMemcpyHostToDevice, s));
+  }
+  // run flags: the running cases (or only the cases in ids)
+  void set_run(const std::vector<int>* ids = nullptr) {
+    for (int i = 0; i < ncase; ++i) h_dyn[i].run = ids ? 0 : running[i];
+    if (ids)
+      for (int i : *ids) h_dyn[i].run = 1;
+  }
   void readback() {
     all(LsReadback<T>{d_read, m});
     CK(cudaMemcpyAsync(h_read, d_read, sizeof(LsRead) * ncase, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
+    sync();
   }
 
   // ----------------------------------------------- one Arnoldi step j
@@ -452,6 +501,7 @@ struct Lockstep : LockstepBase {
   // node is not armed is skipped on the device, and so is every later one.
   void build_cycle(int max_sw) {
     const FgLayout L{m};
+    Cycle& cyc = cycles[max_sw];
     if (cyc.exec) CK(cudaGraphExecDestroy(cyc.exec));
     cyc.exec = nullptr;
     const unsigned long long before = launches;
@@ -521,12 +571,11 @@ struct Lockstep : LockstepBase {
     const cudaError_t e = cudaGraphInstantiate(&cyc.exec, graph, 0);
     cudaGraphDestroy(graph);
     CK(e);
-    cyc.max_sweeps = max_sw;
   }
 
   // one flexible-GMRES(m) cycle of every running case from a zero correction
   void fgmres_cycle(int max_sw) {
-    if (use_cycle_graph && (!cyc.exec || cyc.max_sweeps != max_sw)) {
+    if (use_cycle_graph && !cycles[max_sw].exec) {
       try {
         build_cycle(max_sw);
       } catch (const CudaError&) {
@@ -537,8 +586,10 @@ struct Lockstep : LockstepBase {
       }
     }
     if (use_cycle_graph) {
+      const Cycle& cyc = cycles[max_sw];
       CK(cudaGraphLaunch(cyc.exec, s));
-      launches += cyc.head;  // the executed steps' launches are added by the caller
+      launches += cyc.head;  // the executed steps' launches are added after the cycle
+      cyc_body = cyc.body;
       return;
     }
     const FgLayout L{m};
@@ -561,22 +612,30 @@ struct Lockstep : LockstepBase {
   }
 
   // ------------------------------------------------ the lockstep solve
-  // refine_solve (fugu_gpu.cu) for every case at once
-  void solve(const std::vector<StepSetup>& su, std::vector<KrylovResult>& kr, std::vector<int>& outer) override {
+  // refine_solve (fugu_gpu.cu) for every running case at once, split at its
+  // host checks so that cases can join and leave at every pass
+  unsigned long long cyc_body = 0;  // launches of one executed Arnoldi step of the last cycle
+
+  void reset() override {
+    CK(cudaSetDevice(device));
+    sync();
+    running.assign(ncase, 0);
+  }
+
+  void join(const std::vector<int>& ids, const std::vector<StepSetup>& su) override {
     CK(cudaSetDevice(device));
     q = s;
-    std::vector<LsCaseRun> cr(ncase);
-    for (int i = 0; i < ncase; ++i) {
+    for (int i : ids) {
       fugu_ctx* c = cases[i];
       const fugu_params& p = c->prm;
       LsCaseRun& r = cr[i];
+      r = LsCaseRun{};
       r.adapt = p.pcg_cap_start > 0;
       r.adapt_sw = p.pcd_sweeps_max > p.pcd_sweeps;
       if (r.adapt) r.cap = std::min(std::max(p.pcg_cap_start, c->pcg_cap_state), p.pcg_max_iter);
       if (r.adapt_sw) r.sweeps = std::min(std::max(p.pcd_sweeps, c->pcd_sweeps_state), p.pcd_sweeps_max);
       r.tol = su[i].tol;
       LsDyn& d = h_dyn[i];
-      d.run = 1;
       d.pcg_cap = r.cap > 0 ? r.cap : p.pcg_max_iter;
       d.sweeps = r.sweeps > 0 ? r.sweeps : p.pcd_sweeps;
       d.pen = su[i].pen ? 1 : 0;
@@ -585,6 +644,7 @@ struct Lockstep : LockstepBase {
       d.dt = su[i].dt_eff;
       d.lid = su[i].lid;
     }
+    set_run(&ids);
     upload_dyn();
     plan(0, 1);
     if constexpr (sizeof(T) == 4) e1(LsCvtCoefs<T>{});
@@ -592,85 +652,49 @@ struct Lockstep : LockstepBase {
     all(LsResetKs{});
     one(LsVbcs<T>{LB_X, 0, 0});
     dot(0, OP_REF_NORMB);
-    for (;;) {
-      NvtxRange r_pass("lockstep_defect_correction_pass");
-      plan(0, 1);
-      if (any_periodic)
-        for (int comp = 0; comp < 3; ++comp) one(LsHalo<T>{LB_X, comp, 0, -1});
-      box(LsMatvecOuter<T>{});
-      e1(LsDefect<T>{});
-      dot(1, OP_REF_REL);
-      readback();
-      int nrun = 0, max_sw = 0;
-      for (int i = 0; i < ncase; ++i) {
-        LsCaseRun& r = cr[i];
-        LsDyn& d = h_dyn[i];
-        if (r.done) continue;
-        const double rel = h_read[i].true_rel;
-        r.rel = rel;
-        if (h_read[i].nan || std::isnan(rel)) {
-          r.status = FUGU_NAN;
-          r.done = true;
-        } else if (rel < r.tol) {
-          r.status = FUGU_CONVERGED;
-          r.done = true;
-        } else if (r.outer >= cases[i]->prm.refine_max_outer) {
-          r.status = FUGU_MAXITER;
-          r.done = true;
-        }
-        d.run = r.done ? 0 : 1;
-        if (!r.done) {
-          ++nrun;
-          max_sw = std::max(max_sw, d.sweeps);
-        }
-      }
-      if (!nrun) break;
-      upload_dyn();
-      plan(0, 1);
-      if constexpr (sizeof(T) == 4) e1(LsScaleDefect<T>{});
-      else e1(LsZeroCorrection<T>{});
-      fgmres_cycle(max_sw);
-      plan(0, 1);
-      if constexpr (sizeof(T) == 4) e1(LsAccumulate<T>{});
-      else e1(LsUpdate64<T>{});
-      readback();
-      int steps_run = 0;
-      for (int i = 0; i < ncase; ++i)
-        if (!cr[i].done) steps_run = std::max(steps_run, h_read[i].active ? m : h_read[i].exit_iter);
-      if (use_cycle_graph) launches += cyc.body * (unsigned long long)steps_run;
-      for (int i = 0; i < ncase; ++i) {
-        LsCaseRun& r = cr[i];
-        if (r.done) continue;
-        const fugu_params& p = cases[i]->prm;
-        const LsRead& rd = h_read[i];
-        r.inner_total += rd.active ? m : rd.exit_iter;
-        const double ir = rd.inner_rel;
-        LsDyn& d = h_dyn[i];
-        if (!(ir < p.refine_inner_tol)) {
-          if (r.adapt && r.cap < p.pcg_max_iter) {
-            r.cap = std::min(2 * r.cap, p.pcg_max_iter);
-            d.pcg_cap = r.cap;
-          } else if (r.adapt_sw && r.sweeps < p.pcd_sweeps_max) {
-            r.sweeps = std::min(2 * r.sweeps, p.pcd_sweeps_max);
-            d.sweeps = r.sweeps;
-          }
-        }
-        ++r.outer;
-      }
-      upload_dyn();
-      all(LsResetKs{});
-      one(LsVbcs<T>{LB_X, 0, 0});
+    for (int i : ids) running[i] = 1;
+  }
+
+  std::vector<int> defect() override {
+    NvtxRange r_pass("lockstep_defect_correction_pass");
+    q = s;
+    set_run();
+    upload_dyn();
+    plan(0, 1);
+    if (any_periodic)
+      for (int comp = 0; comp < 3; ++comp) one(LsHalo<T>{LB_X, comp, 0, -1});
+    box(LsMatvecOuter<T>{});
+    e1(LsDefect<T>{});
+    dot(1, OP_REF_REL);
+    readback();
+    std::vector<int> ended;
+    for (int i = 0; i < ncase; ++i) {
+      if (!running[i]) continue;
+      LsCaseRun& r = cr[i];
+      const double rel = h_read[i].true_rel;
+      r.rel = rel;
+      if (h_read[i].nan || std::isnan(rel)) r.status = FUGU_NAN;
+      else if (rel < r.tol) r.status = FUGU_CONVERGED;
+      else if (r.outer >= cases[i]->prm.refine_max_outer) r.status = FUGU_MAXITER;
+      else continue;
+      r.done = true;
+      ended.push_back(i);
     }
-    // the lid of every case (refine_solve's final vbcs with has_lid)
-    for (int i = 0; i < ncase; ++i) h_dyn[i].run = 1;
+    return ended;
+  }
+
+  void finish(const std::vector<int>& ids, std::vector<KrylovResult>& kr, std::vector<int>& outer) override {
+    q = s;
+    for (int i : ids) running[i] = 0;
+    if (ids.empty()) return;
+    // the lid (refine_solve's final vbcs with has_lid)
+    set_run(&ids);
     upload_dyn();
     plan(0, 1);
     one(LsVbcs<T>{LB_X, 0, 1});
-    kr.assign(ncase, KrylovResult{});
-    outer.assign(ncase, 0);
-    for (int i = 0; i < ncase; ++i) {
+    for (int i : ids) {
       fugu_ctx* c = cases[i];
-      LsCaseRun& r = cr[i];
+      const LsCaseRun& r = cr[i];
       if (r.adapt) c->pcg_cap_state = r.cap;
       if (r.adapt_sw) c->pcd_sweeps_state = r.sweeps;
       kr[i].iter = r.inner_total;
@@ -678,6 +702,60 @@ struct Lockstep : LockstepBase {
       kr[i].status = r.status;
       outer[i] = r.outer;
     }
+  }
+
+  bool cycle_launch() override {
+    q = s;
+    int max_sw = 0;
+    bool any = false;
+    for (int i = 0; i < ncase; ++i)
+      if (running[i]) {
+        any = true;
+        max_sw = std::max(max_sw, h_dyn[i].sweeps);
+      }
+    if (!any) return false;
+    set_run();
+    upload_dyn();
+    plan(0, 1);
+    if constexpr (sizeof(T) == 4) e1(LsScaleDefect<T>{});
+    else e1(LsZeroCorrection<T>{});
+    fgmres_cycle(max_sw);
+    plan(0, 1);
+    if constexpr (sizeof(T) == 4) e1(LsAccumulate<T>{});
+    else e1(LsUpdate64<T>{});
+    return true;
+  }
+
+  void cycle_finish() override {
+    readback();
+    int steps_run = 0;
+    for (int i = 0; i < ncase; ++i)
+      if (running[i]) steps_run = std::max(steps_run, h_read[i].active ? m : h_read[i].exit_iter);
+    if (use_cycle_graph) launches += cyc_body * (unsigned long long)steps_run;
+    for (int i = 0; i < ncase; ++i) {
+      if (!running[i]) continue;
+      LsCaseRun& r = cr[i];
+      const fugu_params& p = cases[i]->prm;
+      const LsRead& rd = h_read[i];
+      r.inner_total += rd.active ? m : rd.exit_iter;
+      const double ir = rd.inner_rel;
+      LsDyn& d = h_dyn[i];
+      if (!(ir < p.refine_inner_tol)) {
+        if (r.adapt && r.cap < p.pcg_max_iter) {
+          r.cap = std::min(2 * r.cap, p.pcg_max_iter);
+          d.pcg_cap = r.cap;
+        } else if (r.adapt_sw && r.sweeps < p.pcd_sweeps_max) {
+          r.sweeps = std::min(2 * r.sweeps, p.pcd_sweeps_max);
+          d.sweeps = r.sweeps;
+        }
+      }
+      ++r.outer;
+    }
+    set_run();
+    upload_dyn();
+    plan(0, 1);
+    all(LsResetKs{});
+    one(LsVbcs<T>{LB_X, 0, 0});
   }
 };
 

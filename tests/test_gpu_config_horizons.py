@@ -11,7 +11,7 @@ the error against the FP64 oracle stated per result.
   the lockstep batch in mixed precision against the FP64 oracle, at the
   ensemble's tolerance 1e-8 (state difference within 1e-3: both runs meet
   the residual, and the high density ratios amplify it) and at 1e-11 (the
-  mixed bound 1e-6); fluid-1 volume equal to 1e-12 either way.
+  mixed bound 1e-6); fluid-1 volume equal to 1e-10 and 1e-12.
 - c3, rising bubble 320 x 640, free-slip sides, BDF2, dt = 5e-4, with the
   configuration runner's solver (the PCD with the viscous Schur term and
   red-black SOR): to t = 0.1 (200 steps), mixed against FP64 on the GPU;
@@ -154,7 +154,9 @@ def test_c4_one_case_per_grid_class_lockstep_mixed(gpu, oracle_mod, oracle_runs,
               f"FP64 oracle:", e)
     for case, e in errs.items():
         assert max(e["u"], e["v"], e["p"]) <= (MIXED_BOUND if tol < 1e-8 else C4_TOL_BOUND), (case, e)
-        assert e["volume"] <= 1e-12, (case, e)
+        # fluid-1 volume moves with the velocity field's divergence, which the
+        # two runs share to the tolerance: 1e-12 at 1e-11, 1e-10 at 1e-8
+        assert e["volume"] <= (1e-12 if tol < 1e-8 else 1e-10), (case, e)
 
 
 def test_c3_bubble_mixed_vs_fp64_diagnostics(gpu, oracle_mod):

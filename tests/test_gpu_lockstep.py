@@ -43,12 +43,16 @@ def specs_with_periodic(n):
     return specs
 
 
-def run(specs, prms, prec, lockstep, nsteps=NSTEPS):
+def run(specs, prms, prec, lockstep, nsteps=NSTEPS, one_call=False):
     with Batch([(s["grid"], p, prec) for s, p in zip(specs, prms)], nthreads=4, max_cluster=8,
                lockstep=lockstep) as b:
         for i, s in enumerate(specs):
             initial_bubble_state(b.case(i), s)
-        outs = [b.run(1, DT, k, b.case(0).step_opts(use_bicgstab2=True)) for k in range(1, nsteps + 1)]
+        o = b.case(0).step_opts(use_bicgstab2=True)
+        if one_call:  # every step in one run: the cases move through their steps at their own pace
+            outs = [b.run(nsteps, DT, 1, o)]
+        else:
+            outs = [b.run(1, DT, k, o) for k in range(1, nsteps + 1)]
         states = [b.case(i).download_state(list(STATE_FIELDS)) for i in range(len(specs))]
         launches = b.launches()
     return outs, states, launches
@@ -73,6 +77,30 @@ def test_lockstep_equals_thread_pool_bitwise(gpu, prec, smoother, periodic):
         for k in STATE_FIELDS:
             np.testing.assert_array_equal(states[i][k], ref_states[i][k], err_msg=f"case {i} {k}")
     assert 0 < launches < ref_launches  # one launch per kernel family for all cases
+
+
+@pytest.mark.parametrize("smoother,periodic", [(1, False), (0, True)])
+def test_lockstep_continuous_run_equals_thread_pool_bitwise(gpu, smoother, periodic):
+    """All steps in one run: a case whose solve ends at a pass takes its next
+    step's explicit stages while the others keep solving, and joins the
+    lockstep solve at the following pass, so within the run the cases are at
+    different steps.  Every case still follows its own sequence of operations,
+    so the final states and the last step's statistics equal the thread-pool
+    batch's bit for bit."""
+    specs = specs_with_periodic(6) if periodic else cases.bubble_ensemble(6, grids=SMALL_GRIDS)
+    prms = [ensemble_params(s, **dict(SOLVER, pcd_smoother=smoother)) for s in specs]
+    if periodic:
+        prms[1] = dataclasses.replace(prms[1], free_slip_x=0)
+    nsteps = 4
+    (ref,), ref_states, _ = run(specs, prms, MIXED, lockstep=False, nsteps=nsteps, one_call=True)
+    (out,), states, _ = run(specs, prms, MIXED, lockstep=True, nsteps=nsteps, one_call=True)
+    assert out["status"] == ref["status"] == [0] * len(specs)
+    assert out["max_res"] == ref["max_res"]
+    for i in range(len(specs)):
+        for k in STATS:
+            assert out["last"][i][k] == ref["last"][i][k], (i, k, out["last"][i], ref["last"][i])
+        for k in STATE_FIELDS:
+            np.testing.assert_array_equal(states[i][k], ref_states[i][k], err_msg=f"case {i} {k}")
 
 
 def test_lockstep_rejects_cases_it_cannot_run(gpu):
