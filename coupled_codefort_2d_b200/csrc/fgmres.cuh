@@ -224,17 +224,16 @@ __device__ __forceinline__ void maxpy_body(long n3, T* w, const T* V0, long stri
   __syncthreads();
   for (long q = b * (long)blockDim.x + threadIdx.x; q < n3; q += (long)G * blockDim.x) {
     T x = w[q];
-    int i = 0;
-    // four vectors' loads in flight before the (ordered) dependent updates
-    for (; i + 4 <= nvec; i += 4) {
-      const T v0 = V0[i * stride + q], v1 = V0[(i + 1) * stride + q];
-      const T v2 = V0[(i + 2) * stride + q], v3 = V0[(i + 3) * stride + q];
-      x = madd(s[i], v0, x);
-      x = madd(s[i + 1], v1, x);
-      x = madd(s[i + 2], v2, x);
-      x = madd(s[i + 3], v3, x);
+    // four vectors' loads in flight before the (ordered) dependent updates,
+    // the last group's too (a one-at-a-time tail serialises its loads)
+    for (int i = 0; i < nvec; i += 4) {
+      T v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) v[u] = i + u < nvec ? V0[(i + u) * stride + q] : T(0);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (i + u < nvec) x = madd(s[i + u], v[u], x);
     }
-    for (; i < nvec; ++i) x = madd(s[i], V0[i * stride + q], x);
     w[q] = x;
   }
 }
