@@ -124,7 +124,7 @@ SIGNATURES = {
     "fugu_batch_last_error": (C.c_char_p, [_vp]),
     "fugu_batch_size": (_i, [_vp]),
     "fugu_batch_case": (_i, [_vp, _i, _vp]),
-    "fugu_batch_run": (_i, [_vp, _i] + [_vp] * 6),
+    "fugu_batch_run": (_i, [_vp, _i] + [_vp] * 7),
     "fugu_batch_get_stream": (_i, [_vp, _vp]),
     "fugu_batch_launches": (C.c_ulonglong, [_vp]),
     "fugu_matvec_coupled_t": (_i, [_vp] * 15 + [_d] + [_vp] * 4),
@@ -135,7 +135,8 @@ SIGNATURES = {
 
 
 class FuguBatchOpts(C.Structure):
-    _fields_ = [("nthreads", C.c_int), ("max_cluster", C.c_int), ("max_coop", C.c_int), ("lockstep", C.c_int)]
+    _fields_ = [("nthreads", C.c_int), ("max_cluster", C.c_int), ("max_coop", C.c_int), ("lockstep", C.c_int),
+                ("lockstep_group", C.c_int)]
 
 _lib = None
 

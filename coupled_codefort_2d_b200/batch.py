@@ -4,9 +4,12 @@
 context on the device (its own state, work space and stream); the library
 autotunes the thread-block-cluster size of each case's PCG at creation.  By
 default a pool of host threads steps the cases, largest grid first; with
-``lockstep=True`` the coupled solves of all cases advance together, one launch
-per kernel family serving every case still running, with the same results per
-case.  The reference runs one case per ``mpirun`` and has no counterpart.
+``lockstep=True`` the coupled solves of a group of cases advance together, one
+launch per kernel family serving every case of the group still running, with
+the same results per case.  The groups (cases of one PCG grid class, at most
+``lockstep_group`` of them; 0: no limit) run side by side, each on its own
+stream and host thread.  The reference runs one case per ``mpirun`` and has no
+counterpart.
 """
 from __future__ import annotations
 
@@ -28,12 +31,12 @@ class Batch:
     """``cases``: a list of ``(Grid, Params, precision)``."""
 
     def __init__(self, specs, device: int = 0, nthreads: int = 0, max_cluster: int = 0, max_coop: int = 0,
-                 lockstep: bool = False):
+                 lockstep: bool = False, lockstep_group: int = 0):
         self.L = _lib.lib()
         self.specs = list(specs)
         n = len(self.specs)
         arr = (FuguParams * n)(*[make_params(g, prm, prec) for g, prm, prec in self.specs])
-        opts = FuguBatchOpts(nthreads, max_cluster, max_coop, int(lockstep))
+        opts = FuguBatchOpts(nthreads, max_cluster, max_coop, int(lockstep), int(lockstep_group))
         h = C.c_void_p()
         rc = self.L.fugu_batch_create(arr, n, int(device), C.byref(opts), C.byref(h))
         if rc != 0:
@@ -88,7 +91,9 @@ class Batch:
 
     def run(self, nsteps: int, dt, step0, opts) -> dict:
         """Advance every case ``nsteps`` steps (``dt``, ``step0`` scalars or
-        per-case sequences; ``opts`` one :class:`FuguStepOpts` or a list)."""
+        per-case sequences; ``opts`` one :class:`FuguStepOpts` or a list).
+        Returns per case the last step's statistics, the run's summed
+        statistics (``total``), the largest residual and the status."""
         n = len(self)
         dts = (C.c_double * n)(*np.broadcast_to(np.asarray(dt, dtype=np.float64), (n,)))
         s0 = (C.c_int * n)(*np.broadcast_to(np.asarray(step0, dtype=np.int64), (n,)).tolist())
@@ -97,8 +102,10 @@ class Batch:
         last = (FuguStats * n)()
         mres = (C.c_double * n)()
         status = (C.c_int * n)()
-        rc = self.L.fugu_batch_run(self.h, int(nsteps), dts, s0, oa, last, mres, status)
-        out = {"last": [s.as_dict() for s in last], "max_res": list(mres), "status": list(status)}
+        total = (FuguStats * n)()
+        rc = self.L.fugu_batch_run(self.h, int(nsteps), dts, s0, oa, last, mres, status, total)
+        out = {"last": [s.as_dict() for s in last], "total": [s.as_dict() for s in total], "max_res": list(mres),
+               "status": list(status)}
         if rc != 0:
             raise FuguError(rc, self.L.fugu_batch_last_error(self.h).decode())
         return out

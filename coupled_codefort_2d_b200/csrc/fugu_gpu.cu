@@ -425,6 +425,9 @@ const void* pcgc_fn(int cpt) {
     case 4: return (const void*)k_pcg_cluster<T, 4>;
     case 8: return (const void*)k_pcg_cluster<T, 8>;
     case 16: return (const void*)k_pcg_cluster<T, 16>;
+    case 32:
+      if constexpr (sizeof(T) == 4) return (const void*)k_pcg_cluster<T, 32>;
+      break;
   }
   return nullptr;
 }
@@ -452,8 +455,8 @@ cudaError_t launch_pcg_cluster(PcgClusterArgs<T> a, int C, int cpt, size_t smem,
 }
 // Plan the cluster-resident PCG for precision T: up to 16 CTAs of PCGC_TPB
 // threads, every CTA's rows must fit the shared memory and the register
-// arrays (cpt <= 8 in FP64, <= 16 in FP32), and the device must be able to
-// co-schedule such a cluster.
+// arrays (cpt <= 8 in FP64, <= 32 in FP32 with the lean variant above 16),
+// and the device must be able to co-schedule such a cluster.
 template <typename T>
 void plan_pcg_cluster(fugu_ctx* c, fugu_ctx::ClusterPlan& pl) {
   pl = fugu_ctx::ClusterPlan{};
@@ -467,7 +470,7 @@ void plan_pcg_cluster(fugu_ctx* c, fugu_ctx::ClusterPlan& pl) {
   if (nx > PCGC_TPB) return;
   int cpt = 1;
   while ((long)nx * ((rows_per + cpt - 1) / cpt) > PCGC_TPB) cpt *= 2;
-  const int cpt_max = sizeof(T) == 8 ? 8 : 16;
+  const int cpt_max = sizeof(T) == 8 ? 8 : 32;
   if (cpt > cpt_max) return;
   const void* fn = pcgc_fn<T>(cpt);
   // The dynamic shared-memory limit is a property of the kernel, shared by
@@ -2693,15 +2696,17 @@ struct fugu_batch {
   std::vector<fugu_ctx*> cases;
   std::vector<int> order;
   std::string err;
-  LockstepBase* ls = nullptr;  // the lockstep solver (lockstep = 1)
+  // the lockstep solvers (lockstep = 1): one per group of cases, a group
+  // being cases of one PCG grid class (at most lockstep_group of them), each
+  // group advanced by its own host thread on its own stream
+  std::vector<LockstepBase*> groups;
+  std::vector<std::vector<int>> group_ids;  // the batch indices of each group's cases
+  std::vector<cudaEvent_t> ev_group;        // per group: its ended solves' final BCs are queued
   // the batch stream: a run starts after the work queued on it before the
-  // run and ends before the work queued on it after (the lockstep solver's
-  // own stream, or a stream of the batch)
+  // run and ends before the work queued on it after
   cudaStream_t s = nullptr;
-  bool own_s = false;
   cudaEvent_t ev_start = nullptr;
   std::vector<cudaEvent_t> ev_case;  // per case: its stage of the run is done
-  cudaEvent_t ev_solve = nullptr;    // the lockstep solves are done
 };
 
 namespace {
@@ -2773,6 +2778,19 @@ int tune_cluster(fugu_ctx* c) {
   return best;
 }
 
+// accumulate one step's statistics into a run's totals (sums of the counts,
+// the largest residual, the first error)
+void add_stats(fugu_stats& t, const fugu_stats& s) {
+  t.iter += s.iter;
+  t.outer += s.outer;
+  t.pcg_iters += s.pcg_iters;
+  t.pcg_calls += s.pcg_calls;
+  t.matvecs += s.matvecs;
+  t.svof_iters += s.svof_iters;
+  if (s.res > t.res || std::isnan(s.res)) t.res = s.res;
+  if (t.status == FUGU_CONVERGED && s.status != FUGU_CONVERGED) t.status = s.status;
+}
+
 struct BatchRun {
   int nsteps;
   const double* dt;
@@ -2781,6 +2799,7 @@ struct BatchRun {
   fugu_stats* last;
   double* max_res;
   int* status;
+  fugu_stats* total;
   std::atomic<int> next{0};
 };
 
@@ -2792,15 +2811,18 @@ void batch_worker(fugu_batch* b, BatchRun* r) {
     const int i = b->order[k];
     fugu_ctx* c = b->cases[i];
     double mres = 0.0;
-    fugu_stats st{};
+    fugu_stats st{}, tot{};
+    tot.status = FUGU_CONVERGED;
     const int rc = guard(c, [&] {
       for (int s = 0; s < r->nsteps; ++s) {
         std::memset(&st, 0, sizeof st);
         step(c, r->dt[i], r->step0[i] + s, &r->opts[i], &st);
         if (st.res > mres || std::isnan(st.res)) mres = st.res;
+        add_stats(tot, st);
       }
     });
     if (r->last) r->last[i] = st;
+    if (r->total) r->total[i] = tot;
     if (r->max_res) r->max_res[i] = mres;
     if (r->status) r->status[i] = rc;
   }
@@ -2808,18 +2830,18 @@ void batch_worker(fugu_batch* b, BatchRun* r) {
 
 // Lockstep set-up: every case runs the flexible-GMRES defect correction
 // (refine = 2) in one precision with one smoother and cycle length, and its
-// PCG fits a thread-block cluster.
-int lockstep_create(fugu_batch* b) {
+// PCG fits a thread-block cluster.  The cases are grouped by their PCG's
+// cluster plan (one PCG launch per Arnoldi step and group), in groups of at
+// most group_max cases (0: no limit) in the order of the batch.
+int lockstep_create(fugu_batch* b, int group_max) {
   const int nc = (int)b->cases.size();
-  if (nc > LS_MAX) {
-    b->err = "lockstep batch: at most " + std::to_string(LS_MAX) + " cases";
-    return FUGU_EINVAL;
-  }
   const fugu_params& p0 = b->cases[0]->prm;
+  const int pi = p0.precision == FUGU_MIXED ? 1 : 0;
+  std::map<std::array<long, 4>, std::vector<int>> by_class;
+  std::vector<std::array<long, 4>> class_order;
   for (int i = 0; i < nc; ++i) {
     const fugu_ctx* c = b->cases[i];
     const fugu_params& p = c->prm;
-    const int pi = p.precision == FUGU_MIXED ? 1 : 0;
     std::string why;
     if (p.refine != 2) why = "refine must be 2 (flexible GMRES inside the defect correction)";
     else if (p.precision != p0.precision) why = "every case needs the same precision";
@@ -2830,19 +2852,39 @@ int lockstep_create(fugu_batch* b) {
       b->err = "lockstep batch, case " + std::to_string(i) + ": " + why;
       return FUGU_EINVAL;
     }
+    const fugu_ctx::ClusterPlan& pl = c->pcgc[pi];
+    const std::array<long, 4> key = {pl.C, pl.cpt, pl.rows_per, (long)pl.smem};
+    auto it = by_class.find(key);
+    if (it == by_class.end()) {
+      class_order.push_back(key);
+      it = by_class.emplace(key, std::vector<int>{}).first;
+    }
+    it->second.push_back(i);
+  }
+  const int gmax = group_max > 0 ? std::min(group_max, LS_MAX) : LS_MAX;
+  for (const auto& key : class_order) {
+    const std::vector<int>& ids = by_class[key];
+    for (size_t k = 0; k < ids.size(); k += gmax)
+      b->group_ids.emplace_back(ids.begin() + k, ids.begin() + std::min(ids.size(), k + (size_t)gmax));
   }
   try {
     CK(cudaSetDevice(b->device));
-    if (p0.precision == FUGU_MIXED) {
-      Lockstep<float>* ls = new Lockstep<float>();
-      b->ls = ls;
-      ls->create(b->cases);
-    } else {
-      Lockstep<double>* ls = new Lockstep<double>();
-      b->ls = ls;
-      ls->create(b->cases);
+    for (const std::vector<int>& ids : b->group_ids) {
+      std::vector<fugu_ctx*> cs;
+      for (int i : ids) cs.push_back(b->cases[i]);
+      if (p0.precision == FUGU_MIXED) {
+        Lockstep<float>* ls = new Lockstep<float>();
+        b->groups.push_back(ls);
+        ls->create(cs);
+      } else {
+        Lockstep<double>* ls = new Lockstep<double>();
+        b->groups.push_back(ls);
+        ls->create(cs);
+      }
+      cudaEvent_t e;
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      b->ev_group.push_back(e);
     }
-    CK(cudaEventCreateWithFlags(&b->ev_solve, cudaEventDisableTiming));
   } catch (const CudaError& e) {
     b->err = std::string("lockstep batch: ") + e.what + ": " + cudaGetErrorString(e.e);
     return FUGU_ECUDA;
@@ -2856,35 +2898,37 @@ int lockstep_create(fugu_batch* b) {
 // the batch stream and its events (created with the batch)
 void batch_streams(fugu_batch* b) {
   CK(cudaSetDevice(b->device));
-  if (b->ls) {
-    b->s = b->ls->stream();
-  } else {
-    CK(cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking));
-    b->own_s = true;
-  }
+  CK(cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking));
   CK(cudaEventCreateWithFlags(&b->ev_start, cudaEventDisableTiming));
   b->ev_case.resize(b->cases.size(), nullptr);
   for (auto& e : b->ev_case) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
 }
-// every case stream waits for the work queued on the batch stream so far
+// every case stream and lockstep stream waits for the work queued on the
+// batch stream so far
 void batch_begin(fugu_batch* b) {
   CK(cudaSetDevice(b->device));
   CK(cudaEventRecord(b->ev_start, b->s));
   for (fugu_ctx* c : b->cases) CK(cudaStreamWaitEvent(c->s, b->ev_start, 0));
+  for (LockstepBase* ls : b->groups) CK(cudaStreamWaitEvent(ls->stream(), b->ev_start, 0));
 }
-// the batch stream waits for every case stream's work of the run
+// the batch stream waits for every case stream's and lockstep stream's work
+// of the run
 void batch_end(fugu_batch* b) {
   CK(cudaSetDevice(b->device));
   for (size_t i = 0; i < b->cases.size(); ++i) {
     CK(cudaEventRecord(b->ev_case[i], b->cases[i]->s));
     CK(cudaStreamWaitEvent(b->s, b->ev_case[i], 0));
   }
+  for (size_t g = 0; g < b->groups.size(); ++g) {
+    CK(cudaEventRecord(b->ev_group[g], b->groups[g]->stream()));
+    CK(cudaStreamWaitEvent(b->s, b->ev_group[g], 0));
+  }
 }
 
-// run fn(i) for the cases ids (in that order) from the batch's host threads;
-// returns a status per case of the batch
+// run fn(i) for the cases ids (in that order) from up to nthreads host
+// threads (0: the batch's); returns a status per case of the batch
 template <typename F>
-std::vector<int> for_ids(fugu_batch* b, const std::vector<int>& ids, F fn) {
+std::vector<int> for_ids(fugu_batch* b, const std::vector<int>& ids, F fn, int nthreads = 0) {
   std::vector<int> st(b->cases.size(), FUGU_OK);
   const int n = (int)ids.size();
   std::atomic<int> next{0};
@@ -2896,7 +2940,7 @@ std::vector<int> for_ids(fugu_batch* b, const std::vector<int>& ids, F fn) {
       st[i] = guard(b->cases[i], [&] { fn(i); });
     }
   };
-  const int nt = std::min(b->nthreads, n);
+  const int nt = std::min(nthreads > 0 ? nthreads : b->nthreads, n);
   std::vector<std::thread> pool;
   for (int t = 1; t < nt; ++t) pool.emplace_back(work);
   work();
@@ -2909,112 +2953,140 @@ std::vector<int> for_cases(fugu_batch* b, F fn) {
   return for_ids(b, b->order, fn);
 }
 
-// The lockstep batch run (continuous batching, lockstep_host.cuh): every
-// case goes through nsteps steps; a case whose solve ends at a pass goes
-// through its final BCs and statistics and its next step's explicit stages
-// on its own stream while the other cases' next cycle runs, and joins the
-// lockstep solve again at the following pass.
+// The lockstep batch run (continuous batching, lockstep_host.cuh).  Each
+// group of cases is advanced by its own host thread: every case goes
+// through nsteps steps; a case whose solve ends at a pass goes through its
+// final BCs and statistics and its next step's explicit stages on its own
+// stream while the group's other cases' next cycle runs, and joins the
+// lockstep solve again at the following pass.  The groups do not wait for
+// one another.
 int lockstep_run(fugu_batch* b, int nsteps, const double* dt, const int* step0, const fugu_step_opts* opts,
-                 fugu_stats* last, double* max_res, int* status) {
+                 fugu_stats* last, double* max_res, int* status, fugu_stats* total) {
   const int nc = (int)b->cases.size();
   std::vector<double> mres(nc, 0.0);
   std::vector<int> cst(nc, FUGU_OK);
-  std::vector<fugu_stats> lst(nc);
-  int rc = FUGU_OK;
-  LockstepBase* ls = b->ls;
-  cudaStream_t ls_s = ls->stream();
+  std::vector<fugu_stats> lst(nc), tot(nc);
+  for (auto& t : tot) {
+    std::memset(&t, 0, sizeof t);
+    t.status = FUGU_CONVERGED;
+  }
+  std::atomic<int> rc{FUGU_OK};
+  std::mutex err_mu;
+  auto fail = [&](int code, const std::string& msg) {
+    std::lock_guard<std::mutex> lk(err_mu);
+    if (rc.load() == FUGU_OK) {
+      rc = code;
+      b->err = msg;
+    }
+  };
   try {
-    ls->reset();
+    for (LockstepBase* ls : b->groups) ls->reset();
     batch_begin(b);
   } catch (const CudaError& e) {
     b->err = std::string("batch stream: ") + e.what + ": " + cudaGetErrorString(e.e);
     return FUGU_ECUDA;
   }
   std::vector<int> done(nc, 0);  // steps completed per case
-  std::vector<StepSetup> su(nc);
-  std::vector<KrylovResult> kr(nc);
-  std::vector<int> outer(nc, 0);
-  // a failed case stops the run (its status and the batch's message)
-  auto take = [&](const std::vector<int>& st, const std::vector<int>& ids) {
-    for (int i : ids)
-      if (st[i] != FUGU_OK) {
-        cst[i] = st[i];
-        if (rc == FUGU_OK) {
-          rc = st[i];
-          b->err = "case " + std::to_string(i) + ": " + b->cases[i]->err;
+  const int ng = (int)b->groups.size();
+  const int nt = std::max(1, b->nthreads / ng);  // host threads of a group's per-case work
+  auto run_group = [&](int g) {
+    LockstepBase* ls = b->groups[g];
+    const std::vector<int>& ids = b->group_ids[g];  // local index k: batch case ids[k]
+    const int n = (int)ids.size();
+    cudaStream_t ls_s = ls->stream();
+    std::vector<StepSetup> su(n);
+    std::vector<KrylovResult> kr(n);
+    std::vector<int> outer(n, 0);
+    std::vector<int> loc(nc, -1);
+    for (int k = 0; k < n; ++k) loc[ids[k]] = k;
+    auto take = [&](const std::vector<int>& st, const std::vector<int>& bids) {
+      for (int i : bids)
+        if (st[i] != FUGU_OK) {
+          cst[i] = st[i];
+          fail(st[i], "case " + std::to_string(i) + ": " + b->cases[i]->err);
         }
-      }
-  };
-  // explicit stages of the next step of ids, each on its own stream
-  auto pre = [&](int i) {
-    fugu_ctx* c = b->cases[i];
-    su[i] = step_setup(c, dt[i], step0[i] + done[i], &opts[i]);
-    step_pre(c, dt[i], step0[i] + done[i], &opts[i]);
-    CK(cudaEventRecord(b->ev_case[i], c->s));
-  };
-  std::vector<int> joining;
-  if (nsteps > 0) {
-    joining = b->order;
-    take(for_ids(b, joining, pre), joining);
-  }
-  try {
-    CK(cudaSetDevice(b->device));
-    while (rc == FUGU_OK) {
-      // the cases whose explicit stages were issued join the solve
-      if (!joining.empty()) {
-        for (int i : joining) CK(cudaStreamWaitEvent(ls_s, b->ev_case[i], 0));
-        ls->join(joining, su);
-        joining.clear();
-      }
-      std::vector<int> ended = ls->defect();
-      if (!ended.empty()) {
-        ls->finish(ended, kr, outer);
-        CK(cudaEventRecord(b->ev_solve, ls_s));
-      }
-      const bool cycling = ls->cycle_launch();
-      if (!ended.empty()) {
-        // meanwhile on the host threads: the ended steps' final BCs and
-        // statistics, and the next steps' explicit stages
-        std::vector<int> st = for_ids(b, ended, [&](int i) {
-          fugu_ctx* c = b->cases[i];
-          CK(cudaStreamWaitEvent(c->s, b->ev_solve, 0));
-          std::memset(&lst[i], 0, sizeof(fugu_stats));
-          step_post(c, su[i], kr[i], outer[i], &lst[i]);
-          if (lst[i].res > mres[i] || std::isnan(lst[i].res)) mres[i] = lst[i].res;
-          if (++done[i] < nsteps) pre(i);
-        });
-        take(st, ended);
-        for (int i : ended)
-          if (done[i] < nsteps) joining.push_back(i);
-      }
-      if (cycling) ls->cycle_finish();
-      if (!cycling && joining.empty()) break;
+    };
+    // explicit stages of case i's next step on its own stream
+    auto pre = [&](int i) {
+      fugu_ctx* c = b->cases[i];
+      su[loc[i]] = step_setup(c, dt[i], step0[i] + done[i], &opts[i]);
+      step_pre(c, dt[i], step0[i] + done[i], &opts[i]);
+      CK(cudaEventRecord(b->ev_case[i], c->s));
+    };
+    std::vector<int> joining;  // batch ids
+    if (nsteps > 0) {
+      take(for_ids(b, ids, pre, nt), ids);
+      joining = ids;
     }
-  } catch (const CudaError& e) {
-    b->err = std::string("lockstep solve: ") + e.what + ": " + cudaGetErrorString(e.e);
-    rc = FUGU_ECUDA;
-  } catch (const ApiError& e) {
-    b->err = "lockstep solve: " + e.msg;
-    rc = e.code;
-  }
-  if (rc != FUGU_OK) {
+    try {
+      CK(cudaSetDevice(b->device));
+      while (rc.load() == FUGU_OK) {
+        if (!joining.empty()) {
+          std::vector<int> lj;
+          for (int i : joining) {
+            CK(cudaStreamWaitEvent(ls_s, b->ev_case[i], 0));
+            lj.push_back(loc[i]);
+          }
+          ls->join(lj, su);
+          joining.clear();
+        }
+        const std::vector<int> ended_l = ls->defect();
+        std::vector<int> ended;
+        for (int k : ended_l) ended.push_back(ids[k]);
+        if (!ended.empty()) {
+          ls->finish(ended_l, kr, outer);
+          CK(cudaEventRecord(b->ev_group[g], ls_s));
+        }
+        const bool cycling = ls->cycle_launch();
+        if (!ended.empty()) {
+          // meanwhile on the host threads: the ended steps' final BCs and
+          // statistics, and the next steps' explicit stages
+          std::vector<int> st = for_ids(b, ended, [&](int i) {
+            fugu_ctx* c = b->cases[i];
+            const int k = loc[i];
+            CK(cudaStreamWaitEvent(c->s, b->ev_group[g], 0));
+            std::memset(&lst[i], 0, sizeof(fugu_stats));
+            step_post(c, su[k], kr[k], outer[k], &lst[i]);
+            if (lst[i].res > mres[i] || std::isnan(lst[i].res)) mres[i] = lst[i].res;
+            add_stats(tot[i], lst[i]);
+            if (++done[i] < nsteps) pre(i);
+          }, nt);
+          take(st, ended);
+          for (int i : ended)
+            if (done[i] < nsteps) joining.push_back(i);
+        }
+        if (cycling) ls->cycle_finish();
+        if (!cycling && joining.empty()) break;
+      }
+    } catch (const CudaError& e) {
+      fail(FUGU_ECUDA, std::string("lockstep solve: ") + e.what + ": " + cudaGetErrorString(e.e));
+    } catch (const ApiError& e) {
+      fail(e.code, "lockstep solve: " + e.msg);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int g = 1; g < ng; ++g) pool.emplace_back(run_group, g);
+  if (ng > 0) run_group(0);
+  for (auto& th : pool) th.join();
+  int code = rc.load();
+  if (code != FUGU_OK) {
     for (int i = 0; i < nc; ++i)
-      if (cst[i] == FUGU_OK) cst[i] = rc;
-  }
-  if (rc == FUGU_OK) {
+      if (cst[i] == FUGU_OK) cst[i] = code;
+  } else {
     try {
       batch_end(b);
     } catch (const CudaError& e) {
       b->err = std::string("batch stream: ") + e.what + ": " + cudaGetErrorString(e.e);
-      rc = FUGU_ECUDA;
+      code = FUGU_ECUDA;
     }
   }
   for (int i = 0; i < nc; ++i) {
     if (last) last[i] = lst[i];
     if (max_res) max_res[i] = mres[i];
     if (status) status[i] = cst[i];
+    if (total) total[i] = tot[i];
   }
-  return rc;
+  return code;
 }
 
 }  // namespace
@@ -3072,7 +3144,7 @@ int fugu_batch_create(const fugu_params* params, int ncases, int device, const f
     }
   }
   if (o.lockstep) {
-    const int rc = lockstep_create(b);
+    const int rc = lockstep_create(b, o.lockstep_group);
     if (rc) {
       fprintf(stderr, "fugu_batch_create: %s\n", b->err.c_str());
       fugu_batch_destroy(b);
@@ -3100,13 +3172,13 @@ void fugu_batch_destroy(fugu_batch* b) {
   if (!b) return;
   cudaSetDevice(b->device);
   for (cudaEvent_t e : b->ev_case) cudaEventDestroy(e);
-  if (b->ev_solve) cudaEventDestroy(b->ev_solve);
+  for (cudaEvent_t e : b->ev_group) cudaEventDestroy(e);
   if (b->ev_start) cudaEventDestroy(b->ev_start);
-  if (b->own_s && b->s) {
+  if (b->s) {
     cudaStreamSynchronize(b->s);
     cudaStreamDestroy(b->s);
   }
-  delete b->ls;
+  for (LockstepBase* ls : b->groups) delete ls;
   for (fugu_ctx* c : b->cases) destroy(c);
   delete b;
 }
@@ -3122,13 +3194,13 @@ int fugu_batch_case(fugu_batch* b, int i, fugu_ctx** ctx) {
 }
 
 int fugu_batch_run(fugu_batch* b, int nsteps, const double* dt, const int* step0, const fugu_step_opts* opts,
-                   fugu_stats* last, double* max_res, int* status) {
+                   fugu_stats* last, double* max_res, int* status, fugu_stats* total) {
   if (!b) return FUGU_EINVAL;
   if (nsteps < 0 || !dt || !step0 || !opts) {
     b->err = "fugu_batch_run: NULL dt/step0/opts or nsteps < 0";
     return FUGU_EINVAL;
   }
-  if (b->ls) return lockstep_run(b, nsteps, dt, step0, opts, last, max_res, status);
+  if (!b->groups.empty()) return lockstep_run(b, nsteps, dt, step0, opts, last, max_res, status, total);
   try {
     batch_begin(b);
   } catch (const CudaError& e) {
@@ -3142,6 +3214,7 @@ int fugu_batch_run(fugu_batch* b, int nsteps, const double* dt, const int* step0
   r.opts = opts;
   r.last = last;
   r.max_res = max_res;
+  r.total = total;
   std::vector<int> st(b->cases.size(), FUGU_OK);
   r.status = st.data();
   std::vector<std::thread> pool;
@@ -3171,7 +3244,8 @@ int fugu_batch_get_stream(fugu_batch* b, void** stream) {
 
 unsigned long long fugu_batch_launches(const fugu_batch* b) {
   if (!b) return 0;
-  unsigned long long n = b->ls ? b->ls->launch_count() : 0;
+  unsigned long long n = 0;
+  for (const LockstepBase* ls : b->groups) n += ls->launch_count();
   for (const fugu_ctx* c : b->cases) n += c->launches;
   return n;
 }

@@ -198,24 +198,74 @@ __device__ __forceinline__ void put_partial(double* part, int b, DD v) {
   part[2 * b] = v.hi;
   part[2 * b + 1] = v.lo;
 }
-// rounded sum of n DD partials, identical in every CTA (fixed order)
+// rounded sum of n DD partials, identical in every CTA (fixed order).  Lane
+// l of warp 0 merges partials l, l + 32, l + 64, ... in that order, then a
+// fixed shuffle tree merges the lanes.  The loads of up to eight of a lane's
+// partials are issued together before they are merged (one round trip to
+// L2 per eight instead of one per partial); the order of the merges is the
+// same either way.
+template <int NA>
+__device__ __forceinline__ void merge_partials_dd(const double* const* parts, int n, double* res) {
+  DD v[NA];
+#pragma unroll
+  for (int a = 0; a < NA; ++a) v[a] = DD{0.0, 0.0};
+  for (int k0 = threadIdx.x; k0 < n; k0 += 32 * 8) {
+    DD p[NA][8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int k = k0 + 32 * u;
+#pragma unroll
+      for (int a = 0; a < NA; ++a) {
+        p[a][u] = DD{0.0, 0.0};
+        if (k < n) {
+          p[a][u].hi = __ldcg(parts[a] + 2 * k);
+          p[a][u].lo = __ldcg(parts[a] + 2 * k + 1);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (k0 + 32 * u < n) {
+#pragma unroll
+        for (int a = 0; a < NA; ++a) v[a] = dd_merge(v[a], p[a][u]);
+      }
+  }
+#pragma unroll
+  for (int a = 0; a < NA; ++a) {
+    for (int o = 16; o > 0; o >>= 1) v[a] = dd_merge(v[a], dd_shfl_down(v[a], o));
+    res[a] = v[a].hi + v[a].lo;
+  }
+}
 __device__ __forceinline__ double sum_partials_dd(const double* part, int n) {
   __shared__ double s_res;
   if (threadIdx.x < 32) {
-    DD v{0.0, 0.0};
-    for (int k = threadIdx.x; k < n; k += 32) {
-      DD p;
-      p.hi = __ldcg(part + 2 * k);
-      p.lo = __ldcg(part + 2 * k + 1);
-      v = dd_merge(v, p);
-    }
-    for (int o = 16; o > 0; o >>= 1) v = dd_merge(v, dd_shfl_down(v, o));
-    if (threadIdx.x == 0) s_res = v.hi + v.lo;
+    const double* parts[1] = {part};
+    double r[1];
+    merge_partials_dd<1>(parts, n, r);
+    if (threadIdx.x == 0) s_res = r[0];
   }
   __syncthreads();
   const double r = s_res;
   __syncthreads();
   return r;
+}
+// the rounded sums of two arrays of n DD partials in one pass
+__device__ __forceinline__ void sum_partials_dd2(const double* pa, const double* pb, int n, double& oa,
+                                                 double& ob) {
+  __shared__ double s_res2[2];
+  if (threadIdx.x < 32) {
+    const double* parts[2] = {pa, pb};
+    double r[2];
+    merge_partials_dd<2>(parts, n, r);
+    if (threadIdx.x == 0) {
+      s_res2[0] = r[0];
+      s_res2[1] = r[1];
+    }
+  }
+  __syncthreads();
+  oa = s_res2[0];
+  ob = s_res2[1];
+  __syncthreads();
 }
 
 // deterministic block reduction (sum) of one double per thread; result valid
@@ -266,8 +316,15 @@ __device__ __forceinline__ double sum_partials(const double* part, int n, double
 __device__ __forceinline__ double max_partials(const double* part, int n) {
   __shared__ double s_res;
   if (threadIdx.x < 32) {
+    // loads eight at a time (the maximum does not depend on the order)
     double v = 0.0;
-    for (int k = threadIdx.x; k < n; k += 32) v = fmax(v, __ldcg(part + k));
+    for (int k0 = threadIdx.x; k0 < n; k0 += 32 * 8) {
+      double x[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) x[u] = k0 + 32 * u < n ? __ldcg(part + k0 + 32 * u) : 0.0;
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v = fmax(v, x[u]);
+    }
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
     if (threadIdx.x == 0) s_res = v;
   }

@@ -97,6 +97,8 @@ struct Lockstep : LockstepBase {
   int* h_nact = nullptr;
   std::vector<LsClass> classes;
   std::map<const void*, int> grids;  // persistent grid per family kernel
+  // virtual blocks of each family with every case of the group running
+  long cap_box = 0, cap_e1 = 0, cap_dot = 0, cap_mdot = 0, cap_tile = 0;
   unsigned long long launches = 0;   // kernel launches issued, replays included
   // per Arnoldi step, one graph (the host checks between steps)
   struct Graph {
@@ -232,6 +234,17 @@ struct Lockstep : LockstepBase {
       }
       classes[it->second].cases.push_back(i);
     }
+    for (const LsCase<T>& r : rec) {
+      cap_box += ls_box_blocks(r.g);
+      cap_e1 += ls_e1_blocks(3 * r.n);
+      cap_dot += r.dot_grid;
+      cap_tile += ls_tile_blocks(r.g);
+    }
+    for (int nvec = 1; nvec <= m + 1; ++nvec) {
+      long t = 0;
+      for (const LsCase<T>& r : rec) t += (long)ls_mdot_g(r.nsm, r.mdot_gmax, nvec) * nvec;
+      cap_mdot = std::max(cap_mdot, t);
+    }
     d_cases = dal<LsCase<T>>(ncase);
     CK(cudaMemcpy(d_cases, rec.data(), sizeof(LsCase<T>) * ncase, cudaMemcpyHostToDevice));
     d_dyn = dal<LsDyn>(ncase);
@@ -277,25 +290,31 @@ struct Lockstep : LockstepBase {
       case 4: return (const void*)k_ls_pcg<T, 4>;
       case 8: return (const void*)k_ls_pcg<T, 8>;
       case 16: return (const void*)k_ls_pcg<T, 16>;
+      case 32:
+        if constexpr (sizeof(T) == 4) return (const void*)k_ls_pcg<T, 32>;
+        break;
     }
     throw ApiError{FUGU_EINVAL, "lockstep batch: no PCG kernel for this cluster plan"};
   }
 
   // co-resident CTAs of a family kernel (its persistent grid)
-  int grid_of(const void* fn, int tpb, size_t smem = 0) {
+  // (capped at the most virtual blocks the family can have: a larger grid
+  // would only launch CTAs without work, which a small group pays for on
+  // every launch)
+  int grid_of(const void* fn, int tpb, long cap, size_t smem = 0) {
     auto it = grids.find(fn);
     if (it != grids.end()) return it->second;
     int occ = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, tpb, smem));
-    const int g = nsm * (occ > 0 ? occ : 1);
+    const int g = (int)std::max(1L, std::min((long)nsm * (occ > 0 ? occ : 1), cap));
     grids.emplace(fn, g);
     return g;
   }
   // the persistent grid of every family kernel, taken before any capture
   template <class F>
-  void warm_box() { grid_of((const void*)k_ls_box<T, F>, LS_TPB); }
+  void warm_box() { grid_of((const void*)k_ls_box<T, F>, LS_TPB, cap_box); }
   template <class F>
-  void warm_e1() { grid_of((const void*)k_ls_e1<T, F>, LS_TPB); }
+  void warm_e1() { grid_of((const void*)k_ls_e1<T, F>, LS_TPB, cap_e1); }
   void warm_grids() {
     warm_box<LsMatvecOuter<T>>(); warm_box<LsPoissonCoefs<T>>();
     warm_box<LsSchur<T>>(); warm_box<LsZwork<T>>(); warm_box<LsCross<T>>(); warm_box<LsRbsor<T>>();
@@ -303,26 +322,26 @@ struct Lockstep : LockstepBase {
     warm_e1<LsCvtCoefs<T>>(); warm_e1<LsDefect<T>>(); warm_e1<LsUpdate64<T>>(); warm_e1<LsScaleDefect<T>>();
     warm_e1<LsZeroCorrection<T>>(); warm_e1<LsAccumulate<T>>(); warm_e1<LsFgScale<T>>(); warm_e1<LsZeroPcd<T>>();
     warm_e1<LsJacobiCopy<T>>();
-    grid_of((const void*)k_ls_dot<T>, DOT_TPB);
-    grid_of((const void*)k_ls_mdot<T>, MDOT_TPB);
-    grid_of((const void*)k_ls_maxpy<T>, LS_TPB);
-    grid_of((const void*)k_ls_rbsor<T>, RB_TPB);
+    grid_of((const void*)k_ls_dot<T>, DOT_TPB, cap_dot);
+    grid_of((const void*)k_ls_mdot<T>, MDOT_TPB, cap_mdot);
+    grid_of((const void*)k_ls_maxpy<T>, LS_TPB, cap_e1);
+    grid_of((const void*)k_ls_rbsor<T>, RB_TPB, cap_tile);
     CK(cudaFuncSetAttribute((const void*)k_ls_matvec<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                             mt_matvec_smem<T, RB_TY>()));
-    grid_of((const void*)k_ls_matvec<T>, MT_TPB, mt_matvec_smem<T, RB_TY>());
+    grid_of((const void*)k_ls_matvec<T>, MT_TPB, cap_tile, mt_matvec_smem<T, RB_TY>());
   }
 
   // ------------------------------------------------------- launches
   template <class F>
   void box(F f) {
     const void* fn = (const void*)k_ls_box<T, F>;
-    k_ls_box<T, F><<<grid_of(fn, LS_TPB), LS_TPB, 0, q>>>(d_cases, d_dyn, d_plan, f);
+    k_ls_box<T, F><<<grid_of(fn, LS_TPB, cap_box), LS_TPB, 0, q>>>(d_cases, d_dyn, d_plan, f);
     LSCKL("k_ls_box");
   }
   template <class F>
   void e1(F f) {
     const void* fn = (const void*)k_ls_e1<T, F>;
-    k_ls_e1<T, F><<<grid_of(fn, LS_TPB), LS_TPB, 0, q>>>(d_cases, d_dyn, d_plan, f);
+    k_ls_e1<T, F><<<grid_of(fn, LS_TPB, cap_e1), LS_TPB, 0, q>>>(d_cases, d_dyn, d_plan, f);
     LSCKL("k_ls_e1");
   }
   template <class F>
@@ -341,17 +360,17 @@ struct Lockstep : LockstepBase {
   }
   void dot(int which, int op) {
     const void* fn = (const void*)k_ls_dot<T>;
-    k_ls_dot<T><<<grid_of(fn, DOT_TPB), DOT_TPB, 0, q>>>(d_cases, d_plan, which, OpArgs{op, 0, 0.0});
+    k_ls_dot<T><<<grid_of(fn, DOT_TPB, cap_dot), DOT_TPB, 0, q>>>(d_cases, d_plan, which, OpArgs{op, 0, 0.0});
     LSCKL("k_ls_dot");
   }
   void mdot(int which, int nvec, int op, int j) {
     const void* fn = (const void*)k_ls_mdot<T>;
-    k_ls_mdot<T><<<grid_of(fn, MDOT_TPB), MDOT_TPB, 0, q>>>(d_cases, d_plan, which, nvec, op, j, m);
+    k_ls_mdot<T><<<grid_of(fn, MDOT_TPB, cap_mdot), MDOT_TPB, 0, q>>>(d_cases, d_plan, which, nvec, op, j, m);
     LSCKL("k_ls_mdot");
   }
   void maxpy(int which, int nvec) {
     const void* fn = (const void*)k_ls_maxpy<T>;
-    k_ls_maxpy<T><<<grid_of(fn, LS_TPB), LS_TPB, 0, q>>>(d_cases, d_plan, which, nvec, m);
+    k_ls_maxpy<T><<<grid_of(fn, LS_TPB, cap_e1), LS_TPB, 0, q>>>(d_cases, d_plan, which, nvec, m);
     LSCKL("k_ls_maxpy");
   }
   // the PCD's PCG of every grid class, the classes side by side
@@ -415,7 +434,7 @@ struct Lockstep : LockstepBase {
     if (smoother == 1 && !any_periodic) {  // both colours of a sweep in one launch
       const void* fn = (const void*)k_ls_rbsor<T>;
       for (int sw = 0; sw < max_sw; ++sw) {
-        k_ls_rbsor<T><<<grid_of(fn, RB_TPB), RB_TPB, 0, q>>>(d_cases, d_dyn, d_plan, j, comp, sw);
+        k_ls_rbsor<T><<<grid_of(fn, RB_TPB, cap_tile), RB_TPB, 0, q>>>(d_cases, d_dyn, d_plan, j, comp, sw);
         LSCKL("k_ls_rbsor");
       }
       e1(LsJacobiCopy<T>{j, comp});
@@ -453,7 +472,7 @@ struct Lockstep : LockstepBase {
       for (int comp = 0; comp < 3; ++comp) one(LsHalo<T>{LB_ZJ, comp, j, -1});
     {
       const void* fn = (const void*)k_ls_matvec<T>;
-      k_ls_matvec<T><<<grid_of(fn, MT_TPB), MT_TPB, mt_matvec_smem<T, RB_TY>(), q>>>(d_cases, d_dyn, d_plan, j);
+      k_ls_matvec<T><<<grid_of(fn, MT_TPB, cap_tile), MT_TPB, mt_matvec_smem<T, RB_TY>(), q>>>(d_cases, d_dyn, d_plan, j);
       LSCKL("k_ls_matvec");
     }
     mdot(1, j + 1, FG_PROJ1, j);

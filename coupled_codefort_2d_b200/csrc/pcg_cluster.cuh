@@ -19,6 +19,12 @@
 //   boundary it is formed from the halo z and p, which gives the same bits as
 //   the owner's value.
 //
+// Lean variant (CPT = 32, FP32 only; grids of up to 16 x 512 cells per
+// column strip, such as 320 x 640): five register arrays of 32 cells do not
+// fit, so z is recomputed from r (z = dinv r, the same operation and bits)
+// and p_k is read back from the shared-memory copy the CTA keeps anyway;
+// phi, r and A p stay in registers.
+//
 // Arithmetic and reductions of the FP64 instantiation are those of k_pcg
 // and the oracle (error-free DD sums merged in rank order), so results are
 // bit-exact.  The FP32 instantiation (mixed-precision inner solve) sums its
@@ -74,6 +80,8 @@ struct RAcc {
 
 template <typename T, int CPT>
 __device__ __forceinline__ void pcg_cluster_body(const PcgClusterArgs<T>& a) {
+  constexpr bool LEAN = CPT > 16;
+  static_assert(!LEAN || sizeof(T) == 4, "the lean variant is FP32 only");
   cgc::cluster_group cl = cgc::this_cluster();
   const int C = (int)cl.num_blocks();
   const int rank = (int)cl.block_rank();
@@ -228,7 +236,11 @@ __device__ __forceinline__ void pcg_cluster_body(const PcgClusterArgs<T>& a) {
   }
   for (int q = threadIdx.x; q < R * nx; q += blockDim.x) dis[q] = a.dinv[g.at(q % nx + 1, j0 + q / nx)];
 
-  T phi_r[CPT], r_r[CPT], z_r[CPT], p_r[CPT], ap_r[CPT];
+  T phi_r[CPT], r_r[CPT], ap_r[CPT];
+  T z_r[LEAN ? 1 : CPT], p_r[LEAN ? 1 : CPT];  // (the lean variant does not use them)
+  // z and p_k of own cell c (local row lr): registers, or (lean) recomputed / from pcs
+#define PCGC_Z(c, lr) (LEAN ? dis[(lr) * nx + (i - 1)] * r_r[c] : z_r[LEAN ? 0 : (c)])
+#define PCGC_P(c, lr) (LEAN ? pcs[(lr) * nx + (i - 1)] : p_r[LEAN ? 0 : (c)])
 #define PCGC_CELLS _Pragma("unroll") for (int c = 0; c < CPT; ++c)
 #define PCGC_CELL             \
   if (c >= nr) continue;      \
@@ -290,8 +302,10 @@ __device__ __forceinline__ void pcg_cluster_body(const PcgClusterArgs<T>& a) {
     const T zz = dis[lr * nx + (i - 1)] * rr;
     phi_r[c] = ph;
     r_r[c] = rr;
-    z_r[c] = zz;
-    p_r[c] = zz;
+    if constexpr (!LEAN) {
+      z_r[c] = zz;
+      p_r[c] = zz;
+    }
     push(c, zz, zz);
     rz.add(double(rr) * double(zz));
   }
@@ -304,25 +318,26 @@ __device__ __forceinline__ void pcg_cluster_body(const PcgClusterArgs<T>& a) {
     // phase A: p_k of the own cells, then A p_k
     PCGC_CELLS {
       PCGC_CELL
-      const T pk = (iter == 1) ? z_r[c] : madd(tb, p_r[c], z_r[c]);
-      p_r[c] = pk;
+      const T zk = PCGC_Z(c, lr);
+      const T pk = (iter == 1) ? zk : madd(tb, PCGC_P(c, lr), zk);
+      if constexpr (!LEAN) p_r[c] = pk;
       pcs[lr * nx + (i - 1)] = pk;
     }
     __syncthreads();
     RAcc<T> papd;
     PCGC_CELLS {
       PCGC_CELL
-      const T pk = p_r[c];
+      const T pk = PCGC_P(c, lr);
       const T cE = cxs[lr * (nx + 1) + i], cW = cxs[lr * (nx + 1) + i - 1];
       const T cN = cys[(lr + 1) * nx + (i - 1)], cS = cys[lr * nx + (i - 1)];
       const T pE = pcs[lr * nx + (ie - 1)], pW = pcs[lr * nx + (iw - 1)];
       T pN, pS;
       if (j == ny && !g.py) pN = pk;
-      else if (c + 1 < nr) pN = p_r[c + 1];
+      else if (c + 1 < nr) pN = PCGC_P(c + 1, lr + 1);
       else if (lr + 1 < R) pN = pcs[(lr + 1) * nx + (i - 1)];
       else pN = (iter == 1) ? zt[i - 1] : madd(tb, pt[i - 1], zt[i - 1]);
       if (j == 1 && !g.py) pS = pk;
-      else if (c > 0) pS = p_r[c - 1];
+      else if (c > 0) pS = PCGC_P(c - 1, lr - 1);
       else if (lr > 0) pS = pcs[(lr - 1) * nx + (i - 1)];
       else pS = (iter == 1) ? zb[i - 1] : madd(tb, pb[i - 1], zb[i - 1]);
       // (cE + cW + cN + cS) pk - (((cE pE + cW pW) + cN pN) + cS pS)
@@ -341,10 +356,11 @@ __device__ __forceinline__ void pcg_cluster_body(const PcgClusterArgs<T>& a) {
       PCGC_CELL
       const T rv = madd(-ta, ap_r[c], r_r[c]);
       const T zv = dis[lr * nx + (i - 1)] * rv;
-      phi_r[c] = madd(ta, p_r[c], phi_r[c]);
+      const T pk = PCGC_P(c, lr);
+      phi_r[c] = madd(ta, pk, phi_r[c]);
       r_r[c] = rv;
-      z_r[c] = zv;
-      push(c, zv, p_r[c]);
+      if constexpr (!LEAN) z_r[c] = zv;
+      push(c, zv, pk);
       rrd.add(double(rv) * double(rv));
       rzd.add(double(rv) * double(zv));
     }
@@ -375,6 +391,8 @@ __device__ __forceinline__ void pcg_cluster_body(const PcgClusterArgs<T>& a) {
   cl.sync();  // no CTA leaves while another may still read its shared memory
 #undef PCGC_CELLS
 #undef PCGC_CELL
+#undef PCGC_Z
+#undef PCGC_P
 }
 template <typename T, int CPT>
 __global__ void __launch_bounds__(PCGC_TPB, 1) k_pcg_cluster(PcgClusterArgs<T> a) {

@@ -71,8 +71,7 @@ __device__ __forceinline__ bool grid_allreduce2(Barrier& bar, double* pa, double
   b = block_sum_dd(b, sh);
   if (threadIdx.x == 0) put_partial(pb, blockIdx.x, b);
   if (!grid_sync(bar.gs, bar.nb, bar.gen, bar.lim)) return false;
-  oa = sum_partials_dd(pa, gridDim.x);
-  ob = sum_partials_dd(pb, gridDim.x);
+  sum_partials_dd2(pa, pb, gridDim.x, oa, ob);
   return true;
 }
 

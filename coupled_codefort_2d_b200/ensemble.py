@@ -64,7 +64,7 @@ def solve_bytes(spec: dict, steps: list, solver: dict | None = None, inner_bytes
     distinct array read once and written once per kernel invocation, over the
     case's nx * ny cells (N) and its 3N coupled unknowns.  Counted per step
     from its statistics (``steps``: dicts with iter = Arnoldi steps, outer =
-    defect-correction passes, pcg_iters):
+    defect-correction passes, pcg_iters; per step, or summed over a run):
 
     - PCG: 9 values per cell and iteration (reads of p, cx, cy, dinv, phi, r;
       writes of p, phi, r);
@@ -99,14 +99,18 @@ def solve_bytes(spec: dict, steps: list, solver: dict | None = None, inner_bytes
     return total
 
 
-def run_shard_gpu(specs, idx, nsteps, device, nthreads=0, precision=None, warmup=0, solver=None, lockstep=True):
+def run_shard_gpu(specs, idx, nsteps, device, nthreads=0, precision=None, warmup=0, solver=None, lockstep=True,
+                  lockstep_group=0):
     """Advance the cases ``idx`` on ``device`` and return their per-case
     scalars and the elapsed seconds of the stepping, timed with CUDA events
     on the batch stream (barrier-free; the caller brackets it).  ``warmup``
     untimed steps come first (work space allocation, the adaptive PCG cap
     settling).  ``solver`` overrides the solver settings (default
     ``SOLVER``); ``lockstep`` selects the lockstep batch (one launch per
-    kernel family for all cases) over the thread-pool batch."""
+    kernel family for the cases of a group) over the thread-pool batch,
+    ``lockstep_group`` its largest group (0: one group per PCG grid class).
+    The timed steps are one batch run, so no case waits for the others
+    between its steps."""
     import torch
 
     from ._lib import MIXED
@@ -120,7 +124,7 @@ def run_shard_gpu(specs, idx, nsteps, device, nthreads=0, precision=None, warmup
         return
     sv = SOLVER if solver is None else solver
     with Batch([(s["grid"], ensemble_params(s, **sv), prec) for s in sub], device=device,
-               nthreads=nthreads, lockstep=lockstep) as b:
+               nthreads=nthreads, lockstep=lockstep, lockstep_group=lockstep_group) as b:
         for k, s in enumerate(sub):
             initial_bubble_state(b.case(k), s)
         opts = b.case(0).step_opts(use_bicgstab2=True)
@@ -134,7 +138,7 @@ def run_shard_gpu(specs, idx, nsteps, device, nthreads=0, precision=None, warmup
         n0 = b.launches()
         t0 = time.perf_counter()
         e0.record(stream)
-        outs = [b.run(1, DT, warmup + 1 + k, opts) for k in range(nsteps)]
+        out = b.run(nsteps, DT, warmup + 1, opts)
         e1.record(stream)
         e1.synchronize()
         elapsed = e0.elapsed_time(e1) / 1000.0
@@ -145,12 +149,10 @@ def run_shard_gpu(specs, idx, nsteps, device, nthreads=0, precision=None, warmup
         for k, s in enumerate(sub):
             st = b.case(k).download_state(["c_field", "v_vel"])
             ycm, vr = cases.bubble_centroid_velocity(s["grid"], st["c_field"], st["v_vel"])
-            steps = [o["last"][k] for o in outs]
-            rows.append({"case": s["case"], "status": max((o["status"][k] for o in outs), key=abs),
-                         "max_res": max(o["max_res"][k] for o in outs),
-                         "arnoldi_steps": sum(x["iter"] for x in steps), "outer": sum(x["outer"] for x in steps),
-                         "pcg_iters": sum(x["pcg_iters"] for x in steps),
-                         "bytes": solve_bytes(s, steps, sv, 4 if prec == MIXED else 8),
+            tot = out["total"][k]
+            rows.append({"case": s["case"], "status": out["status"][k], "max_res": out["max_res"][k],
+                         "arnoldi_steps": tot["iter"], "outer": tot["outer"], "pcg_iters": tot["pcg_iters"],
+                         "bytes": solve_bytes(s, [tot], sv, 4 if prec == MIXED else 8),
                          "y_centroid": ycm, "rise_velocity": vr, "host_wall_s": wall,
                          "shard_launches": launches})
         yield "done", (rows, elapsed)
@@ -234,6 +236,8 @@ def main(argv=None):
                     help="replay the Arnoldi steps from CUDA graphs (default: the SOLVER setting)")
     ap.add_argument("--thread-pool", action="store_true",
                     help="step the cases from host threads instead of in lockstep")
+    ap.add_argument("--lockstep-group", type=int, default=0,
+                    help="largest lockstep group (0: one group per PCG grid class)")
     args = ap.parse_args(argv)
     solver = solver_from_args(args)
     import datetime
@@ -253,7 +257,8 @@ def main(argv=None):
     specs = cases.bubble_ensemble(args.cases, seed=args.seed)
     res = run_ensemble(specs, args.steps, rank, world,
                        lambda idx: run_shard_gpu(specs, idx, args.steps, local, args.threads, warmup=args.warmup,
-                                                 solver=solver, lockstep=not args.thread_pool),
+                                                 solver=solver, lockstep=not args.thread_pool,
+                                                 lockstep_group=args.lockstep_group),
                        barrier, max_reduce, gather)
     if world > 1:
         dist.destroy_process_group()
@@ -261,7 +266,7 @@ def main(argv=None):
         rows = res.pop("rows")
         res["failed"] = [r["case"] for r in rows if r["status"] != 0]
         res["max_res"] = max(r["max_res"] for r in rows)
-        res["form"] = "thread pool" if args.thread_pool else "lockstep"
+        res["form"] = "thread pool" if args.thread_pool else f"lockstep (group <= {args.lockstep_group or 'class'})"
         res["launches_rank0"] = rows[0].get("shard_launches") if rows else None
         res["solver"] = solver
         print(json.dumps(res), flush=True)

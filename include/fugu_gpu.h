@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define FUGU_ABI_VERSION 3
+#define FUGU_ABI_VERSION 4
 
 /* return codes */
 #define FUGU_OK 0
@@ -385,8 +385,15 @@ typedef struct {
                        are conditional nodes armed on the device); needs every
                        case at refine = 2 with one precision, pcd_smoother and
                        refine_max_inner, and a PCG that fits a cluster; at most
-                       1024 cases.  Each case's results equal those of the
+                       1024 cases.  Within one fugu_batch_run of several
+                       steps a case whose solve has ended takes its next
+                       step while the others keep solving (continuous
+                       batching).  Each case's results equal those of the
                        thread-pool form (0) bit for bit.                      */
+  int lockstep_group; /* lockstep: the cases are grouped by their PCG's cluster
+                       plan, at most this many per group (0: no limit); each
+                       group runs in lockstep on its own stream and host
+                       thread, and the groups do not wait for one another   */
 } fugu_batch_opts;
 int fugu_batch_create(const fugu_params* params, int ncases, int device, const fugu_batch_opts* opts,
                       fugu_batch** out);
@@ -398,9 +405,12 @@ int fugu_batch_case(fugu_batch* b, int i, fugu_ctx** ctx);
  * step0[i]+nsteps-1 and options opts[i].  Per case (each output may be
  * NULL): last[i] = stats of its last step, max_res[i] = largest final
  * residual over its steps, status[i] = FUGU_OK or the error of the step
- * that stopped it.  Returns FUGU_OK, or the first failing case's code. */
+ * that stopped it, total[i] = its steps' stats summed (iter, outer,
+ * pcg_iters, pcg_calls, matvecs, svof_iters; res the largest, status the
+ * first that is not FUGU_CONVERGED).  Returns FUGU_OK, or the first failing
+ * case's code. */
 int fugu_batch_run(fugu_batch* b, int nsteps, const double* dt, const int* step0, const fugu_step_opts* opts,
-                   fugu_stats* last, double* max_res, int* status);
+                   fugu_stats* last, double* max_res, int* status, fugu_stats* total);
 /* The batch stream (cudaStream_t): all device work of a fugu_batch_run
  * starts after the work queued on it before the call and ends before the
  * work queued on it after the call, so CUDA events recorded on it around a

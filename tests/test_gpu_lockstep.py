@@ -43,9 +43,9 @@ def specs_with_periodic(n):
     return specs
 
 
-def run(specs, prms, prec, lockstep, nsteps=NSTEPS, one_call=False):
+def run(specs, prms, prec, lockstep, nsteps=NSTEPS, one_call=False, group=0):
     with Batch([(s["grid"], p, prec) for s, p in zip(specs, prms)], nthreads=4, max_cluster=8,
-               lockstep=lockstep) as b:
+               lockstep=lockstep, lockstep_group=group) as b:
         for i, s in enumerate(specs):
             initial_bubble_state(b.case(i), s)
         o = b.case(0).step_opts(use_bicgstab2=True)
@@ -79,26 +79,30 @@ def test_lockstep_equals_thread_pool_bitwise(gpu, prec, smoother, periodic):
     assert 0 < launches < ref_launches  # one launch per kernel family for all cases
 
 
-@pytest.mark.parametrize("smoother,periodic", [(1, False), (0, True)])
-def test_lockstep_continuous_run_equals_thread_pool_bitwise(gpu, smoother, periodic):
+@pytest.mark.parametrize("smoother,periodic,group", [(1, False, 0), (0, True, 0), (1, False, 1), (1, False, 2)])
+def test_lockstep_continuous_run_equals_thread_pool_bitwise(gpu, smoother, periodic, group):
     """All steps in one run: a case whose solve ends at a pass takes its next
     step's explicit stages while the others keep solving, and joins the
     lockstep solve at the following pass, so within the run the cases are at
-    different steps.  Every case still follows its own sequence of operations,
-    so the final states and the last step's statistics equal the thread-pool
-    batch's bit for bit."""
+    different steps.  The cases form lockstep groups by PCG grid class (group
+    0: one group per class; 1 and 2: at most that many cases per group), each
+    run by its own host thread.  Every case still follows its own sequence of
+    operations, so the final states, the last step's and the run's summed
+    statistics equal the thread-pool batch's bit for bit."""
     specs = specs_with_periodic(6) if periodic else cases.bubble_ensemble(6, grids=SMALL_GRIDS)
     prms = [ensemble_params(s, **dict(SOLVER, pcd_smoother=smoother)) for s in specs]
     if periodic:
         prms[1] = dataclasses.replace(prms[1], free_slip_x=0)
     nsteps = 4
     (ref,), ref_states, _ = run(specs, prms, MIXED, lockstep=False, nsteps=nsteps, one_call=True)
-    (out,), states, _ = run(specs, prms, MIXED, lockstep=True, nsteps=nsteps, one_call=True)
+    (out,), states, _ = run(specs, prms, MIXED, lockstep=True, nsteps=nsteps, one_call=True, group=group)
     assert out["status"] == ref["status"] == [0] * len(specs)
     assert out["max_res"] == ref["max_res"]
     for i in range(len(specs)):
         for k in STATS:
             assert out["last"][i][k] == ref["last"][i][k], (i, k, out["last"][i], ref["last"][i])
+            assert out["total"][i][k] == ref["total"][i][k], (i, k, out["total"][i], ref["total"][i])
+        assert out["total"][i]["iter"] > out["last"][i]["iter"]
         for k in STATE_FIELDS:
             np.testing.assert_array_equal(states[i][k], ref_states[i][k], err_msg=f"case {i} {k}")
 

@@ -280,6 +280,39 @@ def test_graph_replay_with_grid_wide_pcg(gpu, precision, refine, monkeypatch):
         assert c1["pcg_launches"] < c0["pcg_launches"]
 
 
+def test_lean_cluster_pcg_matches_grid_wide(gpu, monkeypatch):
+    """A 300 x 384 droplet: 16 CTAs of 24 rows, so each thread of the
+    cluster-resident FP32 PCG owns a strip of up to 32 cells, and the lean
+    variant (z recomputed from r, p read from shared memory) runs.  The mixed
+    form solved to 1e-10 with it and with the grid-wide kernel ends within
+    1e-7 of each other (two FP32 inner paths, one FP64 tolerance), and the
+    profile shows which PCG ran."""
+    from oracle import oracle as o
+
+    g = Grid(300, 384, 1.0, 1.28)
+    p = Params(rho1=1.0, rho2=0.1, mu1=0.1, mu2=0.01, sigma=1.0, gx=0.0, gy=0.0, time_order=2,
+               tol_bicgstab2=1e-10, max_iter_bicgstab2=500, refine=2, refine_inner_tol=1e-2, refine_max_inner=30,
+               refine_max_outer=60, krylov_bc_fix=1, pcg_cap_start=40, pcd_sweeps=6, pcd_sweeps_max=24, graphs=1,
+               pcd_visc_scale=1.0)
+    c0 = cases.circle_fraction(g, 0.5, 0.64, 0.25, inside=1.0, ns=4)
+    out = {}
+    for mode in ("cluster", "grid"):
+        if mode == "grid":
+            monkeypatch.setenv("FUGU_PCG", "grid")
+        st = o.new_state(g, c0, p)
+        with Context(g, p, precision=1) as ctx:
+            ctx.upload_state(st)
+            opts = ctx.step_opts(use_bicgstab2=True)
+            stats = [ctx.step(1e-4, s, opts) for s in (1, 2)]
+            prof = ctx.profile(-1)
+            out[mode] = (ctx.download_state(["u_vel", "v_vel", "p_field"]), stats, prof)
+    (sc, hc, pc), (sg, hg, pg) = out["cluster"], out["grid"]
+    assert pc["pcg_cluster_fp32"] == 16 and pg["pcg_cluster_fp32"] == 0
+    assert all(h["status"] == 0 and h["res"] < 1e-10 for h in hc + hg)
+    for k in ("u_vel", "v_vel"):
+        assert rel(sc[k], sg[k]) <= 1e-7, (k, rel(sc[k], sg[k]))
+
+
 def test_checkpoint_restart_bitwise(gpu, oracle_mod):
     """mod_io.f90:169-225 format: the GPU writes the reference's byte layout,
     the oracle reads it back, and a restart reproduces the run bit for bit
