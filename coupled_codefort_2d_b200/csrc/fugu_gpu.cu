@@ -483,7 +483,7 @@ void plan_pcg_cluster(fugu_ctx* c, fugu_ctx::ClusterPlan& pl) {
     cudaGetLastError();
     return;
   }
-  const size_t smem = sizeof(T) * (size_t)pcgc_smem_elems(nx, rows_per);
+  const size_t smem = sizeof(T) * (size_t)pcgc_smem_elems<T>(nx, rows_per, cpt);
   const size_t smem_cap = (size_t)optin - fa.sharedSizeBytes;
   if (smem > smem_cap) return;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_cap) != cudaSuccess ||
@@ -659,6 +659,21 @@ void helmholtz(fugu_ctx* c, bool is_u, T* sol, T* tmp, const T* rhs, const CoefB
                                                      T(dt), T(c->prm.pcd_sor_omega), col, active);
         CKL("k_rbsor");
       }
+    return;
+  }
+  if (!c->g.px && !c->g.py) {
+    // up to JM_K sweeps per launch on staged tiles, alternating between sol
+    // and tmp
+    const dim3 grid((c->g.P + JM_TX - 1) / JM_TX, (c->g.R + JM_TY - 1) / JM_TY);
+    for (int s = 0; s < n_sweeps; s += JM_K) {
+      const int k = std::min(JM_K, n_sweeps - s);
+      k_jacobi_multi<T><<<grid, JM_TPB, sizeof(JmSmem<T>), c->s>>>(
+          c->g, is_u ? 0 : 1, k, cur, nxt, rhs, is_u ? cb.rho_u : cb.rho_v, cb.kappa, cb.zeta, cb.eta, pen, T(dt),
+          T(c->prm.jacobi_omega), active);
+      CKL("k_jacobi_multi");
+      std::swap(cur, nxt);
+    }
+    if (cur != sol) CK(cudaMemcpyAsync(sol, cur, sizeof(T) * c->n, cudaMemcpyDeviceToDevice, c->s));
     return;
   }
   for (int s = 0; s < n_sweeps; ++s) {
@@ -1586,6 +1601,11 @@ void create(fugu_ctx* c) {
   if (c->pcg_grid < 1 || c->svof_grid < 1) throw ApiError{FUGU_ECUDA, "no co-resident grid for persistent kernels"};
   plan_pcg_cluster<double>(c, c->pcgc[0]);
   plan_pcg_cluster<float>(c, c->pcgc[1]);
+  // the multi-sweep Jacobi tiles of FP64 need more than the default 48 KB
+  CK(cudaFuncSetAttribute((const void*)k_jacobi_multi<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)sizeof(JmSmem<double>)));
+  CK(cudaFuncSetAttribute((const void*)k_jacobi_multi<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                          (int)sizeof(JmSmem<float>)));
   const char* env = std::getenv("FUGU_PCG");
   if (env && std::strcmp(env, "cluster") == 0 && !(c->pcgc[0].ok && c->pcgc[1].ok))
     throw ApiError{FUGU_EINVAL, "FUGU_PCG=cluster but this grid does not fit a thread-block cluster"};

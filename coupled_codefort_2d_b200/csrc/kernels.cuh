@@ -835,6 +835,119 @@ __global__ void __launch_bounds__(RB_TPB) k_rbsor_sweep(Geo g, int comp, const T
   rbsor_sweep_tile<T>(g, comp, blockIdx.x, blockIdx.y, uin, uout, rhs, rho, kap, zeta, eta, pen, dt, om, sm);
 }
 
+// ------------------------------------------------ several Jacobi sweeps at once
+// Up to JM_K damped-Jacobi sweeps (solve_helmholtz_u/v's, jacobi_u_vals /
+// jacobi_v_vals) of one velocity component of a wall-bounded case in one
+// launch, per tile of JM_TX x JM_TY faces, from uin into uout.  The tile and
+// a ring of JM_K faces of uin go to shared memory (the ring widened to eight
+// columns either side so that rows start on 16-byte boundaries), the
+// coefficients of the tile and a ring of JM_K - 1 are formed once, and sweep
+// s of nsw updates the tile and a ring of nsw - s faces from the previous
+// sweep's values, alternating between two shared-memory buffers; each face
+// takes the formula with its operand order (owned faces), the right-hand side
+// (wall faces) or keeps its value (other elements), as in k_jacobi_u/v.  So
+// nsw sweeps give the bits of nsw k_jacobi_u/v launches, reading and writing
+// each array once.  Periodic cases refresh their halo between sweeps and
+// keep the one-sweep launches.
+constexpr int JM_TX = 32, JM_TY = 16, JM_K = 6, JM_TPB = 256;
+constexpr int JM_SX = JM_TX + 16, JM_SY = JM_TY + 2 * JM_K;            // staged values
+constexpr int JM_CX = JM_TX + 2 * (JM_K - 1), JM_CY = JM_TY + 2 * (JM_K - 1);  // coefficients
+template <typename T>
+struct JmSmem {
+  T u[2][JM_SY][JM_SX];
+  T cE[JM_CY][JM_CX], cW[JM_CY][JM_CX], cN[JM_CY][JM_CX], cS[JM_CY][JM_CX], dg[JM_CY][JM_CX], rh[JM_CY][JM_CX];
+  unsigned char kind[JM_CY][JM_CX];  // 0 keeps its value, 1 owned face (formula), 2 wall face (= rhs)
+};
+template <typename T>
+__device__ __forceinline__ void jacobi_multi_tile(const Geo& g, int comp, int nsw, int tx, int ty, const T* uin,
+                                                  T* __restrict__ uout, const T* rhs, const T* rho, const T* kap,
+                                                  const T* zeta, const T* eta, const T* pen, T dt, T om,
+                                                  JmSmem<T>& sm) {
+  const int ii0 = tx * JM_TX, jj0 = ty * JM_TY;  // padded coordinates of the tile's first face
+  const int sx0 = ii0 - 8, sy0 = jj0 - JM_K;     // of sm.u[.][0][0]
+  const int cx0 = ii0 - (JM_K - 1), cy0 = jj0 - (JM_K - 1);  // of the coefficient arrays' [0][0]
+  const int nx = g.nx, ny = g.ny;
+  const T ix2 = T(g.idx2), iy2 = T(g.idy2);
+  for (int q = threadIdx.x; q < JM_SX * JM_SY; q += blockDim.x) {
+    const int a = q % JM_SX, b = q / JM_SX;
+    const int ii = sx0 + a, jj = sy0 + b;
+    sm.u[0][b][a] = (ii >= 0 && ii < g.P && jj >= 0 && jj < g.R) ? uin[ii + jj * g.P] : T(0);
+  }
+  for (int q = threadIdx.x; q < JM_CX * JM_CY; q += blockDim.x) {
+    const int a = q % JM_CX, b = q / JM_CX;
+    const int ii = cx0 + a, jj = cy0 + b;
+    const int i = ii - 2, j = jj - 2;
+    unsigned char kd = 0;
+    if (ii >= 0 && ii < g.P && jj >= 0 && jj < g.R) {
+      const int k = ii + jj * g.P;
+      if (comp == 0 && j >= 1 && j <= ny) {
+        if (i >= 1 && i <= nx - 1) {
+          kd = 1;
+          const T e = kap[g.at(i + 1, j)] * ix2, w = kap[k] * ix2;
+          const T nn = (zeta[k] - eta[k]) * iy2, ss = (zeta[g.at(i, j - 1)] - eta[g.at(i, j - 1)]) * iy2;
+          T d = (rho[k] / dt) + e + w + nn + ss;
+          if (pen) d = d + pen[k];
+          sm.cE[b][a] = e; sm.cW[b][a] = w; sm.cN[b][a] = nn; sm.cS[b][a] = ss; sm.dg[b][a] = d;
+        } else if (i == 0 || i == nx) {
+          kd = 2;
+        }
+      } else if (comp == 1 && i >= 1 && i <= nx) {
+        if (j >= 1 && j <= ny - 1) {
+          kd = 1;
+          const T e = (zeta[k] - eta[k]) * ix2, w = (zeta[g.at(i - 1, j)] - eta[g.at(i - 1, j)]) * ix2;
+          const T nn = kap[g.at(i, j + 1)] * iy2, ss = kap[k] * iy2;
+          T d = (rho[k] / dt) + e + w + nn + ss;
+          if (pen) d = d + pen[k];
+          sm.cE[b][a] = e; sm.cW[b][a] = w; sm.cN[b][a] = nn; sm.cS[b][a] = ss; sm.dg[b][a] = d;
+        } else if (j == 0 || j == ny) {
+          kd = 2;
+        }
+      }
+      if (kd) sm.rh[b][a] = rhs[k];
+    }
+    sm.kind[b][a] = kd;
+  }
+  __syncthreads();
+  int cur = 0;
+  for (int sweep = 1; sweep <= nsw; ++sweep) {
+    const int ring = nsw - sweep;  // faces updated around the tile in this sweep
+    const int wx = JM_TX + 2 * ring, wy = JM_TY + 2 * ring;
+    for (int q = threadIdx.x; q < wx * wy; q += blockDim.x) {
+      const int ii = ii0 - ring + q % wx, jj = jj0 - ring + q / wx;  // padded coordinates
+      const int a = ii - cx0, b = jj - cy0;                           // coefficient indices
+      const int ua = ii - sx0, ub = jj - sy0;                         // value indices
+      const unsigned char kd = sm.kind[b][a];
+      const T uo = sm.u[cur][ub][ua];
+      T val = uo;
+      if (kd == 2) {
+        val = sm.rh[b][a];
+      } else if (kd == 1) {
+        const T d = sm.dg[b][a];
+        const T off = madd(sm.cS[b][a], sm.u[cur][ub - 1][ua],
+                           madd(sm.cN[b][a], sm.u[cur][ub + 1][ua],
+                                madd(sm.cW[b][a], sm.u[cur][ub][ua - 1], sm.cE[b][a] * sm.u[cur][ub][ua + 1])));
+        if (d > T(1.0e-15)) val = madd(T(1) - om, uo, om * ((sm.rh[b][a] + off) / d));
+      }
+      sm.u[cur ^ 1][ub][ua] = val;
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+  for (int q = threadIdx.x; q < JM_TX * JM_TY; q += blockDim.x) {
+    const int ii = ii0 + q % JM_TX, jj = jj0 + q / JM_TX;
+    if (ii < g.P && jj < g.R) uout[ii + jj * g.P] = sm.u[cur][jj - sy0][ii - sx0];
+  }
+}
+template <typename T>
+__global__ void __launch_bounds__(JM_TPB) k_jacobi_multi(Geo g, int comp, int nsw, const T* uin, T* __restrict__ uout,
+                                                         const T* rhs, const T* rho, const T* kap, const T* zeta,
+                                                         const T* eta, const T* pen, T dt, T om, const int* active) {
+  if (active && !*active) return;
+  extern __shared__ __align__(16) unsigned char jm_smem[];
+  jacobi_multi_tile<T>(g, comp, nsw, blockIdx.x, blockIdx.y, uin, uout, rhs, rho, kap, zeta, eta, pen, dt, om,
+                       *reinterpret_cast<JmSmem<T>*>(jm_smem));
+}
+
 // ------------------------------------------------------------ Krylov vectors
 // Whole-buffer linear combinations over a coupled triple (u, v, p buffers of
 // n elements each, contiguous in one allocation of 3n).  Coefficients are

@@ -708,7 +708,8 @@ __global__ void __launch_bounds__(PCGC_TPB, 1) k_ls_pcg(const LsCase<T>* cs, con
   a.phi_zero = 1;
   a.rows_per = rows_per;
   a.timed = 0;
-  pcg_cluster_body<T, CPT>(a);
+  if constexpr (pcgc_one_reduction<T>(CPT)) pcg_cluster_body_1r<CPT>(a);
+  else pcg_cluster_body<T, CPT>(a);
 }
 
 }  // namespace fugu
