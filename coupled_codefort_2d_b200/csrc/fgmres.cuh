@@ -123,6 +123,21 @@ __host__ __device__ inline long mdot_items(const Geo& g) {
 }
 
 // CTA (bx, by) of a (Gx, Gy = nvec) grid
+// arms the conditional node of a further Arnoldi step of a cycle graph
+// with "the solve is still active" (run_cycle in fugu_gpu.cu)
+__global__ void k_fg_cond(const int* active, cudaGraphConditionalHandle h) {
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, *active ? 1u : 0u);
+}
+
+// a lane's running sum of its products: error-free (double-double) for the
+// FP64 parity path; the FP32 inner solve needs only a fixed order, so a plain
+// double sum of its (exact) float products serves there at a fraction of the
+// dependent FP64 work
+template <typename T>
+__device__ __forceinline__ void mdot_acc(DD& acc, double x) {
+  if constexpr (sizeof(T) == 8) dd_add(acc, x);
+  else acc.hi += x;
+}
 template <typename T>
 __device__ __forceinline__ void mdot_body(const MdotArgs<T>& a, int bx, int by, int Gx, int Gy) {
   constexpr int NW = MDOT_TPB / 32;
@@ -167,11 +182,11 @@ __device__ __forceinline__ void mdot_body(const MdotArgs<T>& a, int bx, int by, 
         vv[u] = V[base + i0 + 32 * u];
       }
 #pragma unroll
-      for (int u = 0; u < U; ++u) dd_add(acc, (double(wv[u]) * double(vv[u])) * a.vol);
+      for (int u = 0; u < U; ++u) mdot_acc<T>(acc, (double(wv[u]) * double(vv[u])) * a.vol);
     } else {
       for (int i = i0; i < i1; i += 32) {
         const long e = base + i;
-        dd_add(acc, (double(a.w[e]) * double(V[e])) * a.vol);
+        mdot_acc<T>(acc, (double(a.w[e]) * double(V[e])) * a.vol);
       }
     }
   }
