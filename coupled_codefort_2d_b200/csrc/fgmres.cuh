@@ -123,12 +123,6 @@ __host__ __device__ inline long mdot_items(const Geo& g) {
 }
 
 // CTA (bx, by) of a (Gx, Gy = nvec) grid
-// arms the conditional node of a further Arnoldi step of a cycle graph
-// with "the solve is still active" (run_cycle in fugu_gpu.cu)
-__global__ void k_fg_cond(const int* active, cudaGraphConditionalHandle h) {
-  if (threadIdx.x == 0) cudaGraphSetConditional(h, *active ? 1u : 0u);
-}
-
 // a lane's running sum of its products: error-free (double-double) for the
 // FP64 parity path; the FP32 inner solve needs only a fixed order, so a plain
 // double sum of its (exact) float products serves there at a fraction of the

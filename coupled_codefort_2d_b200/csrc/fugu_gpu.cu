@@ -83,6 +83,7 @@ template <typename T>
 struct PcgWork {
   T *cx = nullptr, *cy = nullptr, *dinv = nullptr, *r = nullptr, *z = nullptr, *pb0 = nullptr,
     *pb1 = nullptr, *ap = nullptr;
+  T *w1 = nullptr, *pv = nullptr;  // the FP32 single-reduction grid-wide PCG's two more vectors
 };
 
 template <typename T>
@@ -228,16 +229,6 @@ struct fugu_ctx {
   // one BiCGStab (index 0) / BiCGStab(2) (index 1) iteration per precision,
   // its iteration index on the device (KState::kiter)
   StepGraph kr_graphs[2][2];
-  // one flexible-GMRES cycle as one graph per precision: Arnoldi step 0,
-  // then one conditional IF node per further step, armed on the device
-  struct CycleGraph {
-    StepGraph sg;                 // key, executable graph, step 0's PCG events
-    unsigned long long head = 0;  // kernel launches of step 0
-    unsigned long long body = 0;  // kernel launches of one further step
-  };
-  CycleGraph fg_cycle[2];
-  bool fg_cycle_ok = true;        // cleared (for good) if the conditional graph cannot be built
-  cudaStream_t s2 = nullptr;      // captures the bodies of the conditional nodes
   StepGraph* capturing = nullptr;     // the step graph being captured
   StepGraph* pcg_timed = nullptr;     // replayed with PCG events, not yet read
   // measurement: launch count, CUDA-event timing of the persistent kernels
@@ -615,7 +606,14 @@ void pcg(fugu_ctx* c, PcgWork<T>& w, T* phi, const T* rhs, double tol, int max_i
   } else {
     CK(cudaMemsetAsync(c->gs, 0, sizeof(GridSync), c->s));
     void* args[] = {&a};
-    launch_coop(c, (const void*)k_pcg<T>, c->pcg_grid, args);
+    if constexpr (sizeof(T) == 4) {
+      // the FP32 inner solve: one grid barrier per iteration
+      a.w1 = w.w1;
+      a.pv = w.pv;
+      launch_coop(c, (const void*)k_pcg1<T>, c->pcg_grid, args);
+    } else {
+      launch_coop(c, (const void*)k_pcg<T>, c->pcg_grid, args);
+    }
   }
   ++c->launches;
   if (rec) {
@@ -1080,113 +1078,6 @@ void mdot(fugu_ctx* c, const T* w, const T* V0, int nvec, int op, int j, double 
   CKL("k_mdot");
 }
 
-// Replay a whole flexible-GMRES cycle from one graph: Arnoldi step 0, then
-// per further step j a one-thread kernel that arms a conditional IF node
-// with "the solve is still active" and the node whose body is step j.  A
-// step after the solve's exit is skipped on the device, and the host waits
-// once per cycle instead of once per Arnoldi step.  The graph is captured
-// again when key changes.  The bodies are captured on the context's second
-// stream (the launch helpers issue on c->s, which is swapped with it for the
-// capture).  Kernel launches are counted as if launched one by one (the
-// arming kernels are not counted).  Returns false, and leaves nothing
-// launched, when the runtime cannot build the graph.
-template <typename F>
-bool run_cycle(fugu_ctx* c, fugu_ctx::CycleGraph& cg, std::vector<unsigned char>&& key, bool timed, int m, F step) {
-  fugu_ctx::StepGraph& sg = cg.sg;
-  if (!sg.exec || sg.key != key) {
-    if (sg.exec) {
-      cudaGraphExecDestroy(sg.exec);
-      sg.exec = nullptr;
-    }
-    if (c->pcg_timed == &sg) c->pcg_timed = nullptr;
-    sg.timed = timed;
-    while (timed && sg.ev.size() < 4) {
-      cudaEvent_t a, b;
-      CK(cudaEventCreate(&a));
-      CK(cudaEventCreate(&b));
-      sg.ev.push_back({a, b});
-    }
-    sg.ev_used = 0;
-    fugu_ctx::StepGraph body_sg;  // the bodies record no events
-    const unsigned long long l0 = c->launches;
-    cudaGraph_t graph = nullptr;
-    bool swapped = false;
-    try {
-      CK(cudaStreamBeginCapture(c->s, cudaStreamCaptureModeThreadLocal));
-      c->capturing = &sg;
-      step(0);
-      cg.head = c->launches - l0;
-      for (int j = 1; j < m; ++j) {
-        cudaStreamCaptureStatus cs;
-        cudaGraph_t cgr = nullptr;
-        const cudaGraphNode_t* deps = nullptr;
-        size_t nd = 0;
-        CK(cudaStreamGetCaptureInfo(c->s, &cs, nullptr, &cgr, &deps, &nd));
-        cudaGraphConditionalHandle h;
-        CK(cudaGraphConditionalHandleCreate(&h, cgr, 0, 0));
-        k_fg_cond<<<1, 32, 0, c->s>>>(&c->ks->active, h);
-        CK(cudaGetLastError());
-        CK(cudaStreamGetCaptureInfo(c->s, &cs, nullptr, &cgr, &deps, &nd));
-        cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeIf;
-        cp.conditional.size = 1;
-        cudaGraphNode_t node;
-        CK(cudaGraphAddNode(&node, cgr, deps, nd, &cp));
-        CK(cudaStreamUpdateCaptureDependencies(c->s, &node, 1, cudaStreamSetCaptureDependencies));
-        std::swap(c->s, c->s2);
-        swapped = true;
-        CK(cudaStreamBeginCaptureToGraph(c->s, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                         cudaStreamCaptureModeThreadLocal));
-        c->capturing = &body_sg;
-        const unsigned long long b0 = c->launches;
-        step(j);
-        cg.body = c->launches - b0;
-        cudaGraph_t bout = nullptr;
-        CK(cudaStreamEndCapture(c->s, &bout));
-        std::swap(c->s, c->s2);
-        swapped = false;
-        c->capturing = &sg;
-      }
-      c->capturing = nullptr;
-      CK(cudaStreamEndCapture(c->s, &graph));
-      CK(cudaGraphInstantiate(&sg.exec, graph, 0));
-      cudaGraphDestroy(graph);
-    } catch (...) {
-      // close the captures; a CUDA error means the runtime cannot build the
-      // graph (the caller launches the steps one by one), anything else is
-      // passed on
-      c->capturing = nullptr;
-      if (swapped) {
-        cudaGraph_t junk = nullptr;
-        cudaStreamEndCapture(c->s, &junk);
-        std::swap(c->s, c->s2);
-      }
-      cudaGraph_t junk = nullptr;
-      cudaStreamEndCapture(c->s, &junk);
-      if (junk) cudaGraphDestroy(junk);
-      if (graph) cudaGraphDestroy(graph);
-      cudaGetLastError();
-      c->launches = l0;
-      if (sg.exec) cudaGraphExecDestroy(sg.exec);
-      sg.exec = nullptr;
-      sg.key.clear();
-      try {
-        throw;
-      } catch (const CudaError&) {
-        return false;
-      }
-    }
-    c->launches = l0;
-    sg.key = std::move(key);
-  }
-  if (c->pcg_timed == &sg) graph_prof_read(c);
-  CK(cudaGraphLaunch(sg.exec, c->s));
-  c->launches += cg.head;  // the executed further steps are added by the caller
-  if (sg.timed) c->pcg_timed = &sg;
-  return true;
-}
-
 // flexible GMRES(m), right PCD preconditioning, one cycle from X = 0
 // (extension; the inner solve of refine_solve when refine = 2)
 template <typename T>
@@ -1233,27 +1124,7 @@ KrylovResult fgmres(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const 
     k_fg_scale<T><<<g1, 256, 0, c->s>>>(n3, f.V + (long)(j + 1) * n3, wv.base, f.st + L.inv(), act);
     CKL("k_fg_scale");
   };
-  // graphs = 1 with the cluster-resident PCG: the whole cycle from one graph
-  bool cycled = false;
-  if (graphed && c->pcgc[pi].ok && c->fg_cycle_ok && ks.active && m > 1) {
-    NvtxRange r_it("fgmres_cycle");
-    std::vector<unsigned char> key;
-    key_put(key, m); key_put(key, f.V); key_put(key, f.Z); key_put(key, f.st);
-    key_put(key, wv.base); key_put(key, cb); key_put(key, o); key_put(key, dt); key_put(key, tol);
-    key_put(key, c->pcg_cap_cur); key_put(key, c->pcd_sweeps_cur); key_put(key, c->adj_on);
-    const bool timed = c->prof != 0;  // the PCG of step 0 (outside the conditional nodes)
-    key_put(key, c->prm); key_put(key, timed);
-    fugu_ctx::CycleGraph& cg = c->fg_cycle[pi];
-    cycled = run_cycle(c, cg, std::move(key), timed, m, arnoldi_step_j);
-    if (cycled) {
-      ks = read_ks(c);
-      const int done = ks.active ? m : ks.exit_iter;  // Arnoldi steps the cycle ran
-      if (done > 1) c->launches += cg.body * (unsigned long long)(done - 1);
-    } else {
-      c->fg_cycle_ok = false;
-    }
-  }
-  for (int j = 0; j < m && ks.active && !cycled; ++j) {
+  for (int j = 0; j < m && ks.active; ++j) {
     NvtxRange r_it("arnoldi_step");
     auto arnoldi_step = [&] { arnoldi_step_j(j); };
     if (graphed) {
@@ -1315,6 +1186,7 @@ void ensure_w32(fugu_ctx* c) {
   p.cx = dalloc<float>(c, c->n); p.cy = dalloc<float>(c, c->n); p.dinv = dalloc<float>(c, c->n);
   p.r = dalloc<float>(c, c->n); p.z = dalloc<float>(c, c->n); p.pb0 = dalloc<float>(c, c->n);
   p.pb1 = dalloc<float>(c, c->n); p.ap = dalloc<float>(c, c->n);
+  p.w1 = dalloc<float>(c, c->n); p.pv = dalloc<float>(c, c->n);
   CoefBufs<float>& f = w.cf;
   f.u_adv = dalloc<float>(c, c->n); f.v_adv = dalloc<float>(c, c->n); f.rho_c = dalloc<float>(c, c->n);
   f.rho_u = dalloc<float>(c, c->n); f.rho_v = dalloc<float>(c, c->n); f.kappa = dalloc<float>(c, c->n);
@@ -1706,7 +1578,6 @@ void create(fugu_ctx* c) {
   if (!prop.cooperativeLaunch) throw ApiError{FUGU_ECUDA, "device lacks cooperative launch"};
   c->nsm = prop.multiProcessorCount;
   CK(cudaStreamCreateWithFlags(&c->s, cudaStreamNonBlocking));
-  CK(cudaStreamCreateWithFlags(&c->s2, cudaStreamNonBlocking));
   c->g = make_geo(c->prm);
   c->n = c->g.n();
   c->Xstate = talloc<double>(c);
@@ -1735,6 +1606,8 @@ void create(fugu_ctx* c) {
   const long ncell = (long)c->prm.nx * c->prm.ny;
   c->pcg_grid = coop_grid((const void*)k_pcg<double>, PCG_TPB, c->nsm, ncell, c->max_coop);
   int g32 = coop_grid((const void*)k_pcg<float>, PCG_TPB, c->nsm, ncell, c->max_coop);
+  if (g32 < c->pcg_grid) c->pcg_grid = g32;
+  g32 = coop_grid((const void*)k_pcg1<float>, PCG_TPB, c->nsm, ncell, c->max_coop);
   if (g32 < c->pcg_grid) c->pcg_grid = g32;
   c->svof_grid = coop_grid((const void*)k_svof, PCG_TPB, c->nsm, ncell, c->max_coop);
   if (c->pcg_grid < 1 || c->svof_grid < 1) throw ApiError{FUGU_ECUDA, "no co-resident grid for persistent kernels"};
@@ -1781,13 +1654,11 @@ void destroy(fugu_ctx* c) {
     for (auto& sg : v) drop(sg);
   for (auto& pr : c->kr_graphs)
     for (auto& sg : pr) drop(sg);
-  for (auto& cg : c->fg_cycle) drop(cg.sg);
   for (void* p : c->allocs) cudaFree(p);
   if (c->h_ks) cudaFreeHost(c->h_ks);
   if (c->h_sc) cudaFreeHost(c->h_sc);
   if (c->h_pcg) cudaFreeHost(c->h_pcg);
   if (c->h_int) cudaFreeHost(c->h_int);
-  if (c->s2) cudaStreamDestroy(c->s2);
   if (c->s) cudaStreamDestroy(c->s);
   delete c;
 }

@@ -44,6 +44,8 @@ struct PcgArgs {
   // spin_limit polls (0: FUGU_SPIN_LIMIT).  Both 0 in normal use.
   unsigned int spin_limit;
   int extra_arrivals;
+  T* w1;               // k_pcg1 only: the second w buffer and p (work)
+  T* pv;
 };
 
 // the arrival count and poll limit of one grid-wide launch's barriers
@@ -72,6 +74,35 @@ __device__ __forceinline__ bool grid_allreduce2(Barrier& bar, double* pa, double
   if (threadIdx.x == 0) put_partial(pb, blockIdx.x, b);
   if (!grid_sync(bar.gs, bar.nb, bar.gen, bar.lim)) return false;
   sum_partials_dd2(pa, pb, gridDim.x, oa, ob);
+  return true;
+}
+
+// three sums at one barrier (the single-reduction PCG)
+__device__ __forceinline__ bool grid_allreduce3(Barrier& bar, double* pa, double* pb, double* pc, DD a, DD b, DD c,
+                                                DD* sh, double* out) {
+  a = block_sum_dd(a, sh);
+  if (threadIdx.x == 0) put_partial(pa, blockIdx.x, a);
+  b = block_sum_dd(b, sh);
+  if (threadIdx.x == 0) put_partial(pb, blockIdx.x, b);
+  c = block_sum_dd(c, sh);
+  if (threadIdx.x == 0) put_partial(pc, blockIdx.x, c);
+  if (!grid_sync(bar.gs, bar.nb, bar.gen, bar.lim)) return false;
+  __shared__ double s_res3[3];
+  if (threadIdx.x < 32) {
+    const double* parts[3] = {pa, pb, pc};
+    double r[3];
+    merge_partials_dd<3>(parts, gridDim.x, r);
+    if (threadIdx.x == 0) {
+      s_res3[0] = r[0];
+      s_res3[1] = r[1];
+      s_res3[2] = r[2];
+    }
+  }
+  __syncthreads();
+  out[0] = s_res3[0];
+  out[1] = s_res3[1];
+  out[2] = s_res3[2];
+  __syncthreads();
   return true;
 }
 
@@ -247,6 +278,183 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
 
 // The mean subtraction above uses (phi - mean) in double for both T; for T =
 // double it is exactly phi(i,j) - mean_val of mod_subsolvers.f90:238.
+
+// The FP32 inner solve's grid-wide PCG with one grid barrier per iteration:
+// the single-reduction (Chronopoulos-Gear) arrangement of
+// pcg_cluster_body_1r, for the grids that do not fit one cluster.  With
+// u = M^-1 r, w = A u and s = A p, an iteration is one pass over the cells,
+//   s = w + beta s,  p = u + beta p,  phi += alpha p,  r -= alpha s,
+//   u = M^-1 r,  w = A u,  and the sums (r, u), (w, u), (r, r),
+// then one barrier.  w = A u needs the new u of the neighbouring cells; a
+// thread forms it from the neighbour's previous r, s and w with the owner's
+// expressions (the same bits), so r, s and w are double-buffered by
+// iteration parity (read one set, write the other), and so are the partial
+// sums' slots (a fast CTA may write the next iteration's partial while a
+// slow one still reads this one's).  Buffers: r in r / z, s in pb0 / pb1,
+// w in ap / w1, p in pv.  Stopping test and outputs as k_pcg.
+template <typename T>
+__global__ void __launch_bounds__(512) k_pcg1(PcgArgs<T> a) {
+  if (a.active && !*a.active) return;
+  __shared__ DD sh[32];
+  const Geo g = a.g;
+  const int G = gridDim.x;
+  const long N = (long)g.nx * g.ny;
+  const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long nthr = (long)G * blockDim.x;
+  const bool closed = !g.px && !g.py;
+  Barrier bar{a.gs, (unsigned int)(G + a.extra_arrivals), a.spin_limit ? a.spin_limit : FUGU_SPIN_LIMIT, 0u};
+  auto gave_up = [&]() {
+    if (threadIdx.x == 0) a.out->status = 1;
+  };
+  T* rb[2] = {a.r, a.z};
+  T* sb[2] = {a.pb0, a.pb1};
+  T* wb[2] = {a.ap, a.w1};
+  T* pv = a.pv;
+  double* P0 = a.part;           // setup sum / final mean
+  double* P1 = a.part + 2 * G;   // rhs norm
+  double* PS = a.part + 4 * G;   // two sets of three slots: (r, u), (w, u), (r, r)
+#define CELL_LOOP1 for (long q = tid; q < N; q += nthr)
+#define CELL_IJ1 const int i = 1 + (int)(q % g.nx), j = 1 + (int)(q / g.nx); const int c = g.at(i, j);
+
+  double mean = 0.0;
+  if (closed) {
+    DD s{0.0, 0.0};
+    CELL_LOOP1 { CELL_IJ1 dd_add(s, double(a.rhs[c])); }
+    double tot;
+    if (!grid_allreduce(bar, P0, s, sh, tot)) { gave_up(); return; }
+    mean = tot / (double)(g.nx * g.ny);
+  }
+  DD ss{0.0, 0.0};
+  CELL_LOOP1 {
+    CELL_IJ1
+    const T rw = closed ? T(double(a.rhs[c]) - mean) : a.rhs[c];
+    rb[0][c] = rw;
+    dd_add(ss, double(rw) * double(rw));
+  }
+  double ssum;
+  if (!grid_allreduce(bar, P1, ss, sh, ssum)) { gave_up(); return; }
+  const double rhs_norm = sqrt(ssum);
+  if (rhs_norm < 1.0e-14) {
+    for (long q = tid; q < g.n(); q += nthr) a.phi[q] = T(0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      a.out->iters = 0;
+      a.out->res = 0.0;
+      a.out->calls += 1;
+    }
+    return;
+  }
+  if (!a.phi_zero) {
+    for (long q = tid; q < g.n(); q += nthr) {
+      const int i = (int)(q % g.P) - 2, j = (int)(q / g.P) - 2;
+      if (i < -1 || j < -1 || i > g.nx + 2 || j > g.ny + 2) continue;
+      if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny) continue;
+      const int mi = (i >= 1 && i <= g.nx) ? i : (g.px ? (i < 1 ? i + g.nx : i - g.nx) : (i < 1 ? 1 - i : 2 * g.nx + 1 - i));
+      const int mj = (j >= 1 && j <= g.ny) ? j : (g.py ? (j < 1 ? j + g.ny : j - g.ny) : (j < 1 ? 1 - j : 2 * g.ny + 1 - j));
+      a.phi[q] = a.phi[g.at(mi, mj)];
+    }
+  }
+  // r0 = rhs_work - A phi0 (poisson_ap reads interior cells only); s = p = 0
+  CELL_LOOP1 {
+    CELL_IJ1
+    T rr = rb[0][c];
+    if (!a.phi_zero) {
+      const T* ph = a.phi;
+      rr = rr - poisson_ap<T>(g, a.cx, a.cy, i, j, [&](int x, int y) { return ph[g.at(x, y)]; });
+    }
+    rb[0][c] = rr;
+    sb[0][c] = T(0);
+    pv[c] = T(0);
+  }
+  if (!grid_sync(bar.gs, bar.nb, bar.gen, bar.lim)) { gave_up(); return; }
+  // w0 = A u0 and the first sums
+  double red[3];
+  {
+    DD d0{0.0, 0.0}, d1{0.0, 0.0}, d2{0.0, 0.0};
+    CELL_LOOP1 {
+      CELL_IJ1
+      const T* r0 = rb[0];
+      const T uv = a.dinv[c] * r0[c];
+      const T wv = poisson_ap<T>(g, a.cx, a.cy, i, j, [&](int x, int y) {
+        const int e = g.at(x, y);
+        return a.dinv[e] * __ldcg(r0 + e);
+      });
+      wb[0][c] = wv;
+      const T rv = r0[c];
+      dd_add(d0, double(rv) * double(uv));
+      dd_add(d1, double(wv) * double(uv));
+      dd_add(d2, double(rv) * double(rv));
+    }
+    if (!grid_allreduce3(bar, PS, PS + 2 * G, PS + 4 * G, d0, d1, d2, sh, red)) { gave_up(); return; }
+  }
+  double gam = red[0], del = red[1], res_norm = sqrt(red[2]), alpha = 0.0, beta = 0.0, gam_old = 0.0;
+  int iter;
+  for (iter = 1; iter <= a.max_iter; ++iter) {
+    if (iter == 1) {
+      beta = 0.0;
+      if (fabs(del) < 1.0e-30) break;
+      alpha = gam / del;
+    } else {
+      beta = gam / gam_old;
+      const double den = del - beta * gam / alpha;
+      if (fabs(den) < 1.0e-30) break;
+      alpha = gam / den;
+    }
+    const T tb = T(beta), ta = T(alpha);
+    const int rd = (iter - 1) & 1, wr = iter & 1;
+    const T* ro = rb[rd];
+    const T* so = sb[rd];
+    const T* wo = wb[rd];
+    // u_k of a cell from its previous r, s and w (the owner's expressions)
+    auto unew = [&](int e) {
+      const T sv = madd(tb, __ldcg(so + e), __ldcg(wo + e));
+      const T rv = madd(-ta, sv, __ldcg(ro + e));
+      return a.dinv[e] * rv;
+    };
+    DD d0{0.0, 0.0}, d1{0.0, 0.0}, d2{0.0, 0.0};
+    CELL_LOOP1 {
+      CELL_IJ1
+      const T sk = madd(tb, __ldcg(so + c), __ldcg(wo + c));
+      const T uo = a.dinv[c] * __ldcg(ro + c);
+      const T pk = madd(tb, pv[c], uo);
+      a.phi[c] = madd(ta, pk, a.phi[c]);
+      const T rv = madd(-ta, sk, __ldcg(ro + c));
+      const T uv = a.dinv[c] * rv;
+      pv[c] = pk;
+      sb[wr][c] = sk;
+      rb[wr][c] = rv;
+      const T wv = poisson_ap<T>(g, a.cx, a.cy, i, j, [&](int x, int y) { return unew(g.at(x, y)); });
+      wb[wr][c] = wv;
+      dd_add(d0, double(rv) * double(uv));
+      dd_add(d1, double(wv) * double(uv));
+      dd_add(d2, double(rv) * double(rv));
+    }
+    double* slot = PS + (iter & 1) * 6 * G;
+    if (!grid_allreduce3(bar, slot, slot + 2 * G, slot + 4 * G, d0, d1, d2, sh, red)) { gave_up(); return; }
+    gam_old = gam;
+    gam = red[0];
+    del = red[1];
+    res_norm = sqrt(red[2]);
+    if (res_norm / rhs_norm < a.tol) break;
+  }
+  if (closed) {
+    DD s{0.0, 0.0};
+    CELL_LOOP1 { CELL_IJ1 dd_add(s, double(a.phi[c])); }
+    double tot;
+    if (!grid_allreduce(bar, P0, s, sh, tot)) { gave_up(); return; }
+    const double m = tot / (double)(g.nx * g.ny);
+    CELL_LOOP1 { CELL_IJ1 a.phi[c] = T(double(a.phi[c]) - m); }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const int it = iter < a.max_iter ? iter : a.max_iter;
+    a.out->iters = it;
+    a.out->res = res_norm / rhs_norm;
+    a.out->total_iters += (unsigned long long)it;
+    if (a.timed) a.out->timed_iters += (unsigned long long)it;
+    a.out->calls += 1;
+  }
+#undef CELL_LOOP1
+#undef CELL_IJ1
+}
 
 struct SvofArgs {
   Geo g;
