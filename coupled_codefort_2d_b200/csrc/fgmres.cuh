@@ -233,14 +233,15 @@ __device__ __forceinline__ void maxpy_body(long n3, T* w, const T* V0, long stri
   __syncthreads();
   for (long q = b * (long)blockDim.x + threadIdx.x; q < n3; q += (long)G * blockDim.x) {
     T x = w[q];
-    // four vectors' loads in flight before the (ordered) dependent updates,
-    // the last group's too (a one-at-a-time tail serialises its loads)
-    for (int i = 0; i < nvec; i += 4) {
-      T v[4];
+    // the loads of up to 16 vectors in flight together before the (ordered)
+    // dependent updates: each group of loads costs one memory round trip,
+    // so a projection on up to 16 vectors is one round trip per element
+    for (int i = 0; i < nvec; i += 16) {
+      T v[16];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) v[u] = i + u < nvec ? V0[(i + u) * stride + q] : T(0);
+      for (int u = 0; u < 16; ++u) v[u] = i + u < nvec ? V0[(i + u) * stride + q] : T(0);
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+      for (int u = 0; u < 16; ++u)
         if (i + u < nvec) x = madd(s[i + u], v[u], x);
     }
     w[q] = x;
