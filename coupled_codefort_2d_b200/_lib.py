@@ -45,6 +45,7 @@ class FuguParams(C.Structure):
         ("refine_max_inner", C.c_int), ("refine_max_outer", C.c_int), ("precision", C.c_int),
         ("pcg_cap_start", C.c_int), ("pcd_sweeps_max", C.c_int), ("pcd_smoother", C.c_int),
         ("pcd_sor_omega", C.c_double), ("graphs", C.c_int), ("pcd_visc_scale", C.c_double),
+        ("vec_rows", C.c_int),
     ]
 
 

@@ -51,6 +51,22 @@ def build_driver(verbose: bool = False) -> str:
     return DRIVER
 
 
+ROWBENCH = os.path.join(HERE, "rowbench")
+ROWBENCH_SRC = os.path.join(CSRC, "rowbench.cu")
+
+
+def build_rowbench(verbose: bool = False) -> str:
+    """The row-kernel timing program (csrc/rowbench.cu): the same kernels and
+    flags as the library, as a stand-alone executable."""
+    nvcc = os.environ.get("NVCC", "nvcc")
+    flags = [f for f in NVCC_FLAGS if f not in ("-shared", "-Xcompiler", "-fPIC")]
+    cmd = [nvcc, *flags, "-I", os.path.join(ROOT, "include"), ROWBENCH_SRC, "-o", ROWBENCH]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return ROWBENCH
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if force or _stale():
         nvcc = os.environ.get("NVCC", "nvcc")
@@ -66,4 +82,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True))
+    if "--rowbench" in sys.argv:
+        print(build_rowbench(verbose=True))
+    else:
+        print(build(force="--force" in sys.argv, verbose=True))

@@ -305,7 +305,7 @@ def config_scale(args):
     n = args.n
     g = Grid(n, n)
     prm = Params(rho1=1.0, rho2=0.1, mu1=0.1, mu2=0.01, sigma=1.0, gx=0.0, gy=0.0, time_order=2,
-                 tol_bicgstab2=1e-8, max_iter_bicgstab2=500, **SOLVER)
+                 tol_bicgstab2=1e-8, max_iter_bicgstab2=500, vec_rows=args.vec_rows, **SOLVER)
     steps = args.steps or 1
     c0 = cases.circle_fraction(g, 0.5, 0.5, 0.25, inside=1.0, ns=4)
     prec = {"mixed": MIXED, "fp64": FP64}[args.precision]
@@ -317,6 +317,7 @@ def config_scale(args):
 
     _, stats, secs, _ = _run(g, prm, c0, prec, steps, 1e-4, device=args.device, on_step=probe)
     return {"config": "scale", "workload": f"static_droplet_{n}x{n}", "steps": steps, "precision": args.precision,
+            "vec_rows": args.vec_rows,
             **_summary(stats, secs), **{k: [s[k] for s in stats] for k in ("outer", "iter", "pcg_calls", "pcg_iters",
                                                                                 "svof_iters")},
             "device_bytes_held": peak[0], "device_bytes_total": total}
@@ -332,6 +333,8 @@ def main(argv=None):
                     help="c1-c3: the PCD extensions (default) or the reference's PCD")
     ap.add_argument("--n", type=int, default=2048, help="scale only: cells per side")
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"], help="scale only")
+    ap.add_argument("--vec-rows", type=int, default=0, choices=[-1, 0, 1],
+                    help="scale only: fugu_params.vec_rows (0: vector row kernels from 2^20 box points)")
     ap.add_argument("--sweep", action="store_true",
                     help="c5 only: central differences over h = 1e-8 .. 1e-3 at 80 x 160 (the plateau)")
     args = ap.parse_args(argv)

@@ -224,14 +224,42 @@ __global__ void __launch_bounds__(MDOT_TPB) k_mdot(MdotArgs<T> a) {
 
 // w = (...((w + s_0 V_0) + s_1 V_1) ...) + s_{nvec-1} V_{nvec-1}, s_i = sign * coef[i],
 // over every element of the triple (whole-array, as the reference's array
-// expressions)
+// expressions).  Each element takes the same updates in the same order
+// however the elements are spread over threads, so the two paths below give
+// the same bits.
 template <typename T>
 __device__ __forceinline__ void maxpy_body(long n3, T* w, const T* V0, long stride, const double* coef, int nvec,
                                            double sign, int b, int G) {
   __shared__ T s[MDOT_MAXV];  // the coefficients, converted once per CTA
   for (int i = threadIdx.x; i < nvec; i += blockDim.x) s[i] = T(sign * coef[i]);
   __syncthreads();
-  for (long q = b * (long)blockDim.x + threadIdx.x; q < n3; q += (long)G * blockDim.x) {
+  constexpr int W = VecW<T>::value;
+  const long S = (long)G * blockDim.x;
+  if (n3 % W == 0 && stride % W == 0 && ((reinterpret_cast<uintptr_t>(w) | reinterpret_cast<uintptr_t>(V0)) & 15u) == 0) {
+    // W consecutive elements per thread with 16-byte loads and stores, the
+    // loads of up to eight vectors in flight before their updates: a
+    // thread's elements are a few long, wide round trips rather than many
+    // short ones (at 2048^2 a one-element-per-thread pass was latency-bound)
+    for (long q = (b * (long)blockDim.x + threadIdx.x) * W; q < n3; q += S * W) {
+      T x[W];
+      ldv(w + q, x);
+      for (int i = 0; i < nvec; i += 8) {
+        T v[8][W];
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (i + u < nvec) ldv(V0 + (i + u) * stride + q, v[u]);
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (i + u < nvec) {
+#pragma unroll
+            for (int e = 0; e < W; ++e) x[e] = madd(s[i + u], v[u][e], x[e]);
+          }
+      }
+      stv(w + q, x);
+    }
+    return;
+  }
+  for (long q = b * (long)blockDim.x + threadIdx.x; q < n3; q += S) {
     T x = w[q];
     // the loads of up to 16 vectors in flight together before the (ordered)
     // dependent updates: each group of loads costs one memory round trip,

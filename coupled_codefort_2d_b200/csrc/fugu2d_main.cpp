@@ -11,7 +11,7 @@
 // Extra namelist keys (this build): use_gpu (accepted, the path is the GPU),
 // precision ('fp64' | 'mixed'), refine (logical or 0 / 1 / 2), refine_inner_tol, refine_max_inner,
 // refine_max_outer, pcg_max_iter, pcg_cap_start, pcd_sweeps, pcd_sweeps_max, pcd_smoother
-// ('jacobi' | 'rbsor'), pcd_sor_omega, pcd_visc_scale, graphs (logical), krylov_bc_fix,
+// ('jacobi' | 'rbsor'), pcd_sor_omega, pcd_visc_scale, graphs (logical), vec_rows, krylov_bc_fix,
 // limiter ('vanleer' | 'superbee'),
 // free_slip_x, device.
 //
@@ -54,7 +54,7 @@ struct Settings {
   // extensions
   std::string precision = "fp64", limiter = "vanleer", pcd_smoother = "jacobi";
   int refine = 0, refine_max_inner = 20, refine_max_outer = 30, krylov_bc_fix = 0, free_slip_x = 0, device = 0;
-  int pcg_max_iter = 150, pcg_cap_start = 0, pcd_sweeps = 3, pcd_sweeps_max = 0, graphs = 0;
+  int pcg_max_iter = 150, pcg_cap_start = 0, pcd_sweeps = 3, pcd_sweeps_max = 0, graphs = 0, vec_rows = 0;
   double refine_inner_tol = 1.0e-2, pcd_sor_omega = 1.0, pcd_visc_scale = 0.0;
 };
 
@@ -214,6 +214,7 @@ bool apply(Settings& st, const std::map<std::string, std::string>& kv, std::stri
     else if (k == "pcd_sor_omega") st.pcd_sor_omega = fnum(v);
     else if (k == "pcd_visc_scale") st.pcd_visc_scale = fnum(v);
     else if (k == "graphs") st.graphs = flog(v) ? 1 : 0;
+    else if (k == "vec_rows") st.vec_rows = (int)fnum(v);
     else if (k == "krylov_bc_fix") st.krylov_bc_fix = flog(v) ? 1 : 0;
     else if (k == "free_slip_x") st.free_slip_x = flog(v) ? 1 : 0;
     else if (k == "device") st.device = (int)fnum(v);
@@ -247,7 +248,7 @@ void print_json(const Settings& s) {
          "\"cyl_xc\": %.17g, \"cyl_yc\": %.17g, \"cyl_rad\": %.17g, \"drop_rad\": %.17g, \"chk_prefix\": \"%s\", "
          "\"precision\": \"%s\", \"limiter\": \"%s\", \"refine\": %d, \"krylov_bc_fix\": %d, "
          "\"pcd_sweeps\": %d, \"pcd_sweeps_max\": %d, \"pcd_smoother\": \"%s\", \"pcd_sor_omega\": %.17g, "
-         "\"graphs\": %d, \"pcd_visc_scale\": %.17g}\n",
+         "\"graphs\": %d, \"pcd_visc_scale\": %.17g, \"vec_rows\": %d}\n",
          s.case_type.c_str(), s.Lx, s.Ly, s.Nx_global, s.Ny_global, s.rho1, s.rho2, s.mu1, s.mu2, s.sigma, s.gx,
          s.gy, s.dt, s.t_final, s.cfl_target, s.max_time_steps, s.time_order, s.tol_bicgstab2,
          s.max_iter_bicgstab2, s.alpha_penalty, s.periodic_x ? "true" : "false", s.periodic_y ? "true" : "false",
@@ -255,7 +256,7 @@ void print_json(const Settings& s) {
          s.use_bicgstab2 ? "true" : "false", s.restart ? "true" : "false", s.vtk_freq, s.chk_freq, s.u_lid,
          s.cyl_xc, s.cyl_yc, s.cyl_rad, s.drop_rad, s.chk_prefix.c_str(), s.precision.c_str(), s.limiter.c_str(),
          s.refine, s.krylov_bc_fix, s.pcd_sweeps, s.pcd_sweeps_max, s.pcd_smoother.c_str(), s.pcd_sor_omega,
-         s.graphs, s.pcd_visc_scale);
+         s.graphs, s.pcd_visc_scale, s.vec_rows);
 }
 
 // ---------------------------------------------------------------- fields
@@ -381,6 +382,7 @@ int main(int argc, char** argv) {
   p.pcd_smoother = st.pcd_smoother == "rbsor" ? 1 : 0; p.pcd_sor_omega = st.pcd_sor_omega;
   p.graphs = st.graphs;
   p.pcd_visc_scale = st.pcd_visc_scale;
+  p.vec_rows = st.vec_rows;
   p.precision = st.precision == "mixed" ? FUGU_MIXED : FUGU_FP64;
   fugu_ctx* ctx = nullptr;
   int rc = fugu_create(&p, st.device, &ctx);

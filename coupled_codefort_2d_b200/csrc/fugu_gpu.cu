@@ -633,6 +633,30 @@ void poisson_coefs(fugu_ctx* c, PcgWork<T>& w, const double* rho_u, const double
   CKL("k_poisson_coefs");
 }
 
+// The vectorised row kernels (VW elements of a row per thread, kernels.cuh)
+// run when fugu_params.vec_rows is 1, or 0 with a box of at least auto_min
+// points, and every array they touch is 16-byte aligned.  Same bits as the
+// one-thread-per-element kernels.  The size rule, from CUDA-event timings on
+// a B200 (FP32, us per launch): the PCD steps and single sweeps gain from
+// 1024^2 up (k_pcd_zwork 8.2 -> 6.2, one Jacobi sweep 12.3 -> 10.2) and lose
+// below (a sweep at 512^2 4.7 -> 5.7); against the staged multi-sweep kernel
+// of wall-bounded cases, six vector sweeps lose at 1024^2 (61 against 55)
+// and win at 2048^2 (154 against 187), hence the larger bound there.
+constexpr long VEC_ROWS_AUTO = 1L << 20;
+constexpr long VEC_ROWS_AUTO_WALL_SWEEPS = 1L << 21;
+bool vec_rows_on(const fugu_ctx* c, std::initializer_list<const void*> ps, long auto_min = VEC_ROWS_AUTO) {
+  const int m = c->prm.vec_rows;
+  if (m < 0 || (m == 0 && c->n < auto_min)) return false;
+  for (const void* p : ps)
+    if (reinterpret_cast<uintptr_t>(p) & 15u) return false;
+  return true;
+}
+template <typename T>
+dim3 vec_grid(const Geo& g) {
+  constexpr int cols = VEC_TX * VecW<T>::value;
+  return dim3((g.P + cols - 1) / cols, (g.R + VEC_TY - 1) / VEC_TY);
+}
+
 // damped-Jacobi smoother: n sweeps of solve_helmholtz_{u,v} in place on sol
 template <typename T>
 void helmholtz(fugu_ctx* c, bool is_u, T* sol, T* tmp, const T* rhs, const CoefBufs<T>& cb,
@@ -667,6 +691,23 @@ void helmholtz(fugu_ctx* c, bool is_u, T* sol, T* tmp, const T* rhs, const CoefB
                                                      T(dt), T(c->prm.pcd_sor_omega), col, active);
         CKL("k_rbsor");
       }
+    return;
+  }
+  const T* rho = is_u ? cb.rho_u : cb.rho_v;
+  const bool walls = !c->g.px && !c->g.py;
+  if (vec_rows_on(c, {sol, tmp, rhs, rho, cb.kappa, cb.zeta, cb.eta, pen},
+                  walls ? VEC_ROWS_AUTO_WALL_SWEEPS : VEC_ROWS_AUTO)) {
+    // one sweep per launch, VW faces per thread, alternating buffers
+    const dim3 grid = vec_grid<T>(c->g);
+    for (int s = 0; s < n_sweeps; ++s) {
+      halo(c, cur, is_u ? K_U : K_V, active);
+      k_jacobi_vec<T><<<grid, dim3(VEC_TX, VEC_TY), 0, c->s>>>(c->g, is_u ? 0 : 1, cur, nxt, rhs, rho, cb.kappa,
+                                                               cb.zeta, cb.eta, pen, T(dt), T(c->prm.jacobi_omega),
+                                                               active);
+      CKL("k_jacobi_vec");
+      std::swap(cur, nxt);
+    }
+    if (cur != sol) CK(cudaMemcpyAsync(sol, cur, sizeof(T) * c->n, cudaMemcpyDeviceToDevice, c->s));
     return;
   }
   if (!c->g.px && !c->g.py) {
@@ -711,16 +752,29 @@ void pcd(fugu_ctx* c, KrylovWork<T>& w, const CoefBufs<T>& cb, const SolveOpt& o
   pcg<T>(c, w.pcg, pw.phi, z.p, c->prm.pcg_tol, c->pcg_cap_cur > 0 ? c->pcg_cap_cur : c->prm.pcg_max_iter, true,
          active);
   halo(c, pw.phi, K_CELL, active);
-  k_pcd_schur<T><<<b.grid, b.block, 0, c->s>>>(c->g, pw.phi, cb.u_adv, cb.v_adv, r.p, T(1.0 / dt), cb.kappa, z.p,
-                                                T(c->prm.pcd_visc_scale), active);
+  const bool vec = vec_rows_on(c, {pw.phi, cb.u_adv, cb.v_adv, r.p, cb.kappa, z.p, z.u, z.v, pw.zuw, pw.zvw,
+                                   cb.eta, r.v});
+  const dim3 vg = vec_grid<T>(c->g), vb(VEC_TX, VEC_TY);
+  if (vec)
+    k_pcd_schur_vec<T><<<vg, vb, 0, c->s>>>(c->g, pw.phi, cb.u_adv, cb.v_adv, r.p, T(1.0 / dt), cb.kappa, z.p,
+                                            T(c->prm.pcd_visc_scale), active);
+  else
+    k_pcd_schur<T><<<b.grid, b.block, 0, c->s>>>(c->g, pw.phi, cb.u_adv, cb.v_adv, r.p, T(1.0 / dt), cb.kappa, z.p,
+                                                  T(c->prm.pcd_visc_scale), active);
   CKL("k_pcd_schur");
   halo(c, r.p, K_CELL, active);
-  k_pcd_zwork<T><<<b.grid, b.block, 0, c->s>>>(c->g, z.u, z.v, r.p, pw.zuw, pw.zvw, active);
+  if (vec)
+    k_pcd_zwork_vec<T><<<vg, vb, 0, c->s>>>(c->g, z.u, z.v, r.p, pw.zuw, pw.zvw, active);
+  else
+    k_pcd_zwork<T><<<b.grid, b.block, 0, c->s>>>(c->g, z.u, z.v, r.p, pw.zuw, pw.zvw, active);
   CKL("k_pcd_zwork");
   const int sweeps = c->pcd_sweeps_cur > 0 ? c->pcd_sweeps_cur : c->prm.pcd_sweeps;
   helmholtz<T>(c, false, r.v, pw.tmp, pw.zvw, cb, o, dt, sweeps, active);
   halo(c, r.v, K_V, active);
-  k_pcd_cross<T><<<b.grid, b.block, 0, c->s>>>(c->g, cb.eta, r.v, pw.zuw, active);
+  if (vec)
+    k_pcd_cross_vec<T><<<vg, vb, 0, c->s>>>(c->g, cb.eta, r.v, pw.zuw, active);
+  else
+    k_pcd_cross<T><<<b.grid, b.block, 0, c->s>>>(c->g, cb.eta, r.v, pw.zuw, active);
   CKL("k_pcd_cross");
   helmholtz<T>(c, true, r.u, pw.tmp, pw.zuw, cb, o, dt, sweeps, active);
   halo(c, r.u, K_U, active);
@@ -1556,6 +1610,7 @@ int check_params(const fugu_params* p) {
   if (p->pcd_smoother < 0 || p->pcd_smoother > 1) return FUGU_EINVAL;
   if (p->graphs < 0 || p->graphs > 1) return FUGU_EINVAL;
   if (!(p->pcd_visc_scale >= 0.0 && p->pcd_visc_scale < 1.0e6)) return FUGU_EINVAL;
+  if (p->vec_rows < -1 || p->vec_rows > 1) return FUGU_EINVAL;
   if (p->pcd_smoother == 1 && !(p->pcd_sor_omega > 0.0 && p->pcd_sor_omega < 2.0)) return FUGU_EINVAL;
   return FUGU_OK;
 }
@@ -1719,7 +1774,7 @@ void fugu_params_default(fugu_params* p) {
   p->svof_delta_h = 1.5; p->svof_max_iter = 150; p->svof_tol = 1.0e-7;
   p->refine_inner_tol = 1.0e-2; p->refine_max_inner = 20; p->refine_max_outer = 30;
   p->precision = FUGU_FP64;
-  p->pcd_smoother = 0; p->pcd_sor_omega = 1.0; p->graphs = 0; p->pcd_visc_scale = 0.0;
+  p->pcd_smoother = 0; p->pcd_sor_omega = 1.0; p->graphs = 0; p->pcd_visc_scale = 0.0; p->vec_rows = 0;
 }
 
 const char* fugu_version(void) { return "fugu-b200 1 (sm_100a)"; }

@@ -53,6 +53,27 @@ inline Box box_launch(const Geo& g) {
   return b;
 }
 
+// 16-byte vector access: VecW<T>::value elements (four floats or two
+// doubles) from / to an address that is a multiple of 16 bytes
+template <typename T>
+struct VecW {
+  static constexpr int value = 16 / (int)sizeof(T);
+};
+__device__ __forceinline__ void ldv(const float* p, float* o) {
+  const float4 x = *reinterpret_cast<const float4*>(p);
+  o[0] = x.x; o[1] = x.y; o[2] = x.z; o[3] = x.w;
+}
+__device__ __forceinline__ void ldv(const double* p, double* o) {
+  const double2 x = *reinterpret_cast<const double2*>(p);
+  o[0] = x.x; o[1] = x.y;
+}
+__device__ __forceinline__ void stv(float* p, const float* o) {
+  *reinterpret_cast<float4*>(p) = make_float4(o[0], o[1], o[2], o[3]);
+}
+__device__ __forceinline__ void stv(double* p, const double* o) {
+  *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]);
+}
+
 // a * b + c.  FP32 (the mixed form's inner solve, which needs no bit parity
 // with the oracle): one fused multiply-add, one rounding and one issue slot.
 // Every other type: the product and the sum rounded separately -- the library

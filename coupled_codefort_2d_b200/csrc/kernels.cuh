@@ -542,21 +542,28 @@ __global__ void k_poisson_coefs(Geo g, const double* rho_u, const double* rho_v,
 // PCD Schur step r_p = -((1/dt) phi + u.grad phi) (mod_pcd_precond.f90:54-62);
 // r_p is zero outside the interior (as after r_p = zero).
 // Each PCD step is an element function plus a thin whole-box kernel around it.
-template <typename T>
-__device__ __forceinline__ T pcd_schur_at(const Geo& g, int k, int i, int j, const T* phi, const T* ua,
-                                          const T* va, T inv_dt, const T* kap, const T* zp, T visc) {
+template <typename T, typename V>
+__device__ __forceinline__ T pcd_schur_vals(const Geo& g, int i, int j, const V& phi, const V& ua, const V& va,
+                                            T inv_dt, const V& kap, const V& zp, T visc) {
   T r = T(0);
   if (i >= 1 && i <= g.nx && j >= 1 && j <= g.ny) {
     const T h = T(0.5);
-    const T uavg = h * (ua[k] + ua[g.at(i - 1, j)]);
-    const T vavg = h * (va[k] + va[g.at(i, j - 1)]);
-    const T conv = uavg * (phi[g.at(i + 1, j)] - phi[g.at(i - 1, j)]) * (h * T(g.idx)) +
-                   vavg * (phi[g.at(i, j + 1)] - phi[g.at(i, j - 1)]) * (h * T(g.idy));
-    r = -(inv_dt * phi[k] + conv);
+    const T uavg = h * (ua(i, j) + ua(i - 1, j));
+    const T vavg = h * (va(i, j) + va(i, j - 1));
+    const T conv = uavg * (phi(i + 1, j) - phi(i - 1, j)) * (h * T(g.idx)) +
+                   vavg * (phi(i, j + 1) - phi(i, j - 1)) * (h * T(g.idy));
+    r = -(inv_dt * phi(i, j) + conv);
     // extension (visc > 0): the viscous Cahouet-Chabard part, visc * mu_c * z_p
-    if (visc != T(0)) r = r - ((visc * T(0.5)) * kap[k]) * zp[k];
+    if (visc != T(0)) r = r - ((visc * T(0.5)) * kap(i, j)) * zp(i, j);
   }
   return r;
+}
+template <typename T>
+__device__ __forceinline__ T pcd_schur_at(const Geo& g, int k, int i, int j, const T* phi, const T* ua,
+                                          const T* va, T inv_dt, const T* kap, const T* zp, T visc) {
+  (void)k;
+  return pcd_schur_vals<T>(g, i, j, gview(g, phi), gview(g, ua), gview(g, va), inv_dt, gview(g, kap), gview(g, zp),
+                           visc);
 }
 template <typename T>
 __global__ void k_pcd_schur(Geo g, const T* phi, const T* ua, const T* va, T* rp, T inv_dt, const T* kap,
@@ -567,19 +574,25 @@ __global__ void k_pcd_schur(Geo g, const T* phi, const T* ua, const T* va, T* rp
 }
 
 // velocity residual update z - B_p^T r_p (mod_pcd_precond.f90:66-84)
+template <typename T, typename V>
+__device__ __forceinline__ void pcd_zwork_vals(const Geo& g, int i, int j, T zu, T zv, const V& rp, T& a, T& b) {
+  const int nx = g.nx, ny = g.ny;
+  a = T(0);
+  b = T(0);
+  if (j >= 1 && j <= ny) {
+    if (i >= 1 && i <= nx - 1) a = zu - (rp(i + 1, j) - rp(i, j)) * T(g.idx);
+    else if (i == 0 || i == nx) a = zu;
+  }
+  if (i >= 1 && i <= nx) {
+    if (j >= 1 && j <= ny - 1) b = zv - (rp(i, j + 1) - rp(i, j)) * T(g.idy);
+    else if (j == 0 || j == ny) b = zv;
+  }
+}
 template <typename T>
 __device__ __forceinline__ void pcd_zwork_at(const Geo& g, int k, int i, int j, const T* zu, const T* zv,
                                              const T* rp, T* zuw, T* zvw) {
-  const int nx = g.nx, ny = g.ny;
-  T a = T(0), b = T(0);
-  if (j >= 1 && j <= ny) {
-    if (i >= 1 && i <= nx - 1) a = zu[k] - (rp[g.at(i + 1, j)] - rp[k]) * T(g.idx);
-    else if (i == 0 || i == nx) a = zu[k];
-  }
-  if (i >= 1 && i <= nx) {
-    if (j >= 1 && j <= ny - 1) b = zv[k] - (rp[g.at(i, j + 1)] - rp[k]) * T(g.idy);
-    else if (j == 0 || j == ny) b = zv[k];
-  }
+  T a, b;
+  pcd_zwork_vals<T>(g, i, j, zu[k], zv[k], gview(g, rp), a, b);
   zuw[k] = a;
   zvw[k] = b;
 }
@@ -591,15 +604,20 @@ __global__ void k_pcd_zwork(Geo g, const T* zu, const T* zv, const T* rp, T* zuw
 }
 
 // cross term from r_v into the u residual (mod_pcd_precond.f90:91-98)
+template <typename T, typename V>
+__device__ __forceinline__ T pcd_cross_vals(const Geo& g, int i, int j, const V& eta, const V& rv, T zuw) {
+  if (j >= 1 && j <= g.ny && i >= 1 && i <= g.nx - 1) {
+    const T idx = T(g.idx), idy = T(g.idy);
+    const T cross = -idy * (eta(i, j) * (rv(i + 1, j) - rv(i, j)) * idx -
+                            eta(i, j - 1) * (rv(i + 1, j - 1) - rv(i, j - 1)) * idx);
+    return zuw - cross;
+  }
+  return zuw;
+}
 template <typename T>
 __device__ __forceinline__ void pcd_cross_at(const Geo& g, int k, int i, int j, const T* eta, const T* rv,
                                              T* zuw) {
-  if (j >= 1 && j <= g.ny && i >= 1 && i <= g.nx - 1) {
-    const T idx = T(g.idx), idy = T(g.idy);
-    const T cross = -idy * (eta[k] * (rv[g.at(i + 1, j)] - rv[k]) * idx -
-                            eta[g.at(i, j - 1)] * (rv[g.at(i + 1, j - 1)] - rv[g.at(i, j - 1)]) * idx);
-    zuw[k] = zuw[k] - cross;
-  }
+  if (j >= 1 && j <= g.ny && i >= 1 && i <= g.nx - 1) zuw[k] = pcd_cross_vals<T>(g, i, j, gview(g, eta), gview(g, rv), zuw[k]);
 }
 template <typename T>
 __global__ void k_pcd_cross(Geo g, const T* eta, const T* rv, T* zuw, const int* active) {
@@ -719,6 +737,165 @@ __global__ void k_rbsor_v(Geo g, T* v, const T* rhs, const T* rho_v, const T* ka
   if (!rbsor_v_face(g, i, j, col)) return;
   v[k] = jacobi_v_at<T>(g, k, i, j, v, rhs, rho_v, kap, zeta, eta, pen, dt, om);
 }
+
+// ------------------------------------------------- vectorised row kernels
+// The damped-Jacobi sweep and the PCD's Schur, residual and cross steps with
+// VW = 16 / sizeof(T) consecutive elements of one box row per thread (four
+// floats or two doubles): each array is read and written with 16-byte vector
+// accesses, the rows above and below with vector loads too, and the one
+// neighbour either side of the segment with a scalar load.  The values go to
+// a window of registers (RView) that the element functions above read
+// through, so every face gets the bits of the one-thread-per-face kernels
+// with a quarter (FP32) or half (FP64) of the load instructions.  P is a
+// multiple of 16, so a segment starting at a multiple of VW is 16-byte
+// aligned when the array is (the host checks every pointer before taking
+// these kernels).  Block VEC_TX x VEC_TY threads covers VEC_TX * VW columns.
+constexpr int VEC_TX = 32, VEC_TY = 8;
+// rows j0 - 1, j0, j0 + 1 (slots 0..2) of the columns i0 - 1 .. i0 + W
+template <typename T, int W>
+struct RView {
+  T v[3][W + 2];
+  int i0, j0;
+  __device__ __forceinline__ T operator()(int i, int j) const { return v[j - j0 + 1][i - i0 + 1]; }
+};
+// slot r of the window from the row segment starting at box index k, with
+// the left / right neighbours when asked (and only then read)
+template <typename T, int W>
+__device__ __forceinline__ void rv_row(RView<T, W>& w, int r, const T* p, long k, bool left, bool right) {
+  ldv(p + k, &w.v[r][1]);
+  w.v[r][0] = left ? p[k - 1] : T(0);
+  w.v[r][W + 1] = right ? p[k + W] : T(0);
+}
+#define FUGU_VEC_SEG                                                        \
+  constexpr int W = VecW<T>::value;                                         \
+  const int ii0 = (blockIdx.x * blockDim.x + threadIdx.x) * W;             \
+  const int jj = blockIdx.y * blockDim.y + threadIdx.y;                    \
+  if (ii0 >= g.P || jj >= g.R) return;                                      \
+  const int i0 = ii0 - 2, j = jj - 2;                                       \
+  const long P = g.P;                                                       \
+  const long k0 = ii0 + jj * P;                                             \
+  const bool lft = ii0 > 0, rgt = ii0 + W < g.P;                            \
+  (void)lft; (void)rgt;
+
+// one damped-Jacobi sweep (k_jacobi_u for comp 0, k_jacobi_v for comp 1)
+template <typename T>
+__global__ void __launch_bounds__(VEC_TX * VEC_TY)
+    k_jacobi_vec(Geo g, int comp, const T* __restrict__ uo, T* __restrict__ un, const T* __restrict__ rhs,
+                 const T* __restrict__ rho, const T* __restrict__ kap, const T* __restrict__ zeta,
+                 const T* __restrict__ eta, const T* __restrict__ pen, T dt, T om, const int* active) {
+  if (active && !*active) return;
+  FUGU_VEC_SEG
+  RView<T, W> U, K, Z, E;
+  U.i0 = K.i0 = Z.i0 = E.i0 = i0;
+  U.j0 = K.j0 = Z.j0 = E.j0 = j;
+  T rv[W], bv[W], pv[W];
+  rv_row(U, 1, uo, k0, lft, rgt);
+  ldv(rhs + k0, rv);
+  ldv(rho + k0, bv);
+  if (pen) ldv(pen + k0, pv);
+  // the stencil is read only on owned rows (j in 1..ny for u, 1..jmax for v)
+  if (j >= 1 && j <= (comp == 0 ? g.ny : g.jmax())) {
+    rv_row(U, 0, uo, k0 - P, lft, rgt);
+    rv_row(U, 2, uo, k0 + P, lft, rgt);
+    if (comp == 0) {  // kap(i, j), kap(i + 1, j); zeta, eta at rows j and j - 1
+      rv_row(K, 1, kap, k0, false, rgt);
+      ldv(zeta + k0, &Z.v[1][1]);
+      ldv(zeta + k0 - P, &Z.v[0][1]);
+      ldv(eta + k0, &E.v[1][1]);
+      ldv(eta + k0 - P, &E.v[0][1]);
+    } else {  // kap at rows j and j + 1; zeta, eta at (i, j) and (i - 1, j)
+      ldv(kap + k0, &K.v[1][1]);
+      ldv(kap + k0 + P, &K.v[2][1]);
+      rv_row(Z, 1, zeta, k0, lft, false);
+      rv_row(E, 1, eta, k0, lft, false);
+    }
+  }
+  T out[W];
+#pragma unroll
+  for (int e = 0; e < W; ++e)
+    out[e] = comp == 0 ? jacobi_u_vals<T>(g, e, i0 + e, j, U, K, Z, E, rv, bv, pen ? pv : nullptr, dt, om)
+                       : jacobi_v_vals<T>(g, e, i0 + e, j, U, K, Z, E, rv, bv, pen ? pv : nullptr, dt, om);
+  stv(un + k0, out);
+}
+
+// the PCD's Schur step (k_pcd_schur)
+template <typename T>
+__global__ void __launch_bounds__(VEC_TX * VEC_TY)
+    k_pcd_schur_vec(Geo g, const T* __restrict__ phi, const T* __restrict__ ua, const T* __restrict__ va,
+                    T* __restrict__ rp, T inv_dt, const T* __restrict__ kap, const T* __restrict__ zp, T visc,
+                    const int* active) {
+  if (active && !*active) return;
+  FUGU_VEC_SEG
+  RView<T, W> F, A, B, K, Z;
+  F.i0 = A.i0 = B.i0 = K.i0 = Z.i0 = i0;
+  F.j0 = A.j0 = B.j0 = K.j0 = Z.j0 = j;
+  T out[W];
+  if (j >= 1 && j <= g.ny) {
+    rv_row(F, 0, phi, k0 - P, false, false);
+    rv_row(F, 1, phi, k0, lft, rgt);
+    rv_row(F, 2, phi, k0 + P, false, false);
+    rv_row(A, 1, ua, k0, lft, false);
+    ldv(va + k0, &B.v[1][1]);
+    ldv(va + k0 - P, &B.v[0][1]);
+    if (visc != T(0)) {
+      ldv(kap + k0, &K.v[1][1]);
+      ldv(zp + k0, &Z.v[1][1]);
+    }
+#pragma unroll
+    for (int e = 0; e < W; ++e) out[e] = pcd_schur_vals<T>(g, i0 + e, j, F, A, B, inv_dt, K, Z, visc);
+  } else {
+#pragma unroll
+    for (int e = 0; e < W; ++e) out[e] = T(0);
+  }
+  stv(rp + k0, out);
+}
+
+// the PCD's velocity residual update (k_pcd_zwork)
+template <typename T>
+__global__ void __launch_bounds__(VEC_TX * VEC_TY)
+    k_pcd_zwork_vec(Geo g, const T* __restrict__ zu, const T* __restrict__ zv, const T* __restrict__ rp,
+                    T* __restrict__ zuw, T* __restrict__ zvw, const int* active) {
+  if (active && !*active) return;
+  FUGU_VEC_SEG
+  RView<T, W> R;
+  R.i0 = i0;
+  R.j0 = j;
+  T a[W], b[W], zuv[W], zvv[W];
+  ldv(zu + k0, zuv);
+  ldv(zv + k0, zvv);
+  // rp(i, j), rp(i + 1, j) on the rows j in 1..ny; rp(i, j + 1) on 1..ny-1
+  if (j >= 1 && j <= g.ny) {
+    rv_row(R, 1, rp, k0, false, rgt);
+    if (j <= g.ny - 1) ldv(rp + k0 + P, &R.v[2][1]);
+  }
+#pragma unroll
+  for (int e = 0; e < W; ++e) pcd_zwork_vals<T>(g, i0 + e, j, zuv[e], zvv[e], R, a[e], b[e]);
+  stv(zuw + k0, a);
+  stv(zvw + k0, b);
+}
+
+// the PCD's cross term from r_v into the u residual (k_pcd_cross)
+template <typename T>
+__global__ void __launch_bounds__(VEC_TX * VEC_TY)
+    k_pcd_cross_vec(Geo g, const T* __restrict__ eta, const T* __restrict__ rv, T* __restrict__ zuw,
+                    const int* active) {
+  if (active && !*active) return;
+  FUGU_VEC_SEG
+  if (j < 1 || j > g.ny) return;  // zuw is left as it is outside the rows 1..ny
+  RView<T, W> E, V;
+  E.i0 = V.i0 = i0;
+  E.j0 = V.j0 = j;
+  ldv(eta + k0, &E.v[1][1]);
+  ldv(eta + k0 - P, &E.v[0][1]);
+  rv_row(V, 1, rv, k0, false, rgt);
+  rv_row(V, 0, rv, k0 - P, false, rgt);
+  T z[W];
+  ldv(zuw + k0, z);
+#pragma unroll
+  for (int e = 0; e < W; ++e) z[e] = pcd_cross_vals<T>(g, i0 + e, j, E, V, z[e]);
+  stv(zuw + k0, z);
+}
+#undef FUGU_VEC_SEG
 
 // ------------------------------------------------- fused red-black SOR sweep
 // One whole red-black SOR sweep (both colour passes) of one velocity

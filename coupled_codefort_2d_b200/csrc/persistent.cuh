@@ -18,6 +18,25 @@ struct PcgOut {
   unsigned long long timed_iters;  // accumulated over the launches with timed = 1
 };
 
+// A thread's walk over the interior cells q = tid, tid + nthr, ... with
+// q = (i - 1) + (j - 1) * nx, as (i, j) from the thread's first cell and
+// the stride's (di, dj), advanced by carry: a cell costs two adds and a
+// compare instead of a 64-bit division and remainder, and the cells and
+// their order are those of the plain strided loop (q < nx * ny is j <= ny).
+struct CellWalk {
+  int i0, j0, di, dj;
+  __device__ __forceinline__ CellWalk(long tid, long nthr, int nx)
+      : i0(1 + (int)(tid % nx)), j0(1 + (int)(tid / nx)), di((int)(nthr % nx)), dj((int)(nthr / nx)) {}
+  __device__ __forceinline__ void next(int& i, int& j, int nx) const {
+    i += di;
+    j += dj;
+    if (i > nx) {
+      i -= nx;
+      ++j;
+    }
+  }
+};
+
 template <typename T>
 struct PcgArgs {
   Geo g;
@@ -126,7 +145,6 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
   __shared__ DD sh[32];
   const Geo g = a.g;
   const int G = gridDim.x;
-  const long N = (long)g.nx * g.ny;
   const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long nthr = (long)G * blockDim.x;
   const bool closed = !g.px && !g.py;
@@ -142,8 +160,9 @@ __global__ void __launch_bounds__(512) k_pcg(PcgArgs<T> a) {
   double* PA = a.part + 6 * G;   // p.Ap
   double* PB = a.part + 8 * G;   // r.r
   double* PC = a.part + 10 * G;  // r.z
-#define CELL_LOOP for (long q = tid; q < N; q += nthr)
-#define CELL_IJ const int i = 1 + (int)(q % g.nx), j = 1 + (int)(q / g.nx); const int c = g.at(i, j);
+  const CellWalk cw(tid, nthr, g.nx);
+#define CELL_LOOP for (int i = cw.i0, j = cw.j0; j <= g.ny; cw.next(i, j, g.nx))
+#define CELL_IJ const int c = g.at(i, j);
 
   // (b) zero-mean projection of the right-hand side when no direction is periodic
   double mean = 0.0;
@@ -298,7 +317,6 @@ __global__ void __launch_bounds__(512) k_pcg1(PcgArgs<T> a) {
   __shared__ DD sh[32];
   const Geo g = a.g;
   const int G = gridDim.x;
-  const long N = (long)g.nx * g.ny;
   const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long nthr = (long)G * blockDim.x;
   const bool closed = !g.px && !g.py;
@@ -306,15 +324,18 @@ __global__ void __launch_bounds__(512) k_pcg1(PcgArgs<T> a) {
   auto gave_up = [&]() {
     if (threadIdx.x == 0) a.out->status = 1;
   };
-  T* rb[2] = {a.r, a.z};
-  T* sb[2] = {a.pb0, a.pb1};
-  T* wb[2] = {a.ap, a.w1};
+  // the two sets of r, s and w, picked by parity with selects (an array of
+  // pointers indexed at run time would live in local memory)
+  auto rb = [&](int q) { return q ? a.z : a.r; };
+  auto sb = [&](int q) { return q ? a.pb1 : a.pb0; };
+  auto wb = [&](int q) { return q ? a.w1 : a.ap; };
   T* pv = a.pv;
   double* P0 = a.part;           // setup sum / final mean
   double* P1 = a.part + 2 * G;   // rhs norm
   double* PS = a.part + 4 * G;   // two sets of three slots: (r, u), (w, u), (r, r)
-#define CELL_LOOP1 for (long q = tid; q < N; q += nthr)
-#define CELL_IJ1 const int i = 1 + (int)(q % g.nx), j = 1 + (int)(q / g.nx); const int c = g.at(i, j);
+  const CellWalk cw(tid, nthr, g.nx);
+#define CELL_LOOP1 for (int i = cw.i0, j = cw.j0; j <= g.ny; cw.next(i, j, g.nx))
+#define CELL_IJ1 const int c = g.at(i, j);
 
   double mean = 0.0;
   if (closed) {
@@ -328,7 +349,7 @@ __global__ void __launch_bounds__(512) k_pcg1(PcgArgs<T> a) {
   CELL_LOOP1 {
     CELL_IJ1
     const T rw = closed ? T(double(a.rhs[c]) - mean) : a.rhs[c];
-    rb[0][c] = rw;
+    rb(0)[c] = rw;
     dd_add(ss, double(rw) * double(rw));
   }
   double ssum;
@@ -356,13 +377,13 @@ __global__ void __launch_bounds__(512) k_pcg1(PcgArgs<T> a) {
   // r0 = rhs_work - A phi0 (poisson_ap reads interior cells only); s = p = 0
   CELL_LOOP1 {
     CELL_IJ1
-    T rr = rb[0][c];
+    T rr = rb(0)[c];
     if (!a.phi_zero) {
       const T* ph = a.phi;
       rr = rr - poisson_ap<T>(g, a.cx, a.cy, i, j, [&](int x, int y) { return ph[g.at(x, y)]; });
     }
-    rb[0][c] = rr;
-    sb[0][c] = T(0);
+    rb(0)[c] = rr;
+    sb(0)[c] = T(0);
     pv[c] = T(0);
   }
   if (!grid_sync(bar.gs, bar.nb, bar.gen, bar.lim)) { gave_up(); return; }
@@ -372,13 +393,13 @@ __global__ void __launch_bounds__(512) k_pcg1(PcgArgs<T> a) {
     DD d0{0.0, 0.0}, d1{0.0, 0.0}, d2{0.0, 0.0};
     CELL_LOOP1 {
       CELL_IJ1
-      const T* r0 = rb[0];
+      const T* r0 = rb(0);
       const T uv = a.dinv[c] * r0[c];
       const T wv = poisson_ap<T>(g, a.cx, a.cy, i, j, [&](int x, int y) {
         const int e = g.at(x, y);
         return a.dinv[e] * __ldcg(r0 + e);
       });
-      wb[0][c] = wv;
+      wb(0)[c] = wv;
       const T rv = r0[c];
       dd_add(d0, double(rv) * double(uv));
       dd_add(d1, double(wv) * double(uv));
@@ -401,9 +422,9 @@ __global__ void __launch_bounds__(512) k_pcg1(PcgArgs<T> a) {
     }
     const T tb = T(beta), ta = T(alpha);
     const int rd = (iter - 1) & 1, wr = iter & 1;
-    const T* ro = rb[rd];
-    const T* so = sb[rd];
-    const T* wo = wb[rd];
+    const T* ro = rb(rd);
+    const T* so = sb(rd);
+    const T* wo = wb(rd);
     // u_k of a cell from its previous r, s and w (the owner's expressions)
     auto unew = [&](int e) {
       const T sv = madd(tb, __ldcg(so + e), __ldcg(wo + e));
@@ -413,17 +434,22 @@ __global__ void __launch_bounds__(512) k_pcg1(PcgArgs<T> a) {
     DD d0{0.0, 0.0}, d1{0.0, 0.0}, d2{0.0, 0.0};
     CELL_LOOP1 {
       CELL_IJ1
+      // every load of the cell (its own values and the stencil's) comes
+      // before its first store, so they are issued together: one memory
+      // round trip per cell (a store in between would hold back the loads
+      // after it, since the compiler cannot rule out aliasing)
       const T sk = madd(tb, __ldcg(so + c), __ldcg(wo + c));
       const T uo = a.dinv[c] * __ldcg(ro + c);
       const T pk = madd(tb, pv[c], uo);
-      a.phi[c] = madd(ta, pk, a.phi[c]);
+      const T ph = madd(ta, pk, a.phi[c]);
       const T rv = madd(-ta, sk, __ldcg(ro + c));
       const T uv = a.dinv[c] * rv;
-      pv[c] = pk;
-      sb[wr][c] = sk;
-      rb[wr][c] = rv;
       const T wv = poisson_ap<T>(g, a.cx, a.cy, i, j, [&](int x, int y) { return unew(g.at(x, y)); });
-      wb[wr][c] = wv;
+      a.phi[c] = ph;
+      pv[c] = pk;
+      sb(wr)[c] = sk;
+      rb(wr)[c] = rv;
+      wb(wr)[c] = wv;
       dd_add(d0, double(rv) * double(uv));
       dd_add(d1, double(wv) * double(uv));
       dd_add(d2, double(rv) * double(rv));
@@ -477,9 +503,9 @@ __global__ void __launch_bounds__(512) k_svof(SvofArgs a) {
   __shared__ double sh[32];  // max reduction (exact in any order)
   const Geo g = a.g;
   const int G = gridDim.x;
-  const long N = (long)g.nx * g.ny;
   const long tid = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long nthr = (long)G * blockDim.x;
+  const CellWalk cw(tid, nthr, g.nx);
   unsigned int gen = 0;
   for (long q = tid; q < g.n(); q += nthr) a.out[q] = a.craw[q];
   if (!grid_sync(a.gs, G, gen)) { if (threadIdx.x == 0) *a.status = 1; return; }
@@ -492,14 +518,38 @@ __global__ void __launch_bounds__(512) k_svof(SvofArgs a) {
     const double* src = (it & 1) ? a.out : a.work;
     double* dst = (it & 1) ? a.work : a.out;
     double res = 0.0;
-    for (long q = tid; q < N; q += nthr) {
-      const int i = 1 + (int)(q % g.nx), j = 1 + (int)(q / g.nx);
-      const int c = g.at(i, j);
-      const double old = __ldcg(src + c);
-      const double val = (a.craw[c] + a.cx * (__ldcg(src + g.at(mx(i + 1), j)) + __ldcg(src + g.at(mx(i - 1), j))) +
-                          a.cy * (__ldcg(src + g.at(i, my(j + 1))) + __ldcg(src + g.at(i, my(j - 1))))) / a.diag;
-      dst[c] = val;
-      res = fmax(res, fabs(val - old));
+    // four cells of the walk at a time: every load of the four before the
+    // first store, so they go out together (a store in between would hold
+    // back the loads after it, since src and dst may alias for all the
+    // compiler knows); each cell's expression is unchanged, and the max-norm
+    // is exact in any order
+    for (int i = cw.i0, j = cw.j0; j <= g.ny;) {
+      constexpr int U = 4;
+      int cc[U];
+      bool on[U];
+      double o[U], cr[U], e[U], w[U], n[U], so[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        on[u] = j <= g.ny;
+        if (on[u]) {
+          const int c = g.at(i, j);
+          cc[u] = c;
+          o[u] = __ldcg(src + c);
+          cr[u] = a.craw[c];
+          e[u] = __ldcg(src + g.at(mx(i + 1), j));
+          w[u] = __ldcg(src + g.at(mx(i - 1), j));
+          n[u] = __ldcg(src + g.at(i, my(j + 1)));
+          so[u] = __ldcg(src + g.at(i, my(j - 1)));
+          cw.next(i, j, g.nx);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+        if (on[u]) {
+          const double val = (cr[u] + a.cx * (e[u] + w[u]) + a.cy * (n[u] + so[u])) / a.diag;
+          dst[cc[u]] = val;
+          res = fmax(res, fabs(val - o[u]));
+        }
     }
     res = block_max(res, sh);
     if (threadIdx.x == 0) a.part[blockIdx.x] = res;

@@ -63,6 +63,10 @@ class Params:
     # > 0: the PCD's Schur step adds the viscous (Cahouet-Chabard) term
     # r_p -= pcd_visc_scale * mu_cell * z_p (0 = the reference's PCD)
     pcd_visc_scale: float = 0.0
+    # 1: the damped-Jacobi sweeps and the PCD's Schur, residual and cross
+    # steps take 16-byte vector accesses (same results); -1 never; 0 for
+    # boxes of at least 2^20 points (the sweeps of wall-bounded cases 2^21)
+    vec_rows: int = 0
 
     def with_(self, **kw) -> "Params":
         return replace(self, **kw)

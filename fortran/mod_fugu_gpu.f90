@@ -58,6 +58,7 @@ module mod_fugu_gpu
     real(c_double)  :: pcd_sor_omega
     integer(c_int)  :: graphs
     real(c_double)  :: pcd_visc_scale
+    integer(c_int)  :: vec_rows
   end type
   ! fugu_step_opts: advance_coupled_step's optional arguments, has_* = present()
   type, bind(C) :: fugu_step_opts

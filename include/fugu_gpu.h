@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define FUGU_ABI_VERSION 4
+#define FUGU_ABI_VERSION 5  /* 5: fugu_params.vec_rows */
 
 /* return codes */
 #define FUGU_OK 0
@@ -108,6 +108,13 @@ typedef struct {
                                  complement, r_p -= pcd_visc_scale * mu_c *
                                  z_p with mu_c = kappa / 2 at the cell; 0 =
                                  the reference (mod_pcd_precond.f90:49-64)   */
+  int vec_rows;               /* damped-Jacobi sweeps and the PCD's Schur,
+                                 residual and cross steps with 16-byte
+                                 vector accesses, 16 / sizeof(real) elements
+                                 of a row per thread (same results): 1 on,
+                                 -1 off, 0 on for boxes of >= 2^20 points
+                                 (large grids, where they stream HBM; the
+                                 sweeps of wall-bounded cases from 2^21)    */
 } fugu_params;
 
 /* Optional arguments of advance_coupled_step (src/mod_solver_coupled.f90:137-160):

@@ -108,7 +108,7 @@ def test_comments_commas_and_extensions(driver, tmp_path):
 def test_smoother_and_graph_keys(driver, tmp_path):
     text = """&sim_params
   pcd_smoother = 'RBSOR', pcd_sor_omega = 1.5d0, pcd_sweeps = 6, pcd_sweeps_max = 24, graphs = .true.,
-  pcd_visc_scale = 1.0d0
+  pcd_visc_scale = 1.0d0, vec_rows = 1
 /
 """
     r = run(driver, text, tmp_path)
@@ -116,7 +116,7 @@ def test_smoother_and_graph_keys(driver, tmp_path):
     s = json.loads(r.stdout)
     assert (s["pcd_smoother"], s["pcd_sor_omega"], s["pcd_sweeps"], s["pcd_sweeps_max"], s["graphs"]) == \
         ("rbsor", 1.5, 6, 24, 1)
-    assert s["pcd_visc_scale"] == 1.0
+    assert s["pcd_visc_scale"] == 1.0 and s["vec_rows"] == 1
     r = run(driver, "&sim_params\n  pcd_smoother = 'gauss'\n/\n", tmp_path)
     assert r.returncode == 2 and "pcd_smoother" in r.stderr
 
