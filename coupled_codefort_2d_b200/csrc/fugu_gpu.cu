@@ -2142,7 +2142,10 @@ KrylovResult adjoint_solve_dev(fugu_ctx* c, const CoefBufs<double>& cb, const So
   const int g1 = grid1d(c, c->n);
   k_adj_flip_p<<<g1, 256, 0, c->s>>>(c->n, B.base);  // S g
   CKL("k_adj_flip_p");
-  c->prm.refine = 2;
+  // inner solve: flexible GMRES, or BiCGStab(2) (the reference's solver on
+  // the transposed system) when the context's refine is 1; the defect
+  // correction around it in FP64 either way
+  c->prm.refine = c->prm.refine == 1 ? 1 : 2;
   c->prm.precision = FUGU_FP64;
   if (c->prm.refine_max_inner < 1 || c->prm.refine_max_inner > 127) c->prm.refine_max_inner = 30;
   c->adj_on = true;

@@ -312,9 +312,12 @@ int fugu_matvec_coupled_t(fugu_ctx* ctx, const double* Y_u, const double* Y_v, c
 /* Solve A^T lambda = g to true relative residual tol: the FP64 defect
  * correction around flexible GMRES on S A^T S (S flips the pressure block,
  * which turns A^T back into A's block structure with the velocity block
- * transposed) with the step's PCD as right preconditioner.  st reports the
- * iterations; lambda's pressure block is defined up to the null space of
- * A^T (a constant in a closed or periodic box). */
+ * transposed) with the step's PCD as right preconditioner; when the
+ * context's refine is 1, around BiCGStab(2) instead (the reference's solver,
+ * mod_bicgstab2.f90:270-570, on the transposed system; it inherits that
+ * solver's breakdowns on hard cases).  st reports the iterations; lambda's
+ * pressure block is defined up to the null space of A^T (a constant in a
+ * closed or periodic box). */
 int fugu_adjoint_solve(fugu_ctx* ctx, const double* g_u, const double* g_v, const double* g_p,
                        double* lambda_u, double* lambda_v, double* lambda_p,
                        const double* u_adv, const double* v_adv,

@@ -5,7 +5,8 @@
    coefficients, to 1e-12 relative (the probe reproduces the operator exactly;
    the two sums differ by rounding only).
 2. The adjoint solve is dual to the forward solve: for A X = B and
-   A^T lambda = g, g . X = lambda . B to 1e-9.
+   A^T lambda = g, g . X = lambda . B to 1e-9, with flexible GMRES and with
+   BiCGStab(2) as the inner solver of the defect correction.
 3. The steady two-phase Poiseuille gradient dJ/dmu (J = mean velocity) from
    the adjoint equals central finite differences of the GPU forward solve
    (h = 1e-5 relative) to 1e-6, and the analytic derivative of the two-layer
@@ -73,14 +74,17 @@ def test_transpose_dot_product(gpu, name, extra):
         assert not np.any(a[~m])
 
 
-def test_adjoint_solve_is_dual_to_the_forward_solve(gpu):
+@pytest.mark.parametrize("refine", [2, 1])
+def test_adjoint_solve_is_dual_to_the_forward_solve(gpu, refine):
     """A two-phase system of a step: a circular interface (density ratio 10)
-    and a mild advecting velocity; random right-hand sides."""
+    and a mild advecting velocity; random right-hand sides.  refine 2: both
+    solves are the defect correction around flexible GMRES; refine 1: around
+    BiCGStab(2), the forward solve on A and the adjoint one on S A^T S."""
     from coupled_codefort_2d_b200 import cases
 
     g = Grid(24, 32, periodic_x=True)
     rng = np.random.default_rng(32)
-    prm = two_phase_params(refine=2, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=200,
+    prm = two_phase_params(refine=refine, refine_inner_tol=1e-2, refine_max_inner=30, refine_max_outer=200,
                            krylov_bc_fix=1, tol_bicgstab2=1e-10)
     with Context(g, prm) as ctx:
         c = cases.binary_circle(g, 0.5, 0.5, 0.25, inside=1.0)
