@@ -31,6 +31,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import shutil
 import subprocess
 import sys
 import threading
@@ -470,6 +471,14 @@ def _replica_run(args_tuple):
     return times, res
 
 
+def reference_toolchain():
+    """Where the host could build and run the Fortran/MPI reference: the
+    compilers and launcher its Makefile and README use (None when absent),
+    and the host's cores."""
+    tools = {t: shutil.which(t) for t in ("gfortran", "mpifort", "mpirun")}
+    return {**tools, "cores": os.cpu_count() or 1}
+
+
 def reference_arm(args, rank, world):
     """The reference's CPU path on the host cores: the oracle port (the
     Fortran/MPI reference cannot be built here), one independent replica per
@@ -480,6 +489,7 @@ def reference_arm(args, rank, world):
     from oracle import oracle
 
     oracle.build()
+    tc = reference_toolchain()
     inner = INNER[args.inner]
     cores = os.cpu_count() or 1
     import multiprocessing as mp
@@ -500,7 +510,10 @@ def reference_arm(args, rank, world):
                                    f"{args.steps} timed steps of the {N}^2 droplet, timed inside the replica"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "max_true_residual": max(max(r) for _, r in runs),
-        "note": "Fortran/MPI reference unbuildable here (no gfortran, no MPI); the C oracle restates it",
+        "reference_toolchain": tc,
+        "note": ("the Fortran/MPI reference is not built (probed on this host: "
+                 + ", ".join(f"{t} {'at ' + tc[t] if tc[t] else 'absent'}" for t in ("gfortran", "mpifort", "mpirun"))
+                 + "); the C oracle restates its hot path"),
     }
     print(json.dumps(line), flush=True)
 

@@ -52,3 +52,14 @@ def test_measured_forms_solver_settings():
     assert (r.pcd_visc_scale, r.pcg_cap_start, r.refine, r.graphs, r.tol_bicgstab2) == (0.0, 40, 2, 1, 1e-8)
     b2 = bench.case_params(1)  # BiCGStab(2) inner solve: the reference's fixed PCD
     assert (b2.pcd_visc_scale, b2.pcg_cap_start, b2.pcd_sweeps) == (0.0, 0, 3)
+
+
+def test_reference_toolchain_probe():
+    """The reference arm records, on the host it runs on, whether the Fortran
+    and MPI tools the reference needs exist (this container has none)."""
+    import shutil
+
+    tc = bench.reference_toolchain()
+    assert set(tc) == {"gfortran", "mpifort", "mpirun", "cores"} and tc["cores"] >= 1
+    for t in ("gfortran", "mpifort", "mpirun"):
+        assert tc[t] == shutil.which(t)
