@@ -103,9 +103,9 @@ __device__ __forceinline__ float madd<float>(float a, float b, float c) {
 #endif
 
 struct GridSync {
-  unsigned int count;
-  unsigned int gen;
-  int error;       // 0 ok, 1 barrier timeout
+  unsigned int count;  // arrivals since the launch began (zeroed before every launch)
+  unsigned int gen;    // not used by the barrier below; keeps the 16-byte layout
+  int error;           // 0 ok, 1 barrier timeout
   int pad;
 };
 
@@ -123,30 +123,32 @@ __device__ __forceinline__ int ld_relaxed_i32(const int* p) {
 // Returns true when every CTA arrived; false on timeout / error.  nblocks is
 // the arrival count the barrier waits for (gridDim.x, or one more in the
 // failure-detection test, which makes every wait run out); spin_limit bounds
-// each wait in polls.
+// each wait in polls.  gen counts the launch's barriers so far.
+//
+// The arrival counter only grows within a launch (the host zeroes it before
+// every launch), so barrier gen is complete once it reaches
+// (gen + 1) * nblocks: the last CTA's arrival is itself the release, and no
+// CTA has to reset a counter and publish a new generation after it (two
+// more dependent global operations on the critical path).  A CTA can only
+// arrive at barrier gen + 1 after every CTA arrived at barrier gen, so an
+// early arrival never completes a barrier that is still missing one.
 __device__ __forceinline__ bool grid_sync(GridSync* gs, unsigned int nblocks, unsigned int& gen,
                                           unsigned int spin_limit = FUGU_SPIN_LIMIT) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
+    const unsigned int target = (gen + 1u) * nblocks;
     __threadfence();
-    unsigned int my = gen;
-    unsigned int arrived = atomicAdd(&gs->count, 1u);
-    if (arrived == nblocks - 1) {
-      atomicExch(&gs->count, 0u);
-      __threadfence();
-      atomicAdd(&gs->gen, 1u);
-    } else {
-      unsigned int spins = 0;
-      while (ld_acquire_u32(&gs->gen) == my) {
-        if (++spins > spin_limit || ld_relaxed_i32(&gs->error) != 0) {
-          atomicExch(&gs->error, 1);
-          ok = 0;
-          break;
-        }
-        __nanosleep(40);
+    atomicAdd(&gs->count, 1u);
+    unsigned int spins = 0;
+    while (ld_acquire_u32(&gs->count) < target) {
+      if (++spins > spin_limit || ld_relaxed_i32(&gs->error) != 0) {
+        atomicExch(&gs->error, 1);
+        ok = 0;
+        break;
       }
+      __nanosleep(40);
     }
     __threadfence();
     s_ok = ok;
