@@ -235,7 +235,8 @@ __device__ __forceinline__ void maxpy_body(long n3, T* w, const T* V0, long stri
   __syncthreads();
   constexpr int W = VecW<T>::value;
   const long S = (long)G * blockDim.x;
-  if (n3 % W == 0 && stride % W == 0 && ((reinterpret_cast<uintptr_t>(w) | reinterpret_cast<uintptr_t>(V0)) & 15u) == 0) {
+  const bool aligned = ((reinterpret_cast<uintptr_t>(w) | reinterpret_cast<uintptr_t>(V0)) & 15u) == 0;
+  if (n3 % W == 0 && stride % W == 0 && aligned) {
     // W consecutive elements per thread with 16-byte loads and stores, the
     // loads of up to eight vectors in flight before their updates: a
     // thread's elements are a few long, wide round trips rather than many

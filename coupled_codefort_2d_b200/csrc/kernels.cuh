@@ -617,7 +617,8 @@ __device__ __forceinline__ T pcd_cross_vals(const Geo& g, int i, int j, const V&
 template <typename T>
 __device__ __forceinline__ void pcd_cross_at(const Geo& g, int k, int i, int j, const T* eta, const T* rv,
                                              T* zuw) {
-  if (j >= 1 && j <= g.ny && i >= 1 && i <= g.nx - 1) zuw[k] = pcd_cross_vals<T>(g, i, j, gview(g, eta), gview(g, rv), zuw[k]);
+  if (j >= 1 && j <= g.ny && i >= 1 && i <= g.nx - 1)
+    zuw[k] = pcd_cross_vals<T>(g, i, j, gview(g, eta), gview(g, rv), zuw[k]);
 }
 template <typename T>
 __global__ void k_pcd_cross(Geo g, const T* eta, const T* rv, T* zuw, const int* active) {
