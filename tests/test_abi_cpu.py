@@ -102,6 +102,10 @@ def test_invalid_params_rejected_before_any_device_work(libpath):
     L.fugu_params_default(C.byref(p))
     p.precision = 1  # mixed precision requires refine = 1
     assert L.fugu_create(C.byref(p), 0, C.byref(h)) == -1
+    for bad in (-2, 2):  # vec_rows takes -1, 0 or 1
+        L.fugu_params_default(C.byref(p))
+        p.vec_rows = bad
+        assert L.fugu_create(C.byref(p), 0, C.byref(h)) == -1
     assert L.fugu_create(None, 0, C.byref(h)) == -1
     assert not h.value
 
